@@ -1,0 +1,352 @@
+#!/usr/bin/env python3
+"""Benchmark of tetmag's full field evaluation (demag chain + local field + LLG
+right-hand side) on B200.
+
+A step is one full field evaluation of the 363,609-node permalloy film
+(500x500x20 nm at 2.5 nm, seeded vortex, 20 mT in-plane): divergence, Neumann
+PCG+AMG, dense double-layer BEM matvec, Dirichlet PCG+AMG, gradient, fused
+local field + LLG right-hand side.  The headline path is the mixed one (FP32
+operator values, FP64 vectors / reductions / coarse solve); the plain FP64 path
+is measured in the same run as the speed bar, with the relative error between
+the two.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun each rank evaluates its own replica (independent seed): no
+data-path collective; value = all ranks' evaluations / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "field evals/s & simulated ns/hour vs plain FP64 GPU path at <=1e-5 rel. err"
+UNIT = "field evals/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--workload", default="c2", choices=["c1", "c2", "c4"])
+    p.add_argument("--tol", type=float, default=1e-7)
+    p.add_argument("--sim-ps", type=float, default=2.0, help="simulated ps for the ns/hour figure")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def peak_hbm():
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        d = json.loads(f.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region (read only)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.out = ROOT / f"_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.fh = open(self.out, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device)], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        self.out.unlink(missing_ok=True)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline_sample(w, samples: int = 1):
+    """Oracle field evaluation on the host cores (bounded sample)."""
+    from oracle import cpu_baseline, tetmag_oracle as O
+
+    axis = None if w.ku_axis is None else O.soa_to_rows(w.ku_axis)
+    pb = O.make_problem(w.mesh.xyz, w.mesh.tets, w.mesh.scale, Ms=w.Ms, A=w.A, alpha=w.alpha, Ku=w.Ku,
+                        ku_axis=axis if axis is not None else (0, 0, 1), D=w.D, hext=w.hext, with_bem=False)
+    ev = cpu_baseline.CpuFieldEval(pb)
+    m = O.soa_to_rows(w.m0)
+    ev.calibrate(m)
+    res = [ev.sample(m) for _ in range(samples)]
+    return ev, res
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from tetmag_b200 import workloads
+
+    w = workloads.WORKLOADS[args.workload]()
+    ev, res = cpu_baseline_sample(w, samples=0)
+    m = w.m0.reshape(3, -1).T.copy()
+    for _ in range(args.warmup):
+        ev.sample(m)
+    tot = 0.0
+    parts = []
+    for _ in range(args.steps):
+        r = ev.sample(m)
+        tot += r["total_s"]
+        parts.append(r)
+    value = args.steps / tot
+    cores = ev.threads
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": w.name, "nodes": w.n, "impl": "oracle port on host cores"},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": ev.describe()},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "components_s": {k: float(np.mean([p[k] for p in parts])) for k in
+                         ("local_s", "div_grad_s", "solves_s", "bem_s")},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_gpu(args):
+    import torch
+    from tetmag_b200 import api, workloads
+
+    world, rank, local = dist_env()
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    w = workloads.WORKLOADS[args.workload](seed=2 + 17 * rank) if args.workload != "c4" else \
+        workloads.c4_replica(replica=rank)
+    t0 = time.perf_counter()
+    mo, ctx = workloads.setup_context(w, device=local, mixed=True, tol=args.tol, maxiter=100)
+    setup_s = time.perf_counter() - t0
+    stream = torch.cuda.current_stream(dev)
+    ctx.set_stream(stream.cuda_stream)
+    n = w.n
+    K, W = args.steps, args.warmup
+
+    # W + K distinct states: the seeded initial state with seeded perturbations
+    rng = np.random.default_rng(1000 + rank)
+    base = w.m0.reshape(3, n)
+    states = []
+    for _ in range(W + K):
+        s = base + 0.05 * rng.standard_normal((3, n))
+        s /= np.linalg.norm(s, axis=0, keepdims=True)
+        states.append(s.ravel())
+    S = torch.from_numpy(np.stack(states)).to(dev)
+    ydot = torch.empty(3 * n, dtype=torch.float64, device=dev)
+    hdem = torch.empty(3 * n, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize(dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(mixed: bool, profile: bool):
+        ctx.set_precision(mixed)
+        for k in range(W):
+            ctx.field_eval(S[k], ydot, hdem)
+        torch.cuda.synchronize(dev)
+        barrier()
+        torch.cuda.synchronize(dev)
+        if profile:
+            api.profile_enable(ctx, True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = api.kernel_launches()
+        its = [0, 0]
+        e0.record(stream)
+        for k in range(K):
+            ctx.field_eval(S[W + k], ydot, hdem)
+            st = ctx.stats()
+            its[0] += st["it_neumann"]
+            its[1] += st["it_dirichlet"]
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        ms = e0.elapsed_time(e1)
+        launches = api.kernel_launches() - l0
+        prof = api.profile_read(ctx) if profile else None
+        if profile:
+            api.profile_enable(ctx, False)
+        return max_over_ranks(ms), launches, prof, its
+
+    clocks = Clocks(local)
+    clocks.start()
+    ms_mx, launches, prof, its_mx = timed(True, True)
+    clk = clocks.stop()
+    ms_64, _, _, its_64 = timed(False, False)
+
+    # relative error of the mixed path against the FP64 path, on one state
+    probe = S[W + K - 1]
+    ctx.set_precision(False)
+    ctx.set_solver_params(1e-12, 300)
+    h64 = hdem.clone()
+    y64 = ctx.field_eval(probe, torch.empty_like(ydot), h64)
+    ctx.set_precision(True)
+    ctx.set_solver_params(args.tol, 100)
+    hmx = hdem.clone()
+    ymx = ctx.field_eval(probe, torch.empty_like(ydot), hmx)
+    torch.cuda.synchronize(dev)
+    err_h = float(torch.linalg.norm(hmx - h64) / torch.linalg.norm(h64))
+    err_y = float(torch.linalg.norm(ymx - y64) / torch.linalg.norm(y64))
+
+    # local right-hand side only (frozen demag), mixed
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for k in range(3):
+        ctx.llg_rhs(0.0, S[k], ydot)
+    e0.record(stream)
+    nloc = 50
+    for k in range(nloc):
+        ctx.llg_rhs(0.0, S[k % (W + K)], ydot)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    local_per_s = nloc / (max_over_ranks(e0.elapsed_time(e1)) / 1e3)
+
+    # end to end through the public API with host buffers (H2D of m, D2H of ydot per step)
+    host_states = [np.ascontiguousarray(st) for st in states]
+    yh = np.empty(3 * n)
+    for k in range(W):
+        ctx.field_eval(host_states[k], yh)
+    barrier()
+    t = time.perf_counter()
+    for k in range(K):
+        ctx.field_eval(host_states[W + k], yh)
+    e2e_s = max_over_ranks(time.perf_counter() - t)
+
+    # simulated time: the frozen-demag relaxation loop (0.5 ps segments), mixed
+    mrun = S[0].clone()
+    torch.cuda.synchronize(dev)
+    t = time.perf_counter()
+    rs = ctx.relax(mrun, duration_ps=args.sim_ps, segment_ps=0.5)
+    sim_s = max_over_ranks(time.perf_counter() - t)
+    ns_per_hour = (args.sim_ps * 1e-3) / (sim_s / 3600.0)
+
+    value = world * K / (ms_mx / 1e3)
+    fp64_value = world * K / (ms_64 / 1e3)
+    peak, peak_kind = peak_hbm()
+    kernels = ["local_llg", "divergence", "gradient", "bem_matvec", "cg_spmv"]
+    dom = max(kernels, key=lambda k: prof[k]["total_ms"])
+    d = prof[dom]
+    avg_ms = d["total_ms"] / max(d["launches"], 1)
+    achieved = d["bytes_per_launch"] / (avg_ms / 1e3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get(w.name, {}).get(dom)
+    kshare = {k: round(prof[k]["total_ms"] / ms_mx, 4) for k in prof if k != "demag_chain"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms_mx / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 operators / f64 vectors+reductions", "data": "synthetic",
+        "config": {"workload": w.name, "nodes": n, "boundary_nodes": mo.nb, "nnz": mo.nnz,
+                   "bem": "dense, device-assembled, FP32 on the mixed path", "precision": "mixed",
+                   "cg_tol": args.tol, "states": "W+K distinct seeded perturbed states, warm-started solves",
+                   "l2": "inputs larger than L2 (dense BEM alone is 4*Nb^2 bytes)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single"},
+        "e2e": {"value": world * K / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 3 * n * 8,
+                "d2h_bytes_per_step": 3 * n * 8},
+        "gpu_launches": launches,
+        "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                     "bytes_per_launch": d["bytes_per_launch"], "avg_ms": avg_ms},
+        "clocks": clk,
+        "fp64_value": fp64_value, "speedup_vs_fp64": value / fp64_value,
+        "rel_err_vs_fp64": {"hdem": err_h, "ydot": err_y},
+        "local_rhs_evals_per_s": world * local_per_s,
+        "sim_ns_per_hour": ns_per_hour,
+        "relax": {"sim_ps": args.sim_ps, "wall_s": sim_s, "steps": rs["accepted"], "rejected": rs["rejected"],
+                  "rhs": rs["rhs"]},
+        "cg_iters_per_eval": {"mixed": [i / K for i in its_mx], "fp64": [i / K for i in its_64]},
+        "kernel_time_share": kshare,
+        "setup_s": setup_s,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        ev, res = cpu_baseline_sample(w, samples=1)
+        line["cpu_baseline"] = {"value": 1.0 / res[0]["total_s"], "unit": UNIT, "cores": ev.threads,
+                                "kind": "port", "sample": ev.describe(),
+                                "components_s": {k: res[0][k] for k in
+                                                 ("local_s", "div_grad_s", "solves_s", "bem_s")}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del ctx, mo
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,171 @@
+/*
+ * tmb.h -- C ABI of the tetmag B200 library (libtmb.so).
+ *
+ * A drop-in replacement for the per-step effective-field and LLG
+ * right-hand-side evaluation of tetmag (R-Hertel/tetmag v1.7.7), including
+ * its FEM-BEM demagnetising-field chain.  Plain C types only: caller-owned
+ * buffers, int status codes, an opaque context per mesh.  Every entry point
+ * returns TMB_OK (0) or a positive TMB_ERR_* code; tmb_last_error() gives
+ * the message of the last failure on the calling thread.
+ *
+ * Vectors of nodal 3-vectors use tetmag's layout: SoA / column-major
+ * [x(0..N-1), y(0..N-1), z(0..N-1)], length 3N (main/TheLLG.cpp:156).  Fields
+ * are in A/m, reduced time t*gamma/(1+alpha^2) (specs/SimulationData.cpp:52-57).
+ * Entry points that take a `ptr_kind` accept host (TMB_PTR_HOST) or device
+ * (TMB_PTR_DEVICE) pointers; device-pointer calls are ordered on the context
+ * stream and do not synchronise the host except where stated.
+ *
+ * Threading: a context is used by one host thread at a time.
+ */
+#ifndef TMB_H_
+#define TMB_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TMB_OK 0
+#define TMB_ERR_ARG 1          /* invalid argument or size */
+#define TMB_ERR_CUDA 2         /* CUDA runtime error */
+#define TMB_ERR_NOCONVERGE 3   /* an iterative solve hit its iteration cap */
+#define TMB_ERR_STATE 4        /* call out of order (e.g. no mesh set) */
+#define TMB_ERR_NAN 5          /* NaN / Inf detected (field, torque, solver breakdown) */
+#define TMB_ERR_STEP 6         /* integrator step-size underflow or step cap */
+#define TMB_ERR_INTERNAL 7
+
+#define TMB_FP64 0             /* plain path: FP64 operators and vectors */
+#define TMB_MIXED 1            /* FP32 operator values, FP64 vectors, reductions, coarse solve, step control */
+
+#define TMB_PTR_HOST 0
+#define TMB_PTR_DEVICE 1
+
+typedef struct tmb_ctx tmb_ctx;
+typedef struct tmb_mesh tmb_mesh;
+typedef struct tmb_solver tmb_solver;
+
+const char* tmb_last_error(void);
+int tmb_version(void);
+/* Kernels launched by this library so far, all contexts (no reference counterpart; for benchmarking). */
+int tmb_kernel_launches(long long* count);
+
+/* ---------------------------------------------------------------------------------------
+ * Host mesh preprocessing.  Replaces PreprocessMesh::prepareAllMatrices
+ * (preproc/FEMprocessing.cpp:70-93), MeshBoundary::extractFeatures
+ * (preproc/Boundary.cpp:47-55) and BEMprocessing::calculateSolidAngles
+ * (preproc/BEMprocessing.cpp:358-372).  xyz: N x 3 row-major (mesh units);
+ * tets: E x 4 node ids.
+ * ------------------------------------------------------------------------------------- */
+int tmb_mesh_create(int nx, int ntet, const double* xyz, const int* tets, tmb_mesh** out);
+int tmb_mesh_destroy(tmb_mesh* mesh);
+/* info[0..5] = nx, ntet, nnz (shared operator pattern), nb (boundary nodes), ntri (boundary triangles), 0 */
+int tmb_mesh_info(const tmb_mesh* mesh, long long* info);
+/* CSR arrays of the shared pattern: rowptr[N+1], col[nnz]; each value array has nnz entries.
+ * tg* are tetmag's msh.tGrad* (not negated).  Any output pointer may be NULL. */
+int tmb_mesh_get_operators(const tmb_mesh* mesh, int* rowptr, int* col, double* stiff, double* gx, double* gy,
+                           double* gz, double* tgx, double* tgy, double* tgz, double* node_vol);
+/* bnodes[nb] ascending; tri[3*ntri] global ids; tri_area[ntri]; tri_normal[3*ntri] outward (row-major);
+ * node_area[N]; node_normal[3N] SoA; solid_angle[nb].  Any output pointer may be NULL. */
+int tmb_mesh_get_boundary(const tmb_mesh* mesh, int* bnodes, int* tri, double* tri_area, double* tri_normal,
+                          double* node_area, double* node_normal, double* solid_angle);
+
+/* ---------------------------------------------------------------------------------------
+ * Context: one mesh on one device.
+ * ------------------------------------------------------------------------------------- */
+int tmb_ctx_create(int device, tmb_ctx** out);       /* SetDevice::set (gpu/SetDevice.cu:41-60) */
+int tmb_ctx_destroy(tmb_ctx* ctx);
+int tmb_ctx_set_stream(tmb_ctx* ctx, void* cuda_stream);  /* NULL: the context's own stream */
+int tmb_set_precision(tmb_ctx* ctx, int precision);   /* TMB_FP64 (default) or TMB_MIXED */
+
+/* Operators from a preprocessed mesh, or from tetmag's own MeshData arrays
+ * (main/TheLLG.cpp:88-108 uploads K; main/DemagField.cpp:65-89 keeps grad,
+ * tGrad, the Dirichlet and Neumann matrices).  The caller's CSR must hold K,
+ * grad* and tGrad* on one pattern; node_normal is SoA 3N. */
+int tmb_set_mesh(tmb_ctx* ctx, const tmb_mesh* mesh);
+int tmb_set_operators(tmb_ctx* ctx, int nx, int nnz, const int* rowptr, const int* col, const double* stiff,
+                      const double* gx, const double* gy, const double* gz, const double* tgx, const double* tgy,
+                      const double* tgz, const double* node_vol, int nb, const int* bnodes,
+                      const double* node_area, const double* node_normal);
+
+/* Dense double-layer BEM matrix.  tmb_bem_assemble builds it on the device from the
+ * mesh boundary (BEMprocessing::assembleLaplaceBEMmatrix, preproc/BEMprocessing.cpp:375-411);
+ * tmb_set_bem_dense takes tetmag's MeshData::laplaceBEM (Nb x Nb, column-major). */
+int tmb_bem_assemble(tmb_ctx* ctx, const tmb_mesh* mesh);
+int tmb_set_bem_dense(tmb_ctx* ctx, int nb, const double* B_colmajor);
+int tmb_get_bem_dense(tmb_ctx* ctx, double* B_colmajor);
+
+/* Material per node (SimulationData, specs/SimulationData.cpp:125-163): Js [T], A [J/m]
+ * already divided by scale^2, Ku [J/m^3], ku_axis 3N SoA, D [J/m^2] already divided by
+ * scale (bulk DMI, main/EffFieldCalc.cpp:159-170).  Ku, ku_axis, D may be NULL. */
+int tmb_set_material(tmb_ctx* ctx, const double* Js, const double* A, const double* Ku, const double* ku_axis,
+                     const double* D, double alpha);
+/* Applied field, 3N SoA in A/m (TheLLG::setZeemanField, main/TheLLG.cpp:477-483). */
+int tmb_set_applied_field(tmb_ctx* ctx, const double* hext, int ptr_kind);
+/* precession = 0 selects the "remove precession" dynamics (TheLLG::noPrecession, main/TheLLG.cpp:180-199). */
+int tmb_set_llg_options(tmb_ctx* ctx, int precession);
+/* Relative residual tolerance and iteration cap of both demag solves
+ * ("CG tolerance", specs/ProgramSpecs.cpp:70; maxiter main/AMGCLSolver.cpp:42). */
+int tmb_set_solver_params(tmb_ctx* ctx, double tol, int maxiter);
+
+/* DemagField::calcField (main/DemagField.cpp:92-94): m (3N) -> H_dem (3N).  The result
+ * also becomes the frozen demag field used by the right-hand side. hdem may be NULL. */
+int tmb_demag_field(tmb_ctx* ctx, const double* m, double* hdem, int ptr_kind);
+/* One full field evaluation: the demag chain on m, then the local field and the LLG
+ * right-hand side -- TheLLG::rhs with "freeze demag = false", whose calcDemagField refreshes
+ * H_dem inside the right-hand side (main/TheLLG.cpp:278-283, 458-462).  hdem may be NULL. */
+int tmb_field_eval(tmb_ctx* ctx, const double* m, double* ydot, double* hdem, int ptr_kind);
+/* TheLLG::setHdem (main/TheLLG.cpp:508-510). */
+int tmb_set_demag_frozen(tmb_ctx* ctx, const double* hdem, int ptr_kind);
+/* Total effective field with the frozen demag (TheLLG::totalEffectiveField, main/TheLLG.cpp:238-254). */
+int tmb_effective_field(tmb_ctx* ctx, const double* m, double* h, int ptr_kind);
+/* The CVODE right-hand side (TheLLG::rhs / rhs_d, main/TheLLG.cpp:670-711,
+ * gpu/LLGWrapper.cu:213-228): ydot = -m x H - alpha m x (m x H).  t is reduced time. */
+int tmb_llg_rhs(tmb_ctx* ctx, double t, const double* y, double* ydot, int ptr_kind);
+/* TheLLG::getMaxTorque (main/TheLLG.cpp:426-439): mu0 * max_i |m_i x H_i| with the frozen demag.
+ * Synchronises.  Returns TMB_ERR_NAN if the torque is not finite. */
+int tmb_max_torque(tmb_ctx* ctx, const double* m, double* out, int ptr_kind);
+/* m <- m / |m| per node (TheSimulation::normalizeMag, main/TheSimulation.cpp:404-411). */
+int tmb_normalize(tmb_ctx* ctx, double* m, int ptr_kind);
+
+/* The simulation loop of TheSimulation::start (main/TheSimulation.cpp:231-311) with frozen
+ * demag: per segment of segment_ps, refresh H_dem, integrate the LLG with an adaptive
+ * Dormand-Prince 5(4) stepper on the device (TheLLG::IntegrateODEINT's stepper,
+ * main/TheLLG.cpp:514-572), normalise.  stats[0..11] = accepted steps, rejected steps,
+ * rhs evaluations, demag evaluations, Neumann CG iterations, Dirichlet CG iterations,
+ * final max torque [T], final dt (reduced), segments, 0, 0, 0.  Synchronises. */
+int tmb_relax(tmb_ctx* ctx, double* m, double duration_ps, double segment_ps, double eps_abs, double eps_rel,
+              double* stats, int ptr_kind);
+/* Counters of the last demag evaluation: [0] Neumann iterations, [1] Dirichlet iterations,
+ * [2] Neumann relative residual, [3] Dirichlet relative residual, [4] Neumann status,
+ * [5] Dirichlet status, [6] AMG levels (Neumann), [7] AMG setup ms (both). Synchronises. */
+int tmb_get_stats(tmb_ctx* ctx, double* out);
+
+/* Live profiling with CUDA events on the context stream (no reference counterpart; tetmag's
+ * timers are host wall clocks, main/DemagField.cpp:155-160, utils/Timer.cpp:36-81).
+ * Kernel ids: 0 local field + LLG, 1 divergence, 2 gradient, 3 BEM matvec, 4 Neumann solve,
+ * 5 Dirichlet solve, 6 CG fine-level SpMV, 7 whole demag chain.
+ * tmb_profile_read fills out[3*id + {0,1,2}] = launches, total ms, algorithmic bytes per launch. */
+int tmb_profile_enable(tmb_ctx* ctx, int on);
+int tmb_profile_read(tmb_ctx* ctx, double* out);
+
+/* ---------------------------------------------------------------------------------------
+ * Linear solver plugin (SolverFactory, main/SolverFactory.h:42-65): a "b200" solver
+ * for the row-pinned Neumann and row-replaced Dirichlet matrices of the demag chain.
+ * Rows whose only entry is a unit diagonal are treated as constraints and eliminated
+ * symmetrically, so the remaining system is SPD and solved by PCG with a device
+ * smoothed-aggregation V-cycle.  The previous solution is the initial guess
+ * (as AMGCLSolver::solve, main/AMGCLSolver.cpp:97-103).
+ * ------------------------------------------------------------------------------------- */
+int tmb_solver_create(tmb_ctx* ctx, tmb_solver** out);
+int tmb_solver_destroy(tmb_solver* s);
+int tmb_solver_set_matrix(tmb_solver* s, int n, int nnz, const int* rowptr, const int* col, const double* val);
+int tmb_solver_set_tolerance(tmb_solver* s, double tol, int maxiter);
+int tmb_solver_compute(tmb_solver* s);                 /* setup; SolverFactory::compute */
+int tmb_solver_solve(tmb_solver* s, const double* b, double* x, int ptr_kind);  /* synchronises */
+/* info[0] iterations, [1] relative residual, [2] status (0 ok, 3 not converged, 5 breakdown) */
+int tmb_solver_info(tmb_solver* s, double* info);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TMB_H_ */

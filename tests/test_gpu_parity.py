@@ -1,0 +1,220 @@
+"""GPU parity of the CUDA path (through the C ABI) against the FP64 oracle.
+
+Tolerances (relative L2 over all nodes and components):
+  plain FP64 path   <= 1e-10  (field, demag, right-hand side)
+  mixed path        <= 1e-5   (FP32 operator values, FP64 vectors / reductions)
+  relaxation        |<m>_gpu - <m>_oracle| <= 1e-4
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+import scipy.sparse.linalg as spla
+
+from oracle import tetmag_oracle as O
+from tetmag_b200 import _lib, meshgen, workloads
+from tetmag_b200.api import Context, MeshOps, SolverFactory, TheLLG, DemagField
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).with_name("golden") / "oracle_small.npz"
+FP64_TOL = 1e-10
+MIXED_TOL = 1e-5
+
+
+def rel(a, b):
+    a, b = np.asarray(a).ravel(), np.asarray(b).ravel()
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def oracle_problem(w: workloads.Workload, with_bem=True):
+    axis = None if w.ku_axis is None else O.soa_to_rows(w.ku_axis)
+    return O.make_problem(w.mesh.xyz, w.mesh.tets, w.mesh.scale, Ms=w.Ms, A=w.A, alpha=w.alpha,
+                          Ku=w.Ku, ku_axis=axis if axis is not None else (0, 0, 1), D=w.D, hext=w.hext,
+                          with_bem=with_bem)
+
+
+@pytest.fixture(scope="module")
+def golden():
+    g = np.load(GOLDEN)
+    mo = MeshOps(g["xyz"], g["tets"])
+    ctx = Context(0)
+    ctx.set_mesh(mo)
+    ctx.bem_assemble(mo)
+    n = mo.nx
+    ctx.set_material(np.full(n, O.MU0 * 8e5), np.full(n, 1.3e-11 / 1e-18), Ku=np.full(n, 5e4),
+                     ku_axis=O.rows_to_soa(g["axis"]), D=np.full(n, 3e-3 / 1e-9), alpha=0.3)
+    ctx.set_applied_field(np.ascontiguousarray(g["hext"]))
+    return g, mo, ctx
+
+
+@pytest.fixture(scope="module")
+def c1():
+    w = workloads.c1()
+    mo, ctx = workloads.setup_context(w, tol=1e-13, maxiter=200)
+    pb = oracle_problem(w)
+    return w, mo, ctx, pb, O.DemagOracle(pb)
+
+
+def test_bem_assembly_matches_oracle(golden, c1):
+    g, mo, ctx = golden
+    B = ctx.get_bem_dense()
+    assert np.max(np.abs(B - g["B"])) <= 1e-12 * np.max(np.abs(g["B"]))
+    w, mo1, ctx1, pb, _ = c1
+    B1 = ctx1.get_bem_dense()
+    assert np.max(np.abs(B1 - pb.B)) <= 1e-12 * np.max(np.abs(pb.B))
+    assert np.max(np.abs(B1.sum(axis=1) + 1.0)) < 1e-9          # B.1 = -1 per row
+    assert O.bem_rowsum_error(B1) < 5e-3                          # the reference's own check
+
+
+def test_local_field_and_rhs_fp64(golden):
+    g, mo, ctx = golden
+    m = O.rows_to_soa(g["m"])
+    ctx.set_demag_frozen(O.rows_to_soa(g["hdem"]))
+    H = ctx.effective_field(m)
+    assert rel(H, O.rows_to_soa(g["H"])) <= 1e-12
+    ydot = TheLLG(ctx)(m, 0.0)
+    assert rel(ydot, O.rows_to_soa(g["ydot"])) <= 1e-12
+    assert abs(ctx.max_torque(m) - float(g["torque"])) <= 1e-12 * float(g["torque"])
+
+
+def test_local_field_mixed(golden):
+    g, mo, ctx = golden
+    m = O.rows_to_soa(g["m"])
+    ctx.set_demag_frozen(O.rows_to_soa(g["hdem"]))
+    ctx.set_precision(True)
+    try:
+        H = ctx.effective_field(m)
+    finally:
+        ctx.set_precision(False)
+    assert rel(H, O.rows_to_soa(g["H"])) <= MIXED_TOL
+
+
+def test_demag_fp64_golden(golden):
+    g, mo, ctx = golden
+    ctx.set_solver_params(1e-13, 300)
+    H = DemagField(ctx).calcField(O.rows_to_soa(g["m"]))
+    assert rel(H, O.rows_to_soa(g["hdem"])) <= FP64_TOL
+
+
+def test_demag_fp64_c1(c1):
+    w, mo, ctx, pb, dem = c1
+    ctx.set_precision(False)
+    m = w.m0
+    H = ctx.demag_field(m)
+    Ho = dem.field(O.soa_to_rows(m))
+    assert rel(H, O.rows_to_soa(Ho)) <= FP64_TOL
+    st = ctx.stats()
+    assert st["status_neumann"] == 0 and st["status_dirichlet"] == 0
+    # a second call warm-starts from the previous solution and still matches
+    H2 = ctx.demag_field(m)
+    assert rel(H2, O.rows_to_soa(Ho)) <= FP64_TOL
+
+
+def test_demag_mixed_c1(c1):
+    w, mo, ctx, pb, dem = c1
+    ctx.set_precision(True)
+    ctx.set_solver_params(1e-9, 200)
+    try:
+        for seed in (3, 4):
+            m = meshgen.random_state(w.n, seed)
+            H = ctx.demag_field(m)
+            Ho = dem.field(O.soa_to_rows(m))
+            assert rel(H, O.rows_to_soa(Ho)) <= MIXED_TOL
+    finally:
+        ctx.set_precision(False)
+        ctx.set_solver_params(1e-13, 200)
+
+
+def test_full_rhs_with_demag_c1(c1):
+    w, mo, ctx, pb, dem = c1
+    m = meshgen.random_state(w.n, 9)
+    ctx.demag_field(m)                     # refresh the frozen demag field
+    ydot = ctx.llg_rhs(0.0, m)
+    mr = O.soa_to_rows(m)
+    Ho = O.local_field(pb, mr, dem.field(mr))
+    assert rel(ydot, O.rows_to_soa(O.llg_rhs(pb, mr, Ho))) <= FP64_TOL
+    assert abs(ctx.max_torque(m) - O.max_torque(mr, Ho)) <= 1e-9 * O.max_torque(mr, Ho)
+
+
+def test_solver_plugin_on_reference_matrices(c1):
+    # the row-pinned Neumann and row-replaced Dirichlet matrices of DemagField
+    w, mo, ctx, pb, dem = c1
+    rng = np.random.default_rng(5)
+    for A in (dem.neumann, dem.dirichlet):
+        s = SolverFactory.makeSolver("b200", ctx)
+        s.setMatrix(A)
+        s.setCGTolerance(1e-13)
+        s.maxiter = 300
+        assert s.compute()
+        b = rng.standard_normal(A.shape[0])
+        s.setLoadVector(b)
+        s.solve()
+        assert s.wasSuccessful()
+        x_ref = spla.splu(A.tocsc()).solve(b)
+        assert rel(s.result(), x_ref) <= 1e-10
+
+
+def test_normalize_and_device_pointers(c1):
+    torch = pytest.importorskip("torch")
+    w, mo, ctx, pb, dem = c1
+    m = meshgen.random_state(w.n, 12) * 1.7
+    mt = torch.from_numpy(m.copy()).cuda()
+    ctx.normalize(mt)
+    mh = ctx.normalize(m.copy())
+    assert np.allclose(mt.cpu().numpy(), mh, rtol=0, atol=1e-15)
+    assert np.allclose(np.linalg.norm(O.soa_to_rows(mh), axis=1), 1.0, atol=1e-15)
+    yd = ctx.llg_rhs(0.0, mt)
+    torch.cuda.synchronize()
+    assert rel(yd.cpu().numpy(), ctx.llg_rhs(0.0, mh)) <= 1e-14
+
+
+def test_nan_is_reported(c1):
+    w, mo, ctx, pb, dem = c1
+    m = meshgen.random_state(w.n, 2)
+    m[5] = np.nan
+    with pytest.raises(_lib.TmbError) as e:
+        ctx.max_torque(m)
+    assert e.value.code == _lib.TMB_ERR_NAN
+
+
+def test_relax_short_matches_oracle(c1):
+    w, mo, ctx, pb, dem = c1
+    ctx.set_precision(False)
+    ctx.set_solver_params(1e-12, 200)
+    m = w.m0.copy()
+    st = ctx.relax(m, duration_ps=10.0, segment_ps=0.5)
+    mo_, so = O.relax(pb, w.m0, 10.0, 0.5, demag=dem)
+    assert st["segments"] == so["segments"] == 20
+    assert np.max(np.abs(O.mean_m(pb, O.soa_to_rows(m)) - O.mean_m(pb, mo_))) <= 1e-4
+    assert abs(st["accepted"] - so["accepted"]) <= max(2, 0.02 * so["accepted"])
+    assert np.isfinite(st["max_torque"])
+
+
+def test_full_size_c4_properties():
+    # 28611 nodes / 7002 boundary nodes: size-independent checks at full size
+    w = workloads.c4_replica(replica=0)
+    mo, ctx = workloads.setup_context(w, tol=1e-11, maxiter=200)
+    B = ctx.get_bem_dense()
+    assert np.max(np.abs(B.sum(axis=1) + 1.0)) < 1e-8
+    del B
+    # uniform magnetisation: demag factors of the 200x200x40 nm prism (Aharoni)
+    n = w.n
+    Ms = w.Ms
+    vol = mo.operators()["node_vol"]
+    Nd = []
+    for d in range(3):
+        m = np.zeros(3 * n)
+        m[d * n:(d + 1) * n] = 1.0
+        H = ctx.demag_field(m)
+        E = -(O.MU0 * Ms * vol) @ H[d * n:(d + 1) * n] / 2.0
+        Nd.append(E / (0.5 * O.MU0 * Ms * Ms * vol.sum()))
+    assert abs(sum(Nd) - 1.0) < 0.02
+    assert abs(Nd[2] - O.aharoni_nz(100.0, 100.0, 20.0)) < 0.01
+    # mixed vs FP64 on a random state
+    m = w.m0
+    H64 = ctx.demag_field(m)
+    ctx.set_precision(True)
+    ctx.set_solver_params(1e-9, 200)
+    Hmx = ctx.demag_field(m)
+    assert rel(Hmx, H64) <= MIXED_TOL

@@ -1,0 +1,114 @@
+"""CPU tests of the FP64 oracle: the reference's own known-answer checks,
+analytic identities, and the committed golden vectors."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import tetmag_oracle as O
+from tetmag_b200 import meshgen
+
+GOLDEN = Path(__file__).with_name("golden") / "oracle_small.npz"
+
+
+@pytest.fixture(scope="module")
+def c1():
+    mesh = meshgen.kuhn_cuboid(20, 20, 2, 5.0)
+    fem = O.fem_prepare(mesh.xyz, mesh.tets)
+    bnd = O.extract_boundary(mesh.xyz, mesh.tets)
+    return mesh, fem, bnd
+
+
+def test_c1_sizes(c1):
+    # 21x21x3 nodes, unpruned Kuhn pattern, 962 surface nodes
+    mesh, fem, bnd = c1
+    assert mesh.nx == 1323
+    assert fem.stiff.nnz == 15487
+    assert bnd.bnodes.size == 962
+    assert bnd.tri.shape[0] == 1920
+    assert np.isclose(bnd.tri_area.sum(), 2 * (100 * 100 + 2 * 100 * 10))
+
+
+def test_gradient_operators_exact_on_linear_functions(c1):
+    # PreprocessMesh::testGradientOperators (preproc/FEMprocessing.cpp:288-326), tol 1e-10
+    mesh, fem, _ = c1
+    x, y, z = mesh.xyz.T
+    f = 0.5 * x - 17.0 * y + 13.0 * z + 42.0
+    for d, c in enumerate((0.5, -17.0, 13.0)):
+        g = fem.grad[d] @ f
+        assert np.max(np.abs(g - c)) <= 1e-10 * abs(c)
+
+
+def test_stiffness_and_divergence_annihilate_constants(c1):
+    mesh, fem, _ = c1
+    one = np.ones(mesh.nx)
+    assert np.max(np.abs(fem.stiff @ one)) < 1e-12 * abs(fem.stiff).max()
+    for t in fem.tgrad:  # sum_i grad(phi_i) = 0 per element
+        assert np.max(np.abs(one @ t)) < 1e-12 * abs(t).max()
+
+
+def test_dense_bem_rowsum_known_answer(c1):
+    # BEMprocessing::testLaplaceMatrix (preproc/BEMprocessing.cpp:440-445, 55-72):
+    # sum(B.(-1)) must equal Nb within 5e-3; each row of B sums to -1.
+    mesh, _, bnd = c1
+    B = O.dense_bem(mesh.xyz, mesh.tets, bnd)
+    assert O.bem_rowsum_error(B) < 5e-3
+    assert np.max(np.abs(B.sum(axis=1) + 1.0)) < 1e-9
+
+
+def test_solid_angles_interior(c1):
+    # face nodes see 2 pi, edge nodes pi, corner nodes pi/2
+    mesh, _, bnd = c1
+    sub = O.solid_angles(mesh.xyz, mesh.tets, bnd)
+    assert np.allclose(np.sort(np.unique(np.round(sub / np.pi, 12))), [0.5, 1.0, 2.0])
+
+
+@pytest.mark.parametrize("nc,tol", [(4, 0.03), (8, 0.012)])
+def test_demag_factor_of_a_cube(nc, tol):
+    # uniformly magnetised cube: N = 1/3 (Aharoni), FEM-BEM converges with h
+    mesh = meshgen.kuhn_cuboid(nc, nc, nc, 10.0 / nc)
+    pb = O.make_problem(mesh.xyz, mesh.tets, 1e-9, Ms=8e5, A=1.3e-11, alpha=1.0)
+    dm = O.DemagOracle(pb)
+    m = np.zeros((mesh.nx, 3))
+    m[:, 2] = 1.0
+    H = dm.field(m)
+    Nz = dm.energy(m, H) / (0.5 * pb.Js[0] * 8e5 * pb.fem.node_vol.sum())
+    assert abs(Nz - O.aharoni_nz(5.0, 5.0, 5.0)) < tol
+    assert abs(O.aharoni_nz(5.0, 5.0, 5.0) - 1.0 / 3.0) < 1e-12
+
+
+def test_llg_rhs_is_orthogonal_to_m():
+    rng = np.random.default_rng(3)
+    m = rng.standard_normal((50, 3))
+    m /= np.linalg.norm(m, axis=1, keepdims=True)
+    H = rng.standard_normal((50, 3)) * 1e5
+
+    class P:
+        alpha = 0.5
+
+    ydot = O.llg_rhs(P, m, H)
+    assert np.max(np.abs(np.sum(ydot * m, axis=1))) < 1e-9
+
+
+def test_dp45_on_linear_ode():
+    f = lambda t, y: -y  # noqa: E731
+    y, dt, acc, rej, nrhs = O.dp45_segment(f, np.array([1.0, 2.0]), 0.0, 3.0, 0.1,
+                                          O.StepControl(eps_abs=1e-10, eps_rel=1e-10))
+    assert np.allclose(y, np.exp(-3.0) * np.array([1.0, 2.0]), rtol=1e-8)
+    assert acc > 0 and nrhs == 6 * (acc + rej) + 1
+
+
+def test_golden_vectors():
+    g = np.load(GOLDEN)
+    n = g["xyz"].shape[0]
+    pb = O.make_problem(g["xyz"], g["tets"], 1e-9, Ms=8e5, A=1.3e-11, alpha=0.3, Ku=5e4, ku_axis=g["axis"],
+                        D=3e-3, hext=g["hext"])
+    assert np.max(np.abs(pb.B - g["B"])) < 1e-13
+    m = g["m"]
+    hdem = O.DemagOracle(pb).field(m)
+    assert np.linalg.norm(hdem - g["hdem"]) <= 1e-12 * np.linalg.norm(g["hdem"])
+    H = O.local_field(pb, m, hdem)
+    assert np.linalg.norm(H - g["H"]) <= 1e-12 * np.linalg.norm(g["H"])
+    ydot = O.llg_rhs(pb, m, H)
+    assert np.linalg.norm(ydot - g["ydot"]) <= 1e-12 * np.linalg.norm(g["ydot"])
+    assert n == 210

@@ -1,0 +1,381 @@
+"""Python host API over the C ABI, shaped like tetmag's own classes.
+
+* ``MeshOps``     -- preprocessing (PreprocessMesh / MeshBoundary), C++ in libtmb
+* ``Context``     -- one mesh on one GPU: operators, BEM, material, fields
+* ``DemagField``  -- ``calcField(m)`` as main/DemagField.h:91
+* ``TheLLG``      -- ``__call__(state, t)`` as TheLLG::operator() (main/TheLLG.h:148),
+                     ``rhs(t, y, ydot)`` as the CVODE callback (main/TheLLG.h:141),
+                     ``getMaxTorque(m)`` (main/TheLLG.cpp:426-439)
+* ``SolverFactory.makeSolver("b200")`` -- the solver plugin
+                     (main/SolverFactory.cpp:124-143), with setMatrix /
+                     setLoadVector / setCGTolerance / compute / solve / result /
+                     wasSuccessful / report.
+
+Arrays: numpy float64 (host) or CUDA torch float64 tensors (device pointers,
+ordered on the context stream).  Vectors of nodal 3-vectors are SoA, length 3N.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import check, lib
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _iptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _vec(a):
+    """(void* address, ptr_kind, keepalive) for numpy or torch arrays."""
+    if isinstance(a, np.ndarray):
+        if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+            raise TypeError("expected a C-contiguous float64 numpy array")
+        return a.ctypes.data, L.TMB_PTR_HOST
+    try:
+        import torch
+    except ImportError:  # pragma: no cover
+        torch = None
+    if torch is not None and isinstance(a, torch.Tensor):
+        if a.dtype != torch.float64 or not a.is_contiguous():
+            raise TypeError("expected a contiguous float64 tensor")
+        if a.is_cuda:
+            return a.data_ptr(), L.TMB_PTR_DEVICE
+        return a.data_ptr(), L.TMB_PTR_HOST
+    raise TypeError(f"unsupported array type {type(a)}")
+
+
+class MeshOps:
+    """Host mesh preprocessing in libtmb (tmb_mesh_*)."""
+
+    def __init__(self, xyz: np.ndarray, tets: np.ndarray):
+        self.xyz = _f64(xyz).reshape(-1, 3)
+        self.tets = _i32(tets).reshape(-1, 4)
+        h = C.c_void_p()
+        check(lib().tmb_mesh_create(self.xyz.shape[0], self.tets.shape[0], _dptr(self.xyz), _iptr(self.tets),
+                                    C.byref(h)))
+        self.h = h
+        info = (C.c_longlong * 6)()
+        check(lib().tmb_mesh_info(self.h, info))
+        self.nx, self.ntet, self.nnz, self.nb, self.ntri = (int(info[i]) for i in range(5))
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            lib().tmb_mesh_destroy(h)
+            self.h = None
+
+    def operators(self) -> dict:
+        n, z = self.nx, self.nnz
+        out = dict(rowptr=np.empty(n + 1, np.int32), col=np.empty(z, np.int32), stiff=np.empty(z),
+                   gx=np.empty(z), gy=np.empty(z), gz=np.empty(z), tgx=np.empty(z), tgy=np.empty(z),
+                   tgz=np.empty(z), node_vol=np.empty(n))
+        check(lib().tmb_mesh_get_operators(self.h, _iptr(out["rowptr"]), _iptr(out["col"]), _dptr(out["stiff"]),
+                                           _dptr(out["gx"]), _dptr(out["gy"]), _dptr(out["gz"]), _dptr(out["tgx"]),
+                                           _dptr(out["tgy"]), _dptr(out["tgz"]), _dptr(out["node_vol"])))
+        return out
+
+    def boundary(self) -> dict:
+        n, nb, nt = self.nx, self.nb, self.ntri
+        out = dict(bnodes=np.empty(nb, np.int32), tri=np.empty(3 * nt, np.int32), tri_area=np.empty(nt),
+                   tri_normal=np.empty(3 * nt), node_area=np.empty(n), node_normal=np.empty(3 * n),
+                   solid_angle=np.empty(nb))
+        check(lib().tmb_mesh_get_boundary(self.h, _iptr(out["bnodes"]), _iptr(out["tri"]), _dptr(out["tri_area"]),
+                                          _dptr(out["tri_normal"]), _dptr(out["node_area"]),
+                                          _dptr(out["node_normal"]), _dptr(out["solid_angle"])))
+        return out
+
+
+class Context:
+    """One mesh on one device (tmb_ctx)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(lib().tmb_ctx_create(device, C.byref(h)))
+        self.h = h
+        self.n = 0
+        self.nb = 0
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            lib().tmb_ctx_destroy(h)
+            self.h = None
+
+    # --- setup ---------------------------------------------------------------------------
+    def set_mesh(self, mesh: MeshOps):
+        check(lib().tmb_set_mesh(self.h, mesh.h))
+        self.n, self.nb = mesh.nx, mesh.nb
+        return self
+
+    def set_operators(self, rowptr, col, stiff, grad, tgrad, node_vol, bnodes, node_area, node_normal_soa):
+        rp, cl = _i32(rowptr), _i32(col)
+        arrs = [_f64(stiff)] + [_f64(g) for g in grad] + [_f64(t) for t in tgrad]
+        nv, bn, na, nn = _f64(node_vol), _i32(bnodes), _f64(node_area), _f64(node_normal_soa)
+        n = rp.size - 1
+        check(lib().tmb_set_operators(self.h, n, int(rp[-1]), _iptr(rp), _iptr(cl), *[_dptr(a) for a in arrs],
+                                      _dptr(nv), bn.size, _iptr(bn), _dptr(na), _dptr(nn)))
+        self.n, self.nb = n, bn.size
+        return self
+
+    def bem_assemble(self, mesh: MeshOps):
+        check(lib().tmb_bem_assemble(self.h, mesh.h))
+        return self
+
+    def set_bem_dense(self, B: np.ndarray):
+        Bc = np.asfortranarray(B, dtype=np.float64)
+        check(lib().tmb_set_bem_dense(self.h, Bc.shape[0], Bc.ctypes.data_as(C.POINTER(C.c_double))))
+        return self
+
+    def get_bem_dense(self) -> np.ndarray:
+        B = np.empty((self.nb, self.nb), order="F")
+        check(lib().tmb_get_bem_dense(self.h, B.ctypes.data_as(C.POINTER(C.c_double))))
+        return B
+
+    def set_material(self, Js, A, Ku=None, ku_axis=None, D=None, alpha=1.0):
+        n = self.n
+        js, a = _f64(np.broadcast_to(Js, (n,))), _f64(np.broadcast_to(A, (n,)))
+        ku = None if Ku is None else _f64(np.broadcast_to(Ku, (n,)))
+        ax = None if ku_axis is None else _f64(ku_axis)
+        d = None if D is None else _f64(np.broadcast_to(D, (n,)))
+        check(lib().tmb_set_material(self.h, _dptr(js), _dptr(a), _dptr(ku) if ku is not None else None,
+                                     _dptr(ax) if ax is not None else None, _dptr(d) if d is not None else None,
+                                     float(alpha)))
+        return self
+
+    def set_applied_field(self, hext):
+        p, k = _vec(hext)
+        check(lib().tmb_set_applied_field(self.h, p, k))
+        return self
+
+    def set_precision(self, mixed: bool):
+        check(lib().tmb_set_precision(self.h, L.TMB_MIXED if mixed else L.TMB_FP64))
+        return self
+
+    def set_solver_params(self, tol: float, maxiter: int = 100):
+        check(lib().tmb_set_solver_params(self.h, float(tol), int(maxiter)))
+        return self
+
+    def set_llg_options(self, precession: bool = True):
+        check(lib().tmb_set_llg_options(self.h, 1 if precession else 0))
+        return self
+
+    def set_stream(self, stream_handle: Optional[int]):
+        check(lib().tmb_ctx_set_stream(self.h, C.c_void_p(stream_handle) if stream_handle else None))
+        return self
+
+    # --- evaluation ----------------------------------------------------------------------
+    def _out_like(self, m):
+        if isinstance(m, np.ndarray):
+            return np.empty(3 * self.n)
+        import torch
+        return torch.empty(3 * self.n, dtype=torch.float64, device=m.device)
+
+    def demag_field(self, m, out=None):
+        out = self._out_like(m) if out is None else out
+        pm, k = _vec(m)
+        po, _ = _vec(out)
+        check(lib().tmb_demag_field(self.h, pm, po, k))
+        return out
+
+    def field_eval(self, m, ydot=None, hdem=None):
+        """Full field evaluation (demag chain + local field + LLG right-hand side)."""
+        ydot = self._out_like(m) if ydot is None else ydot
+        pm, k = _vec(m)
+        py, _ = _vec(ydot)
+        ph = _vec(hdem)[0] if hdem is not None else None
+        check(lib().tmb_field_eval(self.h, pm, py, ph, k))
+        return ydot
+
+    def set_demag_frozen(self, hdem):
+        p, k = _vec(hdem)
+        check(lib().tmb_set_demag_frozen(self.h, p, k))
+
+    def effective_field(self, m, out=None):
+        out = self._out_like(m) if out is None else out
+        pm, k = _vec(m)
+        po, _ = _vec(out)
+        check(lib().tmb_effective_field(self.h, pm, po, k))
+        return out
+
+    def llg_rhs(self, t, y, out=None):
+        out = self._out_like(y) if out is None else out
+        py, k = _vec(y)
+        po, _ = _vec(out)
+        check(lib().tmb_llg_rhs(self.h, float(t), py, po, k))
+        return out
+
+    def max_torque(self, m) -> float:
+        v = C.c_double()
+        pm, k = _vec(m)
+        check(lib().tmb_max_torque(self.h, pm, C.byref(v), k))
+        return v.value
+
+    def normalize(self, m):
+        pm, k = _vec(m)
+        check(lib().tmb_normalize(self.h, pm, k))
+        return m
+
+    def relax(self, m, duration_ps, segment_ps=0.5, eps_abs=1e-6, eps_rel=1e-6) -> dict:
+        st = (C.c_double * 12)()
+        pm, k = _vec(m)
+        check(lib().tmb_relax(self.h, pm, float(duration_ps), float(segment_ps), float(eps_abs), float(eps_rel),
+                              st, k))
+        keys = ["accepted", "rejected", "rhs", "demag", "cg_neumann", "cg_dirichlet", "max_torque", "dt",
+                "segments"]
+        return {kk: st[i] for i, kk in enumerate(keys)}
+
+    def stats(self) -> dict:
+        st = (C.c_double * 8)()
+        check(lib().tmb_get_stats(self.h, st))
+        keys = ["it_neumann", "it_dirichlet", "res_neumann", "res_dirichlet", "status_neumann",
+                "status_dirichlet", "amg_levels", "amg_setup_ms"]
+        return {kk: st[i] for i, kk in enumerate(keys)}
+
+
+def kernel_launches() -> int:
+    v = C.c_longlong()
+    check(lib().tmb_kernel_launches(C.byref(v)))
+    return int(v.value)
+
+
+PROFILE_IDS = ["local_llg", "divergence", "gradient", "bem_matvec", "solve_neumann", "solve_dirichlet",
+               "cg_spmv", "demag_chain"]
+
+
+def profile_enable(ctx: "Context", on: bool = True):
+    check(lib().tmb_profile_enable(ctx.h, 1 if on else 0))
+
+
+def profile_read(ctx: "Context") -> dict:
+    st = (C.c_double * (3 * len(PROFILE_IDS)))()
+    check(lib().tmb_profile_read(ctx.h, st))
+    return {k: dict(launches=st[3 * i], total_ms=st[3 * i + 1], bytes_per_launch=st[3 * i + 2])
+            for i, k in enumerate(PROFILE_IDS)}
+
+
+class DemagField:
+    """DemagField::calcField (main/DemagField.cpp:92-94) on the device."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+
+    def calcField(self, m):
+        return self.ctx.demag_field(m)
+
+
+class TheLLG:
+    """TheLLG's right-hand side with frozen demag (main/TheLLG.cpp:119-124, 670-711)."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+
+    def setHdem(self, hdem):
+        self.ctx.set_demag_frozen(hdem)
+
+    def __call__(self, state, t: float = 0.0):
+        return self.ctx.llg_rhs(t, state)
+
+    def rhs(self, t: float, y, ydot) -> int:
+        """CVODE-style callback: fills ydot, returns 0 on success and -1 on failure."""
+        try:
+            self.ctx.llg_rhs(t, y, out=ydot)
+            return 0
+        except L.TmbError:
+            return -1
+
+    def getMaxTorque(self, m) -> float:
+        return self.ctx.max_torque(m)
+
+
+class B200Solver:
+    """The "b200" case of SolverFactory::makeSolver (main/SolverFactory.h:42-65)."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        h = C.c_void_p()
+        check(lib().tmb_solver_create(ctx.h, C.byref(h)))
+        self.h = h
+        self.n = 0
+        self.b = None
+        self.x = None
+        self.tol = 1e-7
+        self.maxiter = 100
+        self.preconditioner = "amg"
+        self._ok = False
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            lib().tmb_solver_destroy(h)
+            self.h = None
+
+    def setMatrix(self, A):
+        import scipy.sparse as sp
+        A = sp.csr_matrix(A)
+        A.sort_indices()
+        rp, cl, v = _i32(A.indptr), _i32(A.indices), _f64(A.data)
+        self.n = A.shape[0]
+        check(lib().tmb_solver_set_matrix(self.h, self.n, int(rp[-1]), _iptr(rp), _iptr(cl), _dptr(v)))
+
+    def setLoadVector(self, b):
+        self.b = _f64(b)
+
+    def setCGTolerance(self, tol: float):
+        self.tol = float(tol)
+
+    def definePreconditioner(self, name: str):
+        self.preconditioner = name
+
+    def compute(self) -> bool:
+        check(lib().tmb_solver_set_tolerance(self.h, self.tol, self.maxiter))
+        check(lib().tmb_solver_compute(self.h))
+        return True
+
+    def solve(self):
+        check(lib().tmb_solver_set_tolerance(self.h, self.tol, self.maxiter))
+        x = np.empty(self.n)
+        code = lib().tmb_solver_solve(self.h, self.b.ctypes.data, x.ctypes.data, L.TMB_PTR_HOST)
+        self._ok = code == L.TMB_OK
+        self.x = x
+        if code not in (L.TMB_OK, L.TMB_ERR_NOCONVERGE):
+            check(code)
+
+    def result(self) -> np.ndarray:
+        return self.x
+
+    def info(self) -> dict:
+        st = (C.c_double * 3)()
+        check(lib().tmb_solver_info(self.h, st))
+        return dict(iterations=int(st[0]), relres=st[1], status=int(st[2]))
+
+    def wasSuccessful(self) -> bool:
+        return self._ok and np.all(np.isfinite(self.x))
+
+    def report(self):
+        i = self.info()
+        print(f"b200 PCG+AMG: {i['iterations']} iterations, relative residual {i['relres']:.3e}, "
+              f"{'successful' if self.wasSuccessful() else 'FAILED'}")
+
+
+class SolverFactory:
+    @staticmethod
+    def makeSolver(kind: str, ctx: Context) -> B200Solver:
+        if kind.lower() != "b200":
+            raise ValueError(f"solver option not understood: {kind}")
+        return B200Solver(ctx)

@@ -1,0 +1,314 @@
+// Field kernels: fused local effective field + LLG right-hand side, the
+// demag divergence and gradient, normalisation and Runge-Kutta vector ops.
+//
+// The fused kernel replaces, per right-hand-side evaluation, the chain of
+// tetmag's GPU path: three exchange SpMVs (gpu/EffFieldGPU.cu:71-86), the
+// uniaxial Thrust passes (:538-560), six tGrad SpMVs + two passes for bulk
+// DMI (:150-162, 596-622), the host-side sum of the field terms
+// (main/TheLLG.cpp:238-254) and the LLG functor (gpu/EffFieldGPU.cu:316-339,
+// 407-430), plus the max-torque reduction (:484-512).  One thread owns one
+// node (row); its SELL-32 row is read once for all three components.
+#include <atomic>
+#include <cmath>
+
+#include "tmb_dev.cuh"
+
+namespace tmb {
+
+namespace {
+
+__device__ __forceinline__ unsigned long long ordered_bits(double v) {
+  // Non-negative doubles order like their bit patterns; NaN maps above +inf.
+  if (v != v) return 0x7FF8000000000000ull;
+  return static_cast<unsigned long long>(__double_as_longlong(v));
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const double w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = (w != w || w > v) ? w : v;
+  }
+  return v;
+}
+
+template <typename V>
+__device__ __forceinline__ double ld(const V* p, int k) {
+  return static_cast<double>(__ldg(p + k));
+}
+
+template <typename V, bool UNI, bool DMI>
+__global__ void __launch_bounds__(kBlock) k_local_field(SellView s, const V* __restrict__ K,
+                                                        const V* __restrict__ tg0, const V* __restrict__ tg1,
+                                                        const V* __restrict__ tg2, LocalFieldArgs a) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  double torque = 0.0;
+  if (row < a.n) {
+    const int n = a.n;
+    const double* __restrict__ mx = a.m;
+    const double* __restrict__ my = a.m + n;
+    const double* __restrict__ mz = a.m + 2 * n;
+    const int sl = row >> 5;
+    const int beg = __ldg(s.soff + sl) + (row & 31);
+    const int end = __ldg(s.soff + sl + 1);
+    double kx = 0.0, ky = 0.0, kz = 0.0;
+    double cxy = 0.0, cxz = 0.0, cyx = 0.0, cyz = 0.0, czx = 0.0, czy = 0.0;
+#pragma unroll 4
+    for (int k = beg; k < end; k += kSlice) {
+      const int j = __ldg(s.col + k);
+      const double v = ld(K, k);
+      const double ax = __ldg(mx + j), ay = __ldg(my + j), az = __ldg(mz + j);
+      kx = fma(v, ax, kx);
+      ky = fma(v, ay, ky);
+      kz = fma(v, az, kz);
+      if (DMI) {
+        const double t0 = ld(tg0, k), t1 = ld(tg1, k), t2 = ld(tg2, k);
+        cxy = fma(t0, ay, cxy);
+        cxz = fma(t0, az, cxz);
+        cyx = fma(t1, ax, cyx);
+        cyz = fma(t1, az, cyz);
+        czx = fma(t2, ax, czx);
+        czy = fma(t2, ay, czy);
+      }
+    }
+    const double m0 = mx[row], m1 = my[row], m2 = mz[row];
+    const double xc = a.xc[row];
+    double H0 = xc * kx, H1 = xc * ky, H2 = xc * kz;
+    if (UNI) {
+      const double e0 = a.kax[row], e1 = a.kax[row + n], e2 = a.kax[row + 2 * n];
+      const double f = a.ku2[row] * (e0 * m0 + e1 * m1 + e2 * m2);
+      H0 = fma(f, e0, H0);
+      H1 = fma(f, e1, H1);
+      H2 = fma(f, e2, H2);
+    }
+    if (DMI) {
+      // curl m with tGrad' = -tGrad (main/EffFieldCalc.cpp:43, 280-298)
+      const double c0 = -(cyz - czy), c1 = -(czx - cxz), c2 = -(cxy - cyx);
+      const double ar = a.area[row];
+      const double n0 = a.nvn[row], n1 = a.nvn[row + n], n2 = a.nvn[row + 2 * n];
+      const double s0 = ar * (m1 * n2 - m2 * n1), s1 = ar * (m2 * n0 - m0 * n2), s2 = ar * (m0 * n1 - m1 * n0);
+      const double ds = a.dmi_s[row];
+      H0 += ds * (s0 - 2.0 * c0);
+      H1 += ds * (s1 - 2.0 * c1);
+      H2 += ds * (s2 - 2.0 * c2);
+    }
+    if (a.hfix) {
+      H0 += a.hfix[row];
+      H1 += a.hfix[row + n];
+      H2 += a.hfix[row + 2 * n];
+    }
+    if (a.hout) {
+      a.hout[row] = H0;
+      a.hout[row + n] = H1;
+      a.hout[row + 2 * n] = H2;
+    }
+    const double x0 = m1 * H2 - m2 * H1, x1 = m2 * H0 - m0 * H2, x2 = m0 * H1 - m1 * H0;  // m x H
+    torque = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
+    if (a.ydot) {
+      const double d0 = m1 * x2 - m2 * x1, d1 = m2 * x0 - m0 * x2, d2 = m0 * x1 - m1 * x0;  // m x (m x H)
+      const double al = a.alpha;
+      if (a.precession) {
+        a.ydot[row] = -x0 - al * d0;
+        a.ydot[row + n] = -x1 - al * d1;
+        a.ydot[row + 2 * n] = -x2 - al * d2;
+      } else {
+        a.ydot[row] = -al * d0;
+        a.ydot[row + n] = -al * d1;
+        a.ydot[row + 2 * n] = -al * d2;
+      }
+    }
+  }
+  if (a.torque_bits) {
+    const double t = warp_max(torque);
+    if ((threadIdx.x & 31) == 0) atomicMax(a.torque_bits, ordered_bits(t));
+  }
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_divergence(SellView s, const V* __restrict__ tg0,
+                                                       const V* __restrict__ tg1, const V* __restrict__ tg2,
+                                                       const double* __restrict__ m, const double* __restrict__ js,
+                                                       double inv_mu0, double* __restrict__ rhs) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= s.n) return;
+  const int n = s.n;
+  const int sl = row >> 5;
+  const int beg = __ldg(s.soff + sl) + (row & 31);
+  const int end = __ldg(s.soff + sl + 1);
+  double acc = 0.0;
+#pragma unroll 4
+  for (int k = beg; k < end; k += kSlice) {
+    const int j = __ldg(s.col + k);
+    const double J = __ldg(js + j);
+    const double t = ld(tg0, k) * __ldg(m + j) + ld(tg1, k) * __ldg(m + n + j) + ld(tg2, k) * __ldg(m + 2 * n + j);
+    acc = fma(t, J, acc);
+  }
+  rhs[row] = acc * inv_mu0;
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_gradient(SellView s, const V* __restrict__ g0, const V* __restrict__ g1,
+                                                     const V* __restrict__ g2, const double* __restrict__ u1,
+                                                     const double* __restrict__ u2, const double* __restrict__ hext,
+                                                     double* __restrict__ hdem, double* __restrict__ hfix) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= s.n) return;
+  const int n = s.n;
+  const int sl = row >> 5;
+  const int beg = __ldg(s.soff + sl) + (row & 31);
+  const int end = __ldg(s.soff + sl + 1);
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+#pragma unroll 4
+  for (int k = beg; k < end; k += kSlice) {
+    const int j = __ldg(s.col + k);
+    const double u = u2 ? __ldg(u1 + j) + __ldg(u2 + j) : __ldg(u1 + j);
+    a0 = fma(ld(g0, k), u, a0);
+    a1 = fma(ld(g1, k), u, a1);
+    a2 = fma(ld(g2, k), u, a2);
+  }
+  if (hdem) {
+    hdem[row] = -a0;
+    hdem[row + n] = -a1;
+    hdem[row + 2 * n] = -a2;
+  }
+  if (hfix) {
+    const double e0 = hext ? hext[row] : 0.0, e1 = hext ? hext[row + n] : 0.0, e2 = hext ? hext[row + 2 * n] : 0.0;
+    hfix[row] = e0 - a0;
+    hfix[row + n] = e1 - a1;
+    hfix[row + 2 * n] = e2 - a2;
+  }
+}
+
+__global__ void k_normalize(int n, double* m) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double a = m[i], b = m[i + n], c = m[i + 2 * n];
+  const double inv = 1.0 / sqrt(a * a + b * b + c * c);
+  m[i] = a * inv;
+  m[i + n] = b * inv;
+  m[i + 2 * n] = c * inv;
+}
+
+struct Ptrs7 {
+  const double* p[7];
+  double c[7];
+};
+
+__global__ void k_rk_combine(int n3, const double* __restrict__ y, Ptrs7 k, int nk, double h, double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n3) return;
+  double acc = 0.0;
+  for (int j = 0; j < nk; ++j)
+    if (k.c[j] != 0.0) acc = fma(k.c[j], k.p[j][i], acc);
+  out[i] = fma(h, acc, y[i]);
+}
+
+__global__ void k_rk_error(int n3, const double* __restrict__ y, const double* __restrict__ k1, Ptrs7 k, int nk,
+                           double h, double eps_abs, double eps_rel, unsigned long long* err_bits) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double r = 0.0;
+  if (i < n3) {
+    double acc = 0.0;
+    for (int j = 0; j < nk; ++j)
+      if (k.c[j] != 0.0) acc = fma(k.c[j], k.p[j][i], acc);
+    const double sc = eps_abs + eps_rel * (fabs(y[i]) + h * fabs(k1[i]));
+    r = fabs(h * acc) / sc;
+  }
+  r = warp_max(r);
+  if ((threadIdx.x & 31) == 0) atomicMax(err_bits, ordered_bits(r));
+}
+
+__global__ void k_fill(double* p, double v, size_t n) {
+  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+__global__ void k_add(int n, const double* a, const double* b, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = a[i] + b[i];
+}
+
+std::atomic<long long> g_launches{0};
+
+}  // namespace
+
+long long launch_count() { return g_launches.load(); }
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+template <typename V>
+void launch_local_field(const SellView& s, const V* K, const V* tg0, const V* tg1, const V* tg2,
+                        const LocalFieldArgs& a, cudaStream_t st) {
+  note_launch();
+  const int g = grid_for(a.n);
+  const bool uni = a.ku2 != nullptr, dmi = a.dmi_s != nullptr;
+  if (uni && dmi) k_local_field<V, true, true><<<g, kBlock, 0, st>>>(s, K, tg0, tg1, tg2, a);
+  else if (uni) k_local_field<V, true, false><<<g, kBlock, 0, st>>>(s, K, tg0, tg1, tg2, a);
+  else if (dmi) k_local_field<V, false, true><<<g, kBlock, 0, st>>>(s, K, tg0, tg1, tg2, a);
+  else k_local_field<V, false, false><<<g, kBlock, 0, st>>>(s, K, tg0, tg1, tg2, a);
+  TMB_CUDA(cudaGetLastError());
+}
+
+template <typename V>
+void launch_divergence(const SellView& s, const V* tg0, const V* tg1, const V* tg2, const double* m,
+                       const double* js, double inv_mu0, double* rhs, cudaStream_t st) {
+  note_launch();
+  k_divergence<V><<<grid_for(s.n), kBlock, 0, st>>>(s, tg0, tg1, tg2, m, js, inv_mu0, rhs);
+  TMB_CUDA(cudaGetLastError());
+}
+
+template <typename V>
+void launch_gradient(const SellView& s, const V* g0, const V* g1, const V* g2, const double* u1,
+                     const double* u2, const double* hext, double* hdem, double* hfix, cudaStream_t st) {
+  note_launch();
+  k_gradient<V><<<grid_for(s.n), kBlock, 0, st>>>(s, g0, g1, g2, u1, u2, hext, hdem, hfix);
+  TMB_CUDA(cudaGetLastError());
+}
+
+void launch_normalize(int n, double* m, cudaStream_t st) {
+  note_launch();
+  k_normalize<<<grid_for(n), kBlock, 0, st>>>(n, m);
+  TMB_CUDA(cudaGetLastError());
+}
+
+void launch_rk_combine(int n3, const double* y, const double* const* k, const double* a, int nk, double h,
+                       double* out, cudaStream_t st) {
+  note_launch();
+  Ptrs7 P{};
+  for (int j = 0; j < nk && j < 7; ++j) { P.p[j] = k[j]; P.c[j] = a[j]; }
+  k_rk_combine<<<grid_for(n3), kBlock, 0, st>>>(n3, y, P, nk, h, out);
+  TMB_CUDA(cudaGetLastError());
+}
+
+void launch_rk_error(int n3, const double* y, const double* k1, const double* const* k, const double* e, int nk,
+                     double h, double eps_abs, double eps_rel, unsigned long long* err_bits, cudaStream_t st) {
+  note_launch();
+  Ptrs7 P{};
+  for (int j = 0; j < nk && j < 7; ++j) { P.p[j] = k[j]; P.c[j] = e[j]; }
+  k_rk_error<<<grid_for(n3), kBlock, 0, st>>>(n3, y, k1, P, nk, h, eps_abs, eps_rel, err_bits);
+  TMB_CUDA(cudaGetLastError());
+}
+
+void launch_fill(double* p, double v, size_t n, cudaStream_t st) {
+  note_launch();
+  if (n == 0) return;
+  k_fill<<<grid_for((long long)n), kBlock, 0, st>>>(p, v, n);
+  TMB_CUDA(cudaGetLastError());
+}
+
+void launch_add(int n, const double* a, const double* b, double* out, cudaStream_t st) {
+  note_launch();
+  k_add<<<grid_for(n), kBlock, 0, st>>>(n, a, b, out);
+  TMB_CUDA(cudaGetLastError());
+}
+
+#define TMB_INST(V)                                                                                         \
+  template void launch_local_field<V>(const SellView&, const V*, const V*, const V*, const V*,             \
+                                      const LocalFieldArgs&, cudaStream_t);                                \
+  template void launch_divergence<V>(const SellView&, const V*, const V*, const V*, const double*,         \
+                                     const double*, double, double*, cudaStream_t);                        \
+  template void launch_gradient<V>(const SellView&, const V*, const V*, const V*, const double*,           \
+                                   const double*, const double*, double*, double*, cudaStream_t);
+TMB_INST(double)
+TMB_INST(float)
+#undef TMB_INST
+
+}  // namespace tmb

@@ -1,0 +1,342 @@
+// Device kernels of the preconditioned CG solver and its AMG V-cycle.
+//
+// These replace the linear-solver plugin of tetmag's demag chain
+// (SolverFactory, main/SolverFactory.h:42-65; the AMGCL-CUDA GPUSolver,
+// gpu/GPUSolver.cu:43-97), which copies b to the device and x back on every
+// solve.  Here the right-hand side is produced on the device, the scalars of
+// CG (rho, alpha, beta, ||r||) live in device memory and are updated by the
+// last block of each reduction kernel, and the host only polls a converged
+// flag.  Dot products are accumulated in FP64 with warp shuffles, a fixed
+// per-block order and a fixed final order (deterministic for a given grid).
+#include "tmb_dev.cuh"
+
+namespace tmb {
+
+namespace {
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Sum over the block; the result is valid in thread 0.
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double sh[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) sh[warp] = v;
+  __syncthreads();
+  const int nw = (blockDim.x + 31) >> 5;
+  if (warp == 0) {
+    v = (lane < nw) ? sh[lane] : 0.0;
+    v = warp_sum(v);
+  }
+  return v;
+}
+
+// Publishes this block's partial sums; returns true in every thread of the last
+// block to finish, which then holds the grid totals in tot[0..K-1] (thread 0).
+template <int K>
+__device__ __forceinline__ bool grid_reduce(const double (&v)[K], double* partials, unsigned int* ticket,
+                                            double (&tot)[K]) {
+  __shared__ bool last;
+  double bs[K];
+#pragma unroll
+  for (int q = 0; q < K; ++q) bs[q] = block_sum(v[q]);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < K; ++q) partials[size_t(q) * gridDim.x + blockIdx.x] = bs[q];
+    __threadfence();
+    const unsigned int t = atomicAdd(ticket, 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+#pragma unroll
+  for (int q = 0; q < K; ++q) {
+    double s = 0.0;
+    for (int i = threadIdx.x; i < int(gridDim.x); i += blockDim.x) s += __ldcg(partials + size_t(q) * gridDim.x + i);
+    tot[q] = block_sum(s);
+  }
+  if (threadIdx.x == 0) *ticket = 0u;
+  return true;
+}
+
+template <typename V>
+__device__ __forceinline__ double sell_row_dot(const SellView& s, const V* __restrict__ val,
+                                               const double* __restrict__ x, int row) {
+  const int sl = row >> 5;
+  const int beg = __ldg(s.soff + sl) + (row & 31);
+  const int end = __ldg(s.soff + sl + 1);
+  double acc = 0.0;
+#pragma unroll 4
+  for (int k = beg; k < end; k += kSlice) acc = fma(static_cast<double>(__ldg(val + k)), __ldg(x + __ldg(s.col + k)), acc);
+  return acc;
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_spmv(SellView s, const V* __restrict__ val, const double* __restrict__ x,
+                                                 double* __restrict__ y, const int* done) {
+  if (done && *done) return;
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row < s.n) y[row] = sell_row_dot(s, val, x, row);
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_residual(SellView s, const V* __restrict__ val,
+                                                     const double* __restrict__ b, const double* __restrict__ x,
+                                                     double* __restrict__ r, const int* done) {
+  if (done && *done) return;
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row < s.n) r[row] = b[row] - sell_row_dot(s, val, x, row);
+}
+
+__global__ void k_jacobi0(int n, const double* __restrict__ dinv, const double* __restrict__ b,
+                          double* __restrict__ x, const int* done) {
+  if (done && *done) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] = dinv[i] * b[i];
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_jacobi(SellView s, const V* __restrict__ val,
+                                                   const double* __restrict__ dinv, const double* __restrict__ b,
+                                                   const double* __restrict__ xin, double* __restrict__ xout,
+                                                   const int* done) {
+  if (done && *done) return;
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row < s.n) xout[row] = xin[row] + dinv[row] * (b[row] - sell_row_dot(s, val, xin, row));
+}
+
+// CSR product for the transfer operators; 4 threads cooperate on a row.
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_csr_spmv(CsrView c, const V* __restrict__ val,
+                                                     const double* __restrict__ x, double* __restrict__ y,
+                                                     int accumulate, const int* done) {
+  if (done && *done) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int row = t >> 2, sub = t & 3;
+  double acc = 0.0;
+  if (row < c.n) {
+    const int beg = __ldg(c.ptr + row), end = __ldg(c.ptr + row + 1);
+    for (int k = beg + sub; k < end; k += 4) acc = fma(static_cast<double>(__ldg(val + k)), __ldg(x + __ldg(c.col + k)), acc);
+  }
+  acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+  acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+  if (row < c.n && sub == 0) y[row] = accumulate ? y[row] + acc : acc;
+}
+
+// x = A_c^-1 b on the coarsest level: one warp per row of the dense FP64 inverse.
+__global__ void k_coarse_solve(int n, const double* __restrict__ inv, const double* __restrict__ b,
+                               double* __restrict__ x, const int* done) {
+  if (done && *done) return;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const double* row = inv + size_t(warp) * n;
+  double acc = 0.0;
+  for (int j = lane; j < n; j += 32) acc = fma(row[j], b[j], acc);
+  acc = warp_sum(acc);
+  if (lane == 0) x[warp] = acc;
+}
+
+template <typename V>
+__global__ void k_cg_init(int n, CsrView lift, const V* __restrict__ lval, const int* __restrict__ cmask,
+                          const double* __restrict__ b, double* __restrict__ bprime, double* __restrict__ x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (cmask[i]) {
+    bprime[i] = b[i];
+    x[i] = b[i];
+  } else {
+    double acc = b[i];
+    for (int k = lift.ptr[i]; k < lift.ptr[i + 1]; ++k) acc -= static_cast<double>(lval[k]) * b[lift.col[k]];
+    bprime[i] = acc;
+  }
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_cg_residual(SellView s, const V* __restrict__ val,
+                                                        const double* __restrict__ bp, const double* __restrict__ x,
+                                                        double* __restrict__ r, CgScalars* S, double* partials) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[2] = {0.0, 0.0};
+  if (row < s.n) {
+    const double ri = bp[row] - sell_row_dot(s, val, x, row);
+    r[row] = ri;
+    v[0] = ri * ri;
+    v[1] = bp[row] * bp[row];
+  }
+  double tot[2];
+  if (grid_reduce<2>(v, partials, &S->ticket[0], tot) && threadIdx.x == 0) {
+    S->rr = tot[0];
+    S->bb = tot[1];
+    S->iter = 0;
+    S->status = 0;
+    if (tot[1] == 0.0) {
+      S->done = 1;
+      S->status = 2;  // zero right-hand side: the host sets x = 0
+    } else {
+      S->done = (tot[0] <= S->tol2 * tot[1]) ? 1 : 0;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_cg_rz(int n, const double* __restrict__ r, const double* __restrict__ z,
+                                                  CgScalars* S, double* partials, int first) {
+  if (S->done) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[1] = {i < n ? r[i] * z[i] : 0.0};
+  double tot[1];
+  if (grid_reduce<1>(v, partials, &S->ticket[1], tot) && threadIdx.x == 0) {
+    if (first) {
+      S->beta = 0.0;
+    } else {
+      S->beta = tot[0] / S->rz;
+    }
+    S->rz = tot[0];
+  }
+}
+
+__global__ void k_cg_pupdate(int n, const double* __restrict__ z, double* __restrict__ p, const CgScalars* S) {
+  if (S->done) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double beta = S->beta;
+  p[i] = (beta == 0.0) ? z[i] : fma(beta, p[i], z[i]);
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_cg_spmv_pq(SellView s, const V* __restrict__ val,
+                                                       const double* __restrict__ p, double* __restrict__ q,
+                                                       CgScalars* S, double* partials) {
+  if (S->done) return;
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[1] = {0.0};
+  if (row < s.n) {
+    const double qi = sell_row_dot(s, val, p, row);
+    q[row] = qi;
+    v[0] = p[row] * qi;
+  }
+  double tot[1];
+  if (grid_reduce<1>(v, partials, &S->ticket[2], tot) && threadIdx.x == 0) {
+    S->pq = tot[0];
+    S->alpha = S->rz / tot[0];
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_cg_update(int n, const double* __restrict__ p,
+                                                      const double* __restrict__ q, double* __restrict__ x,
+                                                      double* __restrict__ r, CgScalars* S, double* partials) {
+  if (S->done) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const double alpha = S->alpha;
+  double v[1] = {0.0};
+  if (i < n) {
+    x[i] = fma(alpha, p[i], x[i]);
+    const double ri = fma(-alpha, q[i], r[i]);
+    r[i] = ri;
+    v[0] = ri * ri;
+  }
+  double tot[1];
+  if (grid_reduce<1>(v, partials, &S->ticket[3], tot) && threadIdx.x == 0) {
+    S->rr = tot[0];
+    S->iter += 1;
+    if (!(tot[0] == tot[0]) || !(S->pq > 0.0)) {
+      S->done = 1;
+      S->status = 5;  // breakdown / NaN
+    } else if (tot[0] <= S->tol2 * S->bb) {
+      S->done = 1;
+    } else if (S->iter >= S->maxit) {
+      S->done = 1;
+      S->status = 3;  // not converged within maxit
+    }
+  }
+}
+
+}  // namespace
+
+template <typename V>
+void launch_spmv(const SellView& s, const V* val, const double* x, double* y, const int* done, cudaStream_t st) {
+  note_launch();
+  k_spmv<V><<<grid_for(s.n), kBlock, 0, st>>>(s, val, x, y, done);
+}
+template <typename V>
+void launch_residual(const SellView& s, const V* val, const double* b, const double* x, double* r,
+                     const int* done, cudaStream_t st) {
+  note_launch();
+  k_residual<V><<<grid_for(s.n), kBlock, 0, st>>>(s, val, b, x, r, done);
+}
+void launch_jacobi0(int n, const double* dinv, const double* b, double* x, const int* done, cudaStream_t st) {
+  note_launch();
+  k_jacobi0<<<grid_for(n), kBlock, 0, st>>>(n, dinv, b, x, done);
+}
+template <typename V>
+void launch_jacobi(const SellView& s, const V* val, const double* dinv, const double* b, const double* xin,
+                   double* xout, const int* done, cudaStream_t st) {
+  note_launch();
+  k_jacobi<V><<<grid_for(s.n), kBlock, 0, st>>>(s, val, dinv, b, xin, xout, done);
+}
+template <typename V>
+void launch_csr_spmv(const CsrView& c, const V* val, const double* x, double* y, bool accumulate,
+                     const int* done, cudaStream_t st) {
+  note_launch();
+  k_csr_spmv<V><<<grid_for(4LL * c.n), kBlock, 0, st>>>(c, val, x, y, accumulate ? 1 : 0, done);
+}
+void launch_coarse_solve(int n, const double* inv, const double* b, double* x, const int* done, cudaStream_t st) {
+  note_launch();
+  k_coarse_solve<<<grid_for(32LL * n), kBlock, 0, st>>>(n, inv, b, x, done);
+}
+template <typename V>
+void launch_cg_init(int n, const CsrView& lift, const V* lval, const int* cmask, const double* b,
+                    double* bprime, double* x, cudaStream_t st) {
+  note_launch();
+  k_cg_init<V><<<grid_for(n), kBlock, 0, st>>>(n, lift, lval, cmask, b, bprime, x);
+}
+template <typename V>
+void launch_cg_residual(const SellView& s, const V* val, const double* bp, const double* x, double* r,
+                        CgScalars* S, double* partials, cudaStream_t st) {
+  note_launch();
+  k_cg_residual<V><<<grid_for(s.n), kBlock, 0, st>>>(s, val, bp, x, r, S, partials);
+}
+void launch_cg_rz(int n, const double* r, const double* z, CgScalars* S, double* partials, bool first,
+                  cudaStream_t st) {
+  note_launch();
+  k_cg_rz<<<grid_for(n), kBlock, 0, st>>>(n, r, z, S, partials, first ? 1 : 0);
+}
+void launch_cg_pupdate(int n, const double* z, double* p, CgScalars* S, cudaStream_t st) {
+  note_launch();
+  k_cg_pupdate<<<grid_for(n), kBlock, 0, st>>>(n, z, p, S);
+}
+template <typename V>
+void launch_cg_spmv_pq(const SellView& s, const V* val, const double* p, double* q, CgScalars* S,
+                       double* partials, cudaStream_t st) {
+  note_launch();
+  k_cg_spmv_pq<V><<<grid_for(s.n), kBlock, 0, st>>>(s, val, p, q, S, partials);
+}
+void launch_cg_update(int n, const double* p, const double* q, double* x, double* r, CgScalars* S,
+                      double* partials, cudaStream_t st) {
+  note_launch();
+  k_cg_update<<<grid_for(n), kBlock, 0, st>>>(n, p, q, x, r, S, partials);
+}
+
+#define TMB_INST(V)                                                                                          \
+  template void launch_spmv<V>(const SellView&, const V*, const double*, double*, const int*, cudaStream_t); \
+  template void launch_residual<V>(const SellView&, const V*, const double*, const double*, double*,        \
+                                   const int*, cudaStream_t);                                               \
+  template void launch_jacobi<V>(const SellView&, const V*, const double*, const double*, const double*,    \
+                                 double*, const int*, cudaStream_t);                                        \
+  template void launch_csr_spmv<V>(const CsrView&, const V*, const double*, double*, bool, const int*,      \
+                                   cudaStream_t);                                                           \
+  template void launch_cg_init<V>(int, const CsrView&, const V*, const int*, const double*, double*,        \
+                                  double*, cudaStream_t);                                                   \
+  template void launch_cg_residual<V>(const SellView&, const V*, const double*, const double*, double*,     \
+                                      CgScalars*, double*, cudaStream_t);                                   \
+  template void launch_cg_spmv_pq<V>(const SellView&, const V*, const double*, double*, CgScalars*,         \
+                                     double*, cudaStream_t);
+TMB_INST(double)
+TMB_INST(float)
+#undef TMB_INST
+
+}  // namespace tmb

@@ -1,0 +1,1369 @@
+// Host runtime of the tetmag B200 library and its C ABI (include/tmb.h).
+//
+// Mirrors the reference's host classes on the hot path:
+//   Solver    <- SolverFactory / AMGCLSolver / GPUSolver (main/SolverFactory.h:42-65,
+//                main/AMGCLSolver.cpp:39-113, gpu/GPUSolver.cu:43-97)
+//   Ctx::demag <- DemagField::calcField (main/DemagField.cpp:92-240)
+//   Ctx::local <- TheLLG::classicVersion / noPrecession + totalEffectiveField
+//                (main/TheLLG.cpp:150-199, 238-254)
+//   Ctx::relax <- TheSimulation::start outer loop (main/TheSimulation.cpp:231-311)
+//                with the Dormand-Prince stepper of TheLLG::IntegrateODEINT
+//                (main/TheLLG.cpp:514-572)
+// Everything between the caller's input and output stays on the device; the
+// host only launches kernels and polls convergence / step-error scalars.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/tmb.h"
+#include "tmb_dev.cuh"
+#include "tmb_host.h"
+
+namespace tmb {
+
+constexpr double kMu0 = 1.256637061435917295376e-6;   // utils/PhysicalConstants.h:39
+constexpr double kGamma0 = 221276.14886372426114160400;  // utils/PhysicalConstants.h:43
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+template <typename T>
+struct DevArray {
+  T* p = nullptr;
+  size_t n = 0;
+  DevArray() = default;
+  DevArray(const DevArray&) = delete;
+  DevArray& operator=(const DevArray&) = delete;
+  DevArray(DevArray&& o) noexcept : p(o.p), n(o.n) {
+    o.p = nullptr;
+    o.n = 0;
+  }
+  DevArray& operator=(DevArray&& o) noexcept {
+    if (this != &o) {
+      reset();
+      p = o.p;
+      n = o.n;
+      o.p = nullptr;
+      o.n = 0;
+    }
+    return *this;
+  }
+  ~DevArray() { reset(); }
+  void reset() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    if (count == n && p) return;
+    reset();
+    if (count) TMB_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    n = count;
+  }
+  void upload(const T* h, size_t count, cudaStream_t st) {
+    alloc(count);
+    if (count) TMB_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, st));
+  }
+  void upload(const std::vector<T>& v, cudaStream_t st) { upload(v.data(), v.size(), st); }
+  void zero(cudaStream_t st) {
+    if (n) TMB_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), st));
+  }
+  void swap(DevArray& o) noexcept {
+    std::swap(p, o.p);
+    std::swap(n, o.n);
+  }
+};
+
+// ------------------------------------------------------------------------------------------
+// SELL-32 construction
+// ------------------------------------------------------------------------------------------
+struct SellHost {
+  int n = 0, nslice = 0;
+  std::vector<int> soff, col;
+  std::vector<int64_t> map;  // CSR position -> SELL position
+};
+
+static SellHost build_sell(int n, const int* ptr, const int* col) {
+  SellHost S;
+  S.n = n;
+  S.nslice = (n + kSlice - 1) / kSlice;
+  S.soff.assign(S.nslice + 1, 0);
+  for (int s = 0; s < S.nslice; ++s) {
+    int w = 0;
+    for (int r = s * kSlice; r < std::min(n, (s + 1) * kSlice); ++r) w = std::max(w, ptr[r + 1] - ptr[r]);
+    const int64_t next = int64_t(S.soff[s]) + int64_t(kSlice) * w;
+    if (next > 0x7fffffffLL) throw Error(TMB_ERR_ARG, "operator too large for int32 SELL offsets");
+    S.soff[s + 1] = int(next);
+  }
+  S.col.assign(S.soff[S.nslice], 0);
+  S.map.assign(ptr[n], 0);
+  for (int s = 0; s < S.nslice; ++s) {
+    const int w = (S.soff[s + 1] - S.soff[s]) / kSlice;
+    for (int lane = 0; lane < kSlice; ++lane) {
+      const int r = s * kSlice + lane;
+      const int len = (r < n) ? ptr[r + 1] - ptr[r] : 0;
+      const int pad = (r < n) ? r : n - 1;
+      for (int k = 0; k < w; ++k) {
+        const int pos = S.soff[s] + k * kSlice + lane;
+        if (k < len) {
+          S.col[pos] = col[ptr[r] + k];
+          S.map[ptr[r] + k] = pos;
+        } else {
+          S.col[pos] = pad;
+        }
+      }
+    }
+  }
+  return S;
+}
+
+template <typename V>
+static std::vector<V> sell_values(const SellHost& S, const double* v) {
+  std::vector<V> out(S.col.size(), V(0));
+  for (size_t k = 0; k < S.map.size(); ++k) out[S.map[k]] = static_cast<V>(v[k]);
+  return out;
+}
+
+struct DevSell {
+  int n = 0, nslice = 0;
+  DevArray<int> soff, col;
+  SellView view() const { return SellView{n, nslice, soff.p, col.p}; }
+  void upload(const SellHost& S, cudaStream_t st) {
+    n = S.n;
+    nslice = S.nslice;
+    soff.upload(S.soff, st);
+    col.upload(S.col, st);
+  }
+};
+
+struct DevCsr {
+  int n = 0;
+  DevArray<int> ptr, col;
+  DevArray<double> v;
+  DevArray<float> vf;
+  CsrView view() const { return CsrView{n, ptr.p, col.p}; }
+  void upload(const Csr& A, cudaStream_t st) {
+    n = A.nrows;
+    ptr.upload(A.ptr, st);
+    col.upload(A.col, st);
+    v.upload(A.val, st);
+    std::vector<float> f(A.val.begin(), A.val.end());
+    vf.upload(f, st);
+  }
+};
+
+struct Ctx;
+
+// ------------------------------------------------------------------------------------------
+// Live kernel profiler: CUDA events around the main kernels on the launching stream.
+// ids: 0 local field + LLG, 1 divergence, 2 gradient, 3 BEM matvec, 4 Neumann solve,
+//      5 Dirichlet solve, 6 CG fine-level SpMV, 7 whole demag chain
+// ------------------------------------------------------------------------------------------
+constexpr int kProfIds = 8;
+struct Prof {
+  bool on = false;
+  struct Rec {
+    int id;
+    cudaEvent_t a, b;
+    double bytes;
+  };
+  std::vector<cudaEvent_t> pool;
+  size_t used = 0;
+  std::vector<Rec> recs;
+  double count[kProfIds] = {}, ms[kProfIds] = {}, bytes[kProfIds] = {};
+  ~Prof() {
+    for (auto e : pool) cudaEventDestroy(e);
+  }
+  cudaEvent_t get() {
+    if (used == pool.size()) {
+      cudaEvent_t e;
+      TMB_CUDA(cudaEventCreate(&e));
+      pool.push_back(e);
+    }
+    return pool[used++];
+  }
+  std::vector<size_t> open;  // indices of records whose end is pending (nesting allowed)
+  void begin(int id, cudaStream_t st, double b) {
+    if (!on) return;
+    Rec r{id, get(), get(), b};
+    TMB_CUDA(cudaEventRecord(r.a, st));
+    open.push_back(recs.size());
+    recs.push_back(r);
+  }
+  void end(cudaStream_t st) {
+    if (!on || open.empty()) return;
+    TMB_CUDA(cudaEventRecord(recs[open.back()].b, st));
+    open.pop_back();
+    if (open.empty() && used > 4000) flush();
+  }
+  void flush() {
+    if (!open.empty()) return;
+    for (const Rec& r : recs) {
+      TMB_CUDA(cudaEventSynchronize(r.b));
+      float t = 0.f;
+      TMB_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
+      count[r.id] += 1;
+      ms[r.id] += t;
+      bytes[r.id] += r.bytes;
+    }
+    recs.clear();
+    used = 0;
+  }
+  void reset() {
+    open.clear();
+    recs.clear();
+    used = 0;
+    for (int i = 0; i < kProfIds; ++i) count[i] = ms[i] = bytes[i] = 0.0;
+  }
+};
+
+// ------------------------------------------------------------------------------------------
+// Solver: PCG + smoothed-aggregation V-cycle for row-constrained SPD systems
+// ------------------------------------------------------------------------------------------
+struct DevLevel {
+  int n = 0;
+  DevSell A;
+  DevArray<double> Ad, dinv, X, R, b, out;
+  DevArray<float> Af;
+  DevCsr P, Rop;
+};
+
+struct Solver {
+  Ctx* ctx;
+  Csr A;                      // as given (rows may be constraints)
+  double tol = 1e-7;
+  int maxit = 100;
+  int check_every = 2;
+  bool computed = false;
+  int n = 0;
+  AmgParams prm;
+  AmgHierarchy H;
+  std::vector<DevLevel> lev;
+  DevArray<double> cinv;
+  int ncoarse = 0;
+  DevCsr lift;
+  DevArray<int> cmask;
+  DevArray<double> x, r, z, p, q, bp, partials;
+  CgScalars* Sd = nullptr;
+  CgScalars* Sh = nullptr;
+  int last_iters = 0, last_status = 0;
+  double last_relres = 0.0;
+  bool has_x = false;
+
+  explicit Solver(Ctx* c) : ctx(c) {}
+  ~Solver() {
+    if (Sd) cudaFree(Sd);
+    if (Sh) cudaFreeHost(Sh);
+  }
+  void set_matrix(int nn, const int* ptr, const int* col, const double* val) {
+    A.nrows = A.ncols = nn;
+    A.ptr.assign(ptr, ptr + nn + 1);
+    A.col.assign(col, col + ptr[nn]);
+    A.val.assign(val, val + ptr[nn]);
+    computed = false;
+  }
+  void compute();
+  void solve(const double* b_dev, int precision);
+  void vcycle(size_t l, const double* b, double* out, int precision, cudaStream_t st);
+  double nnz_fine = 0.0;
+  void ctx_prof_begin(int id, cudaStream_t st, double bytes);
+  void ctx_prof_end(cudaStream_t st);
+};
+
+// ------------------------------------------------------------------------------------------
+// Context
+// ------------------------------------------------------------------------------------------
+struct Ctx {
+  int device = 0;
+  cudaStream_t own = nullptr, stream = nullptr;
+  int precision = TMB_FP64;
+  int n = 0, nb = 0;
+  // operators
+  DevSell pat;
+  DevArray<double> K, g[3], tg[3];
+  DevArray<float> Kf, gf[3], tgf[3];
+  std::vector<int> hptr, hcol, hbnodes;
+  std::vector<double> hK, hvol;
+  DevArray<double> node_vol, area, nvn;
+  DevArray<int> bnodes, bindex;
+  // material
+  bool has_material = false, has_uni = false, has_dmi = false;
+  double alpha = 1.0, gamma = kGamma0;
+  int precession = 1;
+  DevArray<double> js, xc, ku2, kax, dmi_s, hext, hdem, hfix;
+  // BEM
+  DevArray<double> Bd;
+  DevArray<float> Bf;
+  bool has_bem = false;
+  // demag
+  std::unique_ptr<Solver> neu, dir;
+  double tol = 1e-7;
+  int maxit = 100;
+  DevArray<double> rhs, u1, u2, u1b, u2b, bdir;
+  // integrator / scratch
+  DevArray<double> ybuf[2], kst[7], ytmp, in3, out3;
+  DevArray<unsigned long long> bits;
+  unsigned long long* bits_h = nullptr;
+  Prof prof;
+
+  explicit Ctx(int dev) : device(dev) {
+    TMB_CUDA(cudaSetDevice(dev));
+    TMB_CUDA(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
+    stream = own;
+    TMB_CUDA(cudaMallocHost(&bits_h, 4 * sizeof(unsigned long long)));
+    bits.alloc(4);
+  }
+  ~Ctx() {
+    neu.reset();
+    dir.reset();
+    if (bits_h) cudaFreeHost(bits_h);
+    if (own) cudaStreamDestroy(own);
+  }
+  void require_mesh() const {
+    if (n == 0) throw Error(TMB_ERR_STATE, "no mesh operators set");
+  }
+  void require_material() const {
+    if (!has_material) throw Error(TMB_ERR_STATE, "no material set");
+  }
+
+  void set_operators(int nx, const int* ptr, const int* col, const double* K_, const double* const* g_,
+                     const double* const* tg_, const double* vol, int nb_, const int* bn, const double* area_,
+                     const double* nvn_soa);
+  void set_material(const double* Js, const double* A, const double* Ku, const double* axis, const double* D,
+                    double alpha_);
+  void set_bem_rowmajor(const double* Brow_dev_or_null);
+  void ensure_demag();
+  void demag(const double* m_dev);
+  void local(const double* m, double* ydot, double* hout, unsigned long long* torque_bits);
+  double max_torque(const double* m_dev);
+  int integrate_segment(double*& y, double*& yalt, double t0, double t1, double& dt, double eps_abs,
+                        double eps_rel, double* stats);
+  int relax(double* m_dev, double duration_ps, double segment_ps, double eps_abs, double eps_rel, double* stats);
+  double time_scale() const { return gamma / (1.0 + alpha * alpha) * 1e-12; }
+  void sync() { TMB_CUDA(cudaStreamSynchronize(stream)); }
+};
+
+void Solver::ctx_prof_begin(int id, cudaStream_t st, double bytes) { ctx->prof.begin(id, st, bytes); }
+void Solver::ctx_prof_end(cudaStream_t st) { ctx->prof.end(st); }
+
+// ------------------------------------------------------------------------------------------
+// Solver implementation
+// ------------------------------------------------------------------------------------------
+void Solver::compute() {
+  cudaStream_t st = ctx->stream;
+  n = A.nrows;
+  if (n <= 0) throw Error(TMB_ERR_ARG, "solver: empty matrix");
+  // constraints: rows whose only entry is a unit diagonal
+  std::vector<int> cm(n, 0);
+  for (int i = 0; i < n; ++i)
+    if (A.ptr[i + 1] - A.ptr[i] == 1 && A.col[A.ptr[i]] == i && A.val[A.ptr[i]] == 1.0) cm[i] = 1;
+  // symmetric elimination: A' keeps free-free couplings, the free-constrained ones go to the lift
+  Csr Ap, L;
+  Ap.nrows = Ap.ncols = L.nrows = L.ncols = n;
+  Ap.ptr.assign(n + 1, 0);
+  L.ptr.assign(n + 1, 0);
+  for (int i = 0; i < n; ++i) {
+    if (cm[i]) {
+      Ap.col.push_back(i);
+      Ap.val.push_back(1.0);
+    } else {
+      for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
+        const int j = A.col[k];
+        if (cm[j]) {
+          L.col.push_back(j);
+          L.val.push_back(A.val[k]);
+        } else {
+          Ap.col.push_back(j);
+          Ap.val.push_back(A.val[k]);
+        }
+      }
+    }
+    Ap.ptr[i + 1] = int(Ap.col.size());
+    L.ptr[i + 1] = int(L.col.size());
+  }
+  amg_build(Ap, prm, H);
+  nnz_fine = double(Ap.nnz());
+  lev.clear();
+  lev.resize(H.levels.size());
+  for (size_t l = 0; l < H.levels.size(); ++l) {
+    const AmgLevel& hl = H.levels[l];
+    DevLevel& d = lev[l];
+    d.n = hl.A.nrows;
+    SellHost S = build_sell(d.n, hl.A.ptr.data(), hl.A.col.data());
+    d.A.upload(S, st);
+    d.Ad.upload(sell_values<double>(S, hl.A.val.data()), st);
+    d.Af.upload(sell_values<float>(S, hl.A.val.data()), st);
+    d.dinv.upload(hl.dinv, st);
+    d.X.alloc(d.n);
+    d.R.alloc(d.n);
+    if (l > 0) {
+      d.b.alloc(d.n);
+      d.out.alloc(d.n);
+    }
+    if (l + 1 < H.levels.size()) {
+      d.P.upload(hl.P, st);
+      d.Rop.upload(hl.R, st);
+    }
+  }
+  ncoarse = H.ncoarse;
+  cinv.upload(H.coarse_inv, st);
+  lift.upload(L, st);
+  cmask.upload(cm, st);
+  x.alloc(n);
+  x.zero(st);
+  r.alloc(n);
+  z.alloc(n);
+  p.alloc(n);
+  q.alloc(n);
+  bp.alloc(n);
+  partials.alloc(size_t(2) * grid_for(n) + 64);
+  if (!Sd) TMB_CUDA(cudaMalloc(&Sd, sizeof(CgScalars)));
+  if (!Sh) TMB_CUDA(cudaMallocHost(&Sh, sizeof(CgScalars)));
+  std::memset(Sh, 0, sizeof(CgScalars));
+  TMB_CUDA(cudaMemcpyAsync(Sd, Sh, sizeof(CgScalars), cudaMemcpyHostToDevice, st));
+  TMB_CUDA(cudaStreamSynchronize(st));
+  has_x = false;
+  computed = true;
+}
+
+void Solver::vcycle(size_t l, const double* b, double* out, int precision, cudaStream_t st) {
+  DevLevel& L = lev[l];
+  const int* done = &Sd->done;
+  if (l + 1 == lev.size()) {
+    launch_coarse_solve(ncoarse, cinv.p, b, out, done, st);
+    return;
+  }
+  DevLevel& C = lev[l + 1];
+  const SellView A = L.A.view();
+  launch_jacobi0(L.n, L.dinv.p, b, L.X.p, done, st);
+  if (precision == TMB_FP64) launch_residual<double>(A, L.Ad.p, b, L.X.p, L.R.p, done, st);
+  else launch_residual<float>(A, L.Af.p, b, L.X.p, L.R.p, done, st);
+  if (precision == TMB_FP64) launch_csr_spmv<double>(L.Rop.view(), L.Rop.v.p, L.R.p, C.b.p, false, done, st);
+  else launch_csr_spmv<float>(L.Rop.view(), L.Rop.vf.p, L.R.p, C.b.p, false, done, st);
+  vcycle(l + 1, C.b.p, C.out.p, precision, st);
+  if (precision == TMB_FP64) launch_csr_spmv<double>(L.P.view(), L.P.v.p, C.out.p, L.X.p, true, done, st);
+  else launch_csr_spmv<float>(L.P.view(), L.P.vf.p, C.out.p, L.X.p, true, done, st);
+  if (precision == TMB_FP64) launch_jacobi<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, out, done, st);
+  else launch_jacobi<float>(A, L.Af.p, L.dinv.p, b, L.X.p, out, done, st);
+}
+
+void Solver::solve(const double* b_dev, int precision) {
+  if (!computed) throw Error(TMB_ERR_STATE, "solver: compute() not called");
+  cudaStream_t st = ctx->stream;
+  Sh->tol2 = tol * tol;
+  Sh->maxit = maxit;
+  Sh->done = 0;
+  Sh->status = 0;
+  Sh->iter = 0;
+  TMB_CUDA(cudaMemcpyAsync(Sd, Sh, sizeof(CgScalars), cudaMemcpyHostToDevice, st));
+  const SellView A0 = lev[0].A.view();
+  const bool f64 = precision == TMB_FP64;
+  if (f64) launch_cg_init<double>(n, lift.view(), lift.v.p, cmask.p, b_dev, bp.p, x.p, st);
+  else launch_cg_init<float>(n, lift.view(), lift.vf.p, cmask.p, b_dev, bp.p, x.p, st);
+  if (f64) launch_cg_residual<double>(A0, lev[0].Ad.p, bp.p, x.p, r.p, Sd, partials.p, st);
+  else launch_cg_residual<float>(A0, lev[0].Af.p, bp.p, x.p, r.p, Sd, partials.p, st);
+  vcycle(0, r.p, z.p, precision, st);
+  launch_cg_rz(n, r.p, z.p, Sd, partials.p, true, st);
+  for (int it = 0; it < maxit; ++it) {
+    launch_cg_pupdate(n, z.p, p.p, Sd, st);
+    ctx_prof_begin(6, st, nnz_fine * ((f64 ? 8.0 : 4.0) + 4.0) + 3.0 * 8.0 * n);
+    if (f64) launch_cg_spmv_pq<double>(A0, lev[0].Ad.p, p.p, q.p, Sd, partials.p, st);
+    else launch_cg_spmv_pq<float>(A0, lev[0].Af.p, p.p, q.p, Sd, partials.p, st);
+    ctx_prof_end(st);
+    launch_cg_update(n, p.p, q.p, x.p, r.p, Sd, partials.p, st);
+    vcycle(0, r.p, z.p, precision, st);
+    launch_cg_rz(n, r.p, z.p, Sd, partials.p, false, st);
+    if ((it + 1) % check_every == 0 || it + 1 == maxit) {
+      TMB_CUDA(cudaMemcpyAsync(Sh, Sd, sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
+      TMB_CUDA(cudaStreamSynchronize(st));
+      if (Sh->done) break;
+    }
+  }
+  TMB_CUDA(cudaGetLastError());
+  TMB_CUDA(cudaMemcpyAsync(Sh, Sd, sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
+  TMB_CUDA(cudaStreamSynchronize(st));
+  if (Sh->status == 2) x.zero(st);
+  last_iters = Sh->iter;
+  last_status = Sh->status == 2 ? 0 : Sh->status;
+  last_relres = (Sh->bb > 0.0) ? std::sqrt(Sh->rr / Sh->bb) : 0.0;
+  has_x = true;
+}
+
+// ------------------------------------------------------------------------------------------
+// Context implementation
+// ------------------------------------------------------------------------------------------
+void Ctx::set_operators(int nx, const int* ptr, const int* col, const double* K_, const double* const* g_,
+                        const double* const* tg_, const double* vol, int nb_, const int* bn, const double* area_,
+                        const double* nvn_soa) {
+  if (nx <= 0 || nb_ < 0) throw Error(TMB_ERR_ARG, "set_operators: bad sizes");
+  cudaStream_t st = stream;
+  n = nx;
+  nb = nb_;
+  const int nnz = ptr[nx];
+  hptr.assign(ptr, ptr + nx + 1);
+  hcol.assign(col, col + nnz);
+  hK.assign(K_, K_ + nnz);
+  hvol.assign(vol, vol + nx);
+  hbnodes.assign(bn, bn + nb_);
+  SellHost S = build_sell(nx, ptr, col);
+  pat.upload(S, st);
+  K.upload(sell_values<double>(S, K_), st);
+  Kf.upload(sell_values<float>(S, K_), st);
+  for (int d = 0; d < 3; ++d) {
+    g[d].upload(sell_values<double>(S, g_[d]), st);
+    gf[d].upload(sell_values<float>(S, g_[d]), st);
+    tg[d].upload(sell_values<double>(S, tg_[d]), st);
+    tgf[d].upload(sell_values<float>(S, tg_[d]), st);
+  }
+  node_vol.upload(vol, nx, st);
+  area.upload(area_, nx, st);
+  nvn.upload(nvn_soa, size_t(3) * nx, st);
+  bnodes.upload(bn, nb_, st);
+  std::vector<int> bi(nx, -1);
+  for (int i = 0; i < nb_; ++i) bi[bn[i]] = i;
+  bindex.upload(bi, st);
+  for (auto* a : {&hext, &hdem, &hfix}) {
+    a->alloc(size_t(3) * nx);
+    a->zero(st);
+  }
+  has_material = false;
+  has_bem = false;
+  neu.reset();
+  dir.reset();
+  sync();
+}
+
+void Ctx::set_material(const double* Js, const double* A, const double* Ku, const double* axis, const double* D,
+                       double alpha_) {
+  require_mesh();
+  cudaStream_t st = stream;
+  alpha = alpha_;
+  std::vector<double> ij(n), vxc(n), vku(n, 0.0), vdm(n, 0.0);
+  has_uni = false;
+  has_dmi = false;
+  for (int i = 0; i < n; ++i) {
+    const double v = 1.0 / Js[i];
+    ij[i] = std::isfinite(v) ? v : 0.0;  // main/TheLLG.cpp:110
+    vxc[i] = -2.0 * A[i] / hvol[i] * ij[i];
+    if (Ku) {
+      vku[i] = 2.0 * Ku[i] * ij[i];
+      has_uni |= (Ku[i] != 0.0);
+    }
+    if (D) {
+      vdm[i] = D[i] / hvol[i] * ij[i];
+      has_dmi |= (D[i] != 0.0);
+    }
+  }
+  js.upload(Js, n, st);
+  xc.upload(vxc, st);
+  ku2.upload(vku, st);
+  dmi_s.upload(vdm, st);
+  if (axis) {
+    kax.upload(axis, size_t(3) * n, st);
+  } else {
+    kax.alloc(size_t(3) * n);
+    kax.zero(st);
+  }
+  has_material = true;
+  sync();
+}
+
+void Ctx::set_bem_rowmajor(const double* /*unused*/) {}
+
+void Ctx::ensure_demag() {
+  require_mesh();
+  require_material();
+  if (!has_bem) throw Error(TMB_ERR_STATE, "no BEM matrix set");
+  if (neu && dir) return;
+  // Neumann matrix: K with row N/2 replaced by the unit row (DemagField.cpp:80, 204-220)
+  // Dirichlet matrix: K with boundary rows replaced by unit rows (FEMprocessing.cpp:329-369)
+  const int k = n / 2;
+  std::vector<char> isb(n, 0);
+  for (int b : hbnodes) isb[b] = 1;
+  auto build = [&](auto pinned) {
+    std::vector<int> p(n + 1, 0), c;
+    std::vector<double> v;
+    c.reserve(hcol.size());
+    v.reserve(hcol.size());
+    for (int i = 0; i < n; ++i) {
+      if (pinned(i)) {
+        c.push_back(i);
+        v.push_back(1.0);
+      } else {
+        for (int q = hptr[i]; q < hptr[i + 1]; ++q) {
+          c.push_back(hcol[q]);
+          v.push_back(hK[q]);
+        }
+      }
+      p[i + 1] = int(c.size());
+    }
+    auto s = std::make_unique<Solver>(this);
+    s->set_matrix(n, p.data(), c.data(), v.data());
+    s->tol = tol;
+    s->maxit = maxit;
+    s->compute();
+    return s;
+  };
+  neu = build([&](int i) { return i == k; });
+  dir = build([&](int i) { return isb[i] != 0; });
+  for (auto* a : {&rhs, &u1, &u2, &bdir}) a->alloc(n);
+  u1b.alloc(nb);
+  u2b.alloc(nb);
+}
+
+void Ctx::demag(const double* m) {
+  ensure_demag();
+  cudaStream_t st = stream;
+  neu->tol = dir->tol = tol;
+  neu->maxit = dir->maxit = maxit;
+  const SellView S = pat.view();
+  const bool f64 = precision == TMB_FP64;
+  const double sv = f64 ? 8.0 : 4.0, z = double(hptr[n]), N = double(n), B = double(nb);
+  prof.begin(7, st, 0.0);
+  prof.begin(1, st, z * (3 * sv + 4) + N * 8 * 5);
+  if (f64) launch_divergence<double>(S, tg[0].p, tg[1].p, tg[2].p, m, js.p, 1.0 / kMu0, rhs.p, st);
+  else launch_divergence<float>(S, tgf[0].p, tgf[1].p, tgf[2].p, m, js.p, 1.0 / kMu0, rhs.p, st);
+  prof.end(st);
+  prof.begin(4, st, 0.0);
+  neu->solve(rhs.p, precision);
+  prof.end(st);
+  launch_gather(nb, neu->x.p, bnodes.p, u1b.p, st);
+  prof.begin(3, st, B * B * sv + 2 * B * 8);
+  if (f64) launch_bem_gemv<double>(nb, Bd.p, u1b.p, nullptr, u2b.p, st);
+  else launch_bem_gemv<float>(nb, Bf.p, u1b.p, nullptr, u2b.p, st);
+  prof.end(st);
+  launch_dirichlet_values(n, bindex.p, u2b.p, bdir.p, st);
+  prof.begin(5, st, 0.0);
+  dir->solve(bdir.p, precision);
+  prof.end(st);
+  prof.begin(2, st, z * (3 * sv + 4) + N * 8 * 11);
+  if (f64) launch_gradient<double>(S, g[0].p, g[1].p, g[2].p, neu->x.p, dir->x.p, hext.p, hdem.p, hfix.p, st);
+  else launch_gradient<float>(S, gf[0].p, gf[1].p, gf[2].p, neu->x.p, dir->x.p, hext.p, hdem.p, hfix.p, st);
+  prof.end(st);
+  prof.end(st);
+  TMB_CUDA(cudaGetLastError());
+  if (neu->last_status == 5 || dir->last_status == 5) throw Error(TMB_ERR_NAN, "demag solve broke down (NaN)");
+  if (neu->last_status == 3 || dir->last_status == 3)
+    throw Error(TMB_ERR_NOCONVERGE, "demag solve did not converge within maxiter");
+}
+
+void Ctx::local(const double* m, double* ydot, double* hout, unsigned long long* tq) {
+  require_mesh();
+  require_material();
+  LocalFieldArgs a;
+  a.n = n;
+  a.m = m;
+  a.hfix = hfix.p;
+  a.xc = xc.p;
+  a.ku2 = has_uni ? ku2.p : nullptr;
+  a.kax = kax.p;
+  a.dmi_s = has_dmi ? dmi_s.p : nullptr;
+  a.area = area.p;
+  a.nvn = nvn.p;
+  a.alpha = alpha;
+  a.precession = precession;
+  a.ydot = ydot;
+  a.hout = hout;
+  a.torque_bits = tq;
+  const SellView S = pat.view();
+  const double sv = precision == TMB_FP64 ? 8.0 : 4.0, z = double(hptr[n]), N = double(n);
+  double bytes = z * (sv + 4) + N * 8 * (3 + 3 + 1) + (ydot ? N * 24 : 0.0) + (hout ? N * 24 : 0.0);
+  if (a.ku2) bytes += N * 8 * 4;
+  if (a.dmi_s) bytes += z * 3 * sv + N * 8 * 5;
+  prof.begin(0, stream, bytes);
+  if (precision == TMB_FP64) launch_local_field<double>(S, K.p, tg[0].p, tg[1].p, tg[2].p, a, stream);
+  else launch_local_field<float>(S, Kf.p, tgf[0].p, tgf[1].p, tgf[2].p, a, stream);
+  prof.end(stream);
+}
+
+static double bits_to_double(unsigned long long b) {
+  double d;
+  std::memcpy(&d, &b, sizeof d);
+  return d;
+}
+
+double Ctx::max_torque(const double* m) {
+  TMB_CUDA(cudaMemsetAsync(bits.p, 0, sizeof(unsigned long long), stream));
+  local(m, nullptr, nullptr, bits.p);
+  TMB_CUDA(cudaMemcpyAsync(bits_h, bits.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
+  sync();
+  return bits_to_double(bits_h[0]) * kMu0;
+}
+
+// Dormand & Prince (1980) 5(4) tableau; the stage-7 input is the 5th-order solution (FSAL).
+static const double kDpA[7][6] = {
+    {0, 0, 0, 0, 0, 0},
+    {1.0 / 5, 0, 0, 0, 0, 0},
+    {3.0 / 40, 9.0 / 40, 0, 0, 0, 0},
+    {44.0 / 45, -56.0 / 15, 32.0 / 9, 0, 0, 0},
+    {19372.0 / 6561, -25360.0 / 2187, 64448.0 / 6561, -212.0 / 729, 0, 0},
+    {9017.0 / 3168, -355.0 / 33, 46732.0 / 5247, 49.0 / 176, -5103.0 / 18656, 0},
+    {35.0 / 384, 0, 500.0 / 1113, 125.0 / 192, -2187.0 / 6784, 11.0 / 84}};
+static const double kDpE[7] = {35.0 / 384 - 5179.0 / 57600, 0.0, 500.0 / 1113 - 7571.0 / 16695,
+                               125.0 / 192 - 393.0 / 640, -2187.0 / 6784 + 92097.0 / 339200,
+                               11.0 / 84 - 187.0 / 2100, -1.0 / 40};
+
+// Adaptive segment with odeint's controlled_runge_kutta error control and step adjustment.
+int Ctx::integrate_segment(double*& y, double*& yalt, double t0, double t1, double& dt, double eps_abs,
+                           double eps_rel, double* stats) {
+  const int n3 = 3 * n;
+  cudaStream_t st = stream;
+  double t = t0;
+  local(y, kst[0].p, nullptr, nullptr);
+  stats[2] += 1;
+  const long long max_steps = 50000000LL;
+  long long steps = 0;
+  while (t < t1) {
+    if (++steps > max_steps) throw Error(TMB_ERR_STEP, "integrator step cap reached");
+    bool last = false;
+    double h = dt;
+    if (t + h >= t1) {
+      h = t1 - t;
+      last = true;
+    }
+    if (!(h > 0.0) || h < 1e-300) throw Error(TMB_ERR_STEP, "integrator step size underflow");
+    const double* kp[7];
+    for (int j = 0; j < 7; ++j) kp[j] = kst[j].p;
+    for (int s = 1; s < 7; ++s) {
+      double* dst = (s == 6) ? yalt : ytmp.p;
+      launch_rk_combine(n3, y, kp, kDpA[s], s, h, dst, st);
+      local(dst, kst[s].p, nullptr, nullptr);
+      stats[2] += 1;
+    }
+    TMB_CUDA(cudaMemsetAsync(bits.p + 1, 0, sizeof(unsigned long long), st));
+    launch_rk_error(n3, y, kst[0].p, kp, kDpE, 7, h, eps_abs, eps_rel, bits.p + 1, st);
+    TMB_CUDA(cudaMemcpyAsync(bits_h + 1, bits.p + 1, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    sync();
+    const double err = bits_to_double(bits_h[1]);
+    if (!std::isfinite(err) || err > 1.0) {
+      const double e = std::isfinite(err) ? err : 1e30;
+      dt = h * std::max(0.9 * std::pow(e, -1.0 / 3.0), 0.2);
+      stats[1] += 1;
+      continue;
+    }
+    t = last ? t1 : t + h;
+    std::swap(y, yalt);
+    kst[0].swap(kst[6]);
+    stats[0] += 1;
+    const double dtn = (err < 0.5) ? h * 0.9 * std::pow(std::max(err, std::pow(5.0, -5.0)), -1.0 / 5.0) : h;
+    if (!last) dt = dtn;
+    else dt = (h < dt) ? std::max(dt, dtn) : dtn;
+  }
+  return TMB_OK;
+}
+
+int Ctx::relax(double* m, double duration_ps, double segment_ps, double eps_abs, double eps_rel, double* stats) {
+  require_mesh();
+  require_material();
+  const int n3 = 3 * n;
+  cudaStream_t st = stream;
+  for (auto& b : ybuf) b.alloc(n3);
+  for (auto& k : kst) k.alloc(n3);
+  ytmp.alloc(n3);
+  TMB_CUDA(cudaMemcpyAsync(ybuf[0].p, m, sizeof(double) * n3, cudaMemcpyDeviceToDevice, st));
+  double* y = ybuf[0].p;
+  double* yalt = ybuf[1].p;
+  launch_normalize(n, y, st);
+  const double ts = time_scale();
+  double dt = std::min(segment_ps * ts, ts);
+  for (int i = 0; i < 12; ++i) stats[i] = 0.0;
+  double t_ps = 0.0;
+  const bool with_demag = has_bem;
+  while (t_ps < duration_ps - 1e-12) {
+    if (with_demag) {
+      demag(y);
+      stats[3] += 1;
+      stats[4] += neu->last_iters;
+      stats[5] += dir->last_iters;
+    }
+    const double seg = std::min(segment_ps, duration_ps - t_ps);
+    integrate_segment(y, yalt, t_ps * ts, (t_ps + seg) * ts, dt, eps_abs, eps_rel, stats);
+    launch_normalize(n, y, st);
+    t_ps += seg;
+    stats[8] += 1;
+  }
+  if (with_demag) {
+    demag(y);
+    stats[3] += 1;
+  }
+  stats[6] = max_torque(y);
+  stats[7] = dt;
+  TMB_CUDA(cudaMemcpyAsync(m, y, sizeof(double) * n3, cudaMemcpyDeviceToDevice, st));
+  sync();
+  if (!std::isfinite(stats[6])) throw Error(TMB_ERR_NAN, "torque is not finite");
+  return TMB_OK;
+}
+
+}  // namespace tmb
+
+// ==========================================================================================
+// C ABI
+// ==========================================================================================
+using namespace tmb;
+
+struct tmb_ctx {
+  std::unique_ptr<Ctx> c;
+};
+struct tmb_mesh {
+  MeshHost m;
+};
+struct tmb_solver {
+  Ctx* ctx;
+  std::unique_ptr<Solver> s;
+};
+
+static thread_local std::string g_last_error;
+
+static int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define TMB_API_BEGIN try {
+#define TMB_API_END                                                  \
+  }                                                                  \
+  catch (const Error& e) {                                           \
+    return fail(e.code, e.what());                                   \
+  }                                                                  \
+  catch (const std::bad_alloc&) {                                    \
+    return fail(TMB_ERR_INTERNAL, "host allocation failed");         \
+  }                                                                  \
+  catch (const std::exception& e) {                                  \
+    const std::string w = e.what();                                  \
+    return fail(w.rfind("CUDA", 0) == 0 ? TMB_ERR_CUDA : TMB_ERR_INTERNAL, w); \
+  }                                                                  \
+  return TMB_OK;
+
+#define TMB_CHECK_ARG(cond, msg) \
+  if (!(cond)) return fail(TMB_ERR_ARG, msg);
+
+// Stages a host (or device) 3N vector into a device buffer.
+static const double* stage_in(Ctx& c, DevArray<double>& buf, const double* p, size_t count, int kind) {
+  if (kind == TMB_PTR_DEVICE) return p;
+  buf.alloc(count);
+  TMB_CUDA(cudaMemcpyAsync(buf.p, p, count * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+  return buf.p;
+}
+
+extern "C" {
+
+const char* tmb_last_error(void) { return g_last_error.c_str(); }
+int tmb_version(void) { return 10000; }
+
+int tmb_kernel_launches(long long* count) {
+  TMB_CHECK_ARG(count, "tmb_kernel_launches: null argument");
+  *count = launch_count();
+  return TMB_OK;
+}
+
+int tmb_mesh_create(int nx, int ntet, const double* xyz, const int* tets, tmb_mesh** out) {
+  TMB_CHECK_ARG(out && xyz && tets && nx > 0 && ntet > 0, "tmb_mesh_create: bad arguments");
+  TMB_API_BEGIN
+  for (long long i = 0; i < 4LL * ntet; ++i)
+    if (tets[i] < 0 || tets[i] >= nx) return fail(TMB_ERR_ARG, "tmb_mesh_create: node index out of range");
+  auto* h = new tmb_mesh();
+  h->m.nx = nx;
+  h->m.ntet = ntet;
+  h->m.xyz.assign(xyz, xyz + size_t(3) * nx);
+  h->m.tets.assign(tets, tets + size_t(4) * ntet);
+  try {
+    fem_prepare(h->m);
+    extract_boundary(h->m);
+    compute_solid_angles(h->m);
+  } catch (...) {
+    delete h;
+    throw;
+  }
+  *out = h;
+  TMB_API_END
+}
+
+int tmb_mesh_destroy(tmb_mesh* mesh) {
+  delete mesh;
+  return TMB_OK;
+}
+
+int tmb_mesh_info(const tmb_mesh* mesh, long long* info) {
+  TMB_CHECK_ARG(mesh && info, "tmb_mesh_info: null argument");
+  info[0] = mesh->m.nx;
+  info[1] = mesh->m.ntet;
+  info[2] = mesh->m.fem.ptr.empty() ? 0 : mesh->m.fem.ptr.back();
+  info[3] = (long long)mesh->m.bnd.bnodes.size();
+  info[4] = (long long)mesh->m.bnd.tri_tet.size();
+  info[5] = 0;
+  return TMB_OK;
+}
+
+int tmb_mesh_get_operators(const tmb_mesh* mesh, int* rowptr, int* col, double* stiff, double* gx, double* gy,
+                           double* gz, double* tgx, double* tgy, double* tgz, double* node_vol) {
+  TMB_CHECK_ARG(mesh, "tmb_mesh_get_operators: null mesh");
+  const FemOperators& F = mesh->m.fem;
+  auto cp = [](auto* dst, const auto& src) {
+    if (dst) std::copy(src.begin(), src.end(), dst);
+  };
+  cp(rowptr, F.ptr);
+  cp(col, F.col);
+  cp(stiff, F.stiff);
+  cp(gx, F.grad[0]);
+  cp(gy, F.grad[1]);
+  cp(gz, F.grad[2]);
+  cp(tgx, F.tgrad[0]);
+  cp(tgy, F.tgrad[1]);
+  cp(tgz, F.tgrad[2]);
+  cp(node_vol, F.node_vol);
+  return TMB_OK;
+}
+
+int tmb_mesh_get_boundary(const tmb_mesh* mesh, int* bnodes, int* tri, double* tri_area, double* tri_normal,
+                          double* node_area, double* node_normal, double* solid_angle) {
+  TMB_CHECK_ARG(mesh, "tmb_mesh_get_boundary: null mesh");
+  const BoundaryData& B = mesh->m.bnd;
+  const int n = mesh->m.nx;
+  auto cp = [](auto* dst, const auto& src) {
+    if (dst) std::copy(src.begin(), src.end(), dst);
+  };
+  cp(bnodes, B.bnodes);
+  cp(tri, B.tri);
+  cp(tri_area, B.tri_area);
+  cp(tri_normal, B.tri_normal);
+  cp(node_area, B.node_area);
+  cp(solid_angle, B.solid_angle);
+  if (node_normal)
+    for (int i = 0; i < n; ++i)
+      for (int d = 0; d < 3; ++d) node_normal[size_t(d) * n + i] = B.node_normal[size_t(i) * 3 + d];
+  return TMB_OK;
+}
+
+int tmb_ctx_create(int device, tmb_ctx** out) {
+  TMB_CHECK_ARG(out, "tmb_ctx_create: null out");
+  TMB_API_BEGIN
+  int count = 0;
+  TMB_CUDA(cudaGetDeviceCount(&count));
+  if (device < 0 || device >= count) return fail(TMB_ERR_ARG, "tmb_ctx_create: no such device");
+  auto* h = new tmb_ctx();
+  try {
+    h->c = std::make_unique<Ctx>(device);
+  } catch (...) {
+    delete h;
+    throw;
+  }
+  *out = h;
+  TMB_API_END
+}
+
+int tmb_ctx_destroy(tmb_ctx* ctx) {
+  if (ctx) {
+    cudaSetDevice(ctx->c->device);
+    delete ctx;
+  }
+  return TMB_OK;
+}
+
+int tmb_ctx_set_stream(tmb_ctx* ctx, void* stream) {
+  TMB_CHECK_ARG(ctx, "null context");
+  ctx->c->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->c->own;
+  return TMB_OK;
+}
+
+int tmb_set_precision(tmb_ctx* ctx, int precision) {
+  TMB_CHECK_ARG(ctx, "null context");
+  TMB_CHECK_ARG(precision == TMB_FP64 || precision == TMB_MIXED, "tmb_set_precision: unknown precision");
+  ctx->c->precision = precision;
+  return TMB_OK;
+}
+
+int tmb_set_mesh(tmb_ctx* ctx, const tmb_mesh* mesh) {
+  TMB_CHECK_ARG(ctx && mesh, "tmb_set_mesh: null argument");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  TMB_CUDA(cudaSetDevice(c.device));
+  const MeshHost& M = mesh->m;
+  const double* g[3] = {M.fem.grad[0].data(), M.fem.grad[1].data(), M.fem.grad[2].data()};
+  const double* tg[3] = {M.fem.tgrad[0].data(), M.fem.tgrad[1].data(), M.fem.tgrad[2].data()};
+  std::vector<double> nvn(size_t(3) * M.nx);
+  for (int i = 0; i < M.nx; ++i)
+    for (int d = 0; d < 3; ++d) nvn[size_t(d) * M.nx + i] = M.bnd.node_normal[size_t(i) * 3 + d];
+  c.set_operators(M.nx, M.fem.ptr.data(), M.fem.col.data(), M.fem.stiff.data(), g, tg, M.fem.node_vol.data(),
+                  int(M.bnd.bnodes.size()), M.bnd.bnodes.data(), M.bnd.node_area.data(), nvn.data());
+  TMB_API_END
+}
+
+int tmb_set_operators(tmb_ctx* ctx, int nx, int nnz, const int* rowptr, const int* col, const double* stiff,
+                      const double* gx, const double* gy, const double* gz, const double* tgx, const double* tgy,
+                      const double* tgz, const double* node_vol, int nb, const int* bnodes,
+                      const double* node_area, const double* node_normal) {
+  TMB_CHECK_ARG(ctx && rowptr && col && stiff && gx && gy && gz && tgx && tgy && tgz && node_vol && bnodes &&
+                    node_area && node_normal,
+                "tmb_set_operators: null argument");
+  TMB_CHECK_ARG(nx > 0 && nnz > 0 && rowptr[nx] == nnz && nb >= 0 && nb <= nx, "tmb_set_operators: bad sizes");
+  TMB_API_BEGIN
+  for (int i = 0; i < nnz; ++i)
+    if (col[i] < 0 || col[i] >= nx) return fail(TMB_ERR_ARG, "tmb_set_operators: column out of range");
+  for (int i = 0; i < nb; ++i)
+    if (bnodes[i] < 0 || bnodes[i] >= nx) return fail(TMB_ERR_ARG, "tmb_set_operators: boundary node out of range");
+  TMB_CUDA(cudaSetDevice(ctx->c->device));
+  const double* g[3] = {gx, gy, gz};
+  const double* tg[3] = {tgx, tgy, tgz};
+  ctx->c->set_operators(nx, rowptr, col, stiff, g, tg, node_vol, nb, bnodes, node_area, node_normal);
+  TMB_API_END
+}
+
+int tmb_bem_assemble(tmb_ctx* ctx, const tmb_mesh* mesh) {
+  TMB_CHECK_ARG(ctx && mesh, "tmb_bem_assemble: null argument");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  c.require_mesh();
+  const MeshHost& M = mesh->m;
+  const BoundaryData& B = M.bnd;
+  const int nb = int(B.bnodes.size()), nt = int(B.tri_tet.size());
+  if (nb != c.nb || M.nx != c.n) return fail(TMB_ERR_ARG, "tmb_bem_assemble: mesh differs from the context's");
+  TMB_CUDA(cudaSetDevice(c.device));
+  std::vector<double> bxyz(size_t(3) * nb);
+  for (int i = 0; i < nb; ++i)
+    for (int d = 0; d < 3; ++d) bxyz[size_t(3) * i + d] = M.xyz[size_t(3) * B.bnodes[i] + d];
+  std::vector<int> tri(size_t(3) * nt);
+  for (size_t k = 0; k < tri.size(); ++k) tri[k] = B.bindex[B.tri[k]];
+  DevArray<double> dx, da, dn, ds;
+  DevArray<int> dt;
+  dx.upload(bxyz, c.stream);
+  dt.upload(tri, c.stream);
+  da.upload(B.tri_area, c.stream);
+  dn.upload(B.tri_normal, c.stream);
+  ds.upload(B.solid_angle, c.stream);
+  const size_t ld = bem_ld(nb);
+  c.Bd.alloc(ld * nb);
+  launch_bem_assemble(nb, nt, dx.p, dt.p, da.p, dn.p, ds.p, c.Bd.p, c.stream);
+  c.Bf.alloc(ld * nb);
+  launch_to_float(c.Bd.p, c.Bf.p, ld * nb, c.stream);
+  c.sync();
+  c.has_bem = true;
+  c.neu.reset();
+  c.dir.reset();
+  TMB_API_END
+}
+
+int tmb_set_bem_dense(tmb_ctx* ctx, int nb, const double* B_colmajor) {
+  TMB_CHECK_ARG(ctx && B_colmajor, "tmb_set_bem_dense: null argument");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  c.require_mesh();
+  if (nb != c.nb) return fail(TMB_ERR_ARG, "tmb_set_bem_dense: nb differs from the boundary node count");
+  TMB_CUDA(cudaSetDevice(c.device));
+  const size_t ld = bem_ld(nb);
+  std::vector<double> rowmajor(ld * nb, 0.0);
+  for (int j = 0; j < nb; ++j)
+    for (int i = 0; i < nb; ++i) rowmajor[size_t(i) * ld + j] = B_colmajor[size_t(j) * nb + i];
+  c.Bd.upload(rowmajor, c.stream);
+  c.Bf.alloc(ld * nb);
+  launch_to_float(c.Bd.p, c.Bf.p, ld * nb, c.stream);
+  c.sync();
+  c.has_bem = true;
+  c.neu.reset();
+  c.dir.reset();
+  TMB_API_END
+}
+
+int tmb_get_bem_dense(tmb_ctx* ctx, double* B_colmajor) {
+  TMB_CHECK_ARG(ctx && B_colmajor, "tmb_get_bem_dense: null argument");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  if (!c.has_bem) return fail(TMB_ERR_STATE, "no BEM matrix set");
+  const int nb = c.nb;
+  const size_t ld = bem_ld(nb);
+  std::vector<double> rowmajor(ld * nb);
+  TMB_CUDA(cudaMemcpyAsync(rowmajor.data(), c.Bd.p, sizeof(double) * ld * nb, cudaMemcpyDeviceToHost, c.stream));
+  c.sync();
+  for (int j = 0; j < nb; ++j)
+    for (int i = 0; i < nb; ++i) B_colmajor[size_t(j) * nb + i] = rowmajor[size_t(i) * ld + j];
+  TMB_API_END
+}
+
+int tmb_set_material(tmb_ctx* ctx, const double* Js, const double* A, const double* Ku, const double* ku_axis,
+                     const double* D, double alpha) {
+  TMB_CHECK_ARG(ctx && Js && A, "tmb_set_material: Js and A are required");
+  TMB_CHECK_ARG(std::isfinite(alpha) && alpha >= 0.0, "tmb_set_material: alpha must be finite and >= 0");
+  TMB_API_BEGIN
+  TMB_CUDA(cudaSetDevice(ctx->c->device));
+  ctx->c->set_material(Js, A, Ku, ku_axis, D, alpha);
+  TMB_API_END
+}
+
+int tmb_set_applied_field(tmb_ctx* ctx, const double* hext, int ptr_kind) {
+  TMB_CHECK_ARG(ctx && hext, "tmb_set_applied_field: null argument");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  c.require_mesh();
+  const size_t n3 = size_t(3) * c.n;
+  TMB_CUDA(cudaMemcpyAsync(c.hext.p, hext, n3 * sizeof(double),
+                           ptr_kind == TMB_PTR_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c.stream));
+  launch_add(int(n3), c.hext.p, c.hdem.p, c.hfix.p, c.stream);
+  c.sync();
+  TMB_API_END
+}
+
+int tmb_set_llg_options(tmb_ctx* ctx, int precession) {
+  TMB_CHECK_ARG(ctx, "null context");
+  ctx->c->precession = precession ? 1 : 0;
+  return TMB_OK;
+}
+
+int tmb_set_solver_params(tmb_ctx* ctx, double tol, int maxiter) {
+  TMB_CHECK_ARG(ctx, "null context");
+  TMB_CHECK_ARG(tol > 0.0 && tol < 1.0 && maxiter > 0, "tmb_set_solver_params: need 0 < tol < 1, maxiter > 0");
+  ctx->c->tol = tol;
+  ctx->c->maxit = maxiter;
+  return TMB_OK;
+}
+
+int tmb_demag_field(tmb_ctx* ctx, const double* m, double* hdem, int ptr_kind) {
+  TMB_CHECK_ARG(ctx && m, "tmb_demag_field: null argument");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  c.require_mesh();
+  const size_t n3 = size_t(3) * c.n;
+  const double* md = stage_in(c, c.in3, m, n3, ptr_kind);
+  c.demag(md);
+  if (hdem)
+    TMB_CUDA(cudaMemcpyAsync(hdem, c.hdem.p, n3 * sizeof(double),
+                             ptr_kind == TMB_PTR_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                             c.stream));
+  if (ptr_kind != TMB_PTR_DEVICE) c.sync();
+  TMB_API_END
+}
+
+int tmb_field_eval(tmb_ctx* ctx, const double* m, double* ydot, double* hdem, int ptr_kind) {
+  TMB_CHECK_ARG(ctx && m && ydot, "tmb_field_eval: null argument");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  c.require_mesh();
+  const size_t n3 = size_t(3) * c.n;
+  const double* md = stage_in(c, c.in3, m, n3, ptr_kind);
+  c.demag(md);
+  if (ptr_kind == TMB_PTR_DEVICE) {
+    c.local(md, ydot, nullptr, nullptr);
+    if (hdem) TMB_CUDA(cudaMemcpyAsync(hdem, c.hdem.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
+  } else {
+    c.out3.alloc(n3);
+    c.local(md, c.out3.p, nullptr, nullptr);
+    TMB_CUDA(cudaMemcpyAsync(ydot, c.out3.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    if (hdem) TMB_CUDA(cudaMemcpyAsync(hdem, c.hdem.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+  }
+  TMB_API_END
+}
+
+int tmb_set_demag_frozen(tmb_ctx* ctx, const double* hdem, int ptr_kind) {
+  TMB_CHECK_ARG(ctx && hdem, "tmb_set_demag_frozen: null argument");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  c.require_mesh();
+  const size_t n3 = size_t(3) * c.n;
+  TMB_CUDA(cudaMemcpyAsync(c.hdem.p, hdem, n3 * sizeof(double),
+                           ptr_kind == TMB_PTR_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c.stream));
+  launch_add(int(n3), c.hext.p, c.hdem.p, c.hfix.p, c.stream);
+  if (ptr_kind != TMB_PTR_DEVICE) c.sync();
+  TMB_API_END
+}
+
+int tmb_effective_field(tmb_ctx* ctx, const double* m, double* h, int ptr_kind) {
+  TMB_CHECK_ARG(ctx && m && h, "tmb_effective_field: null argument");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  c.require_mesh();
+  const size_t n3 = size_t(3) * c.n;
+  const double* md = stage_in(c, c.in3, m, n3, ptr_kind);
+  if (ptr_kind == TMB_PTR_DEVICE) {
+    c.local(md, nullptr, h, nullptr);
+  } else {
+    c.out3.alloc(n3);
+    c.local(md, nullptr, c.out3.p, nullptr);
+    TMB_CUDA(cudaMemcpyAsync(h, c.out3.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+  }
+  TMB_API_END
+}
+
+int tmb_llg_rhs(tmb_ctx* ctx, double t, const double* y, double* ydot, int ptr_kind) {
+  (void)t;  // the frozen-demag right-hand side does not depend on t explicitly
+  TMB_CHECK_ARG(ctx && y && ydot, "tmb_llg_rhs: null argument");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  c.require_mesh();
+  const size_t n3 = size_t(3) * c.n;
+  const double* yd = stage_in(c, c.in3, y, n3, ptr_kind);
+  if (ptr_kind == TMB_PTR_DEVICE) {
+    c.local(yd, ydot, nullptr, nullptr);
+  } else {
+    c.out3.alloc(n3);
+    c.local(yd, c.out3.p, nullptr, nullptr);
+    TMB_CUDA(cudaMemcpyAsync(ydot, c.out3.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+  }
+  TMB_API_END
+}
+
+int tmb_max_torque(tmb_ctx* ctx, const double* m, double* out, int ptr_kind) {
+  TMB_CHECK_ARG(ctx && m && out, "tmb_max_torque: null argument");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  c.require_mesh();
+  const double* md = stage_in(c, c.in3, m, size_t(3) * c.n, ptr_kind);
+  *out = c.max_torque(md);
+  if (!std::isfinite(*out)) return fail(TMB_ERR_NAN, "tmb_max_torque: torque is not finite");
+  TMB_API_END
+}
+
+int tmb_normalize(tmb_ctx* ctx, double* m, int ptr_kind) {
+  TMB_CHECK_ARG(ctx && m, "tmb_normalize: null argument");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  c.require_mesh();
+  const size_t n3 = size_t(3) * c.n;
+  if (ptr_kind == TMB_PTR_DEVICE) {
+    launch_normalize(c.n, m, c.stream);
+  } else {
+    c.in3.alloc(n3);
+    TMB_CUDA(cudaMemcpyAsync(c.in3.p, m, n3 * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    launch_normalize(c.n, c.in3.p, c.stream);
+    TMB_CUDA(cudaMemcpyAsync(m, c.in3.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+  }
+  TMB_API_END
+}
+
+int tmb_relax(tmb_ctx* ctx, double* m, double duration_ps, double segment_ps, double eps_abs, double eps_rel,
+              double* stats, int ptr_kind) {
+  TMB_CHECK_ARG(ctx && m && stats, "tmb_relax: null argument");
+  TMB_CHECK_ARG(duration_ps >= 0.0 && segment_ps > 0.0 && eps_abs > 0.0 && eps_rel >= 0.0,
+                "tmb_relax: bad time or tolerance arguments");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  c.require_mesh();
+  const size_t n3 = size_t(3) * c.n;
+  if (ptr_kind == TMB_PTR_DEVICE) {
+    c.relax(m, duration_ps, segment_ps, eps_abs, eps_rel, stats);
+  } else {
+    c.in3.alloc(n3);
+    TMB_CUDA(cudaMemcpyAsync(c.in3.p, m, n3 * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    c.relax(c.in3.p, duration_ps, segment_ps, eps_abs, eps_rel, stats);
+    TMB_CUDA(cudaMemcpyAsync(m, c.in3.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+  }
+  TMB_API_END
+}
+
+int tmb_get_stats(tmb_ctx* ctx, double* out) {
+  TMB_CHECK_ARG(ctx && out, "tmb_get_stats: null argument");
+  Ctx& c = *ctx->c;
+  for (int i = 0; i < 8; ++i) out[i] = 0.0;
+  if (c.neu && c.dir) {
+    out[0] = c.neu->last_iters;
+    out[1] = c.dir->last_iters;
+    out[2] = c.neu->last_relres;
+    out[3] = c.dir->last_relres;
+    out[4] = c.neu->last_status;
+    out[5] = c.dir->last_status;
+    out[6] = double(c.neu->H.levels.size());
+    out[7] = c.neu->H.setup_ms + c.dir->H.setup_ms;
+  }
+  return TMB_OK;
+}
+
+int tmb_profile_enable(tmb_ctx* ctx, int on) {
+  TMB_CHECK_ARG(ctx, "null context");
+  TMB_API_BEGIN
+  ctx->c->prof.reset();
+  ctx->c->prof.on = on != 0;
+  TMB_API_END
+}
+
+int tmb_profile_read(tmb_ctx* ctx, double* out) {
+  TMB_CHECK_ARG(ctx && out, "tmb_profile_read: null argument");
+  TMB_API_BEGIN
+  Prof& P = ctx->c->prof;
+  P.flush();
+  for (int i = 0; i < kProfIds; ++i) {
+    out[3 * i] = P.count[i];
+    out[3 * i + 1] = P.ms[i];
+    out[3 * i + 2] = P.count[i] > 0 ? P.bytes[i] / P.count[i] : 0.0;
+  }
+  TMB_API_END
+}
+
+int tmb_solver_create(tmb_ctx* ctx, tmb_solver** out) {
+  TMB_CHECK_ARG(ctx && out, "tmb_solver_create: null argument");
+  TMB_API_BEGIN
+  auto* s = new tmb_solver();
+  s->ctx = ctx->c.get();
+  s->s = std::make_unique<Solver>(s->ctx);
+  *out = s;
+  TMB_API_END
+}
+
+int tmb_solver_destroy(tmb_solver* s) {
+  delete s;
+  return TMB_OK;
+}
+
+int tmb_solver_set_matrix(tmb_solver* s, int n, int nnz, const int* rowptr, const int* col, const double* val) {
+  TMB_CHECK_ARG(s && rowptr && col && val && n > 0 && nnz > 0 && rowptr[0] == 0 && rowptr[n] == nnz,
+                "tmb_solver_set_matrix: bad arguments");
+  TMB_API_BEGIN
+  for (int i = 0; i < n; ++i)
+    if (rowptr[i + 1] < rowptr[i]) return fail(TMB_ERR_ARG, "tmb_solver_set_matrix: rowptr not monotone");
+  for (int k = 0; k < nnz; ++k)
+    if (col[k] < 0 || col[k] >= n) return fail(TMB_ERR_ARG, "tmb_solver_set_matrix: column out of range");
+  s->s->set_matrix(n, rowptr, col, val);
+  TMB_API_END
+}
+
+int tmb_solver_set_tolerance(tmb_solver* s, double tol, int maxiter) {
+  TMB_CHECK_ARG(s && tol > 0.0 && tol < 1.0 && maxiter > 0, "tmb_solver_set_tolerance: bad arguments");
+  s->s->tol = tol;
+  s->s->maxit = maxiter;
+  return TMB_OK;
+}
+
+int tmb_solver_compute(tmb_solver* s) {
+  TMB_CHECK_ARG(s, "null solver");
+  TMB_API_BEGIN
+  TMB_CUDA(cudaSetDevice(s->ctx->device));
+  s->s->compute();
+  TMB_API_END
+}
+
+int tmb_solver_solve(tmb_solver* s, const double* b, double* x, int ptr_kind) {
+  TMB_CHECK_ARG(s && b && x, "tmb_solver_solve: null argument");
+  TMB_API_BEGIN
+  Solver& S = *s->s;
+  Ctx& c = *s->ctx;
+  if (!S.computed) return fail(TMB_ERR_STATE, "tmb_solver_solve: compute() not called");
+  const size_t n = size_t(S.n);
+  DevArray<double> tmp;
+  const double* bd = stage_in(c, tmp, b, n, ptr_kind);
+  S.solve(bd, c.precision);
+  TMB_CUDA(cudaMemcpyAsync(x, S.x.p, n * sizeof(double),
+                           ptr_kind == TMB_PTR_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c.stream));
+  c.sync();
+  if (S.last_status == 3) return fail(TMB_ERR_NOCONVERGE, "tmb_solver_solve: not converged within maxiter");
+  if (S.last_status == 5) return fail(TMB_ERR_NAN, "tmb_solver_solve: breakdown (NaN or non-positive p.Ap)");
+  TMB_API_END
+}
+
+int tmb_solver_info(tmb_solver* s, double* info) {
+  TMB_CHECK_ARG(s && info, "tmb_solver_info: null argument");
+  info[0] = s->s->last_iters;
+  info[1] = s->s->last_relres;
+  info[2] = s->s->last_status;
+  return TMB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,143 @@
+// Device data structures and kernel launchers of the tetmag B200 library.
+//
+// Sparse operators are stored in SELL-32: rows are grouped in slices of 32
+// consecutive rows; a slice is stored column-major with the width of its
+// longest row, so thread r of a warp reads element k of row r at
+// soff[slice] + 32*k + lane -- every load of a warp is one contiguous,
+// 128/256-byte segment.  Padding entries point at the row itself with value 0.
+// Several operators with the same pattern (K, grad_{x,y,z}, tGrad_{x,y,z})
+// share one index array and keep one value array each, so a kernel that needs
+// several of them (bulk DMI, divergence, gradient) reads the indices once.
+//
+// Values are FP64 (the plain path) or FP32 (the mixed path); vectors and all
+// accumulations are FP64 in both.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+namespace tmb {
+
+#define TMB_CUDA(call)                                                                          \
+  do {                                                                                          \
+    cudaError_t _e = (call);                                                                    \
+    if (_e != cudaSuccess)                                                                      \
+      throw std::runtime_error(std::string("CUDA error ") + cudaGetErrorString(_e) + " at " +   \
+                               __FILE__ + ":" + std::to_string(__LINE__));                      \
+  } while (0)
+
+constexpr int kSlice = 32;
+constexpr int kBlock = 256;
+
+struct SellView {
+  int n;             // rows
+  int nslice;
+  const int* soff;   // nslice + 1 element offsets (multiples of 32)
+  const int* col;    // padded column indices
+};
+
+struct CsrView {
+  int n;
+  const int* ptr;
+  const int* col;
+};
+
+// Scalars of one PCG solve, resident on the device so that no kernel needs
+// the host between iterations.
+struct CgScalars {
+  double rz, rz_new, pq, rr, bb, alpha, beta, tol2;
+  int iter, done, maxit, status;
+  unsigned int ticket[4];
+};
+
+// --- launchers (k_field.cu) --------------------------------------------------------------
+struct LocalFieldArgs {
+  int n;
+  const double* m;          // 3N SoA state
+  const double* hfix;       // 3N field added as is (applied + frozen demag), may be null
+  const double* xc;         // N  exchange row scale  -2 A_i / V_i / Js_i
+  const double* ku2;        // N  2 Ku_i / Js_i, null without uniaxial anisotropy
+  const double* kax;        // 3N SoA easy axis
+  const double* dmi_s;      // N  D_i / V_i / Js_i, null without bulk DMI
+  const double* area;       // N  boundary node area (bulk DMI surface term)
+  const double* nvn;        // 3N SoA node normal
+  double alpha;
+  int precession;
+  double* ydot;             // 3N out, may be null
+  double* hout;             // 3N out (total field), may be null
+  unsigned long long* torque_bits;  // max |m x H| (ordered bits), may be null
+};
+
+template <typename V>
+void launch_local_field(const SellView& s, const V* K, const V* tg0, const V* tg1, const V* tg2,
+                        const LocalFieldArgs& a, cudaStream_t st);
+
+template <typename V>
+void launch_divergence(const SellView& s, const V* tg0, const V* tg1, const V* tg2, const double* m,
+                       const double* js, double inv_mu0, double* rhs, cudaStream_t st);
+
+template <typename V>
+void launch_gradient(const SellView& s, const V* g0, const V* g1, const V* g2, const double* u1,
+                     const double* u2, const double* hext, double* hdem, double* hfix, cudaStream_t st);
+
+void launch_normalize(int n, double* m, cudaStream_t st);
+void launch_rk_combine(int n3, const double* y, const double* const* k, const double* a, int nk, double h,
+                       double* out, cudaStream_t st);
+void launch_rk_error(int n3, const double* y, const double* k1, const double* const* k, const double* e, int nk,
+                     double h, double eps_abs, double eps_rel, unsigned long long* err_bits, cudaStream_t st);
+void launch_fill(double* p, double v, size_t n, cudaStream_t st);
+void launch_add(int n, const double* a, const double* b, double* out, cudaStream_t st);
+
+// --- launchers (k_solver.cu) -------------------------------------------------------------
+template <typename V>
+void launch_spmv(const SellView& s, const V* val, const double* x, double* y, const int* done, cudaStream_t st);
+template <typename V>
+void launch_residual(const SellView& s, const V* val, const double* b, const double* x, double* r,
+                     const int* done, cudaStream_t st);
+void launch_jacobi0(int n, const double* dinv, const double* b, double* x, const int* done, cudaStream_t st);
+template <typename V>
+void launch_jacobi(const SellView& s, const V* val, const double* dinv, const double* b, const double* xin,
+                   double* xout, const int* done, cudaStream_t st);
+template <typename V>
+void launch_csr_spmv(const CsrView& c, const V* val, const double* x, double* y, bool accumulate,
+                     const int* done, cudaStream_t st);
+void launch_coarse_solve(int n, const double* inv, const double* b, double* x, const int* done, cudaStream_t st);
+
+template <typename V>
+void launch_cg_init(int n, const CsrView& lift, const V* lval, const int* cmask, const double* b,
+                    double* bprime, double* x, cudaStream_t st);
+template <typename V>
+void launch_cg_residual(const SellView& s, const V* val, const double* bp, const double* x, double* r,
+                        CgScalars* S, double* partials, cudaStream_t st);
+void launch_cg_rz(int n, const double* r, const double* z, CgScalars* S, double* partials, bool first,
+                  cudaStream_t st);
+void launch_cg_pupdate(int n, const double* z, double* p, CgScalars* S, cudaStream_t st);
+template <typename V>
+void launch_cg_spmv_pq(const SellView& s, const V* val, const double* p, double* q, CgScalars* S,
+                       double* partials, cudaStream_t st);
+void launch_cg_update(int n, const double* p, const double* q, double* x, double* r, CgScalars* S,
+                      double* partials, cudaStream_t st);
+
+// --- launchers (k_bem.cu) ----------------------------------------------------------------
+void launch_bem_assemble(int nb, int ntri, const double* bxyz, const int* tri, const double* area,
+                         const double* nrm, const double* solid, double* B, cudaStream_t st);
+void launch_to_float(const double* src, float* dst, size_t n, cudaStream_t st);
+template <typename V>
+void launch_bem_gemv(int nb, const V* B, const double* u1, const int* bnodes, double* u2b, cudaStream_t st);
+void launch_dirichlet_values(int n, const int* bindex, const double* u2b, double* b, cudaStream_t st);
+void launch_gather(int nb, const double* u, const int* idx, double* out, cudaStream_t st);
+size_t bem_ld(int nb);  // leading dimension (elements) of the row-major device BEM matrix
+
+// Count of kernel launches issued by this library (all contexts), for benchmarking.
+long long launch_count();
+void note_launch();
+
+inline int grid_for(long long n, int block = kBlock) {
+  long long g = (n + block - 1) / block;
+  return int(g < 1 ? 1 : g);
+}
+
+}  // namespace tmb

@@ -1,0 +1,91 @@
+// Host-side data structures of the tetmag B200 library (internal header).
+//
+// The mesh preprocessing here produces the operators that tetmag's
+// PreprocessMesh / MeshBoundary / BEMprocessing hand to TheLLG and DemagField
+// (MeshData, specs/MeshData.h:41-63): the stiffness matrix K, the nodal
+// gradient operators grad_{x,y,z}, the weak-divergence operators
+// tGrad_{x,y,z}, node volumes, boundary nodes, boundary triangles with
+// outward normals, node areas and node normals, and the interior solid angle
+// at every boundary node.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace tmb {
+
+// Compressed sparse row matrix, int32 indices, sorted columns per row.
+struct Csr {
+  int nrows = 0, ncols = 0;
+  std::vector<int> ptr, col;
+  std::vector<double> val;
+  int64_t nnz() const { return ptr.empty() ? 0 : ptr.back(); }
+};
+
+// All seven FEM operators share one sparsity pattern: every (i, j) node
+// pair of every element (preproc/FEMprocessing.cpp:237-252, 256-286).
+struct FemOperators {
+  int nx = 0;
+  std::vector<int> ptr, col;               // shared CSR pattern
+  std::vector<double> stiff;               // K
+  std::vector<double> grad[3];             // volume-averaged nodal gradient
+  std::vector<double> tgrad[3];            // weak divergence (not negated)
+  std::vector<double> node_vol;            // lumped node volume
+  std::vector<double> elem_vol;
+};
+
+struct BoundaryData {
+  std::vector<int> bnodes;                 // ascending global ids (Nb)
+  std::vector<int> bindex;                 // N -> boundary index or -1
+  std::vector<int> tri;                    // T x 3 global ids, ascending per triangle
+  std::vector<int> tri_tet;                // owning tetrahedron
+  std::vector<double> tri_area;            // T
+  std::vector<double> tri_normal;          // T x 3 outward unit normal
+  std::vector<double> node_area;           // N
+  std::vector<double> node_normal;         // N x 3 (row-major), 0 off the boundary
+  std::vector<double> solid_angle;         // Nb interior solid angle
+};
+
+struct MeshHost {
+  int nx = 0, ntet = 0;
+  std::vector<double> xyz;                 // N x 3 row-major
+  std::vector<int> tets;                   // E x 4
+  FemOperators fem;
+  BoundaryData bnd;
+};
+
+// setup.cpp
+void fem_prepare(MeshHost& m);
+void extract_boundary(MeshHost& m);
+void compute_solid_angles(MeshHost& m);
+double solid_angle(const double* x, const double* t1, const double* t2, const double* t3);
+
+// amg.cpp -- smoothed-aggregation hierarchy built on the host.
+struct AmgLevel {
+  Csr A;                                   // level operator
+  Csr P;                                   // prolongation to this level from the next (n_l x n_{l+1})
+  Csr R;                                   // restriction (P^T)
+  std::vector<double> dinv;                // damped inverse diagonal for the Jacobi smoother
+};
+
+struct AmgParams {
+  double eps_strong = 0.08;                // strength threshold (AMGCL default)
+  double relax = 0.75;                     // prolongation-smoother factor (main/AMGCLSolver.cpp:40)
+  int coarse_enough = 200;                 // dense FP64 solve below this size
+  int max_levels = 12;
+  double jacobi_omega = 0.8;               // smoother damping (times 1/rho estimate)
+};
+
+struct AmgHierarchy {
+  std::vector<AmgLevel> levels;            // levels[0].A is the fine operator
+  int ncoarse = 0;
+  std::vector<double> coarse_inv;          // dense ncoarse x ncoarse inverse (row-major), FP64
+  double setup_ms = 0.0;
+};
+
+void amg_build(const Csr& A, const AmgParams& prm, AmgHierarchy& H);
+void csr_transpose(const Csr& A, Csr& T);
+void csr_multiply(const Csr& A, const Csr& B, Csr& C);
+
+}  // namespace tmb

@@ -1,0 +1,158 @@
+"""Seeded synthetic meshes and initial states for the tetmag workloads.
+
+tetmag reads its tetrahedral meshes from legacy VTK / gmsh files
+(io/MeshReaderInterface.cpp:68-82) and its initial magnetisation from
+specs/InitMag.cpp:44-247.  The workloads here are generated instead:
+
+* ``kuhn_cuboid`` -- a structured cuboid whose cubic cells are each split into
+  six tetrahedra around the (1,1,1) diagonal (Kuhn / Freudenthal split).  All
+  cells use the same split, so the mesh is conforming.  Coordinates are in
+  mesh units (nm for ``scale = 1e-9``), centred on the origin like the
+  vortex initial state of specs/InitMag.cpp:203-225 expects.
+* ``jittered_disk`` -- an unstructured disk from a seeded Delaunay
+  tetrahedralisation of a jittered lattice (the interfacial-DMI workload).
+* initial states: uniform random on the unit sphere, and a vortex with a
+  seeded core position.
+
+Node numbering of the cuboid is ``i + nx*(j + ny*k)`` (x fastest).
+"""
+from __future__ import annotations
+
+import itertools
+from dataclasses import dataclass
+
+import numpy as np
+
+
+@dataclass
+class Mesh:
+    xyz: np.ndarray      # (N, 3) float64, mesh units
+    tets: np.ndarray     # (E, 4) int32
+    scale: float = 1e-9  # metres per mesh unit (the ``scale`` key of simulation.cfg)
+    name: str = "mesh"
+
+    @property
+    def nx(self) -> int:
+        return int(self.xyz.shape[0])
+
+
+def kuhn_cuboid(ncx: int, ncy: int, ncz: int, h: float, scale: float = 1e-9,
+                name: str = "cuboid") -> Mesh:
+    """Cuboid of ncx*ncy*ncz cubes of edge h, each cube split into 6 tets."""
+    nx, ny, nz = ncx + 1, ncy + 1, ncz + 1
+    gx = (np.arange(nx) - 0.5 * ncx) * h
+    gy = (np.arange(ny) - 0.5 * ncy) * h
+    gz = (np.arange(nz) - 0.5 * ncz) * h
+    Z, Y, X = np.meshgrid(gz, gy, gx, indexing="ij")
+    xyz = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1).astype(np.float64)
+
+    ci, cj, ck = np.meshgrid(np.arange(ncx), np.arange(ncy), np.arange(ncz), indexing="ij")
+    ci, cj, ck = ci.ravel(), cj.ravel(), ck.ravel()
+
+    def node(di, dj, dk):
+        return (ci + di) + nx * ((cj + dj) + ny * (ck + dk))
+
+    tets = []
+    for perm in itertools.permutations(range(3)):
+        off = np.zeros(3, dtype=int)
+        verts = [node(0, 0, 0)]
+        for ax in perm:
+            off[ax] = 1
+            verts.append(node(*off))
+        tets.append(np.stack(verts, axis=1))
+    tets = np.concatenate(tets, axis=0).astype(np.int32)
+    # order elements cell by cell (memory locality of the element loop)
+    cell = np.tile(np.arange(ci.size), 6)
+    order = np.argsort(cell, kind="stable")
+    return Mesh(xyz=xyz, tets=np.ascontiguousarray(tets[order]), scale=scale, name=name)
+
+
+def jittered_disk(diameter: float, thickness: float, h: float, seed: int,
+                  jitter: float = 0.3, scale: float = 1e-9, name: str = "disk") -> Mesh:
+    """Seeded Delaunay disk: jittered lattice points inside a cylinder.
+
+    Boundary points (rim circle rings and the two faces) are placed without
+    jitter in the normal direction so the surface stays a clean cylinder.
+    Slivers (tets with |volume| < 1e-3 h^3) are removed.
+    """
+    from scipy.spatial import Delaunay
+
+    rng = np.random.default_rng(seed)
+    R = 0.5 * diameter
+    nz = max(1, int(round(thickness / h)))
+    zs = np.linspace(-0.5 * thickness, 0.5 * thickness, nz + 1)
+    pts = []
+    n_ring = max(8, int(round(2 * np.pi * R / h)))
+    for iz, z in enumerate(zs):
+        # interior lattice points of this layer
+        g = np.arange(-R, R + 1e-9, h)
+        X, Y = np.meshgrid(g, g, indexing="ij")
+        X = X.ravel(); Y = Y.ravel()
+        X = X + jitter * h * rng.uniform(-1, 1, X.size)
+        Y = Y + jitter * h * rng.uniform(-1, 1, Y.size)
+        keep = X * X + Y * Y < (R - 0.5 * h) ** 2
+        zz = np.full(int(keep.sum()), z)
+        if 0 < iz < nz:
+            zz = zz + jitter * h * rng.uniform(-1, 1, zz.size) * 0.5
+        pts.append(np.stack([X[keep], Y[keep], zz], axis=1))
+        phi = 2 * np.pi * (np.arange(n_ring) + 0.5 * (iz % 2)) / n_ring
+        pts.append(np.stack([R * np.cos(phi), R * np.sin(phi), np.full(n_ring, z)], axis=1))
+    xyz = np.concatenate(pts, axis=0)
+    tri = Delaunay(xyz)
+    tets = tri.simplices.astype(np.int32)
+    p = xyz[tets]
+    vol = np.einsum("ij,ij->i", np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0]), p[:, 3] - p[:, 0]) / 6.0
+    tets = tets[np.abs(vol) > 1e-3 * h ** 3]
+    used = np.unique(tets)
+    remap = -np.ones(xyz.shape[0], dtype=np.int64)
+    remap[used] = np.arange(used.size)
+    return Mesh(xyz=np.ascontiguousarray(xyz[used]), tets=remap[tets].astype(np.int32),
+                scale=scale, name=name)
+
+
+def random_state(n: int, seed: int) -> np.ndarray:
+    """i.i.d. directions uniform on S^2 (normalised Gaussian triples), SoA (3N,)."""
+    rng = np.random.default_rng(seed)
+    g = rng.standard_normal((n, 3))
+    g /= np.linalg.norm(g, axis=1, keepdims=True)
+    return np.ascontiguousarray(g.T.ravel())
+
+
+def vortex_state(xyz: np.ndarray, seed: int, core_radius: float = 10.0,
+                 polarity: float = 1.0, chirality: float = 1.0) -> np.ndarray:
+    """In-plane vortex with a seeded core position in the central half.
+
+    Follows the shape of the ``vortex`` initial state (specs/InitMag.cpp:203-225):
+    curling in-plane magnetisation around the core; here the core has a smooth
+    out-of-plane profile m_z = p*exp(-(r/rc)^2) instead of a hard disc.
+    """
+    rng = np.random.default_rng(seed)
+    lo, hi = xyz[:, :2].min(axis=0), xyz[:, :2].max(axis=0)
+    centre = 0.5 * (lo + hi) + 0.25 * (hi - lo) * rng.uniform(-1, 1, 2)
+    d = xyz[:, :2] - centre
+    r = np.linalg.norm(d, axis=1)
+    mz = polarity * np.exp(-(r / core_radius) ** 2)
+    inpl = np.sqrt(np.maximum(0.0, 1.0 - mz * mz))
+    rs = np.where(r > 0, r, 1.0)
+    mx = -chirality * d[:, 1] / rs * inpl
+    my = chirality * d[:, 0] / rs * inpl
+    m = np.stack([mx, my, mz], axis=1)
+    m /= np.linalg.norm(m, axis=1, keepdims=True)
+    return np.ascontiguousarray(m.T.ravel()), centre
+
+
+def uniform_state(n: int, direction=(1.0, 0.0, 0.0)) -> np.ndarray:
+    d = np.asarray(direction, dtype=np.float64)
+    d = d / np.linalg.norm(d)
+    return np.ascontiguousarray(np.repeat(d, n))
+
+
+def field_from_angles(n: int, b_tesla: float, theta_deg: float, phi_deg: float) -> np.ndarray:
+    """Uniform applied field in A/m, SoA (3N,): B/mu0 along (theta, phi).
+
+    Same convention as fieldFromAngles (main/TheLLG.cpp:442-449).
+    """
+    mu0 = 1.256637061435917295376e-6
+    th, ph = np.deg2rad(theta_deg), np.deg2rad(phi_deg)
+    d = np.array([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)])
+    return np.ascontiguousarray(np.repeat(d * (b_tesla / mu0), n))

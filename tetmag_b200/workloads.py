@@ -1,0 +1,108 @@
+"""Seeded synthetic workloads of the tetmag field path and their device setup.
+
+Each workload restates one measurement configuration: mesh, material,
+applied field, initial state and run length.  ``setup_context`` drives the
+library end to end: C++ preprocessing (MeshOps), device BEM assembly, material
+and applied field.  Material units follow specs/SimulationData.cpp:45-57
+(Js = mu0 Ms in T; A / scale^2; D / scale).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import meshgen
+from .meshgen import Mesh
+
+MU0 = 1.256637061435917295376e-6
+
+
+@dataclass
+class Workload:
+    name: str
+    mesh: Mesh
+    Ms: float
+    A: float
+    alpha: float
+    m0: np.ndarray                         # 3N SoA
+    hext: np.ndarray                       # 3N SoA, A/m
+    Ku: float = 0.0
+    ku_axis: Optional[np.ndarray] = None   # 3N SoA
+    D: float = 0.0
+    duration_ps: float = 1000.0
+    segment_ps: float = 0.5
+    info: dict = field(default_factory=dict)
+
+    @property
+    def n(self) -> int:
+        return self.mesh.nx
+
+    def material_arrays(self):
+        n, s = self.n, self.mesh.scale
+        Js = np.full(n, MU0 * self.Ms)
+        A = np.full(n, self.A / s ** 2)
+        Ku = np.full(n, self.Ku) if self.Ku != 0.0 else None
+        D = np.full(n, self.D / s) if self.D != 0.0 else None
+        return Js, A, Ku, self.ku_axis, D
+
+
+def cuboid_random(ncx: int, ncy: int, ncz: int, h: float, seed: int = 1, alpha: float = 1.0,
+                  name: str = "cuboid") -> Workload:
+    mesh = meshgen.kuhn_cuboid(ncx, ncy, ncz, h, name=name)
+    return Workload(name=name, mesh=mesh, Ms=8.0e5, A=1.3e-11, alpha=alpha,
+                    m0=meshgen.random_state(mesh.nx, seed), hext=np.zeros(3 * mesh.nx))
+
+
+def c1(seed: int = 1) -> Workload:
+    """Permalloy cuboid 100x100x10 nm, 5 nm Kuhn cells (21x21x3 = 1323 nodes), dense BEM,
+    alpha = 1, zero field, random initial state, relax 1 ns."""
+    w = cuboid_random(20, 20, 2, 5.0, seed=seed, alpha=1.0, name="c1_cuboid_100x100x10nm_h5")
+    w.duration_ps = 1000.0
+    return w
+
+
+def c2(seed: int = 2) -> Workload:
+    """Permalloy cuboid 500x500x20 nm, 2.5 nm Kuhn cells (201x201x9 = 363609 nodes),
+    alpha = 0.02, 20 mT at 10 deg in-plane, seeded vortex, 2 ns."""
+    mesh = meshgen.kuhn_cuboid(200, 200, 8, 2.5, name="c2_cuboid_500x500x20nm_h2.5")
+    m0, centre = meshgen.vortex_state(mesh.xyz, seed=seed, core_radius=10.0)
+    return Workload(name=mesh.name, mesh=mesh, Ms=8.0e5, A=1.3e-11, alpha=0.02, m0=m0,
+                    hext=meshgen.field_from_angles(mesh.nx, 0.020, 90.0, 10.0), duration_ps=2000.0,
+                    info=dict(vortex_centre_nm=centre.tolist()))
+
+
+def c4_replica(seed: int = 4, replica: int = 0) -> Workload:
+    """Cuboid 200x200x40 nm, 4 nm Kuhn cells (51x51x11 = 28611 nodes, 7002 boundary nodes);
+    one of 64 replicas: seeded random m0 and 0-50 mT at a random direction, alpha = 0.5, 1 ns."""
+    mesh = meshgen.kuhn_cuboid(50, 50, 10, 4.0, name="c4_cuboid_200x200x40nm_h4")
+    rng = np.random.default_rng([seed, replica])
+    b = rng.uniform(0.0, 0.050)
+    d = rng.standard_normal(3)
+    d /= np.linalg.norm(d)
+    th, ph = np.degrees(np.arccos(d[2])), np.degrees(np.arctan2(d[1], d[0]))
+    return Workload(name=mesh.name, mesh=mesh, Ms=8.0e5, A=1.3e-11, alpha=0.5,
+                    m0=meshgen.random_state(mesh.nx, int(rng.integers(1 << 31))),
+                    hext=meshgen.field_from_angles(mesh.nx, b, th, ph), duration_ps=1000.0,
+                    info=dict(replica=replica, b_tesla=b))
+
+
+WORKLOADS = {"c1": c1, "c2": c2, "c4": c4_replica}
+
+
+def setup_context(w: Workload, device: int = 0, mixed: bool = False, tol: float = 1e-7, maxiter: int = 100,
+                  mesh_ops=None):
+    """MeshOps + Context with operators, device-assembled dense BEM, material and field."""
+    from .api import Context, MeshOps
+
+    mo = mesh_ops if mesh_ops is not None else MeshOps(w.mesh.xyz, w.mesh.tets)
+    ctx = Context(device)
+    ctx.set_mesh(mo)
+    ctx.bem_assemble(mo)
+    Js, A, Ku, axis, D = w.material_arrays()
+    ctx.set_material(Js, A, Ku=Ku, ku_axis=axis, D=D, alpha=w.alpha)
+    ctx.set_applied_field(np.ascontiguousarray(w.hext, dtype=np.float64))
+    ctx.set_precision(mixed)
+    ctx.set_solver_params(tol, maxiter)
+    return mo, ctx
