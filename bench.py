@@ -42,7 +42,8 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--workload", default="c2", choices=["c1", "c2", "c4"])
+    p.add_argument("--workload", default="c2",
+                   help="c1, c2, c4, or cuboid:NXxNYxNZxH (Kuhn cuboid of NX*NY*NZ cells of edge H nm)")
     p.add_argument("--tol", type=float, default=1e-7)
     p.add_argument("--sim-ps", type=float, default=2.0, help="simulated ps for the ns/hour figure")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -106,6 +107,20 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def make_workload(name: str, rank: int):
+    """The named configuration; each rank gets its own seed (independent replicas)."""
+    from tetmag_b200 import workloads
+
+    if name == "c4":
+        return workloads.c4_replica(replica=rank)
+    if name.startswith("cuboid:"):
+        nx, ny, nz, h = name.split(":", 1)[1].split("x")
+        w = workloads.cuboid_random(int(nx), int(ny), int(nz), float(h), seed=7 + rank, alpha=0.5,
+                                    name=f"cuboid_{nx}x{ny}x{nz}_h{h}")
+        return w
+    return workloads.WORKLOADS[name](seed=2 + 17 * rank)
+
+
 def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -133,7 +148,7 @@ def run_reference(args):
         return
     from tetmag_b200 import workloads
 
-    w = workloads.WORKLOADS[args.workload]()
+    w = make_workload(args.workload, 0)
     ev, res = cpu_baseline_sample(w, samples=0)
     m = w.m0.reshape(3, -1).T.copy()
     for _ in range(args.warmup):
@@ -174,13 +189,14 @@ def run_gpu(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
-    w = workloads.WORKLOADS[args.workload](seed=2 + 17 * rank) if args.workload != "c4" else \
-        workloads.c4_replica(replica=rank)
+    w = make_workload(args.workload, rank)
     t0 = time.perf_counter()
     mo, ctx = workloads.setup_context(w, device=local, mixed=True, tol=args.tol, maxiter=100)
     setup_s = time.perf_counter() - t0
-    stream = torch.cuda.current_stream(dev)
+    # one non-default stream for the library's kernels and the timing events
+    stream = torch.cuda.Stream(dev)
     ctx.set_stream(stream.cuda_stream)
+    torch.cuda.set_stream(stream)
     n = w.n
     K, W = args.steps, args.warmup
 
@@ -238,9 +254,12 @@ def run_gpu(args):
 
     clocks = Clocks(local)
     clocks.start()
-    ms_mx, launches, prof, its_mx = timed(True, True)
+    ms_mx, launches, _, its_mx = timed(True, False)
     clk = clocks.stop()
     ms_64, _, _, its_64 = timed(False, False)
+    # per-kernel CUDA-event timing in a separate pass over the same K states (with the
+    # profiler on, the PCG runs kernel by kernel instead of from CUDA graphs)
+    _, _, prof, _ = timed(True, True)
 
     # relative error of the mixed path against the FP64 path, on one state
     probe = S[W + K - 1]
@@ -325,6 +344,11 @@ def run_gpu(args):
                   "rhs": rs["rhs"]},
         "cg_iters_per_eval": {"mixed": [i / K for i in its_mx], "fp64": [i / K for i in its_64]},
         "kernel_time_share": kshare,
+        "kernels": {k: {"launches": prof[k]["launches"],
+                        "avg_us": 1e3 * prof[k]["total_ms"] / max(prof[k]["launches"], 1),
+                        "gbs": (prof[k]["bytes_per_launch"] / (prof[k]["total_ms"] / max(prof[k]["launches"], 1) / 1e3)
+                                / 1e9) if prof[k]["total_ms"] > 0 and prof[k]["bytes_per_launch"] > 0 else None}
+                    for k in kernels},
         "setup_s": setup_s,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -21,6 +21,8 @@ INCLUDE = PKG.parent / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-fopenmp,-O3", f"-I{INCLUDE}", f"-I{CSRC}"]
+# per-file flags: the BEM assembly follows the restated operation order without contraction
+EXTRA = {"k_bem_assemble.cu": ["-fmad=false"]}
 
 
 def nvcc() -> str:
@@ -46,9 +48,7 @@ def _compile(src: Path, verbose: bool) -> Path:
     obj = OUT / (src.name + ".o")
     if not _needs(obj, src):
         return obj
-    cmd = [nvcc(), *ARCH, *COMMON, "-c", str(src), "-o", str(obj)]
-    if src.suffix == ".cpp":
-        cmd[1:1] = ["-x", "cu"] if False else []
+    cmd = [nvcc(), *ARCH, *COMMON, *EXTRA.get(src.name, []), "-c", str(src), "-o", str(obj)]
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -253,6 +253,14 @@ void amg_build(const Csr& A0, const AmgParams& prm, AmgHierarchy& H) {
       std::vector<double> dense(size_t(n) * n, 0.0);
       for (int i = 0; i < n; ++i)
         for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) dense[size_t(i) * n + A.col[k]] += A.val[k];
+      if (prm.singular) {
+        // constants span the null space on every level (P 1 = 1 since A 1 = 0): invert
+        // A_c + a 1 1^T, which acts as the pseudo-inverse on the range of A_c
+        double tr = 0.0;
+        for (int i = 0; i < n; ++i) tr += dense[size_t(i) * n + i];
+        const double a = tr / (double(n) * n);
+        for (auto& v : dense) v += a;
+      }
       dense_inverse(dense, n);
       H.coarse_inv.swap(dense);
       L.A = std::move(A);

@@ -233,6 +233,7 @@ std::atomic<long long> g_launches{0};
 
 long long launch_count() { return g_launches.load(); }
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void note_launches(long long k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 
 template <typename V>
 void launch_local_field(const SellView& s, const V* K, const V* tg0, const V* tg1, const V* tg2,

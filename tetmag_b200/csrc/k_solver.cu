@@ -110,6 +110,30 @@ __global__ void __launch_bounds__(kBlock) k_jacobi(SellView s, const V* __restri
   if (row < s.n) xout[row] = xin[row] + dinv[row] * (b[row] - sell_row_dot(s, val, xin, row));
 }
 
+// First smoothing sweep from zero fused with the residual: x = D_w^-1 b, r = b - A x,
+// gathering D_w^-1 b on the fly instead of reading back x.
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_jacobi0_residual(SellView s, const V* __restrict__ val,
+                                                             const double* __restrict__ dinv,
+                                                             const double* __restrict__ b, double* __restrict__ x,
+                                                             double* __restrict__ r, const int* done) {
+  if (done && *done) return;
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= s.n) return;
+  const int sl = row >> 5;
+  const int beg = __ldg(s.soff + sl) + (row & 31);
+  const int end = __ldg(s.soff + sl + 1);
+  double acc = 0.0;
+#pragma unroll 4
+  for (int k = beg; k < end; k += kSlice) {
+    const int j = __ldg(s.col + k);
+    acc = fma(static_cast<double>(__ldg(val + k)), __ldg(dinv + j) * __ldg(b + j), acc);
+  }
+  const double bi = b[row];
+  x[row] = dinv[row] * bi;
+  r[row] = bi - acc;
+}
+
 // CSR product for the transfer operators; 4 threads cooperate on a row.
 template <typename V>
 __global__ void __launch_bounds__(kBlock) k_csr_spmv(CsrView c, const V* __restrict__ val,
@@ -196,6 +220,68 @@ __global__ void __launch_bounds__(kBlock) k_cg_rz(int n, const double* __restric
       S->beta = tot[0] / S->rz;
     }
     S->rz = tot[0];
+  }
+}
+
+// Last post-smoothing sweep of the finest level fused with rho = r.z:
+// z = x + D_w^-1 (r - A x); the last block sets beta = rho_new / rho (0 on the first pass).
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_jacobi_rz(SellView s, const V* __restrict__ val,
+                                                      const double* __restrict__ dinv, const double* __restrict__ r,
+                                                      const double* __restrict__ xin, double* __restrict__ z,
+                                                      CgScalars* S, double* partials, int first) {
+  if (S->done) return;
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[1] = {0.0};
+  if (row < s.n) {
+    const double ri = r[row];
+    const double zi = xin[row] + dinv[row] * (ri - sell_row_dot(s, val, xin, row));
+    z[row] = zi;
+    v[0] = ri * zi;
+  }
+  double tot[1];
+  if (grid_reduce<1>(v, partials, &S->ticket[1], tot) && threadIdx.x == 0) {
+    S->beta = first ? 0.0 : tot[0] / S->rz;
+    S->rz = tot[0];
+  }
+}
+
+// q = A p_new with p_new = z + beta p_old formed on the fly (two gathers), p_new written
+// for the own row into a second buffer; p.Ap reduced, the last block sets alpha.
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_cg_dir_spmv(SellView s, const V* __restrict__ val,
+                                                        const double* __restrict__ z,
+                                                        const double* __restrict__ p_old, double* __restrict__ p_new,
+                                                        double* __restrict__ q, CgScalars* S, double* partials) {
+  if (S->done) return;
+  const double beta = S->beta;
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[1] = {0.0};
+  if (row < s.n) {
+    const int sl = row >> 5;
+    const int beg = __ldg(s.soff + sl) + (row & 31);
+    const int end = __ldg(s.soff + sl + 1);
+    double acc = 0.0;
+    if (beta == 0.0) {
+#pragma unroll 4
+      for (int k = beg; k < end; k += kSlice)
+        acc = fma(static_cast<double>(__ldg(val + k)), __ldg(z + __ldg(s.col + k)), acc);
+    } else {
+#pragma unroll 4
+      for (int k = beg; k < end; k += kSlice) {
+        const int j = __ldg(s.col + k);
+        acc = fma(static_cast<double>(__ldg(val + k)), fma(beta, __ldg(p_old + j), __ldg(z + j)), acc);
+      }
+    }
+    const double pi = (beta == 0.0) ? z[row] : fma(beta, p_old[row], z[row]);
+    p_new[row] = pi;
+    q[row] = acc;
+    v[0] = pi * acc;
+  }
+  double tot[1];
+  if (grid_reduce<1>(v, partials, &S->ticket[2], tot) && threadIdx.x == 0) {
+    S->pq = tot[0];
+    S->alpha = S->rz / tot[0];
   }
 }
 
@@ -315,6 +401,25 @@ void launch_cg_spmv_pq(const SellView& s, const V* val, const double* p, double*
   note_launch();
   k_cg_spmv_pq<V><<<grid_for(s.n), kBlock, 0, st>>>(s, val, p, q, S, partials);
 }
+template <typename V>
+void launch_jacobi0_residual(const SellView& s, const V* val, const double* dinv, const double* b, double* x,
+                             double* r, const int* done, cudaStream_t st) {
+  note_launch();
+  k_jacobi0_residual<V><<<grid_for(s.n), kBlock, 0, st>>>(s, val, dinv, b, x, r, done);
+}
+template <typename V>
+void launch_jacobi_rz(const SellView& s, const V* val, const double* dinv, const double* r, const double* xin,
+                      double* z, CgScalars* S, double* partials, bool first, cudaStream_t st) {
+  note_launch();
+  k_jacobi_rz<V><<<grid_for(s.n), kBlock, 0, st>>>(s, val, dinv, r, xin, z, S, partials, first ? 1 : 0);
+}
+template <typename V>
+void launch_cg_dir_spmv(const SellView& s, const V* val, const double* z, const double* p_old, double* p_new,
+                        double* q, CgScalars* S, double* partials, cudaStream_t st) {
+  note_launch();
+  k_cg_dir_spmv<V><<<grid_for(s.n), kBlock, 0, st>>>(s, val, z, p_old, p_new, q, S, partials);
+}
+
 void launch_cg_update(int n, const double* p, const double* q, double* x, double* r, CgScalars* S,
                       double* partials, cudaStream_t st) {
   note_launch();
@@ -334,7 +439,13 @@ void launch_cg_update(int n, const double* p, const double* q, double* x, double
   template void launch_cg_residual<V>(const SellView&, const V*, const double*, const double*, double*,     \
                                       CgScalars*, double*, cudaStream_t);                                   \
   template void launch_cg_spmv_pq<V>(const SellView&, const V*, const double*, double*, CgScalars*,         \
-                                     double*, cudaStream_t);
+                                     double*, cudaStream_t);                                                \
+  template void launch_jacobi0_residual<V>(const SellView&, const V*, const double*, const double*, double*, \
+                                           double*, const int*, cudaStream_t);                              \
+  template void launch_jacobi_rz<V>(const SellView&, const V*, const double*, const double*, const double*, \
+                                    double*, CgScalars*, double*, bool, cudaStream_t);                      \
+  template void launch_cg_dir_spmv<V>(const SellView&, const V*, const double*, const double*, double*,     \
+                                      double*, CgScalars*, double*, cudaStream_t);
 TMB_INST(double)
 TMB_INST(float)
 #undef TMB_INST

@@ -251,7 +251,7 @@ struct Solver {
   int ncoarse = 0;
   DevCsr lift;
   DevArray<int> cmask;
-  DevArray<double> x, r, z, p, q, bp, partials;
+  DevArray<double> x, r, z, p[2], q, bp, partials;
   CgScalars* Sd = nullptr;
   CgScalars* Sh = nullptr;
   int last_iters = 0, last_status = 0;
@@ -260,6 +260,7 @@ struct Solver {
 
   explicit Solver(Ctx* c) : ctx(c) {}
   ~Solver() {
+    drop_graphs();
     if (Sd) cudaFree(Sd);
     if (Sh) cudaFreeHost(Sh);
   }
@@ -272,10 +273,27 @@ struct Solver {
   }
   void compute();
   void solve(const double* b_dev, int precision);
-  void vcycle(size_t l, const double* b, double* out, int precision, cudaStream_t st);
+  void vcycle(size_t l, const double* b, double* out, int precision, cudaStream_t st, int rz_mode);
+  void precondition_rz(int precision, cudaStream_t st, bool first);
+  int pcur = 0;  // which of p[0], p[1] holds the current direction
   double nnz_fine = 0.0;
   void ctx_prof_begin(int id, cudaStream_t st, double bytes);
   void ctx_prof_end(cudaStream_t st);
+  bool ctx_prof_on() const;
+  // one PCG iteration: direction update, A p with p.Ap, x/r update with r.r, V-cycle, r.z
+  void iteration_body(int precision, cudaStream_t st, bool profile);
+  // CUDA graph of kGraphIters iteration bodies per precision, captured on first use
+  static constexpr int kGraphIters = 2;
+  cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
+  long long graph_nodes[2] = {0, 0};
+  cudaGraphExec_t graph_for(int precision);
+  void drop_graphs() {
+    for (auto& g : graph_exec)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+  }
 };
 
 // ------------------------------------------------------------------------------------------
@@ -308,6 +326,7 @@ struct Ctx {
   double tol = 1e-7;
   int maxit = 100;
   DevArray<double> rhs, u1, u2, u1b, u2b, bdir;
+  DevArray<float> u1bf;
   // integrator / scratch
   DevArray<double> ybuf[2], kst[7], ytmp, in3, out3;
   DevArray<unsigned long long> bits;
@@ -353,6 +372,44 @@ struct Ctx {
 
 void Solver::ctx_prof_begin(int id, cudaStream_t st, double bytes) { ctx->prof.begin(id, st, bytes); }
 void Solver::ctx_prof_end(cudaStream_t st) { ctx->prof.end(st); }
+bool Solver::ctx_prof_on() const { return ctx->prof.on; }
+
+void Solver::iteration_body(int precision, cudaStream_t st, bool profile) {
+  const SellView A0 = lev[0].A.view();
+  const bool f64 = precision == TMB_FP64;
+  double* pold = p[pcur].p;
+  double* pnew = p[pcur ^ 1].p;
+  pcur ^= 1;
+  // direction update fused into A p: gathers z and p_old (two 8-byte gathers per entry)
+  if (profile) ctx_prof_begin(6, st, nnz_fine * ((f64 ? 8.0 : 4.0) + 4.0) + 5.0 * 8.0 * n);
+  if (f64) launch_cg_dir_spmv<double>(A0, lev[0].Ad.p, z.p, pold, pnew, q.p, Sd, partials.p, st);
+  else launch_cg_dir_spmv<float>(A0, lev[0].Af.p, z.p, pold, pnew, q.p, Sd, partials.p, st);
+  if (profile) ctx_prof_end(st);
+  launch_cg_update(n, pnew, q.p, x.p, r.p, Sd, partials.p, st);
+  precondition_rz(precision, st, false);
+}
+
+cudaGraphExec_t Solver::graph_for(int precision) {
+  if (graph_exec[precision]) return graph_exec[precision];
+  cudaStream_t st = ctx->stream;
+  cudaGraph_t graph = nullptr;
+  const long long before = launch_count();
+  TMB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  try {
+    for (int q = 0; q < kGraphIters; ++q) iteration_body(precision, st, false);
+  } catch (...) {
+    cudaStreamEndCapture(st, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  TMB_CUDA(cudaStreamEndCapture(st, &graph));
+  graph_nodes[precision] = launch_count() - before;
+  note_launches(-graph_nodes[precision]);  // captured, not launched
+  const cudaError_t e = cudaGraphInstantiate(&graph_exec[precision], graph, 0);
+  cudaGraphDestroy(graph);
+  TMB_CUDA(e);
+  return graph_exec[precision];
+}
 
 // ------------------------------------------------------------------------------------------
 // Solver implementation
@@ -389,6 +446,7 @@ void Solver::compute() {
     Ap.ptr[i + 1] = int(Ap.col.size());
     L.ptr[i + 1] = int(L.col.size());
   }
+  drop_graphs();  // captured graphs hold the previous buffers
   amg_build(Ap, prm, H);
   nnz_fine = double(Ap.nnz());
   lev.clear();
@@ -421,7 +479,8 @@ void Solver::compute() {
   x.zero(st);
   r.alloc(n);
   z.alloc(n);
-  p.alloc(n);
+  p[0].alloc(n);
+  p[1].alloc(n);
   q.alloc(n);
   bp.alloc(n);
   partials.alloc(size_t(2) * grid_for(n) + 64);
@@ -434,7 +493,7 @@ void Solver::compute() {
   computed = true;
 }
 
-void Solver::vcycle(size_t l, const double* b, double* out, int precision, cudaStream_t st) {
+void Solver::vcycle(size_t l, const double* b, double* out, int precision, cudaStream_t st, int rz_mode) {
   DevLevel& L = lev[l];
   const int* done = &Sd->done;
   if (l + 1 == lev.size()) {
@@ -443,16 +502,32 @@ void Solver::vcycle(size_t l, const double* b, double* out, int precision, cudaS
   }
   DevLevel& C = lev[l + 1];
   const SellView A = L.A.view();
-  launch_jacobi0(L.n, L.dinv.p, b, L.X.p, done, st);
-  if (precision == TMB_FP64) launch_residual<double>(A, L.Ad.p, b, L.X.p, L.R.p, done, st);
-  else launch_residual<float>(A, L.Af.p, b, L.X.p, L.R.p, done, st);
-  if (precision == TMB_FP64) launch_csr_spmv<double>(L.Rop.view(), L.Rop.v.p, L.R.p, C.b.p, false, done, st);
+  const bool f64 = precision == TMB_FP64;
+  if (f64) launch_jacobi0_residual<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, L.R.p, done, st);
+  else launch_jacobi0_residual<float>(A, L.Af.p, L.dinv.p, b, L.X.p, L.R.p, done, st);
+  if (f64) launch_csr_spmv<double>(L.Rop.view(), L.Rop.v.p, L.R.p, C.b.p, false, done, st);
   else launch_csr_spmv<float>(L.Rop.view(), L.Rop.vf.p, L.R.p, C.b.p, false, done, st);
-  vcycle(l + 1, C.b.p, C.out.p, precision, st);
-  if (precision == TMB_FP64) launch_csr_spmv<double>(L.P.view(), L.P.v.p, C.out.p, L.X.p, true, done, st);
+  vcycle(l + 1, C.b.p, C.out.p, precision, st, -1);
+  if (f64) launch_csr_spmv<double>(L.P.view(), L.P.v.p, C.out.p, L.X.p, true, done, st);
   else launch_csr_spmv<float>(L.P.view(), L.P.vf.p, C.out.p, L.X.p, true, done, st);
-  if (precision == TMB_FP64) launch_jacobi<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, out, done, st);
-  else launch_jacobi<float>(A, L.Af.p, L.dinv.p, b, L.X.p, out, done, st);
+  if (l == 0 && rz_mode >= 0) {
+    // finest level: the post-smoothing sweep also reduces r.z for the next CG direction
+    if (f64) launch_jacobi_rz<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, out, Sd, partials.p, rz_mode == 1, st);
+    else launch_jacobi_rz<float>(A, L.Af.p, L.dinv.p, b, L.X.p, out, Sd, partials.p, rz_mode == 1, st);
+  } else {
+    if (f64) launch_jacobi<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, out, done, st);
+    else launch_jacobi<float>(A, L.Af.p, L.dinv.p, b, L.X.p, out, done, st);
+  }
+}
+
+// Preconditioner application z = M r followed by rho = r.z (first: beta = 0).
+void Solver::precondition_rz(int precision, cudaStream_t st, bool first) {
+  if (lev.size() > 1) {
+    vcycle(0, r.p, z.p, precision, st, first ? 1 : 0);
+  } else {
+    vcycle(0, r.p, z.p, precision, st, -1);
+    launch_cg_rz(n, r.p, z.p, Sd, partials.p, first, st);
+  }
 }
 
 void Solver::solve(const double* b_dev, int precision) {
@@ -470,21 +545,35 @@ void Solver::solve(const double* b_dev, int precision) {
   else launch_cg_init<float>(n, lift.view(), lift.vf.p, cmask.p, b_dev, bp.p, x.p, st);
   if (f64) launch_cg_residual<double>(A0, lev[0].Ad.p, bp.p, x.p, r.p, Sd, partials.p, st);
   else launch_cg_residual<float>(A0, lev[0].Af.p, bp.p, x.p, r.p, Sd, partials.p, st);
-  vcycle(0, r.p, z.p, precision, st);
-  launch_cg_rz(n, r.p, z.p, Sd, partials.p, true, st);
-  for (int it = 0; it < maxit; ++it) {
-    launch_cg_pupdate(n, z.p, p.p, Sd, st);
-    ctx_prof_begin(6, st, nnz_fine * ((f64 ? 8.0 : 4.0) + 4.0) + 3.0 * 8.0 * n);
-    if (f64) launch_cg_spmv_pq<double>(A0, lev[0].Ad.p, p.p, q.p, Sd, partials.p, st);
-    else launch_cg_spmv_pq<float>(A0, lev[0].Af.p, p.p, q.p, Sd, partials.p, st);
-    ctx_prof_end(st);
-    launch_cg_update(n, p.p, q.p, x.p, r.p, Sd, partials.p, st);
-    vcycle(0, r.p, z.p, precision, st);
-    launch_cg_rz(n, r.p, z.p, Sd, partials.p, false, st);
-    if ((it + 1) % check_every == 0 || it + 1 == maxit) {
+  precondition_rz(precision, st, true);
+  pcur = 0;  // graphs are captured with the direction starting in p[0]
+  if (!ctx_prof_on()) {
+    // Graph path: kGraphIters iterations per graph launch; the first batch covers the
+    // previous solve's iteration count, then the done flag is polled after every launch.
+    // Kernels after convergence return at once (they read the done flag).
+    cudaGraphExec_t g = graph_for(precision);
+    const int batches = (maxit + kGraphIters - 1) / kGraphIters;
+    int first = std::max(1, (last_iters + kGraphIters - 1) / kGraphIters);
+    int launched = 0;
+    while (launched < batches) {
+      const int nlaunch = std::min(batches - launched, launched == 0 ? first : 1);
+      for (int q = 0; q < nlaunch; ++q) {
+        TMB_CUDA(cudaGraphLaunch(g, st));
+        note_launches(graph_nodes[precision]);
+      }
+      launched += nlaunch;
       TMB_CUDA(cudaMemcpyAsync(Sh, Sd, sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
       TMB_CUDA(cudaStreamSynchronize(st));
       if (Sh->done) break;
+    }
+  } else {
+    for (int it = 0; it < maxit; ++it) {
+      iteration_body(precision, st, true);
+      if ((it + 1) % check_every == 0 || it + 1 == maxit) {
+        TMB_CUDA(cudaMemcpyAsync(Sh, Sd, sizeof(CgScalars), cudaMemcpyDeviceToHost, st));
+        TMB_CUDA(cudaStreamSynchronize(st));
+        if (Sh->done) break;
+      }
     }
   }
   TMB_CUDA(cudaGetLastError());
@@ -616,6 +705,7 @@ void Ctx::ensure_demag() {
   dir = build([&](int i) { return isb[i] != 0; });
   for (auto* a : {&rhs, &u1, &u2, &bdir}) a->alloc(n);
   u1b.alloc(nb);
+  u1bf.alloc(nb);
   u2b.alloc(nb);
 }
 
@@ -635,10 +725,11 @@ void Ctx::demag(const double* m) {
   prof.begin(4, st, 0.0);
   neu->solve(rhs.p, precision);
   prof.end(st);
-  launch_gather(nb, neu->x.p, bnodes.p, u1b.p, st);
-  prof.begin(3, st, B * B * sv + 2 * B * 8);
-  if (f64) launch_bem_gemv<double>(nb, Bd.p, u1b.p, nullptr, u2b.p, st);
-  else launch_bem_gemv<float>(nb, Bf.p, u1b.p, nullptr, u2b.p, st);
+  if (f64) launch_gather<double>(nb, neu->x.p, bnodes.p, u1b.p, st);
+  else launch_gather<float>(nb, neu->x.p, bnodes.p, u1bf.p, st);
+  prof.begin(3, st, B * B * sv + B * (sv + 8));
+  if (f64) launch_bem_gemv<double>(nb, Bd.p, u1b.p, u2b.p, st);
+  else launch_bem_gemv<float>(nb, Bf.p, u1bf.p, u2b.p, st);
   prof.end(st);
   launch_dirichlet_values(n, bindex.p, u2b.p, bdir.p, st);
   prof.begin(5, st, 0.0);

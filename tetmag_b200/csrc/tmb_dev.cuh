@@ -120,20 +120,76 @@ void launch_cg_spmv_pq(const SellView& s, const V* val, const double* p, double*
                        double* partials, cudaStream_t st);
 void launch_cg_update(int n, const double* p, const double* q, double* x, double* r, CgScalars* S,
                       double* partials, cudaStream_t st);
+// fused variants used by the PCG iteration
+template <typename V>
+void launch_jacobi0_residual(const SellView& s, const V* val, const double* dinv, const double* b, double* x,
+                             double* r, const int* done, cudaStream_t st);
+template <typename V>
+void launch_jacobi_rz(const SellView& s, const V* val, const double* dinv, const double* r, const double* xin,
+                      double* z, CgScalars* S, double* partials, bool first, cudaStream_t st);
+template <typename V>
+void launch_cg_dir_spmv(const SellView& s, const V* val, const double* z, const double* p_old, double* p_new,
+                        double* q, CgScalars* S, double* partials, cudaStream_t st);
 
 // --- launchers (k_bem.cu) ----------------------------------------------------------------
 void launch_bem_assemble(int nb, int ntri, const double* bxyz, const int* tri, const double* area,
                          const double* nrm, const double* solid, double* B, cudaStream_t st);
 void launch_to_float(const double* src, float* dst, size_t n, cudaStream_t st);
 template <typename V>
-void launch_bem_gemv(int nb, const V* B, const double* u1, const int* bnodes, double* u2b, cudaStream_t st);
+void launch_bem_gemv(int nb, const V* B, const V* xb, double* u2b, cudaStream_t st);
 void launch_dirichlet_values(int n, const int* bindex, const double* u2b, double* b, cudaStream_t st);
-void launch_gather(int nb, const double* u, const int* idx, double* out, cudaStream_t st);
+template <typename V>
+void launch_gather(int nb, const double* u, const int* idx, V* out, cudaStream_t st);
 size_t bem_ld(int nb);  // leading dimension (elements) of the row-major device BEM matrix
+
+// --- hierarchical BEM matrix (k_hmatrix.cu) ---------------------------------------------
+struct HBlockDev {
+  int rb, m, cb, n;        // row / column range in cluster order
+  long long off;           // dense tile offset (column-major m x n), near blocks
+  long long uoff, voff;    // ACA scratch offsets (kmax columns each), admissible blocks
+  long long used_off;      // offset of the m row flags in the ACA scratch
+};
+struct HNearRow {
+  int rb, m, first, last;  // leaf row cluster and its near blocks [first, last)
+};
+struct HFarGroup {
+  int rb, m, first, last;  // row cluster and its admissible blocks [first, last)
+};
+template <typename T>
+struct HMatView {
+  int nb = 0, nrows = 0, ngroups = 0, max_group_m = 0;
+  long long nterms = 0;
+  const int* gidx = nullptr;             // permuted position -> boundary node (mesh numbering)
+  const HNearRow* near_rows = nullptr;
+  const HBlockDev* near = nullptr;
+  const T* D = nullptr;                  // dense tiles
+  const HBlockDev* far = nullptr;
+  const int* rank = nullptr;
+  const long long* uoff = nullptr;       // compact U offsets (column-major m x rank)
+  const long long* voff = nullptr;       // compact V offsets (column-major n x rank)
+  const long long* toff = nullptr;       // offsets of t_b in the term buffer
+  const int2* terms = nullptr;           // (block, column) per low-rank term
+  const T* U = nullptr;
+  const T* V = nullptr;
+  const HFarGroup* groups = nullptr;
+};
+void launch_h_near_gather(int nblk, const HBlockDev* blk, const double* B, size_t ld, const int* perm, double* d64,
+                          float* d32, cudaStream_t st);
+void launch_h_aca(int nblk, const HBlockDev* blk, const double* B, size_t ld, const int* perm, double* Us,
+                  double* Vs, unsigned char* used, int kmax, double eps_tight, double eps_loose, int* out_rank,
+                  cudaStream_t st);
+template <typename T>
+void launch_h_compact(int nblk, const HBlockDev* blk, const double* Us, const double* Vs, const long long* du,
+                      const long long* dv, const int* rank, T* U, T* V, cudaStream_t st);
+// y (cluster order, FP64) = H u[boundary]; then b[node] = y[pos[node]] (0 off the boundary)
+template <typename T>
+void launch_h_matvec(const HMatView<T>& H, const double* u, double* y, double* t, T* xp, const int* pos, int n,
+                     double* bdir, cudaStream_t st);
 
 // Count of kernel launches issued by this library (all contexts), for benchmarking.
 long long launch_count();
 void note_launch();
+void note_launches(long long k);  // k kernels launched at once (a CUDA graph)
 
 inline int grid_for(long long n, int block = kBlock) {
   long long g = (n + block - 1) / block;
