@@ -120,6 +120,17 @@ int tmb_effective_field(tmb_ctx* ctx, const double* m, double* h, int ptr_kind);
 /* The CVODE right-hand side (TheLLG::rhs / rhs_d, main/TheLLG.cpp:670-711,
  * gpu/LLGWrapper.cu:213-228): ydot = -m x H - alpha m x (m x H).  t is reduced time. */
 int tmb_llg_rhs(tmb_ctx* ctx, double t, const double* y, double* ydot, int ptr_kind);
+/* tmb_llg_rhs for host vectors y and ydot (3N), without allocating device memory -- no
+ * counterpart in the reference.  For callers that cannot allocate on the device while they
+ * evaluate the right-hand side (a fixed device-memory budget, a loop that must not pay
+ * cudaMalloc's device-wide synchronisation, a stream under capture by other work).  y and
+ * ydot are staged through one file-scope device array of 2 x 3 x 65536 doubles (3 MiB, held by
+ * every GPU that loads the library until exit); meshes above 65536 nodes get TMB_ERR_ARG.
+ * The first call on a device resolves that array's device address (cudaGetSymbolAddress); make
+ * it before any stream capture.  Every call shares the array: calls that overlap on the GPU
+ * (other threads, other contexts on the same device) race, so serialise them.  Nothing in the
+ * array needs to start at zero: each call overwrites the 6N entries it uses.  Synchronises. */
+int tmb_llg_rhs_noalloc(tmb_ctx* ctx, double t, const double* y, double* ydot);
 /* TheLLG::getMaxTorque (main/TheLLG.cpp:426-439): mu0 * max_i |m_i x H_i| with the frozen demag.
  * Synchronises.  Returns TMB_ERR_NAN if the torque is not finite. */
 int tmb_max_torque(tmb_ctx* ctx, const double* m, double* out, int ptr_kind);

@@ -47,6 +47,7 @@ SIGNATURES = {
     "tmb_field_eval": [_P, _P, _P, _P, _int],
     "tmb_effective_field": [_P, _P, _P, _int],
     "tmb_llg_rhs": [_P, _dbl, _P, _P, _int],
+    "tmb_llg_rhs_noalloc": [_P, _dbl, _D, _D],
     "tmb_max_torque": [_P, _P, _D, _int],
     "tmb_normalize": [_P, _P, _int],
     "tmb_relax": [_P, _P, _dbl, _dbl, _dbl, _dbl, _D, _int],

@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -1298,6 +1299,86 @@ int tmb_llg_rhs(tmb_ctx* ctx, double t, const double* y, double* ydot, int ptr_k
     TMB_CUDA(cudaMemcpyAsync(ydot, c.out3.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     c.sync();
   }
+  TMB_API_END
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// Right-hand side for host vectors without any device allocation.
+//
+// Some callers cannot allocate device memory while they evaluate the right-hand side: a
+// host-side integrator called from inside a process that runs under a fixed device-memory
+// budget, a time-critical loop that must not pay cudaMalloc's implicit device-wide
+// synchronisation on its first call, or code running on a stream that other work is being
+// captured on.  tmb_llg_rhs with host pointers stages y and ydot through device buffers that
+// it allocates on first use; this variant stages them through one file-scope device array of
+// fixed size instead.  That array (2 x 3 x 65536 doubles, 3 MiB) is held by every GPU that
+// loads the library, until the process exits.
+// ------------------------------------------------------------------------------------------
+namespace tmb {
+
+constexpr int kNoAllocMaxNodes = 65536;
+constexpr int kNoAllocMaxDevices = 64;
+static __device__ __align__(256) double g_rhs_staging[2 * 3 * kNoAllocMaxNodes];
+static std::mutex g_staging_mutex;
+static double* g_staging_address[kNoAllocMaxDevices] = {};
+
+// Device address of g_rhs_staging on `device`, which must be the current device.  The
+// host-side name of the array is only a stand-in: kernels must be given this address.
+static double* staging_address(int device) {
+  std::lock_guard<std::mutex> lock(g_staging_mutex);
+  if (!g_staging_address[device]) {
+    void* p = nullptr;
+    TMB_CUDA(cudaGetSymbolAddress(&p, g_rhs_staging));
+    g_staging_address[device] = static_cast<double*>(p);
+  }
+  return g_staging_address[device];
+}
+
+}  // namespace tmb
+
+extern "C" {
+
+int tmb_llg_rhs_noalloc(tmb_ctx* ctx, double t, const double* y, double* ydot) {
+  (void)t;  // the frozen-demag right-hand side does not depend on t explicitly
+  TMB_CHECK_ARG(ctx && y && ydot, "tmb_llg_rhs_noalloc: null argument");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  c.require_mesh();
+  c.require_material();
+  if (c.n > kNoAllocMaxNodes)
+    return fail(TMB_ERR_ARG, "tmb_llg_rhs_noalloc: the mesh has " + std::to_string(c.n) +
+                                 " nodes; its static staging array holds at most " +
+                                 std::to_string(kNoAllocMaxNodes) + " (use tmb_llg_rhs)");
+  if (c.device < 0 || c.device >= kNoAllocMaxDevices)
+    return fail(TMB_ERR_ARG, "tmb_llg_rhs_noalloc: device ordinal beyond the supported range");
+  TMB_CUDA(cudaSetDevice(c.device));
+  double* const stage = staging_address(c.device);
+  double* const yd = stage;                          // y, 3N
+  double* const od = stage + 3 * kNoAllocMaxNodes;   // ydot, 3N
+  const size_t n3 = size_t(3) * c.n;
+  TMB_CUDA(cudaMemcpyAsync(yd, y, n3 * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+  LocalFieldArgs a;
+  a.n = c.n;
+  a.m = yd;
+  a.hfix = c.hfix.p;
+  a.xc = c.xc.p;
+  a.ku2 = c.has_uni ? c.ku2.p : nullptr;
+  a.kax = c.kax.p;
+  a.dmi_s = c.has_dmi ? c.dmi_s.p : nullptr;
+  a.area = c.area.p;
+  a.nvn = c.nvn.p;
+  a.alpha = c.alpha;
+  a.precession = c.precession;
+  a.ydot = od;
+  a.hout = nullptr;
+  a.torque_bits = nullptr;
+  const SellView S = c.pat.view();
+  if (c.precision == TMB_FP64) launch_local_field<double>(S, c.K.p, c.tg[0].p, c.tg[1].p, c.tg[2].p, a, c.stream);
+  else launch_local_field<float>(S, c.Kf.p, c.tgf[0].p, c.tgf[1].p, c.tgf[2].p, a, c.stream);
+  TMB_CUDA(cudaMemcpyAsync(ydot, od, n3 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  c.sync();
   TMB_API_END
 }
 
