@@ -47,6 +47,8 @@ def parse():
     p.add_argument("--tol", type=float, default=1e-7)
     p.add_argument("--sim-ps", type=float, default=2.0, help="simulated ps for the ns/hour figure")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--bem", default="dense", choices=["hmatrix", "dense"],
+                   help="BEM form of the timed paths (the dense FP64 path is always measured too)")
     return p.parse_args()
 
 
@@ -191,7 +193,10 @@ def run_gpu(args):
 
     w = make_workload(args.workload, rank)
     t0 = time.perf_counter()
-    mo, ctx = workloads.setup_context(w, device=local, mixed=True, tol=args.tol, maxiter=100)
+    hier = args.bem == "hmatrix"
+    mo, ctx = workloads.setup_context(w, device=local, mixed=True, tol=args.tol, maxiter=100, hmatrix=hier,
+                                      keep_dense=True)
+    bem_info = ctx.bem_info() if hier else None
     setup_s = time.perf_counter() - t0
     # one non-default stream for the library's kernels and the timing events
     stream = torch.cuda.Stream(dev)
@@ -224,8 +229,10 @@ def run_gpu(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    def timed(mixed: bool, profile: bool):
+    def timed(mixed: bool, profile: bool, dense: bool = False):
         ctx.set_precision(mixed)
+        if hier:
+            ctx.set_bem_mode(not dense)
         for k in range(W):
             ctx.field_eval(S[k], ydot, hdem)
         torch.cuda.synchronize(dev)
@@ -236,6 +243,8 @@ def run_gpu(args):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         l0 = api.kernel_launches()
         its = [0, 0]
+        tag = f"timed_{'mixed' if mixed else 'fp64'}{'_dense' if dense else ''}{'_prof' if profile else ''}"
+        torch.cuda.nvtx.range_push(tag)
         e0.record(stream)
         for k in range(K):
             ctx.field_eval(S[W + k], ydot, hdem)
@@ -244,6 +253,7 @@ def run_gpu(args):
             its[1] += st["it_dirichlet"]
         e1.record(stream)
         torch.cuda.synchronize(dev)
+        torch.cuda.nvtx.range_pop()
         barrier()
         ms = e0.elapsed_time(e1)
         launches = api.kernel_launches() - l0
@@ -257,23 +267,35 @@ def run_gpu(args):
     ms_mx, launches, _, its_mx = timed(True, False)
     clk = clocks.stop()
     ms_64, _, _, its_64 = timed(False, False)
+    ms_64d = timed(False, False, dense=True)[0] if hier else ms_64
     # per-kernel CUDA-event timing in a separate pass over the same K states (with the
     # profiler on, the PCG runs kernel by kernel instead of from CUDA graphs)
     _, _, prof, _ = timed(True, True)
 
     # relative error of the mixed path against the FP64 path, on one state
+    # reference: plain FP64 with the dense BEM, solved to 1e-12
     probe = S[W + K - 1]
     ctx.set_precision(False)
+    if hier:
+        ctx.set_bem_mode(False)
     ctx.set_solver_params(1e-12, 300)
     h64 = hdem.clone()
     y64 = ctx.field_eval(probe, torch.empty_like(ydot), h64)
+    if hier:
+        ctx.set_bem_mode(True)
+    h64h = hdem.clone()
+    y64h = ctx.field_eval(probe, torch.empty_like(ydot), h64h)
     ctx.set_precision(True)
     ctx.set_solver_params(args.tol, 100)
     hmx = hdem.clone()
     ymx = ctx.field_eval(probe, torch.empty_like(ydot), hmx)
     torch.cuda.synchronize(dev)
-    err_h = float(torch.linalg.norm(hmx - h64) / torch.linalg.norm(h64))
-    err_y = float(torch.linalg.norm(ymx - y64) / torch.linalg.norm(y64))
+
+    def relerr(a, b):
+        return float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+
+    err_h, err_y = relerr(hmx, h64), relerr(ymx, y64)
+    err_h64, err_y64 = relerr(h64h, h64), relerr(y64h, y64)
 
     # local right-hand side only (frozen demag), mixed
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -325,7 +347,10 @@ def run_gpu(args):
         "ms_per_step": ms_mx / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 operators / f64 vectors+reductions", "data": "synthetic",
         "config": {"workload": w.name, "nodes": n, "boundary_nodes": mo.nb, "nnz": mo.nnz,
-                   "bem": "dense, device-assembled, FP32 on the mixed path", "precision": "mixed",
+                   "bem": ("hierarchical (leaf 32, eta 2, ACA: FP32 terms to 1e-6 on the mixed path, FP64 "
+                           "terms to 1e-7 on the plain path), compressed from the device-assembled dense "
+                           "matrix" if hier else "dense, device-assembled, FP32 on the mixed path"),
+                   "precision": "mixed",
                    "cg_tol": args.tol, "states": "W+K distinct seeded perturbed states, warm-started solves",
                    "l2": "inputs larger than L2 (dense BEM alone is 4*Nb^2 bytes)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single"},
@@ -337,7 +362,10 @@ def run_gpu(args):
                      "bytes_per_launch": d["bytes_per_launch"], "avg_ms": avg_ms},
         "clocks": clk,
         "fp64_value": fp64_value, "speedup_vs_fp64": value / fp64_value,
-        "rel_err_vs_fp64": {"hdem": err_h, "ydot": err_y},
+        "fp64_dense_value": world * K / (ms_64d / 1e3), "speedup_vs_fp64_dense": ms_64d / ms_mx,
+        "rel_err_vs_fp64": {"hdem": err_h, "ydot": err_y, "reference": "FP64, dense BEM, CG to 1e-12"},
+        "rel_err_fp64_hier_vs_dense": {"hdem": err_h64, "ydot": err_y64},
+        "bem_info": bem_info,
         "local_rhs_evals_per_s": world * local_per_s,
         "sim_ns_per_hour": ns_per_hour,
         "relax": {"sim_ps": args.sim_ps, "wall_s": sim_s, "steps": rs["accepted"], "rejected": rs["rejected"],

@@ -93,6 +93,23 @@ int tmb_bem_assemble(tmb_ctx* ctx, const tmb_mesh* mesh);
 int tmb_set_bem_dense(tmb_ctx* ctx, int nb, const double* B_colmajor);
 int tmb_get_bem_dense(tmb_ctx* ctx, double* B_colmajor);
 
+/* Hierarchical compression of the dense matrix (replaces H2Lib's setupH2MatrixC /
+ * H2_mvp_sub, main/h2interface.c:77-95, 373-399): cluster tree over bxyz (Nb x 3, boundary
+ * order) with leaf size `leaf` (<= 32; tetmag uses clf = 32), admissibility
+ * min(diam) <= eta * dist (tetmag: eta = 2), dense leaf tiles and adaptive-cross-approximation
+ * low-rank blocks: FP32 terms to eps_mixed for the mixed path, FP64 terms to eps_fp64 for the
+ * plain path (at most kmax terms per block).  bnormal (Nb x 3 node normals, may be NULL) lets
+ * the cluster tree separate faces of different orientation first, so that every low-rank block
+ * couples one smooth piece of surface to another.  Needs the dense FP64 matrix on the device
+ * (tmb_bem_assemble / tmb_set_bem_dense); keep_dense = 0 releases it afterwards.  The demag
+ * chain then uses the hierarchical matvec (tmb_set_bem_mode switches back). */
+int tmb_bem_compress(tmb_ctx* ctx, const double* bxyz, const double* bnormal, int leaf, double eta,
+                     double eps_mixed, double eps_fp64, int kmax, int keep_dense);
+int tmb_set_bem_mode(tmb_ctx* ctx, int mode);  /* 0 dense, 1 hierarchical */
+/* out[0..11]: mode, dense tiles, low-rank blocks, FP64 terms, FP32 terms, FP64 bytes, FP32 bytes,
+ * dense entries (Nb^2), blocks at the rank cap, max FP64 rank, compression ms, built flag */
+int tmb_bem_info(tmb_ctx* ctx, double* out);
+
 /* Material per node (SimulationData, specs/SimulationData.cpp:125-163): Js [T], A [J/m]
  * already divided by scale^2, Ku [J/m^3], ku_axis 3N SoA, D [J/m^2] already divided by
  * scale (bulk DMI, main/EffFieldCalc.cpp:159-170).  Ku, ku_axis, D may be NULL. */

@@ -218,3 +218,35 @@ def test_full_size_c4_properties():
     ctx.set_solver_params(1e-9, 200)
     Hmx = ctx.demag_field(m)
     assert rel(Hmx, H64) <= MIXED_TOL
+
+
+def test_hierarchical_bem_matches_dense_c4():
+    # 7002 boundary nodes: leaf 32, eta 2; FP64 terms to 1e-7, FP32 terms to 1e-6.  On this film
+    # the admissible blocks pairing top+bottom-face clusters need the ACA residual check.
+    w = workloads.c4_replica(replica=1)
+    mo, ctx = workloads.setup_context(w, tol=1e-12, maxiter=300, hmatrix=True, keep_dense=True)
+    info = ctx.bem_info()
+    assert info["built"] == 1 and info["mode"] == 1
+    assert info["bytes_fp32"] < 0.5 * 4 * info["dense_entries"]
+    m = w.m0
+    ctx.set_bem_mode(False)
+    H_dense = ctx.demag_field(m)
+    ctx.set_bem_mode(True)
+    H_h64 = ctx.demag_field(m)
+    assert rel(H_h64, H_dense) <= 1e-6
+    ctx.set_precision(True)
+    ctx.set_solver_params(1e-9, 300)
+    H_h32 = ctx.demag_field(m)
+    assert rel(H_h32, H_dense) <= MIXED_TOL
+
+
+def test_hierarchical_bem_c1_against_oracle(c1):
+    w, mo, ctx, pb, dem = c1
+    ctx2 = workloads.setup_context(w, tol=1e-12, maxiter=300, hmatrix=True, keep_dense=False, mesh_ops=mo)[1]
+    assert ctx2.bem_info()["built"] == 1
+    m = meshgen.random_state(w.n, 17)
+    Ho = O.rows_to_soa(dem.field(O.soa_to_rows(m)))
+    assert rel(ctx2.demag_field(m), Ho) <= 1e-6
+    ctx2.set_precision(True)
+    ctx2.set_solver_params(1e-9, 300)
+    assert rel(ctx2.demag_field(m), Ho) <= MIXED_TOL

@@ -38,6 +38,9 @@ SIGNATURES = {
     "tmb_bem_assemble": [_P, _P],
     "tmb_set_bem_dense": [_P, _int, _D],
     "tmb_get_bem_dense": [_P, _D],
+    "tmb_bem_compress": [_P, _D, _D, _int, _dbl, _dbl, _dbl, _int, _int],
+    "tmb_set_bem_mode": [_P, _int],
+    "tmb_bem_info": [_P, _D],
     "tmb_set_material": [_P, _D, _D, _D, _D, _D, _dbl],
     "tmb_set_applied_field": [_P, _P, _int],
     "tmb_set_llg_options": [_P, _int],

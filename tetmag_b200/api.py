@@ -147,6 +147,27 @@ class Context:
         check(lib().tmb_get_bem_dense(self.h, B.ctypes.data_as(C.POINTER(C.c_double))))
         return B
 
+    def bem_compress(self, bxyz, bnormal=None, leaf=32, eta=2.0, eps_mixed=1e-6, eps_fp64=1e-7, kmax=64,
+                     keep_dense=True):
+        """Hierarchical BEM (cluster tree + ACA) from the device-assembled dense matrix."""
+        b = _f64(bxyz).reshape(-1, 3)
+        nrm = None if bnormal is None else _f64(bnormal).reshape(-1, 3)
+        check(lib().tmb_bem_compress(self.h, _dptr(b), _dptr(nrm) if nrm is not None else None, int(leaf),
+                                     float(eta), float(eps_mixed), float(eps_fp64), int(kmax),
+                                     1 if keep_dense else 0))
+        return self
+
+    def set_bem_mode(self, hierarchical: bool):
+        check(lib().tmb_set_bem_mode(self.h, 1 if hierarchical else 0))
+        return self
+
+    def bem_info(self) -> dict:
+        st = (C.c_double * 12)()
+        check(lib().tmb_bem_info(self.h, st))
+        keys = ["mode", "dense_tiles", "lowrank_blocks", "terms_fp64", "terms_fp32", "bytes_fp64", "bytes_fp32",
+                "dense_entries", "blocks_at_cap", "max_rank_fp64", "compress_ms", "built"]
+        return {k: st[i] for i, k in enumerate(keys)}
+
     def set_material(self, Js, A, Ku=None, ku_axis=None, D=None, alpha=1.0):
         n = self.n
         js, a = _f64(np.broadcast_to(Js, (n,))), _f64(np.broadcast_to(A, (n,)))

@@ -83,25 +83,55 @@ __global__ void k_h_near_gather(const HBlockDev* __restrict__ blk, const double*
   }
 }
 
-// Adaptive cross approximation of one admissible block per CTA.
+// Largest residual |A_ij - sum_l U_il V_lj| over unvisited rows (a strided sample of about
+// 128 rows on larger blocks); CTA-wide, every thread receives value and row.
+__device__ void aca_verify(const HBlockDev& b, const double* __restrict__ B, size_t ld, const int* __restrict__ perm,
+                           const double* U, const double* V, const unsigned char* usd, int k, int pass, double* shv,
+                           int* shi, double& val, int& row) {
+  const int m = b.m, n = b.n;
+  const int stride = (m > 128) ? (m + 127) / 128 : 1;
+  const int offset = pass % stride;
+  const int nrows = (m - offset + stride - 1) / stride;
+  double best = 0.0;
+  int bi = 0x7fffffff;
+  for (long long t = threadIdx.x; t < (long long)nrows * n; t += blockDim.x) {
+    const int i = offset + int(t / n) * stride;
+    const int j = int(t % n);
+    if (usd[i]) continue;
+    double r = entry(B, ld, perm, b.rb + i, b.cb + j);
+    for (int l = 0; l < k; ++l) r -= U[size_t(l) * m + i] * V[size_t(l) * n + j];
+    if (fabs(r) > best || (fabs(r) == best && i < bi)) {
+      best = fabs(r);
+      bi = i;
+    }
+  }
+  cta_argmax(best, bi, shv, shi, val, row);
+}
+
+// Adaptive cross approximation of one admissible block per CTA.  Partial pivoting can miss
+// parts of a block whose rows couple to disjoint column sets (on a film, top-face rows see
+// only bottom-face columns and vice versa), so each time the loose tolerance is reached the
+// residual is checked on the unvisited rows, and the approximation restarts from the worst
+// one if it is significant; the same check guards the final (tight) stop.
 __global__ void __launch_bounds__(256) k_h_aca(const HBlockDev* __restrict__ blk, const double* __restrict__ B,
                                                size_t ld, const int* __restrict__ perm, double* __restrict__ Us,
                                                double* __restrict__ Vs, unsigned char* __restrict__ used, int kmax,
                                                double eps_tight, double eps_loose, int* __restrict__ out_rank) {
+  constexpr int kMaxPasses = 8;
   __shared__ double shv[32];
   __shared__ int shi[32];
   __shared__ double shd[32];
-  const int bidx = blockIdx.x;
-  const HBlockDev b = blk[bidx];
+  const HBlockDev b = blk[blockIdx.x];
   const int m = b.m, n = b.n;
   double* U = Us + b.uoff;  // kmax columns of length m
   double* V = Vs + b.voff;  // kmax columns of length n
   unsigned char* usd = used + b.used_off;
   for (int i = threadIdx.x; i < m; i += blockDim.x) usd[i] = 0;
   __syncthreads();
-  int k = 0, k_loose = -1, k_tight = -1, checks = 0, status = 0, istar = 0;
+  int k = 0, k_loose = -1, k_tight = -1, status = 0, istar = 0, passes = 0;
+  bool verified = false;
   double norm2 = 0.0;
-  // next unvisited row after `from` (cyclic), -1 if every row was visited
+  // first unvisited row after `from` (cyclic), -1 if every row was visited
   auto next_unvisited = [&](int from) {
     for (int q = 1; q <= m; ++q)
       if (!usd[(from + q) % m]) return (from + q) % m;
@@ -130,72 +160,78 @@ __global__ void __launch_bounds__(256) k_h_aca(const HBlockDev* __restrict__ blk
     cta_argmax(lb, lj, shv, shi, piv_abs, jstar);
     if (threadIdx.x == 0) usd[istar] = 1;
     __syncthreads();
-    const double scale = (k > 0) ? sqrt(fabs(norm2) / (double(m) * n)) : 0.0;
-    if (piv_abs == 0.0 || piv_abs <= 1e-14 * scale) {
-      // nothing left in this row
-      int nxt;
-      if (k_tight >= 0) {  // converged: this was a verification row
-        if (++checks > 6) break;
-        nxt = next_unvisited(int((unsigned(bidx) * 2654435761u + unsigned(checks) * 40503u) % unsigned(m)));
+    const double rms = (k > 0) ? sqrt(fabs(norm2) / (double(m) * n)) : 0.0;
+    int nxt = -1;
+    bool converged = k_tight >= 0;
+    if (piv_abs == 0.0 || piv_abs <= 1e-14 * rms) {
+      if (!converged) nxt = next_unvisited(istar);  // nothing left in this row
+    } else {
+      const double piv = v[jstar];
+      __syncthreads();
+      for (int j = threadIdx.x; j < n; j += blockDim.x) v[j] /= piv;
+      __syncthreads();
+      // residual of column jstar -> U[:, k]
+      double* u = U + size_t(k) * m;
+      double li_best = 0.0, uu_part = 0.0, vv_part = 0.0;
+      int li = 0x7fffffff;
+      for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        double c = entry(B, ld, perm, b.rb + i, b.cb + jstar);
+        for (int l = 0; l < k; ++l) c -= V[size_t(l) * n + jstar] * U[size_t(l) * m + i];
+        u[i] = c;
+        uu_part += c * c;
+        if (!usd[i] && (fabs(c) > li_best || (fabs(c) == li_best && i < li))) {
+          li_best = fabs(c);
+          li = i;
+        }
+      }
+      for (int j = threadIdx.x; j < n; j += blockDim.x) vv_part += v[j] * v[j];
+      const double uu = cta_sum(uu_part, shd);
+      const double vv = cta_sum(vv_part, shd);
+      double cross = 0.0;
+      for (int l = 0; l < k; ++l) {
+        double pu = 0.0, pv = 0.0;
+        for (int i = threadIdx.x; i < m; i += blockDim.x) pu += u[i] * U[size_t(l) * m + i];
+        for (int j = threadIdx.x; j < n; j += blockDim.x) pv += v[j] * V[size_t(l) * n + j];
+        cross += cta_sum(pu, shd) * cta_sum(pv, shd);
+      }
+      norm2 += uu * vv + 2.0 * cross;
+      ++k;
+      const double term = sqrt(uu * vv), fro = sqrt(fabs(norm2));
+      if (term <= eps_tight * fro) {
+        if (k_tight < 0) k_tight = k;
       } else {
-        nxt = next_unvisited(istar);
+        k_tight = -1;
       }
-      if (nxt < 0) break;
-      istar = nxt;
-      continue;
-    }
-    const double piv = v[jstar];
-    __syncthreads();
-    for (int j = threadIdx.x; j < n; j += blockDim.x) v[j] /= piv;
-    __syncthreads();
-    // residual of column jstar -> U[:, k]
-    double* u = U + size_t(k) * m;
-    double li_best = 0.0, uu_part = 0.0, vv_part = 0.0;
-    int li = 0x7fffffff;
-    for (int i = threadIdx.x; i < m; i += blockDim.x) {
-      double c = entry(B, ld, perm, b.rb + i, b.cb + jstar);
-      for (int l = 0; l < k; ++l) c -= V[size_t(l) * n + jstar] * U[size_t(l) * m + i];
-      u[i] = c;
-      uu_part += c * c;
-      if (!usd[i] && (fabs(c) > li_best || (fabs(c) == li_best && i < li))) {
-        li_best = fabs(c);
-        li = i;
+      if (term <= eps_loose * fro) {
+        if (k_loose < 0) k_loose = k;
+      } else {
+        k_loose = -1;
+        verified = false;
       }
+      converged = k_tight >= 0;
+      double best;
+      int inext;
+      cta_argmax(li_best, li, shv, shi, best, inext);
+      if (k_loose >= 0 && !verified && passes < kMaxPasses) {
+        double val;
+        int row;
+        aca_verify(b, B, ld, perm, U, V, usd, k, passes++, shv, shi, val, row);
+        if (row != 0x7fffffff && val > eps_loose * sqrt(fabs(norm2) / (double(m) * n))) {
+          k_loose = k_tight = -1;  // a part of the block is still missing: restart there
+          istar = row;
+          continue;
+        }
+        verified = true;
+      }
+      if (!converged) nxt = (inext != 0x7fffffff && best > 0.0) ? inext : next_unvisited(istar);
     }
-    for (int j = threadIdx.x; j < n; j += blockDim.x) vv_part += v[j] * v[j];
-    const double uu = cta_sum(uu_part, shd);
-    const double vv = cta_sum(vv_part, shd);
-    double cross = 0.0;
-    for (int l = 0; l < k; ++l) {
-      double pu = 0.0, pv = 0.0;
-      for (int i = threadIdx.x; i < m; i += blockDim.x) pu += u[i] * U[size_t(l) * m + i];
-      for (int j = threadIdx.x; j < n; j += blockDim.x) pv += v[j] * V[size_t(l) * n + j];
-      cross += cta_sum(pu, shd) * cta_sum(pv, shd);
-    }
-    norm2 += uu * vv + 2.0 * cross;
-    ++k;
-    const double term = sqrt(uu * vv), fro = sqrt(fabs(norm2));
-    if (term <= eps_tight * fro) {
-      if (k_tight < 0) k_tight = k;
-    } else {
-      k_tight = -1;  // (re)opened by this term
-    }
-    if (term <= eps_loose * fro) {
-      if (k_loose < 0) k_loose = k;
-    } else {
-      k_loose = -1;
-    }
-    double best;
-    int inext;
-    cta_argmax(li_best, li, shv, shi, best, inext);
-    int nxt;
-    if (k_tight >= 0) {  // converged: verify on a few unvisited rows before stopping
-      if (++checks > 6) break;
-      nxt = next_unvisited(int((unsigned(bidx) * 2654435761u + unsigned(checks) * 40503u) % unsigned(m)));
-    } else if (inext != 0x7fffffff && best > 0.0) {
-      nxt = inext;
-    } else {
-      nxt = next_unvisited(istar);
+    if (converged && nxt < 0) {
+      if (passes >= kMaxPasses) break;
+      double val;
+      int row;
+      aca_verify(b, B, ld, perm, U, V, usd, k, passes++, shv, shi, val, row);
+      if (row == 0x7fffffff || val <= eps_tight * sqrt(fabs(norm2) / (double(m) * n))) break;
+      nxt = row;
     }
     if (nxt < 0) break;
     istar = nxt;
@@ -203,9 +239,9 @@ __global__ void __launch_bounds__(256) k_h_aca(const HBlockDev* __restrict__ blk
   if (threadIdx.x == 0) {
     if (k_tight < 0) k_tight = k;
     if (k_loose < 0 || k_loose > k_tight) k_loose = k_tight;
-    out_rank[3 * bidx] = k_tight;
-    out_rank[3 * bidx + 1] = k_loose;
-    out_rank[3 * bidx + 2] = status;
+    out_rank[3 * blockIdx.x] = k_tight;
+    out_rank[3 * blockIdx.x + 1] = k_loose;
+    out_rank[3 * blockIdx.x + 2] = status;
   }
 }
 

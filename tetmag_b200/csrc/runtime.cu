@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -322,6 +323,30 @@ struct Ctx {
   DevArray<double> Bd;
   DevArray<float> Bf;
   bool has_bem = false;
+  // hierarchical BEM (tmb_bem_compress)
+  struct HMat {
+    bool built = false;
+    int nnear = 0, nfar = 0, nrows = 0, ngroups = 0, max_group_m = 0, failed = 0;
+    long long terms[2] = {0, 0};          // [0] FP64 (tight), [1] FP32 (loose)
+    double bytes[2] = {0, 0}, ms = 0.0;
+    int max_rank = 0;
+    DevArray<int> gidx, pos;
+    DevArray<HBlockDev> nearb, farb;
+    DevArray<HNearRow> rows;
+    DevArray<HFarGroup> groups;
+    DevArray<double> D64, U64, V64, t64, y, xp64;
+    DevArray<float> D32, U32, V32, xp32;
+    DevArray<int> rank[2];
+    DevArray<long long> uoff[2], voff[2], toff[2];
+    DevArray<int2> term[2];
+    DevArray<double> t32;
+  } H;
+  int bem_mode = 0;  // 0 dense, 1 hierarchical
+  void h_compress(const double* bxyz, const double* bnrm, int leaf, double eta, double eps_mixed, double eps_fp64,
+                  int kmax,
+                  bool keep_dense);
+  template <typename T>
+  HMatView<T> h_view(int which) const;
   // demag
   std::unique_ptr<Solver> neu, dir;
   double tol = 1e-7;
@@ -626,6 +651,8 @@ void Ctx::set_operators(int nx, const int* ptr, const int* col, const double* K_
   }
   has_material = false;
   has_bem = false;
+  H = HMat{};
+  bem_mode = 0;
   neu.reset();
   dir.reset();
   sync();
@@ -726,13 +753,22 @@ void Ctx::demag(const double* m) {
   prof.begin(4, st, 0.0);
   neu->solve(rhs.p, precision);
   prof.end(st);
-  if (f64) launch_gather<double>(nb, neu->x.p, bnodes.p, u1b.p, st);
-  else launch_gather<float>(nb, neu->x.p, bnodes.p, u1bf.p, st);
-  prof.begin(3, st, B * B * sv + B * (sv + 8));
-  if (f64) launch_bem_gemv<double>(nb, Bd.p, u1b.p, u2b.p, st);
-  else launch_bem_gemv<float>(nb, Bf.p, u1bf.p, u2b.p, st);
-  prof.end(st);
-  launch_dirichlet_values(n, bindex.p, u2b.p, bdir.p, st);
+  if (bem_mode == 1) {
+    // hierarchical matvec in cluster order, scattered straight into the Dirichlet load
+    const int w = f64 ? 0 : 1;
+    prof.begin(3, st, H.bytes[w] + B * (sv + 8 + 8));
+    if (f64) launch_h_matvec<double>(h_view<double>(0), neu->x.p, H.y.p, H.t64.p, H.xp64.p, H.pos.p, n, bdir.p, st);
+    else launch_h_matvec<float>(h_view<float>(1), neu->x.p, H.y.p, H.t32.p, H.xp32.p, H.pos.p, n, bdir.p, st);
+    prof.end(st);
+  } else {
+    if (f64) launch_gather<double>(nb, neu->x.p, bnodes.p, u1b.p, st);
+    else launch_gather<float>(nb, neu->x.p, bnodes.p, u1bf.p, st);
+    prof.begin(3, st, B * B * sv + B * (sv + 8));
+    if (f64) launch_bem_gemv<double>(nb, Bd.p, u1b.p, u2b.p, st);
+    else launch_bem_gemv<float>(nb, Bf.p, u1bf.p, u2b.p, st);
+    prof.end(st);
+    launch_dirichlet_values(n, bindex.p, u2b.p, bdir.p, st);
+  }
   prof.begin(5, st, 0.0);
   dir->solve(bdir.p, precision);
   prof.end(st);
@@ -745,6 +781,183 @@ void Ctx::demag(const double* m) {
   if (neu->last_status == 5 || dir->last_status == 5) throw Error(TMB_ERR_NAN, "demag solve broke down (NaN)");
   if (neu->last_status == 3 || dir->last_status == 3)
     throw Error(TMB_ERR_NOCONVERGE, "demag solve did not converge within maxiter");
+}
+
+template <typename T>
+HMatView<T> Ctx::h_view(int w) const {
+  HMatView<T> v;
+  v.nb = nb;
+  v.nrows = H.nrows;
+  v.ngroups = H.ngroups;
+  v.max_group_m = H.max_group_m;
+  v.nterms = H.terms[w];
+  v.gidx = H.gidx.p;
+  v.near_rows = H.rows.p;
+  v.near = H.nearb.p;
+  v.far = H.farb.p;
+  v.rank = H.rank[w].p;
+  v.uoff = H.uoff[w].p;
+  v.voff = H.voff[w].p;
+  v.toff = H.toff[w].p;
+  v.terms = H.term[w].p;
+  v.groups = H.groups.p;
+  if constexpr (sizeof(T) == 8) {
+    v.D = H.D64.p;
+    v.U = H.U64.p;
+    v.V = H.V64.p;
+  } else {
+    v.D = H.D32.p;
+    v.U = H.U32.p;
+    v.V = H.V32.p;
+  }
+  return v;
+}
+
+// Compresses the device-assembled dense FP64 BEM matrix into the hierarchical form:
+// dense leaf tiles plus ACA low-rank blocks, FP64 terms to eps_fp64 and FP32 terms to eps_mixed.
+void Ctx::h_compress(const double* bxyz, const double* bnrm, int leaf, double eta, double eps_mixed,
+                     double eps_fp64, int kmax, bool keep_dense) {
+  require_mesh();
+  if (!has_bem || !Bd.p) throw Error(TMB_ERR_STATE, "tmb_bem_compress: needs the dense FP64 BEM matrix on the device");
+  if (leaf < 2 || leaf > 32) throw Error(TMB_ERR_ARG, "tmb_bem_compress: leaf size must be in [2, 32]");
+  if (!(eta > 0.0) || !(eps_mixed > 0.0) || !(eps_fp64 > 0.0) || kmax < 1)
+    throw Error(TMB_ERR_ARG, "tmb_bem_compress: bad eta / tolerance / rank cap");
+  const auto t0 = std::chrono::steady_clock::now();
+  cudaStream_t st = stream;
+  HPartition P;
+  // admissible blocks above 1024 rows or columns are subdivided: bounds the ACA work per CTA
+  h_partition(bxyz, bnrm, nb, leaf, eta, 1024, P);
+  // dense leaf tiles, grouped by leaf row cluster
+  std::vector<HBlockDev> nearb;
+  std::vector<HNearRow> rows;
+  long long doff = 0;
+  for (size_t q = 0; q < P.near.size(); ++q) {
+    const HCluster& ct = P.clusters[P.near[q].first];
+    const HCluster& cs = P.clusters[P.near[q].second];
+    HBlockDev b{ct.begin, ct.end - ct.begin, cs.begin, cs.end - cs.begin, doff, 0, 0, 0};
+    doff += (long long)b.m * b.n;
+    if (rows.empty() || rows.back().rb != b.rb) rows.push_back(HNearRow{b.rb, b.m, int(q), int(q) + 1});
+    else rows.back().last = int(q) + 1;
+    nearb.push_back(b);
+  }
+  long long covered = 0;
+  for (const auto& r : rows) covered += r.m;
+  if (covered != nb) throw Error(TMB_ERR_INTERNAL, "H-matrix: leaf rows do not cover the boundary");
+  // admissible blocks with ACA scratch offsets, grouped by row cluster
+  std::vector<HBlockDev> farb;
+  std::vector<HFarGroup> groups;
+  long long us = 0, vs = 0, fl = 0;
+  int last_cluster = -1;
+  for (size_t q = 0; q < P.far.size(); ++q) {
+    const HCluster& ct = P.clusters[P.far[q].first];
+    const HCluster& cs = P.clusters[P.far[q].second];
+    HBlockDev b{ct.begin, ct.end - ct.begin, cs.begin, cs.end - cs.begin, 0, us, vs, fl};
+    us += (long long)kmax * b.m;
+    vs += (long long)kmax * b.n;
+    fl += b.m;
+    if (P.far[q].first != last_cluster) {
+      groups.push_back(HFarGroup{b.rb, b.m, int(q), int(q) + 1});
+      last_cluster = P.far[q].first;
+    } else {
+      groups.back().last = int(q) + 1;
+    }
+    farb.push_back(b);
+  }
+  if (groups.size() > 65535) throw Error(TMB_ERR_ARG, "tmb_bem_compress: too many row clusters for one launch");
+  H = HMat{};
+  H.nnear = int(nearb.size());
+  H.nfar = int(farb.size());
+  H.nrows = int(rows.size());
+  H.ngroups = int(groups.size());
+  for (const auto& g : groups) H.max_group_m = std::max(H.max_group_m, g.m);
+  std::vector<int> gidx(nb), pos(n, -1);
+  for (int i = 0; i < nb; ++i) {
+    gidx[i] = hbnodes[P.perm[i]];
+    pos[gidx[i]] = i;
+  }
+  H.gidx.upload(gidx, st);
+  H.pos.upload(pos, st);
+  DevArray<int> dperm;
+  dperm.upload(P.perm, st);
+  H.nearb.upload(nearb, st);
+  H.rows.upload(rows, st);
+  H.farb.upload(farb, st);
+  H.groups.upload(groups, st);
+  const size_t ld = bem_ld(nb);
+  H.D64.alloc(size_t(doff));
+  H.D32.alloc(size_t(doff));
+  launch_h_near_gather(H.nnear, H.nearb.p, Bd.p, ld, dperm.p, H.D64.p, H.D32.p, st);
+  // adaptive cross approximation of every admissible block
+  std::vector<int> ranks(size_t(3) * H.nfar, 0);
+  if (H.nfar > 0) {
+    DevArray<double> Us, Vs;
+    DevArray<unsigned char> used;
+    DevArray<int> dr;
+    Us.alloc(size_t(us));
+    Vs.alloc(size_t(vs));
+    used.alloc(size_t(fl));
+    dr.alloc(size_t(3) * H.nfar);
+    launch_h_aca(H.nfar, H.farb.p, Bd.p, ld, dperm.p, Us.p, Vs.p, used.p, kmax, eps_fp64, eps_mixed, dr.p, st);
+    TMB_CUDA(cudaMemcpyAsync(ranks.data(), dr.p, sizeof(int) * ranks.size(), cudaMemcpyDeviceToHost, st));
+    sync();
+    for (int w = 0; w < 2; ++w) {
+      std::vector<int> rk(H.nfar);
+      std::vector<long long> uo(H.nfar), vo(H.nfar), to(H.nfar);
+      std::vector<int2> terms;
+      long long su = 0, sv = 0, stt = 0;
+      for (int q = 0; q < H.nfar; ++q) {
+        rk[q] = ranks[size_t(3) * q + w];
+        uo[q] = su;
+        vo[q] = sv;
+        to[q] = stt;
+        su += (long long)rk[q] * farb[q].m;
+        sv += (long long)rk[q] * farb[q].n;
+        stt += rk[q];
+        for (int l = 0; l < rk[q]; ++l) terms.push_back(make_int2(q, l));
+      }
+      H.terms[w] = stt;
+      H.rank[w].upload(rk, st);
+      H.uoff[w].upload(uo, st);
+      H.voff[w].upload(vo, st);
+      H.toff[w].upload(to, st);
+      H.term[w].upload(terms, st);
+      if (w == 0) {
+        H.U64.alloc(size_t(std::max(su, 1LL)));
+        H.V64.alloc(size_t(std::max(sv, 1LL)));
+        H.t64.alloc(size_t(std::max(stt, 1LL)));
+        launch_h_compact<double>(H.nfar, H.farb.p, Us.p, Vs.p, H.uoff[0].p, H.voff[0].p, H.rank[0].p, H.U64.p,
+                                 H.V64.p, st);
+      } else {
+        H.U32.alloc(size_t(std::max(su, 1LL)));
+        H.V32.alloc(size_t(std::max(sv, 1LL)));
+        H.t32.alloc(size_t(std::max(stt, 1LL)));
+        launch_h_compact<float>(H.nfar, H.farb.p, Us.p, Vs.p, H.uoff[1].p, H.voff[1].p, H.rank[1].p, H.U32.p,
+                                H.V32.p, st);
+      }
+      H.bytes[w] = double(doff) * (w == 0 ? 8 : 4) + double(su + sv) * (w == 0 ? 8 : 4) +
+                   double(H.nnear + H.nfar) * sizeof(HBlockDev);
+    }
+    sync();
+  } else {
+    H.bytes[0] = double(doff) * 8;
+    H.bytes[1] = double(doff) * 4;
+    H.t64.alloc(1);
+    H.t32.alloc(1);
+  }
+  for (int q = 0; q < H.nfar; ++q) {
+    H.failed += ranks[size_t(3) * q + 2] != 0;
+    H.max_rank = std::max(H.max_rank, ranks[size_t(3) * q]);
+  }
+  H.y.alloc(nb);
+  H.xp64.alloc(nb);
+  H.xp32.alloc(nb);
+  H.built = true;
+  bem_mode = 1;
+  if (!keep_dense) {
+    Bd.reset();
+    Bf.reset();
+  }
+  H.ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
 void Ctx::local(const double* m, double* ydot, double* hout, unsigned long long* tq) {
@@ -1137,6 +1350,8 @@ int tmb_bem_assemble(tmb_ctx* ctx, const tmb_mesh* mesh) {
   launch_to_float(c.Bd.p, c.Bf.p, ld * nb, c.stream);
   c.sync();
   c.has_bem = true;
+  c.H = Ctx::HMat{};
+  c.bem_mode = 0;
   c.neu.reset();
   c.dir.reset();
   TMB_API_END
@@ -1158,6 +1373,8 @@ int tmb_set_bem_dense(tmb_ctx* ctx, int nb, const double* B_colmajor) {
   launch_to_float(c.Bd.p, c.Bf.p, ld * nb, c.stream);
   c.sync();
   c.has_bem = true;
+  c.H = Ctx::HMat{};
+  c.bem_mode = 0;
   c.neu.reset();
   c.dir.reset();
   TMB_API_END
@@ -1176,6 +1393,44 @@ int tmb_get_bem_dense(tmb_ctx* ctx, double* B_colmajor) {
   for (int j = 0; j < nb; ++j)
     for (int i = 0; i < nb; ++i) B_colmajor[size_t(j) * nb + i] = rowmajor[size_t(i) * ld + j];
   TMB_API_END
+}
+
+int tmb_bem_compress(tmb_ctx* ctx, const double* bxyz, const double* bnormal, int leaf, double eta,
+                     double eps_mixed, double eps_fp64, int kmax, int keep_dense) {
+  TMB_CHECK_ARG(ctx && bxyz, "tmb_bem_compress: null argument");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  TMB_CUDA(cudaSetDevice(c.device));
+  c.h_compress(bxyz, bnormal, leaf, eta, eps_mixed, eps_fp64, kmax, keep_dense != 0);
+  TMB_API_END
+}
+
+int tmb_set_bem_mode(tmb_ctx* ctx, int mode) {
+  TMB_CHECK_ARG(ctx && (mode == 0 || mode == 1), "tmb_set_bem_mode: mode is 0 (dense) or 1 (hierarchical)");
+  Ctx& c = *ctx->c;
+  if (mode == 1 && !c.H.built) return fail(TMB_ERR_STATE, "tmb_set_bem_mode: no hierarchical matrix built");
+  if (mode == 0 && (!c.Bd.p || !c.Bf.p)) return fail(TMB_ERR_STATE, "tmb_set_bem_mode: the dense matrix was released");
+  c.bem_mode = mode;
+  return TMB_OK;
+}
+
+int tmb_bem_info(tmb_ctx* ctx, double* out) {
+  TMB_CHECK_ARG(ctx && out, "tmb_bem_info: null argument");
+  const Ctx& c = *ctx->c;
+  const auto& H = c.H;
+  out[0] = c.bem_mode;
+  out[1] = H.nnear;
+  out[2] = H.nfar;
+  out[3] = double(H.terms[0]);
+  out[4] = double(H.terms[1]);
+  out[5] = H.bytes[0];
+  out[6] = H.bytes[1];
+  out[7] = double(c.nb) * double(c.nb);
+  out[8] = H.failed;
+  out[9] = H.max_rank;
+  out[10] = H.ms;
+  out[11] = H.built ? 1.0 : 0.0;
+  return TMB_OK;
 }
 
 int tmb_set_material(tmb_ctx* ctx, const double* Js, const double* A, const double* Ku, const double* ku_axis,

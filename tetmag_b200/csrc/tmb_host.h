@@ -104,7 +104,9 @@ struct HPartition {
   std::vector<std::pair<int, int>> far;      // admissible pairs -> low rank
 };
 
-void h_partition(const double* bxyz, int nb, int leaf, double eta, HPartition& P);
+// bnrm (Nb x 3 node normals, may be null) makes faces of different orientation separate first
+void h_partition(const double* bxyz, const double* bnrm, int nb, int leaf, double eta, int max_block,
+                 HPartition& P);
 void csr_transpose(const Csr& A, Csr& T);
 void csr_multiply(const Csr& A, const Csr& B, Csr& C);
 

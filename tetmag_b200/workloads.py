@@ -92,14 +92,22 @@ WORKLOADS = {"c1": c1, "c2": c2, "c4": c4_replica}
 
 
 def setup_context(w: Workload, device: int = 0, mixed: bool = False, tol: float = 1e-7, maxiter: int = 100,
-                  mesh_ops=None):
-    """MeshOps + Context with operators, device-assembled dense BEM, material and field."""
+                  mesh_ops=None, hmatrix: bool = False, keep_dense: bool = True, eps_mixed: float = 1e-6,
+                  eps_fp64: float = 1e-7, kmax: int = 64, normal_split: bool = True):
+    """MeshOps + Context with operators, device-assembled BEM (dense, optionally compressed to the
+    hierarchical form with leaf 32 and eta 2), material and applied field."""
     from .api import Context, MeshOps
 
     mo = mesh_ops if mesh_ops is not None else MeshOps(w.mesh.xyz, w.mesh.tets)
     ctx = Context(device)
     ctx.set_mesh(mo)
     ctx.bem_assemble(mo)
+    if hmatrix:
+        bd = mo.boundary()
+        bn = bd["bnodes"]
+        nrm = bd["node_normal"].reshape(3, -1).T[bn] if normal_split else None
+        ctx.bem_compress(w.mesh.xyz[bn], bnormal=nrm, leaf=32, eta=2.0, eps_mixed=eps_mixed, eps_fp64=eps_fp64,
+                         kmax=kmax, keep_dense=keep_dense)
     Js, A, Ku, axis, D = w.material_arrays()
     ctx.set_material(Js, A, Ku=Ku, ku_axis=axis, D=D, alpha=w.alpha)
     ctx.set_applied_field(np.ascontiguousarray(w.hext, dtype=np.float64))
