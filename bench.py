@@ -47,7 +47,7 @@ def parse():
     p.add_argument("--tol", type=float, default=1e-7)
     p.add_argument("--sim-ps", type=float, default=2.0, help="simulated ps for the ns/hour figure")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--bem", default="dense", choices=["hmatrix", "dense"],
+    p.add_argument("--bem", default="dense", choices=["hmatrix", "hmatrix-dense", "dense"],
                    help="BEM form of the timed paths (the dense FP64 path is always measured too)")
     return p.parse_args()
 
@@ -115,6 +115,10 @@ def make_workload(name: str, rank: int):
 
     if name == "c4":
         return workloads.c4_replica(replica=rank)
+    if name == "c4x64":
+        return workloads.c4_batch(replicas=64, seed=4 + 1000 * rank)
+    if name == "c3":
+        return workloads.c3_dots(ndots=256, seed=3 + 1000 * rank)
     if name.startswith("cuboid:"):
         nx, ny, nz, h = name.split(":", 1)[1].split("x")
         w = workloads.cuboid_random(int(nx), int(ny), int(nz), float(h), seed=7 + rank, alpha=0.5,
@@ -131,9 +135,14 @@ def dist_env():
 
 
 def cpu_baseline_sample(w, samples: int = 1):
-    """Oracle field evaluation on the host cores (bounded sample)."""
+    """Oracle field evaluation on the host cores (bounded sample).  For a batched workload the
+    sample is one instance (the median-sized one) and the rate is per instance."""
     from oracle import cpu_baseline, tetmag_oracle as O
+    from tetmag_b200 import workloads
 
+    if w.components is not None:
+        sizes = np.diff(w.components)
+        w = workloads.component(w, int(np.argsort(sizes)[len(sizes) // 2]))
     axis = None if w.ku_axis is None else O.soa_to_rows(w.ku_axis)
     pb = O.make_problem(w.mesh.xyz, w.mesh.tets, w.mesh.scale, Ms=w.Ms, A=w.A, alpha=w.alpha, Ku=w.Ku,
                         ku_axis=axis if axis is not None else (0, 0, 1), D=w.D, hext=w.hext, with_bem=False)
@@ -141,7 +150,7 @@ def cpu_baseline_sample(w, samples: int = 1):
     m = O.soa_to_rows(w.m0)
     ev.calibrate(m)
     res = [ev.sample(m) for _ in range(samples)]
-    return ev, res
+    return ev, res, m
 
 
 def run_reference(args):
@@ -151,8 +160,7 @@ def run_reference(args):
     from tetmag_b200 import workloads
 
     w = make_workload(args.workload, 0)
-    ev, res = cpu_baseline_sample(w, samples=0)
-    m = w.m0.reshape(3, -1).T.copy()
+    ev, res, m = cpu_baseline_sample(w, samples=0)
     for _ in range(args.warmup):
         ev.sample(m)
     tot = 0.0
@@ -192,11 +200,15 @@ def run_gpu(args):
     dev = torch.device("cuda", local)
 
     w = make_workload(args.workload, rank)
+    ninst = workloads.instances(w)         # batched instances in the context (field evals per call)
     t0 = time.perf_counter()
-    hier = args.bem == "hmatrix"
-    mo, ctx = workloads.setup_context(w, device=local, mixed=True, tol=args.tol, maxiter=100, hmatrix=hier,
+    hier = args.bem != "dense"
+    mo, ctx = workloads.setup_context(w, device=local, mixed=True, tol=args.tol, maxiter=100,
+                                      hmatrix={"hmatrix": "mesh", "hmatrix-dense": True}.get(args.bem, False),
                                       keep_dense=True)
     bem_info = ctx.bem_info() if hier else None
+    if hier:
+        bem_info["verify"] = ctx.bem_verify()
     setup_s = time.perf_counter() - t0
     # one non-default stream for the library's kernels and the timing events
     stream = torch.cuda.Stream(dev)
@@ -307,7 +319,7 @@ def run_gpu(args):
         ctx.llg_rhs(0.0, S[k % (W + K)], ydot)
     e1.record(stream)
     torch.cuda.synchronize(dev)
-    local_per_s = nloc / (max_over_ranks(e0.elapsed_time(e1)) / 1e3)
+    local_per_s = ninst * nloc / (max_over_ranks(e0.elapsed_time(e1)) / 1e3)
 
     # end to end through the public API with host buffers (H2D of m, D2H of ydot per step)
     host_states = [np.ascontiguousarray(st) for st in states]
@@ -326,10 +338,10 @@ def run_gpu(args):
     t = time.perf_counter()
     rs = ctx.relax(mrun, duration_ps=args.sim_ps, segment_ps=0.5)
     sim_s = max_over_ranks(time.perf_counter() - t)
-    ns_per_hour = (args.sim_ps * 1e-3) / (sim_s / 3600.0)
+    ns_per_hour = ninst * (args.sim_ps * 1e-3) / (sim_s / 3600.0)
 
-    value = world * K / (ms_mx / 1e3)
-    fp64_value = world * K / (ms_64 / 1e3)
+    value = world * ninst * K / (ms_mx / 1e3)
+    fp64_value = world * ninst * K / (ms_64 / 1e3)
     peak, peak_kind = peak_hbm()
     kernels = ["local_llg", "divergence", "gradient", "bem_matvec", "cg_spmv"]
     dom = max(kernels, key=lambda k: prof[k]["total_ms"])
@@ -346,15 +358,21 @@ def run_gpu(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_mx / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 operators / f64 vectors+reductions", "data": "synthetic",
-        "config": {"workload": w.name, "nodes": n, "boundary_nodes": mo.nb, "nnz": mo.nnz,
+        "config": {"workload": w.name, "nodes": n, "boundary_nodes": mo.nb, "nnz": mo.nnz, "instances": ninst,
+                   "batched": (None if ninst == 1 else
+                               ("replicas of one mesh sharing one BEM matrix (boundary matvec = one GEMM)"
+                                if w.shared_bem else "uneven meshes, one BEM block each, one batched matvec")
+                               + "; one CG and one step size for the batch; value counts instance evals"),
                    "bem": ("hierarchical (leaf 32, eta 2, ACA: FP32 terms to 1e-6 on the mixed path, FP64 "
-                           "terms to 1e-7 on the plain path), compressed from the device-assembled dense "
-                           "matrix" if hier else "dense, device-assembled, FP32 on the mixed path"),
+                           "terms to 1e-7 on the plain path), " +
+                           ("built from the mesh boundary" if args.bem == "hmatrix" else
+                            "compressed from the device-assembled dense matrix")
+                           if hier else "dense, device-assembled, FP32 on the mixed path"),
                    "precision": "mixed",
                    "cg_tol": args.tol, "states": "W+K distinct seeded perturbed states, warm-started solves",
                    "l2": "inputs larger than L2 (dense BEM alone is 4*Nb^2 bytes)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single"},
-        "e2e": {"value": world * K / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 3 * n * 8,
+        "e2e": {"value": world * ninst * K / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 3 * n * 8,
                 "d2h_bytes_per_step": 3 * n * 8},
         "gpu_launches": launches,
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -362,12 +380,12 @@ def run_gpu(args):
                      "bytes_per_launch": d["bytes_per_launch"], "avg_ms": avg_ms},
         "clocks": clk,
         "fp64_value": fp64_value, "speedup_vs_fp64": value / fp64_value,
-        "fp64_dense_value": world * K / (ms_64d / 1e3), "speedup_vs_fp64_dense": ms_64d / ms_mx,
+        "fp64_dense_value": world * ninst * K / (ms_64d / 1e3), "speedup_vs_fp64_dense": ms_64d / ms_mx,
         "rel_err_vs_fp64": {"hdem": err_h, "ydot": err_y, "reference": "FP64, dense BEM, CG to 1e-12"},
         "rel_err_fp64_hier_vs_dense": {"hdem": err_h64, "ydot": err_y64},
         "bem_info": bem_info,
         "local_rhs_evals_per_s": world * local_per_s,
-        "sim_ns_per_hour": ns_per_hour,
+        "sim_ns_per_hour": world * ns_per_hour,
         "relax": {"sim_ps": args.sim_ps, "wall_s": sim_s, "steps": rs["accepted"], "rejected": rs["rejected"],
                   "rhs": rs["rhs"]},
         "cg_iters_per_eval": {"mixed": [i / K for i in its_mx], "fp64": [i / K for i in its_64]},
@@ -380,7 +398,7 @@ def run_gpu(args):
         "setup_s": setup_s,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        ev, res = cpu_baseline_sample(w, samples=1)
+        ev, res, _ = cpu_baseline_sample(w, samples=1)
         line["cpu_baseline"] = {"value": 1.0 / res[0]["total_s"], "unit": UNIT, "cores": ev.threads,
                                 "kind": "port", "sample": ev.describe(),
                                 "components_s": {k: res[0][k] for k in

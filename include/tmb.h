@@ -90,7 +90,25 @@ int tmb_set_operators(tmb_ctx* ctx, int nx, int nnz, const int* rowptr, const in
  * mesh boundary (BEMprocessing::assembleLaplaceBEMmatrix, preproc/BEMprocessing.cpp:375-411);
  * tmb_set_bem_dense takes tetmag's MeshData::laplaceBEM (Nb x Nb, column-major). */
 int tmb_bem_assemble(tmb_ctx* ctx, const tmb_mesh* mesh);
+/* formula 0: tmb_bem_assemble (tetmag's arithmetic).  formula 1: the same weights in a
+ * far-field-accurate arithmetic (solid angle by atan2 of the triple product, log1p edge terms):
+ * tetmag's acos form drifts from the exact weights several hundred nm from a nm-sized triangle
+ * (row sums of a 500 nm film's matrix miss -1 by up to ~1e-3); this form keeps them to ~1e-13.
+ * No tetmag counterpart; it is the FP64 reference for the hierarchical matrix. */
+int tmb_bem_assemble_ex(tmb_ctx* ctx, const tmb_mesh* mesh, int formula);
 int tmb_set_bem_dense(tmb_ctx* ctx, int nb, const double* B_colmajor);
+/* Batched instances in one context: the mesh given to tmb_set_mesh / tmb_set_operators is a
+ * disjoint union of ncomp meshes, component c owning nodes [node_offsets[c], node_offsets[c+1])
+ * (the operators must not couple components).  Each component is one tetmag problem: its own
+ * pinned Neumann node (node N_c / 2 of the component, main/DemagField.cpp:80) and its own dense
+ * BEM block, assembled by tmb_bem_assemble(_ex) afterwards; the boundary matvec runs for all
+ * components in one launch.  shared_bem = 1 declares the components identical copies of one
+ * mesh (checked: operators and boundary numbering) that share one BEM block: the matvec is then
+ * one GEMM, B times the replicas' boundary values.  Solves, step control and torques are taken
+ * over all components together (one set of CG iterations and one step size for the batch).
+ * No tetmag counterpart (tetmag runs one mesh per process).  Call before tmb_bem_assemble; the
+ * hierarchical BEM and tmb_set_bem_dense / tmb_get_bem_dense need ncomp = 1. */
+int tmb_set_components(tmb_ctx* ctx, int ncomp, const int* node_offsets, int shared_bem);
 int tmb_get_bem_dense(tmb_ctx* ctx, double* B_colmajor);
 
 /* Hierarchical compression of the dense matrix (replaces H2Lib's setupH2MatrixC /
@@ -98,23 +116,44 @@ int tmb_get_bem_dense(tmb_ctx* ctx, double* B_colmajor);
  * order) with leaf size `leaf` (<= 32; tetmag uses clf = 32), admissibility
  * min(diam) <= eta * dist (tetmag: eta = 2), dense leaf tiles and adaptive-cross-approximation
  * low-rank blocks: FP32 terms to eps_mixed for the mixed path, FP64 terms to eps_fp64 for the
- * plain path (at most kmax terms per block).  bnormal (Nb x 3 node normals, may be NULL) lets
+ * plain path (at most kmax <= 128 terms per block).  bnormal (Nb x 3 node normals, may be NULL) lets
  * the cluster tree separate faces of different orientation first, so that every low-rank block
  * couples one smooth piece of surface to another.  Needs the dense FP64 matrix on the device
  * (tmb_bem_assemble / tmb_set_bem_dense); keep_dense = 0 releases it afterwards.  The demag
  * chain then uses the hierarchical matvec (tmb_set_bem_mode switches back). */
 int tmb_bem_compress(tmb_ctx* ctx, const double* bxyz, const double* bnormal, int leaf, double eta,
                      double eps_mixed, double eps_fp64, int kmax, int keep_dense);
+/* Hierarchical matrix straight from the mesh boundary, without the dense matrix: same
+ * partition and ranks as tmb_bem_compress (the cluster tree splits faces by node-normal
+ * orientation), dense tiles with tetmag's Lindholm arithmetic, and low-rank blocks from entries
+ * evaluated on the device in a far-field-accurate form of the same weights (the reference form
+ * loses up to ~10% of a weight several hundred nm from a nm-sized triangle, which is noise
+ * that cross approximation cannot compress).  This is the c2-sized path where H2Lib's own
+ * assembly replaces the dense matrix (setupH2MatrixC, main/h2interface.c:315-399). */
+int tmb_bem_build_h(tmb_ctx* ctx, const tmb_mesh* mesh, int leaf, double eta, double eps_mixed, double eps_fp64,
+                    int kmax);
 int tmb_set_bem_mode(tmb_ctx* ctx, int mode);  /* 0 dense, 1 hierarchical */
 /* out[0..11]: mode, dense tiles, low-rank blocks, FP64 terms, FP32 terms, FP64 bytes, FP32 bytes,
  * dense entries (Nb^2), blocks at the rank cap, max FP64 rank, compression ms, built flag */
 int tmb_bem_info(tmb_ctx* ctx, double* out);
+/* Accuracy of the low-rank blocks against the dense FP64 matrix (still on the device:
+ * keep_dense = 1) for a fixed probe vector.  out[0..3]: relative error of the low-rank part
+ * with FP64 terms, with FP32 terms, worst block relative error FP64, FP32.  block_out (may be
+ * NULL; 6 per low-rank block, partition order): |A x|, FP64 error, FP32 error, FP64 rank, FP32
+ * rank, 1 if the block hit the rank cap.  Diagnostic only: tetmag's call path has no
+ * counterpart. */
+int tmb_bem_verify(tmb_ctx* ctx, double* block_out, double* out);
 
 /* Material per node (SimulationData, specs/SimulationData.cpp:125-163): Js [T], A [J/m]
  * already divided by scale^2, Ku [J/m^3], ku_axis 3N SoA, D [J/m^2] already divided by
  * scale (bulk DMI, main/EffFieldCalc.cpp:159-170).  Ku, ku_axis, D may be NULL. */
 int tmb_set_material(tmb_ctx* ctx, const double* Js, const double* A, const double* Ku, const double* ku_axis,
                      const double* D, double alpha);
+/* DMI form applied with the material's D: 0 bulk (tetmag's, main/EffFieldCalc.cpp:159-170, the
+ * default), 1 interfacial (thin films with the interface normal along z; no tetmag
+ * counterpart): H = -(1/V) dE/dm of E = sum_i V_i D_i [m_z div m - (m . grad) m_z]_i with
+ * tetmag's nodal gradient operators, divided by Js. */
+int tmb_set_dmi_kind(tmb_ctx* ctx, int kind);
 /* Applied field, 3N SoA in A/m (TheLLG::setZeemanField, main/TheLLG.cpp:477-483). */
 int tmb_set_applied_field(tmb_ctx* ctx, const double* hext, int ptr_kind);
 /* precession = 0 selects the "remove precession" dynamics (TheLLG::noPrecession, main/TheLLG.cpp:180-199). */

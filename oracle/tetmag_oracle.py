@@ -273,6 +273,41 @@ def lindholm_weights(x0, p0, p1, p2, area, nv):
     return L
 
 
+def lindholm_weights_accurate(x0, p0, p1, p2, area, nv):
+    """The weights of ``lindholm_weights`` in a far-field-accurate arithmetic (the form the
+    device uses for the low-rank blocks of its hierarchical matrix; not a reference function).
+
+    The solid angle is 2 atan2(N, D) with N = |e01 x e02| chi0 (Van Oosterom & Strackee,
+    IEEE Trans. Biomed. Eng. 30, 125 (1983)) instead of 2 acos(arg), edges are vertex
+    differences and the edge logarithms use log1p, so that the cancellation of the two terms of
+    a weight (about r / h) works on full-precision inputs.
+    """
+    p = np.stack([p0, p1, p2], axis=1)
+    e = np.roll(p, -1, axis=1) - p                       # edges p_{i+1} - p_i
+    c = np.cross(p1 - p0, p2 - p0)
+    cn = np.linalg.norm(c, axis=-1)
+    chi = c / cn[:, None]
+    s = np.linalg.norm(e, axis=-1)
+    xi = e / s[..., None]
+    rv = p - x0[:, None, :]
+    rho = np.linalg.norm(rv, axis=-1)
+    chi0 = np.sum(chi * rv[:, 0, :], axis=-1)
+    d01 = np.sum(rv[:, 0] * rv[:, 1], -1)
+    d02 = np.sum(rv[:, 0] * rv[:, 2], -1)
+    d12 = np.sum(rv[:, 1] * rv[:, 2], -1)
+    D = rho[:, 0] * rho[:, 1] * rho[:, 2] + d01 * rho[:, 2] + d02 * rho[:, 1] + d12 * rho[:, 0]
+    omega = 2.0 * np.arctan2(cn * chi0, D)
+    P = np.log1p(2.0 * s / (rho + np.roll(rho, -1, axis=1) - s))
+    eta0 = np.sum(np.cross(chi[:, None, :], xi) * rv, axis=-1)
+    gamma = np.einsum("mid,mjd->mij", np.roll(xi, -1, axis=1), xi)
+    gP = np.einsum("mij,mj->mi", gamma, P)
+    L = np.roll(s, -1, axis=1) / (8.0 * PI * area[:, None]) * (np.roll(eta0, -1, axis=1) * omega[:, None]
+                                                             - chi0[:, None] * gP)
+    flip = np.sum(nv * chi, axis=-1) < 0.0
+    L[flip] = -L[flip]
+    return L
+
+
 def dense_bem(xyz, tets, bnd: Boundary, sub: Optional[np.ndarray] = None,
               rows: Optional[np.ndarray] = None, chunk_pairs: int = 2_000_000) -> np.ndarray:
     """BEMprocessing::assembleLaplaceBEMmatrix (:375-411) -> (Nb, Nb) FP64.

@@ -240,6 +240,65 @@ def test_hierarchical_bem_matches_dense_c4():
     assert rel(H_h32, H_dense) <= MIXED_TOL
 
 
+def test_accurate_dense_assembly_c4():
+    # the far-field-accurate weights keep the exact identity B.1 = -1 per row; on this 200 nm
+    # cuboid the reference arithmetic is still close to them
+    w = workloads.c4_replica(replica=0)
+    mo = MeshOps(w.mesh.xyz, w.mesh.tets)
+    ctx = Context(0)
+    ctx.set_mesh(mo)
+    ctx.bem_assemble(mo, accurate=True)
+    Ba = ctx.get_bem_dense()
+    assert np.max(np.abs(Ba.sum(axis=1) + 1.0)) < 1e-11
+    ctx.bem_assemble(mo)
+    Br = ctx.get_bem_dense()
+    assert np.max(np.abs(Ba - Br)) < 1e-7 * np.max(np.abs(Br))
+
+
+def test_hierarchical_bem_from_mesh_c4():
+    # built from the mesh boundary (no dense matrix): low-rank blocks from the accurate far-field
+    # weights, dense tiles with the reference arithmetic; compared with the dense path on the
+    # accurate matrix
+    w = workloads.c4_replica(replica=2)
+    mo, ctx = workloads.setup_context(w, tol=1e-12, maxiter=300, hmatrix="mesh", keep_dense=True)
+    info = ctx.bem_info()
+    assert info["built"] == 1 and info["mode"] == 1
+    v = ctx.bem_verify()
+    assert v["rel_err_fp64"] <= 3e-6 and v["rel_err_fp32"] <= 1e-5
+    m = w.m0
+    ctx.set_bem_mode(False)
+    H_dense = ctx.demag_field(m)
+    ctx.set_bem_mode(True)
+    assert rel(ctx.demag_field(m), H_dense) <= 1e-6
+    ctx.set_precision(True)
+    ctx.set_solver_params(1e-9, 300)
+    assert rel(ctx.demag_field(m), H_dense) <= MIXED_TOL
+
+
+def test_hierarchical_from_mesh_all_dense_tiles_equal_dense_c1(c1):
+    # with a vanishing admissibility parameter every block is a dense tile assembled from the
+    # mesh: the matvec must reproduce the dense assembly to round-off
+    w, mo, ctx, pb, dem = c1
+    ctx2 = workloads.setup_context(w, tol=1e-12, maxiter=300, mesh_ops=mo)[1]
+    ctx2.bem_build_h(mo, leaf=32, eta=1e-9)
+    info = ctx2.bem_info()
+    assert info["lowrank_blocks"] == 0 and info["dense_tiles"] > 0
+    m = meshgen.random_state(w.n, 5)
+    H_tiles = ctx2.demag_field(m)
+    ctx2.set_bem_mode(False)
+    assert rel(H_tiles, ctx2.demag_field(m)) <= 1e-12
+
+
+def test_hierarchical_from_mesh_without_dense_c1_against_oracle(c1):
+    w, mo, ctx, pb, dem = c1
+    ctx2 = workloads.setup_context(w, tol=1e-12, maxiter=300, hmatrix="mesh", keep_dense=False, mesh_ops=mo)[1]
+    with pytest.raises(_lib.TmbError):
+        ctx2.set_bem_mode(False)
+    m = meshgen.random_state(w.n, 19)
+    Ho = O.rows_to_soa(dem.field(O.soa_to_rows(m)))
+    assert rel(ctx2.demag_field(m), Ho) <= 1e-6
+
+
 def test_hierarchical_bem_c1_against_oracle(c1):
     w, mo, ctx, pb, dem = c1
     ctx2 = workloads.setup_context(w, tol=1e-12, maxiter=300, hmatrix=True, keep_dense=False, mesh_ops=mo)[1]
@@ -250,3 +309,107 @@ def test_hierarchical_bem_c1_against_oracle(c1):
     ctx2.set_precision(True)
     ctx2.set_solver_params(1e-9, 300)
     assert rel(ctx2.demag_field(m), Ho) <= MIXED_TOL
+
+
+def _separate(meshes, m0s, hexts, axes, Ku, alpha, tol=1e-13):
+    """Demag field and right-hand side of each instance in its own single-mesh context."""
+    out = []
+    for mesh, m0, hx, ax in zip(meshes, m0s, hexts, axes):
+        w = workloads.Workload(name="one", mesh=mesh, Ms=8.0e5, A=1.3e-11, alpha=alpha, m0=m0, hext=hx, Ku=Ku,
+                               ku_axis=ax)
+        ctx = workloads.setup_context(w, tol=tol, maxiter=300)[1]
+        h = ctx.demag_field(m0)
+        out.append((h, ctx.llg_rhs(0.0, m0)))
+    return out
+
+
+def test_components_uneven_dots_match_separate_contexts():
+    # three dots of different sizes as one batched context (each with its own BEM block) against
+    # three single-mesh contexts; one of them also against the oracle
+    meshes = [meshgen.kuhn_cuboid(6, 5, 2, 2.5), meshgen.kuhn_cuboid(9, 7, 3, 2.2), meshgen.kuhn_cuboid(4, 8, 5, 2.8)]
+    m0s = [meshgen.random_state(m.nx, 40 + i) for i, m in enumerate(meshes)]
+    hx = [meshgen.field_from_angles(m.nx, 0.03 * (i + 1), 30.0 * i, 50.0) for i, m in enumerate(meshes)]
+    rng = np.random.default_rng(8)
+    axes = []
+    for m in meshes:
+        a = rng.standard_normal(3)
+        axes.append(np.repeat(a / np.linalg.norm(a), m.nx))
+    mesh, off = meshgen.union(meshes)
+    w = workloads.Workload(name="dots", mesh=mesh, Ms=8.0e5, A=1.3e-11, alpha=0.1, m0=meshgen.soa_stack(m0s),
+                           hext=meshgen.soa_stack(hx), Ku=5e4, ku_axis=meshgen.soa_stack(axes), components=off)
+    mo, ctx = workloads.setup_context(w, tol=1e-13, maxiter=300)
+    H = meshgen.soa_split(ctx.demag_field(w.m0), off)
+    Y = meshgen.soa_split(ctx.llg_rhs(0.0, w.m0), off)
+    ref = _separate(meshes, m0s, hx, axes, 5e4, 0.1)
+    for c in range(3):
+        assert rel(H[c], ref[c][0]) <= 1e-10
+        assert rel(Y[c], ref[c][1]) <= 1e-10
+    pb = O.make_problem(meshes[1].xyz, meshes[1].tets, 1e-9, Ms=8e5, A=1.3e-11, alpha=0.1, Ku=5e4,
+                        ku_axis=O.soa_to_rows(axes[1]), D=0.0, hext=hx[1])
+    Ho = O.DemagOracle(pb).field(O.soa_to_rows(m0s[1]))
+    assert rel(H[1], O.rows_to_soa(Ho)) <= FP64_TOL
+    ctx.set_precision(True)
+    ctx.set_solver_params(1e-9, 300)
+    Hm = meshgen.soa_split(ctx.demag_field(w.m0), off)
+    for c in range(3):
+        assert rel(Hm[c], ref[c][0]) <= MIXED_TOL
+
+
+def test_shared_bem_replicas_gemm_match_separate_contexts():
+    # five replicas of one cuboid sharing one BEM matrix (boundary matvec as one GEMM), each with
+    # its own m0 and applied field
+    base = meshgen.kuhn_cuboid(12, 10, 3, 3.0)
+    R = 5
+    m0s = [meshgen.random_state(base.nx, 60 + r) for r in range(R)]
+    hx = [meshgen.field_from_angles(base.nx, 0.01 * r, 20.0 * r, 10.0 * r) for r in range(R)]
+    mesh, off = meshgen.union([base] * R)
+    w = workloads.Workload(name="reps", mesh=mesh, Ms=8.0e5, A=1.3e-11, alpha=0.5, m0=meshgen.soa_stack(m0s),
+                           hext=meshgen.soa_stack(hx), components=off, shared_bem=True)
+    mo, ctx = workloads.setup_context(w, tol=1e-13, maxiter=300)
+    H = meshgen.soa_split(ctx.demag_field(w.m0), off)
+    ref = _separate([base] * R, m0s, hx, [None] * R, 0.0, 0.5)
+    for r in range(R):
+        assert rel(H[r], ref[r][0]) <= 1e-10
+    ctx.set_precision(True)
+    ctx.set_solver_params(1e-9, 300)
+    Hm = meshgen.soa_split(ctx.demag_field(w.m0), off)
+    for r in range(R):
+        assert rel(Hm[r], ref[r][0]) <= MIXED_TOL
+    # identical replicas must give identical fields
+    mesh2, off2 = meshgen.union([base] * 3)
+    w2 = workloads.Workload(name="same", mesh=mesh2, Ms=8.0e5, A=1.3e-11, alpha=0.5,
+                            m0=meshgen.soa_stack([m0s[0]] * 3), hext=meshgen.soa_stack([hx[1]] * 3),
+                            components=off2, shared_bem=True)
+    ctx2 = workloads.setup_context(w2, tol=1e-13, maxiter=300)[1]
+    H2 = meshgen.soa_split(ctx2.demag_field(w2.m0), off2)
+    assert rel(H2[2], H2[0]) <= 1e-12
+
+
+def test_components_reject_coupled_operators(c1):
+    w, mo, ctx, pb, dem = c1
+    ctx2 = Context(0)
+    ctx2.set_mesh(mo)
+    with pytest.raises(_lib.TmbError):
+        ctx2.set_components([0, w.n // 2, w.n])       # splits one connected mesh
+
+
+def test_interfacial_dmi_local_field(golden):
+    # interfacial DMI (no reference counterpart) against the oracle's exact energy gradient,
+    # both precisions; then back to the bulk form
+    g, mo, ctx = golden
+    m = O.rows_to_soa(g["m"])
+    pb = O.make_problem(g["xyz"], g["tets"], 1e-9, Ms=8e5, A=1.3e-11, alpha=0.3, Ku=5e4, ku_axis=g["axis"],
+                        D=3e-3, hext=np.ascontiguousarray(g["hext"]), with_bem=False, dmi_kind="interfacial")
+    Ho = O.local_field(pb, g["m"], g["hdem"])
+    ctx.set_demag_frozen(O.rows_to_soa(g["hdem"]))
+    ctx.set_dmi_kind(True)
+    try:
+        H = ctx.effective_field(m)
+        assert rel(H, O.rows_to_soa(Ho)) <= 1e-12
+        assert rel(TheLLG(ctx)(m, 0.0), O.rows_to_soa(O.llg_rhs(pb, g["m"], Ho))) <= 1e-12
+        ctx.set_precision(True)
+        assert rel(ctx.effective_field(m), O.rows_to_soa(Ho)) <= MIXED_TOL
+    finally:
+        ctx.set_precision(False)
+        ctx.set_dmi_kind(False)
+    assert rel(ctx.effective_field(m), O.rows_to_soa(g["H"])) <= 1e-12

@@ -77,3 +77,20 @@ def test_cpp_preprocessing_matches_oracle(kind):
     idx = np.array([key[tuple(t)] for t in tri])
     assert np.allclose(bd["tri_normal"].reshape(-1, 3), bnd.tri_normal[idx], atol=1e-13)
     assert np.allclose(bd["tri_area"], bnd.tri_area[idx], rtol=1e-13)
+
+
+def test_union_and_soa_round_trip():
+    a, b = meshgen.kuhn_cuboid(3, 2, 2, 2.0), meshgen.kuhn_cuboid(2, 4, 1, 3.0)
+    u, off = meshgen.union([a, b])
+    assert list(off) == [0, a.nx, a.nx + b.nx]
+    assert u.tets.max() == a.nx + b.nx - 1 and u.tets[len(a.tets):].min() == a.nx
+    va, vb = np.arange(3.0 * a.nx), 1000 + np.arange(3.0 * b.nx)
+    s = meshgen.soa_stack([va, vb])
+    assert np.array_equal(s[:a.nx], va[:a.nx]) and np.array_equal(s[a.nx:a.nx + b.nx], vb[:b.nx])
+    ra, rb = meshgen.soa_split(s, off)
+    assert np.array_equal(ra, va) and np.array_equal(rb, vb)
+    # the preprocessing of the union is the union of the preprocessing
+    mu, ma = MeshOps(u.xyz, u.tets), MeshOps(a.xyz, a.tets)
+    assert mu.nb == ma.nb + MeshOps(b.xyz, b.tets).nb
+    Ku, Ka = mu.operators(), ma.operators()
+    assert np.allclose(Ku["stiff"][:Ka["rowptr"][-1]], Ka["stiff"], rtol=0, atol=0)

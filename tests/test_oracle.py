@@ -112,3 +112,86 @@ def test_golden_vectors():
     ydot = O.llg_rhs(pb, m, H)
     assert np.linalg.norm(ydot - g["ydot"]) <= 1e-12 * np.linalg.norm(g["ydot"])
     assert n == 210
+
+
+def _lindholm_mp(x0, p, nv, dps=50):
+    """Lindholm weights in 50-digit arithmetic (mpmath): the exact values both forms approximate."""
+    mp = pytest.importorskip("mpmath")
+    mp.mp.dps = dps
+    X = [mp.mpf(float(v)) for v in x0]
+    P = [[mp.mpf(float(v)) for v in q] for q in p]
+    sub = lambda a, b: [a[i] - b[i] for i in range(3)]  # noqa: E731
+    dot = lambda a, b: sum(a[i] * b[i] for i in range(3))  # noqa: E731
+    cross = lambda a, b: [a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]]  # noqa: E731
+    c = cross(sub(P[1], P[0]), sub(P[2], P[0]))
+    cn = mp.sqrt(dot(c, c))
+    chi = [v / cn for v in c]
+    rv = [sub(P[i], X) for i in range(3)]
+    xi = [sub(P[(i + 1) % 3], P[i]) for i in range(3)]
+    s = [mp.sqrt(dot(v, v)) for v in xi]
+    xi = [[v / s[i] for v in xi[i]] for i in range(3)]
+    rho = [mp.sqrt(dot(v, v)) for v in rv]
+    chi0 = dot(chi, rv[0])
+    D = rho[0] * rho[1] * rho[2] + dot(rv[0], rv[1]) * rho[2] + dot(rv[0], rv[2]) * rho[1] + dot(rv[1], rv[2]) * rho[0]
+    om = 2 * mp.atan2(cn * chi0, D)
+    Pl = [mp.log((rho[i] + rho[(i + 1) % 3] + s[i]) / (rho[i] + rho[(i + 1) % 3] - s[i])) for i in range(3)]
+    L = []
+    for i in range(3):
+        a = (i + 1) % 3
+        gP = sum(dot(xi[a], xi[j]) * Pl[j] for j in range(3))
+        L.append(s[a] / (8 * mp.pi * cn / 2) * (dot(cross(chi, xi[a]), rv[a]) * om - chi0 * gP))
+    if dot([mp.mpf(float(v)) for v in nv], chi) < 0:
+        L = [-v for v in L]
+    return np.array([float(v) for v in L])
+
+
+def test_far_field_lindholm_weights():
+    # A 2.5 nm bottom-face triangle seen from the top face of a 20 nm film, 10-420 nm away:
+    # the reference arithmetic (acos solid angle) loses accuracy with distance (about 10% at
+    # 420 nm); the far-field form used for the low-rank blocks stays within 1e-9 relative.
+    h = 2.5
+    ref_err, acc_err = [], []
+    for dist in (10.0, 50.0, 100.0, 200.0, 420.0):
+        x0 = np.array([[0.0, 0.0, 10.0]])
+        p = np.array([[dist, 0.0, -10.0], [dist + h, 0.0, -10.0], [dist, h, -10.0]])
+        nv = np.array([[0.0, 0.0, -1.0]])
+        area = np.array([h * h / 2])
+        exact = _lindholm_mp(x0[0], p, nv[0])
+        args = (x0, p[None, 0], p[None, 1], p[None, 2], area, nv)
+        ref_err.append(np.max(np.abs(O.lindholm_weights(*args)[0] - exact)) / np.max(np.abs(exact)))
+        acc_err.append(np.max(np.abs(O.lindholm_weights_accurate(*args)[0] - exact)) / np.max(np.abs(exact)))
+    assert max(acc_err) < 1e-9
+    assert ref_err[-1] > 1e-3                  # the reason the far blocks use the other form
+    # random geometries, including observers close to the triangle's plane
+    rng = np.random.default_rng(3)
+    for trial in range(40):
+        p0 = rng.uniform(-5, 5, 3)
+        p = np.array([p0, p0 + 3 * rng.standard_normal(3), p0 + 3 * rng.standard_normal(3)])
+        d = rng.standard_normal(3)
+        x0 = p0 + 10 ** rng.uniform(0.5, 2.5) * d / np.linalg.norm(d)
+        nv = np.cross(p[1] - p[0], p[2] - p[0])
+        area = np.array([0.5 * np.linalg.norm(nv)])
+        exact = _lindholm_mp(x0, p, nv)
+        La = O.lindholm_weights_accurate(x0[None], p[None, 0], p[None, 1], p[None, 2], area, nv[None])[0]
+        assert np.max(np.abs(La - exact)) <= 1e-9 * np.max(np.abs(exact))
+
+
+def test_interfacial_dmi_field_is_energy_gradient():
+    # the interfacial-DMI field (no reference counterpart) is -(1/V) dE/dm of its discrete energy:
+    # checked by central differences of the energy on a small prism
+    from tetmag_b200 import meshgen
+    mesh = meshgen.kuhn_cuboid(4, 3, 2, 3.0)
+    pb = O.make_problem(mesh.xyz, mesh.tets, 1e-9, Ms=3.84e5, A=8.78e-12, alpha=0.3, D=1.58e-3,
+                        with_bem=False, dmi_kind="interfacial")
+    m = O.soa_to_rows(meshgen.random_state(mesh.nx, 5))
+    H = O.interfacial_dmi_field(pb, m)
+    V = pb.fem.node_vol
+    rng = np.random.default_rng(0)
+    for _ in range(12):
+        i, d = int(rng.integers(mesh.nx)), int(rng.integers(3))
+        eps = 1e-6
+        mp, mm = m.copy(), m.copy()
+        mp[i, d] += eps
+        mm[i, d] -= eps
+        dE = (O.interfacial_dmi_energy(pb, mp) - O.interfacial_dmi_energy(pb, mm)) / (2 * eps)
+        assert abs(-dE / V[i] - H[i, d]) <= 1e-7 * np.max(np.abs(H))

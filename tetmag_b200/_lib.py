@@ -36,12 +36,17 @@ SIGNATURES = {
     "tmb_set_mesh": [_P, _P],
     "tmb_set_operators": [_P, _int, _int, _I, _I, _D, _D, _D, _D, _D, _D, _D, _D, _int, _I, _D, _D],
     "tmb_bem_assemble": [_P, _P],
+    "tmb_bem_assemble_ex": [_P, _P, _int],
     "tmb_set_bem_dense": [_P, _int, _D],
+    "tmb_set_components": [_P, _int, _I, _int],
     "tmb_get_bem_dense": [_P, _D],
     "tmb_bem_compress": [_P, _D, _D, _int, _dbl, _dbl, _dbl, _int, _int],
+    "tmb_bem_build_h": [_P, _P, _int, _dbl, _dbl, _dbl, _int],
     "tmb_set_bem_mode": [_P, _int],
     "tmb_bem_info": [_P, _D],
+    "tmb_bem_verify": [_P, _D, _D],
     "tmb_set_material": [_P, _D, _D, _D, _D, _D, _dbl],
+    "tmb_set_dmi_kind": [_P, _int],
     "tmb_set_applied_field": [_P, _P, _int],
     "tmb_set_llg_options": [_P, _int],
     "tmb_set_solver_params": [_P, _dbl, _int],

@@ -133,8 +133,16 @@ class Context:
         self.n, self.nb = n, bn.size
         return self
 
-    def bem_assemble(self, mesh: MeshOps):
-        check(lib().tmb_bem_assemble(self.h, mesh.h))
+    def bem_assemble(self, mesh: MeshOps, accurate: bool = False):
+        """Dense BEM on the device: tetmag's Lindholm arithmetic, or (accurate) the far-field-accurate
+        form of the same weights."""
+        check(lib().tmb_bem_assemble_ex(self.h, mesh.h, 1 if accurate else 0))
+        return self
+
+    def set_components(self, node_offsets, shared_bem: bool = False):
+        """The mesh is a disjoint union of components (batched instances); see tmb_set_components."""
+        off = _i32(node_offsets)
+        check(lib().tmb_set_components(self.h, off.size - 1, _iptr(off), 1 if shared_bem else 0))
         return self
 
     def set_bem_dense(self, B: np.ndarray):
@@ -157,6 +165,12 @@ class Context:
                                      1 if keep_dense else 0))
         return self
 
+    def bem_build_h(self, mesh: MeshOps, leaf=32, eta=2.0, eps_mixed=1e-6, eps_fp64=1e-7, kmax=64):
+        """Hierarchical BEM built from the mesh boundary, no dense matrix needed."""
+        check(lib().tmb_bem_build_h(self.h, mesh.h, int(leaf), float(eta), float(eps_mixed), float(eps_fp64),
+                                    int(kmax)))
+        return self
+
     def set_bem_mode(self, hierarchical: bool):
         check(lib().tmb_set_bem_mode(self.h, 1 if hierarchical else 0))
         return self
@@ -167,6 +181,23 @@ class Context:
         keys = ["mode", "dense_tiles", "lowrank_blocks", "terms_fp64", "terms_fp32", "bytes_fp64", "bytes_fp32",
                 "dense_entries", "blocks_at_cap", "max_rank_fp64", "compress_ms", "built"]
         return {k: st[i] for i, k in enumerate(keys)}
+
+    def bem_verify(self, per_block: bool = False):
+        """Probe-vector accuracy of the low-rank blocks against the dense FP64 matrix.
+        Returns a dict (rel_err_fp64, rel_err_fp32, worst_block_fp64, worst_block_fp32) and,
+        with per_block, an (nblocks, 6) array: |A x|, FP64 error, FP32 error, ranks, cap flag."""
+        out = (C.c_double * 4)()
+        blk = None
+        if per_block:
+            blk = np.zeros((int(self.bem_info()["lowrank_blocks"]), 6))
+        check(lib().tmb_bem_verify(self.h, _dptr(blk) if blk is not None else None, out))
+        res = dict(zip(["rel_err_fp64", "rel_err_fp32", "worst_block_fp64", "worst_block_fp32"], list(out)))
+        return (res, blk) if per_block else res
+
+    def set_dmi_kind(self, interfacial: bool):
+        """DMI form of the material's D: bulk (tetmag's) or interfacial."""
+        check(lib().tmb_set_dmi_kind(self.h, 1 if interfacial else 0))
+        return self
 
     def set_material(self, Js, A, Ku=None, ku_axis=None, D=None, alpha=1.0):
         n = self.n

@@ -83,6 +83,121 @@ __global__ void __launch_bounds__(kBlock) k_gemv_rows(int nb, size_t ld, const V
   }
 }
 
+// x_pad[pos[i]] = u[bnodes[i]]: boundary values of every component at 32-element aligned offsets.
+template <typename V>
+__global__ void k_gather_pad(int nb, const double* __restrict__ u, const int* __restrict__ idx,
+                             const int* __restrict__ pos, V* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nb) out[pos[i]] = static_cast<V>(u[idx[i]]);
+}
+
+// Batched dense matvecs of components with their own matrices (uneven sizes): one warp per
+// tile of up to R consecutive rows of one component, the same inner loop as k_gemv_rows.
+template <typename V, int R>
+__global__ void __launch_bounds__(kBlock) k_gemv_tiles(int ntiles, const GemvTile* __restrict__ tiles,
+                                                       const V* __restrict__ B, const V* __restrict__ x,
+                                                       double* __restrict__ y) {
+  using VT = typename Vec16<V>::T;
+  constexpr int W = Vec16<V>::W;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= ntiles) return;
+  const GemvTile T = tiles[warp];
+  const VT* rows[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) rows[r] = reinterpret_cast<const VT*>(B + T.b + size_t(min(r, T.nrows - 1)) * T.ld);
+  const V* xs = x + T.x;
+  const VT* xv = reinterpret_cast<const VT*>(xs);
+  const int nv = T.ncols / W;
+  double acc[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) acc[r] = 0.0;
+#pragma unroll 2
+  for (int j = lane; j < nv; j += 32) {
+    const VT xx = __ldg(xv + j);
+    VT b[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) b[r] = __ldcs(rows[r] + j);
+#pragma unroll
+    for (int r = 0; r < R; ++r) acc[r] += Vec16<V>::dot(b[r], xx);
+  }
+  for (int j = nv * W + lane; j < T.ncols; j += 32) {
+    const double xsj = double(xs[j]);
+#pragma unroll
+    for (int r = 0; r < R; ++r) acc[r] = fma(double(reinterpret_cast<const V*>(rows[r])[j]), xsj, acc[r]);
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    double a = acc[r];
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0 && r < T.nrows) y[T.y + r] = a;
+  }
+}
+
+// Replicas sharing one matrix: Y = B X with B (nbc x nbc, row-major, leading dimension ld) and
+// X the replicas' boundary values (column c at c * xs).  CTA tile 64 rows x 64 replicas over a
+// K range of kchunk columns (split-K partial sums are added atomically into a zeroed Y); thread
+// tile 4 x 4; each 32-wide K step is accumulated in the value type, then added into FP64.
+template <typename V>
+__global__ void __launch_bounds__(256) k_bem_gemm(int nbc, int ncomp, size_t ld, const V* __restrict__ B,
+                                                  const V* __restrict__ X, int xs, double* __restrict__ Y,
+                                                  int kchunk) {
+  constexpr int TM = 64, TN = 64, TK = 32;
+  __shared__ __align__(16) V As[TK][TM + 4];
+  __shared__ __align__(16) V Xs[TK][TN + 4];
+  const int m0 = blockIdx.x * TM, c0 = blockIdx.y * TN;
+  const int k0 = blockIdx.z * kchunk, k1 = min(nbc, k0 + kchunk);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+  for (int kb = k0; kb < k1; kb += TK) {
+    for (int e = threadIdx.x; e < TM * TK; e += 256) {
+      const int r = e / TK, k = e % TK, gr = m0 + r, gk = kb + k;
+      As[k][r] = (gr < nbc && gk < k1) ? B[size_t(gr) * ld + gk] : V(0);
+    }
+    for (int e = threadIdx.x; e < TN * TK; e += 256) {
+      const int c = e / TK, k = e % TK, gc = c0 + c, gk = kb + k;
+      Xs[k][c] = (gc < ncomp && gk < k1) ? X[size_t(gc) * xs + gk] : V(0);
+    }
+    __syncthreads();
+    V part[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) part[i][j] = V(0);
+#pragma unroll 8
+    for (int k = 0; k < TK; ++k) {
+      V a[4], xv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        a[i] = As[k][ty * 4 + i];
+        xv[i] = Xs[k][tx * 4 + i];
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) part[i][j] = fma(a[i], xv[j], part[i][j]);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] += double(part[i][j]);
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int r = m0 + ty * 4 + i, c = c0 + tx * 4 + j;
+      if (r < nbc && c < ncomp) {
+        if (gridDim.z > 1) atomicAdd(&Y[size_t(c) * nbc + r], acc[i][j]);
+        else Y[size_t(c) * nbc + r] = acc[i][j];
+      }
+    }
+}
+
 __global__ void k_dirichlet_values(int n, const int* __restrict__ bindex, const double* __restrict__ u2b,
                                    double* __restrict__ b) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -117,6 +232,37 @@ void launch_bem_gemv(int nb, const V* B, const V* xb, double* u2b, cudaStream_t 
   TMB_CUDA(cudaGetLastError());
 }
 
+template <typename V>
+void launch_gather_pad(int nb, const double* u, const int* idx, const int* pos, V* out, cudaStream_t st) {
+  note_launch();
+  k_gather_pad<V><<<grid_for(nb), kBlock, 0, st>>>(nb, u, idx, pos, out);
+  TMB_CUDA(cudaGetLastError());
+}
+
+template <typename V>
+void launch_bem_gemv_tiles(int ntiles, const GemvTile* tiles, int rows_per_tile, const V* B, const V* x, double* y,
+                           cudaStream_t st) {
+  if (ntiles == 0) return;
+  note_launch();
+  if (rows_per_tile == 4) k_gemv_tiles<V, 4><<<grid_for(32LL * ntiles), kBlock, 0, st>>>(ntiles, tiles, B, x, y);
+  else k_gemv_tiles<V, 1><<<grid_for(32LL * ntiles), kBlock, 0, st>>>(ntiles, tiles, B, x, y);
+  TMB_CUDA(cudaGetLastError());
+}
+
+template <typename V>
+void launch_bem_gemm(int nbc, int ncomp, const V* B, const V* X, int xs, double* Y, int num_sms, cudaStream_t st) {
+  const int mt = (nbc + 63) / 64, ct = (ncomp + 63) / 64;
+  // split K until there are about four CTAs per SM
+  int split = 1;
+  while (split < 16 && mt * ct * split < 4 * num_sms && nbc / (split * 2) >= 256) split *= 2;
+  const int kchunk = ((nbc + split - 1) / split + 31) / 32 * 32;
+  split = (nbc + kchunk - 1) / kchunk;
+  if (split > 1) TMB_CUDA(cudaMemsetAsync(Y, 0, sizeof(double) * size_t(nbc) * ncomp, st));
+  note_launch();
+  k_bem_gemm<V><<<dim3(mt, ct, split), 256, 0, st>>>(nbc, ncomp, bem_ld(nbc), B, X, xs, Y, kchunk);
+  TMB_CUDA(cudaGetLastError());
+}
+
 void launch_dirichlet_values(int n, const int* bindex, const double* u2b, double* b, cudaStream_t st) {
   note_launch();
   k_dirichlet_values<<<grid_for(n), kBlock, 0, st>>>(n, bindex, u2b, b);
@@ -126,6 +272,14 @@ void launch_dirichlet_values(int n, const int* bindex, const double* u2b, double
 template void launch_bem_gemv<double>(int, const double*, const double*, double*, cudaStream_t);
 template void launch_bem_gemv<float>(int, const float*, const float*, double*, cudaStream_t);
 template void launch_gather<double>(int, const double*, const int*, double*, cudaStream_t);
+template void launch_gather_pad<double>(int, const double*, const int*, const int*, double*, cudaStream_t);
+template void launch_gather_pad<float>(int, const double*, const int*, const int*, float*, cudaStream_t);
+template void launch_bem_gemv_tiles<double>(int, const GemvTile*, int, const double*, const double*, double*,
+                                            cudaStream_t);
+template void launch_bem_gemv_tiles<float>(int, const GemvTile*, int, const float*, const float*, double*,
+                                           cudaStream_t);
+template void launch_bem_gemm<double>(int, int, const double*, const double*, int, double*, int, cudaStream_t);
+template void launch_bem_gemm<float>(int, int, const float*, const float*, int, double*, int, cudaStream_t);
 template void launch_gather<float>(int, const double*, const int*, float*, cudaStream_t);
 
 }  // namespace tmb

@@ -14,6 +14,7 @@
 // restatement used as the test oracle.
 #include <cmath>
 
+#include "lindholm_accurate.cuh"
 #include "tmb_dev.cuh"
 
 namespace tmb {
@@ -78,8 +79,9 @@ __device__ void lindholm(const double* x0, const double (*p)[3], double area, co
   }
 }
 
-// One CTA per row; row accumulated in shared memory (small Nb) or in global memory.
-template <bool SHARED_ROW>
+// One CTA per row; row accumulated in shared memory (small Nb) or in global memory.  ACCURATE
+// selects the far-field-accurate weights of lindholm_accurate.cuh instead of the reference form.
+template <bool SHARED_ROW, bool ACCURATE>
 __global__ void __launch_bounds__(kBlock) k_bem_assemble(int nb, int ntri, const double* __restrict__ bxyz,
                                                          const int* __restrict__ tri, const double* __restrict__ area,
                                                          const double* __restrict__ nrm,
@@ -103,7 +105,8 @@ __global__ void __launch_bounds__(kBlock) k_bem_assemble(int nb, int ntri, const
       p[2][d] = bxyz[3 * c + d];
     }
     double L[3];
-    lindholm(x0, p, area[t], nrm + 3 * t, L);
+    if (ACCURATE) lindholm_accurate(x0, p, area[t], nrm + 3 * t, L);
+    else lindholm(x0, p, area[t], nrm + 3 * t, L);
     if (SHARED_ROW) {
       atomicAdd(&srow[a], L[0]);
       atomicAdd(&srow[b], L[1]);
@@ -122,19 +125,60 @@ __global__ void __launch_bounds__(kBlock) k_bem_assemble(int nb, int ntri, const
   if (threadIdx.x == 0) out[row] = solid[row] / (4.0 * kPi) - 1.0;
 }
 
+// Dense tiles of the hierarchical matrix straight from the boundary mesh, with the same
+// arithmetic as the dense assembly: entry (i, j) of a tile sums the weight of position j over
+// the triangles touching j that do not contain i; the diagonal is Omega / (4 pi) - 1.
+__global__ void __launch_bounds__(kBlock) k_h_near_mesh(const HBlockDev* __restrict__ blk, HSource g,
+                                                        double* __restrict__ d64, float* __restrict__ d32) {
+  const HBlockDev b = blk[blockIdx.x];
+  const int mn = b.m * b.n;
+  for (int t = threadIdx.x; t < mn; t += blockDim.x) {
+    const int i = b.rb + t % b.m, j = b.cb + t / b.m;  // column-major tile
+    double v = 0.0;
+    if (i == j) {
+      v = g.solid[i] / (4.0 * kPi) - 1.0;
+    } else {
+      const double x0[3] = {g.xp[3 * i], g.xp[3 * i + 1], g.xp[3 * i + 2]};
+      for (int k = g.adj_ptr[j]; k < g.adj_ptr[j + 1]; ++k) {
+        const int2 a = g.adj[k];
+        const int* vt = g.tri + 3 * a.x;
+        if (vt[0] == i || vt[1] == i || vt[2] == i) continue;
+        double p[3][3];
+        for (int q = 0; q < 3; ++q)
+          for (int d = 0; d < 3; ++d) p[q][d] = g.xp[3 * vt[q] + d];
+        double L[3];
+        lindholm(x0, p, g.tarea[a.x], g.tnrm + 3 * a.x, L);
+        v += L[a.y];
+      }
+    }
+    d64[b.off + t] = v;
+    d32[b.off + t] = static_cast<float>(v);
+  }
+}
+
 }  // namespace
 
+void launch_h_near_mesh(int nblk, const HBlockDev* blk, const HSource& src, double* d64, float* d32,
+                        cudaStream_t st) {
+  if (nblk == 0) return;
+  note_launch();
+  k_h_near_mesh<<<nblk, kBlock, 0, st>>>(blk, src, d64, d32);
+  TMB_CUDA(cudaGetLastError());
+}
+
 void launch_bem_assemble(int nb, int ntri, const double* bxyz, const int* tri, const double* area,
-                         const double* nrm, const double* solid, double* B, cudaStream_t st) {
+                         const double* nrm, const double* solid, double* B, bool accurate, cudaStream_t st) {
   note_launch();
   const size_t ld = bem_ld(nb);
   const size_t smem = size_t(nb) * sizeof(double);
   if (smem <= 200 * 1024) {
-    TMB_CUDA(cudaFuncSetAttribute(k_bem_assemble<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    k_bem_assemble<true><<<nb, kBlock, smem, st>>>(nb, ntri, bxyz, tri, area, nrm, solid, B, ld);
+    auto k = accurate ? k_bem_assemble<true, true> : k_bem_assemble<true, false>;
+    TMB_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    k<<<nb, kBlock, smem, st>>>(nb, ntri, bxyz, tri, area, nrm, solid, B, ld);
   } else {
     TMB_CUDA(cudaMemsetAsync(B, 0, sizeof(double) * ld * nb, st));
-    k_bem_assemble<false><<<nb, kBlock, 0, st>>>(nb, ntri, bxyz, tri, area, nrm, solid, B, ld);
+    auto k = accurate ? k_bem_assemble<false, true> : k_bem_assemble<false, false>;
+    k<<<nb, kBlock, 0, st>>>(nb, ntri, bxyz, tri, area, nrm, solid, B, ld);
   }
   TMB_CUDA(cudaGetLastError());
 }

@@ -36,10 +36,12 @@ __device__ __forceinline__ double ld(const V* p, int k) {
   return static_cast<double>(__ldg(p + k));
 }
 
-template <typename V, bool UNI, bool DMI>
+// DMI: 0 none, 1 bulk (tetmag), 2 interfacial (no tetmag counterpart; see the epilogue).
+template <typename V, bool UNI, int DMI>
 __global__ void __launch_bounds__(kBlock) k_local_field(SellView s, const V* __restrict__ K,
                                                         const V* __restrict__ tg0, const V* __restrict__ tg1,
-                                                        const V* __restrict__ tg2, LocalFieldArgs a) {
+                                                        const V* __restrict__ tg2, const V* __restrict__ gr0,
+                                                        const V* __restrict__ gr1, LocalFieldArgs a) {
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
   double torque = 0.0;
   if (row < a.n) {
@@ -60,7 +62,7 @@ __global__ void __launch_bounds__(kBlock) k_local_field(SellView s, const V* __r
       kx = fma(v, ax, kx);
       ky = fma(v, ay, ky);
       kz = fma(v, az, kz);
-      if (DMI) {
+      if (DMI == 1) {
         const double t0 = ld(tg0, k), t1 = ld(tg1, k), t2 = ld(tg2, k);
         cxy = fma(t0, ay, cxy);
         cxz = fma(t0, az, cxz);
@@ -68,6 +70,18 @@ __global__ void __launch_bounds__(kBlock) k_local_field(SellView s, const V* __r
         cyz = fma(t1, az, cyz);
         czx = fma(t2, ax, czx);
         czy = fma(t2, ay, czy);
+      }
+      if (DMI == 2) {
+        // grad_x, grad_y on m (cxz = gx mz, cyz = gy mz, czx = gx mx + gy my) and the transposes
+        // through tGrad = (V grad)^T on D m (cxy = tgx D mz, cyx = tgy D mz, czy = tgx D mx + tgy D my)
+        const double g0 = ld(gr0, k), g1 = ld(gr1, k), t0 = ld(tg0, k), t1 = ld(tg1, k);
+        const double dj = __ldg(a.idm_d + j);
+        cxz = fma(g0, az, cxz);
+        cyz = fma(g1, az, cyz);
+        czx = fma(g0, ax, fma(g1, ay, czx));
+        cxy = fma(t0, dj * az, cxy);
+        cyx = fma(t1, dj * az, cyx);
+        czy = fma(t0, dj * ax, fma(t1, dj * ay, czy));
       }
     }
     const double m0 = mx[row], m1 = my[row], m2 = mz[row];
@@ -80,7 +94,15 @@ __global__ void __launch_bounds__(kBlock) k_local_field(SellView s, const V* __r
       H1 = fma(f, e1, H1);
       H2 = fma(f, e2, H2);
     }
-    if (DMI) {
+    if (DMI == 2) {
+      // interfacial DMI, E = sum_i V_i D_i [m_z div m - (m . grad) m_z]_i with the nodal gradient
+      // operators; H = -(1/V) dE/dm (exact gradient of the discrete energy), divided by Js
+      const double da = a.idm_a[row], db = a.idm_b[row];  // D_i / Js_i, 1 / (V_i Js_i)
+      H0 += da * cxz - db * cxy;
+      H1 += da * cyz - db * cyx;
+      H2 += db * czy - da * czx;
+    }
+    if (DMI == 1) {
       // curl m with tGrad' = -tGrad (main/EffFieldCalc.cpp:43, 280-298)
       const double c0 = -(cyz - czy), c1 = -(czx - cxz), c2 = -(cxy - cyx);
       const double ar = a.area[row];
@@ -236,15 +258,23 @@ void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 void note_launches(long long k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 
 template <typename V>
-void launch_local_field(const SellView& s, const V* K, const V* tg0, const V* tg1, const V* tg2,
-                        const LocalFieldArgs& a, cudaStream_t st) {
+void launch_local_field(const SellView& s, const V* K, const V* tg0, const V* tg1, const V* tg2, const V* gr0,
+                        const V* gr1, const LocalFieldArgs& a, cudaStream_t st) {
   note_launch();
   const int g = grid_for(a.n);
-  const bool uni = a.ku2 != nullptr, dmi = a.dmi_s != nullptr;
-  if (uni && dmi) k_local_field<V, true, true><<<g, kBlock, 0, st>>>(s, K, tg0, tg1, tg2, a);
-  else if (uni) k_local_field<V, true, false><<<g, kBlock, 0, st>>>(s, K, tg0, tg1, tg2, a);
-  else if (dmi) k_local_field<V, false, true><<<g, kBlock, 0, st>>>(s, K, tg0, tg1, tg2, a);
-  else k_local_field<V, false, false><<<g, kBlock, 0, st>>>(s, K, tg0, tg1, tg2, a);
+  const bool uni = a.ku2 != nullptr;
+  const int dmi = a.idm_a ? 2 : (a.dmi_s ? 1 : 0);
+#define TMB_LF(U, D) k_local_field<V, U, D><<<g, kBlock, 0, st>>>(s, K, tg0, tg1, tg2, gr0, gr1, a)
+  if (uni) {
+    if (dmi == 2) TMB_LF(true, 2);
+    else if (dmi == 1) TMB_LF(true, 1);
+    else TMB_LF(true, 0);
+  } else {
+    if (dmi == 2) TMB_LF(false, 2);
+    else if (dmi == 1) TMB_LF(false, 1);
+    else TMB_LF(false, 0);
+  }
+#undef TMB_LF
   TMB_CUDA(cudaGetLastError());
 }
 
@@ -302,8 +332,8 @@ void launch_add(int n, const double* a, const double* b, double* out, cudaStream
 }
 
 #define TMB_INST(V)                                                                                         \
-  template void launch_local_field<V>(const SellView&, const V*, const V*, const V*, const V*,             \
-                                      const LocalFieldArgs&, cudaStream_t);                                \
+  template void launch_local_field<V>(const SellView&, const V*, const V*, const V*, const V*, const V*,   \
+                                      const V*, const LocalFieldArgs&, cudaStream_t);                      \
   template void launch_divergence<V>(const SellView&, const V*, const V*, const V*, const double*,         \
                                      const double*, double, double*, cudaStream_t);                        \
   template void launch_gradient<V>(const SellView&, const V*, const V*, const V*, const double*,           \

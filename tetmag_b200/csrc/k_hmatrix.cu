@@ -3,20 +3,22 @@
 // Replaces the H2Lib path of tetmag's demag chain (DemagField::h2MVP ->
 // H2_mvp_sub, main/DemagField.cpp:139-142, main/h2interface.c:77-95).  The
 // partition comes from hmatrix.cpp; here:
-//   * inadmissible leaf blocks are copied out of the device-assembled dense FP64
-//     matrix into column-major dense tiles (FP64 and FP32 copies);
+//   * inadmissible leaf blocks become column-major dense tiles (FP64 and FP32 copies),
+//     copied out of the dense FP64 matrix or assembled from the boundary mesh;
 //   * every admissible block is compressed by adaptive cross approximation with
 //     partial pivoting (Bebendorf, Numer. Math. 86 (2000) 565-589), one CTA per
-//     block, reading entries of the dense matrix.  Two ranks are recorded: the
+//     block, reading entries of the dense matrix or evaluating them from the mesh
+//     (accurate far-field Lindholm weights, below).  Two ranks are recorded: the
 //     first k meeting the loose tolerance (stored in FP32 for the mixed path) and
 //     the first k meeting the tight tolerance (stored in FP64 for the plain path).
 //     After convergence a few unvisited rows are checked and, if any still has a
 //     significant residual, the approximation continues from that row;
 //   * the matvec y = H x works in the cluster-tree order: dense tiles by leaf row
-//     cluster (plain stores), then t_b = V_b^T x_sigma per low-rank block, then
-//     y_tau += U_b t_b with one atomic add per row and row cluster.
+//     cluster (plain stores), then per row cluster tau, for each of its low-rank blocks,
+//     t_b = V_b^T x_sigma and y_tau += U_b t_b, with one atomic add per row and row cluster.
 #include <cmath>
 
+#include "lindholm_accurate.cuh"
 #include "tmb_dev.cuh"
 
 namespace tmb {
@@ -67,17 +69,49 @@ __device__ void cta_argmax(double v, int idx, double* shv, int* shi, double& bes
     }
 }
 
-__device__ __forceinline__ double entry(const double* B, size_t ld, const int* perm, int gi, int gj) {
-  return B[size_t(perm[gi]) * ld + perm[gj]];
-}
+// Entry (i, j) of the dense matrix in cluster order.
+struct DenseEntry {
+  const double* B;
+  size_t ld;
+  const int* perm;
+  __device__ __forceinline__ double operator()(int i, int j) const { return B[size_t(perm[i]) * ld + perm[j]]; }
+};
 
-__global__ void k_h_near_gather(const HBlockDev* __restrict__ blk, const double* __restrict__ B, size_t ld,
-                                const int* __restrict__ perm, double* __restrict__ d64, float* __restrict__ d32) {
+// Entry (i, j), i != j, evaluated from the boundary mesh: the weights of position j over the
+// triangles that touch j and do not contain i (preproc/BEMprocessing.cpp:375-411), in the
+// far-field-accurate arithmetic of lindholm_accurate.cuh.
+struct MeshEntry {
+  const double* xp;
+  const int* tri;
+  const double* tarea;
+  const double* tnrm;
+  const int* adj_ptr;
+  const int2* adj;
+  __device__ double operator()(int i, int j) const {
+    const double x0[3] = {xp[3 * i], xp[3 * i + 1], xp[3 * i + 2]};
+    double s = 0.0;
+    for (int k = adj_ptr[j]; k < adj_ptr[j + 1]; ++k) {
+      const int2 a = adj[k];
+      const int* v = tri + 3 * a.x;
+      if (v[0] == i || v[1] == i || v[2] == i) continue;
+      double p[3][3];
+      for (int q = 0; q < 3; ++q)
+        for (int d = 0; d < 3; ++d) p[q][d] = xp[3 * v[q] + d];
+      double L[3];
+      lindholm_accurate(x0, p, tarea[a.x], tnrm + 3 * a.x, L);
+      s += (a.y == 0) ? L[0] : (a.y == 1) ? L[1] : L[2];
+    }
+    return s;
+  }
+};
+
+__global__ void k_h_near_gather(const HBlockDev* __restrict__ blk, DenseEntry E, double* __restrict__ d64,
+                                float* __restrict__ d32) {
   const HBlockDev b = blk[blockIdx.x];
   const int mn = b.m * b.n;
   for (int t = threadIdx.x; t < mn; t += blockDim.x) {
     const int i = t % b.m, j = t / b.m;  // column-major tile
-    const double v = entry(B, ld, perm, b.rb + i, b.cb + j);
+    const double v = E(b.rb + i, b.cb + j);
     d64[b.off + t] = v;
     d32[b.off + t] = static_cast<float>(v);
   }
@@ -85,9 +119,9 @@ __global__ void k_h_near_gather(const HBlockDev* __restrict__ blk, const double*
 
 // Largest residual |A_ij - sum_l U_il V_lj| over unvisited rows (a strided sample of about
 // 128 rows on larger blocks); CTA-wide, every thread receives value and row.
-__device__ void aca_verify(const HBlockDev& b, const double* __restrict__ B, size_t ld, const int* __restrict__ perm,
-                           const double* U, const double* V, const unsigned char* usd, int k, int pass, double* shv,
-                           int* shi, double& val, int& row) {
+template <typename E>
+__device__ void aca_verify(const HBlockDev& b, const E& entry, const double* U, const double* V,
+                           const unsigned char* usd, int k, int pass, double* shv, int* shi, double& val, int& row) {
   const int m = b.m, n = b.n;
   const int stride = (m > 128) ? (m + 127) / 128 : 1;
   const int offset = pass % stride;
@@ -98,7 +132,7 @@ __device__ void aca_verify(const HBlockDev& b, const double* __restrict__ B, siz
     const int i = offset + int(t / n) * stride;
     const int j = int(t % n);
     if (usd[i]) continue;
-    double r = entry(B, ld, perm, b.rb + i, b.cb + j);
+    double r = entry(b.rb + i, b.cb + j);
     for (int l = 0; l < k; ++l) r -= U[size_t(l) * m + i] * V[size_t(l) * n + j];
     if (fabs(r) > best || (fabs(r) == best && i < bi)) {
       best = fabs(r);
@@ -113,8 +147,8 @@ __device__ void aca_verify(const HBlockDev& b, const double* __restrict__ B, siz
 // only bottom-face columns and vice versa), so each time the loose tolerance is reached the
 // residual is checked on the unvisited rows, and the approximation restarts from the worst
 // one if it is significant; the same check guards the final (tight) stop.
-__global__ void __launch_bounds__(256) k_h_aca(const HBlockDev* __restrict__ blk, const double* __restrict__ B,
-                                               size_t ld, const int* __restrict__ perm, double* __restrict__ Us,
+template <typename E>
+__global__ void __launch_bounds__(256) k_h_aca(const HBlockDev* __restrict__ blk, E entry, double* __restrict__ Us,
                                                double* __restrict__ Vs, unsigned char* __restrict__ used, int kmax,
                                                double eps_tight, double eps_loose, int* __restrict__ out_rank) {
   constexpr int kMaxPasses = 8;
@@ -147,7 +181,7 @@ __global__ void __launch_bounds__(256) k_h_aca(const HBlockDev* __restrict__ blk
     double lb = 0.0;
     int lj = 0x7fffffff;
     for (int j = threadIdx.x; j < n; j += blockDim.x) {
-      double r = entry(B, ld, perm, b.rb + istar, b.cb + j);
+      double r = entry(b.rb + istar, b.cb + j);
       for (int l = 0; l < k; ++l) r -= U[size_t(l) * m + istar] * V[size_t(l) * n + j];
       v[j] = r;
       if (fabs(r) > lb || (fabs(r) == lb && j < lj)) {
@@ -175,7 +209,7 @@ __global__ void __launch_bounds__(256) k_h_aca(const HBlockDev* __restrict__ blk
       double li_best = 0.0, uu_part = 0.0, vv_part = 0.0;
       int li = 0x7fffffff;
       for (int i = threadIdx.x; i < m; i += blockDim.x) {
-        double c = entry(B, ld, perm, b.rb + i, b.cb + jstar);
+        double c = entry(b.rb + i, b.cb + jstar);
         for (int l = 0; l < k; ++l) c -= V[size_t(l) * n + jstar] * U[size_t(l) * m + i];
         u[i] = c;
         uu_part += c * c;
@@ -215,7 +249,7 @@ __global__ void __launch_bounds__(256) k_h_aca(const HBlockDev* __restrict__ blk
       if (k_loose >= 0 && !verified && passes < kMaxPasses) {
         double val;
         int row;
-        aca_verify(b, B, ld, perm, U, V, usd, k, passes++, shv, shi, val, row);
+        aca_verify(b, entry, U, V, usd, k, passes++, shv, shi, val, row);
         if (row != 0x7fffffff && val > eps_loose * sqrt(fabs(norm2) / (double(m) * n))) {
           k_loose = k_tight = -1;  // a part of the block is still missing: restart there
           istar = row;
@@ -229,7 +263,7 @@ __global__ void __launch_bounds__(256) k_h_aca(const HBlockDev* __restrict__ blk
       if (passes >= kMaxPasses) break;
       double val;
       int row;
-      aca_verify(b, B, ld, perm, U, V, usd, k, passes++, shv, shi, val, row);
+      aca_verify(b, entry, U, V, usd, k, passes++, shv, shi, val, row);
       if (row == 0x7fffffff || val <= eps_tight * sqrt(fabs(norm2) / (double(m) * n))) break;
       nxt = row;
     }
@@ -290,42 +324,127 @@ __global__ void __launch_bounds__(256) k_h_near(const HNearRow* __restrict__ row
   }
 }
 
-// t_b = V_b^T x_sigma for every low-rank block: one warp per term (block, column l).
+// Low-rank part, one CTA per work item (a run of admissible blocks b = (tau, sigma) of one row
+// cluster tau, bounded in size so the CTAs are balanced): for each block t = V_b^T x_sigma (a
+// warp per term, t in shared memory), then y_tau += U_b t accumulated in registers, each thread
+// owning a row and a slice of the terms; one atomic add per row at the end.  Every U and V entry
+// is read once per matvec.
 template <typename T>
-__global__ void __launch_bounds__(256) k_h_far_vt(const int2* __restrict__ terms, long long nterms,
-                                                  const HBlockDev* __restrict__ blk, const long long* __restrict__ voff,
-                                                  const long long* __restrict__ toff, const T* __restrict__ V,
-                                                  const T* __restrict__ xp, double* __restrict__ t) {
-  const long long w = (static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (w >= nterms) return;
-  const int2 bl = terms[w];
-  const HBlockDev b = blk[bl.x];
-  const T* v = V + voff[bl.x] + (long long)bl.y * b.n;
-  double a = 0.0;
-  for (int j = lane; j < b.n; j += 32) a = fma(double(v[j]), double(xp[b.cb + j]), a);
-  a = warp_sum_d(a);
-  if (lane == 0) t[toff[bl.x] + bl.y] = a;
-}
-
-// y_tau += sum_b U_b t_b over the low-rank blocks of each row cluster; one thread per row.
-template <typename T>
-__global__ void __launch_bounds__(256) k_h_far_u(const HFarGroup* __restrict__ grp, const HBlockDev* __restrict__ blk,
-                                                 const int* __restrict__ rank, const long long* __restrict__ uoff,
-                                                 const long long* __restrict__ toff, const T* __restrict__ U,
-                                                 const double* __restrict__ t, double* __restrict__ y) {
-  const HFarGroup g = grp[blockIdx.y];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= g.m) return;
-  double a = 0.0;
+__global__ void __launch_bounds__(256) k_h_far(const HFarGroup* __restrict__ grp, const HBlockDev* __restrict__ blk,
+                                               const int* __restrict__ rank, const long long* __restrict__ uoff,
+                                               const long long* __restrict__ voff, const T* __restrict__ U,
+                                               const T* __restrict__ V, const T* __restrict__ xp,
+                                               double* __restrict__ y) {
+  __shared__ double ts[128];
+  __shared__ double red[256];
+  const HFarGroup g = grp[blockIdx.x];
+  const int m = g.m;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // m <= 256: thread -> (row, term slice); m > 256: thread -> rows threadIdx.x + 256 r
+  const int slices = m >= 256 ? 1 : 256 / m;
+  const int row = m >= 256 ? threadIdx.x : threadIdx.x % m;
+  const int slice = m >= 256 ? 0 : threadIdx.x / m;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
   for (int q = g.first; q < g.last; ++q) {
     const int k = rank[q];
-    const T* u = U + uoff[q] + i;
-    const double* tb = t + toff[q];
-    const int m = blk[q].m;
-    for (int l = 0; l < k; ++l) a = fma(double(u[(long long)l * m]), tb[l], a);
+    if (k == 0) continue;
+    const int n = blk[q].n, cb = blk[q].cb;
+    const T* v = V + voff[q];
+    for (int l = warp; l < k; l += 8) {
+      const T* vl = v + (long long)l * n;
+      double a = 0.0;
+#pragma unroll 4
+      for (int j = lane; j < n; j += 32) a = fma(double(vl[j]), double(xp[cb + j]), a);
+      a = warp_sum_d(a);
+      if (lane == 0) ts[l] = a;
+    }
+    __syncthreads();
+    const T* u = U + uoff[q];
+    if (m >= 256) {
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int i = row + 256 * r;
+        if (i < m) {
+#pragma unroll 4
+          for (int l = 0; l < k; ++l) acc[r] = fma(double(u[(long long)l * m + i]), ts[l], acc[r]);
+        }
+      }
+    } else if (slice < slices) {
+#pragma unroll 4
+      for (int l = slice; l < k; l += slices) acc[0] = fma(double(u[(long long)l * m + row]), ts[l], acc[0]);
+    }
+    __syncthreads();
   }
-  if (a != 0.0) atomicAdd(&y[g.rb + i], a);
+  if (m >= 256) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int i = row + 256 * r;
+      if (i < m) atomicAdd(&y[g.rb + i], acc[r]);
+    }
+  } else {
+    red[threadIdx.x] = acc[0];
+    __syncthreads();
+    if (threadIdx.x < m) {
+      double s = 0.0;
+      for (int sl = 0; sl < slices; ++sl) s += red[sl * m + threadIdx.x];
+      atomicAdd(&y[g.rb + threadIdx.x], s);
+    }
+  }
+}
+
+// Deterministic probe value in [-1, 1) for position j (cluster order): splitmix64 of j.
+__device__ __forceinline__ double probe_value(long long j) {
+  unsigned long long z = static_cast<unsigned long long>(j) + 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  z ^= z >> 31;
+  return double(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+
+// Accuracy of every low-rank block against the entries it was built from, one CTA per block:
+// y = A_b x_sigma for the probe vector x, then out = {|y|^2, |y - U64 V64^T x|^2, |y - U32 V32^T x|^2}.
+template <typename E>
+__global__ void __launch_bounds__(256) k_h_verify(const HBlockDev* __restrict__ blk, E entry, const int* __restrict__ rk64,
+                                                  const long long* __restrict__ uo64, const long long* __restrict__ vo64,
+                                                  const double* __restrict__ U64, const double* __restrict__ V64,
+                                                  const int* __restrict__ rk32, const long long* __restrict__ uo32,
+                                                  const long long* __restrict__ vo32, const float* __restrict__ U32,
+                                                  const float* __restrict__ V32, double* __restrict__ out) {
+  __shared__ double t64[128], t32[128], shd[32];
+  const HBlockDev b = blk[blockIdx.x];
+  const int k64 = rk64[blockIdx.x], k32 = rk32[blockIdx.x];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int l = warp; l < k64 + k32; l += 8) {
+    const bool f = l < k64;
+    const int q = f ? l : l - k64;
+    double a = 0.0;
+    for (int j = lane; j < b.n; j += 32) {
+      const double v = f ? V64[vo64[blockIdx.x] + (long long)q * b.n + j] : double(V32[vo32[blockIdx.x] + (long long)q * b.n + j]);
+      a = fma(v, probe_value(b.cb + j), a);
+    }
+    a = warp_sum_d(a);
+    if (lane == 0) (f ? t64 : t32)[q] = a;
+  }
+  __syncthreads();
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int i = threadIdx.x; i < b.m; i += blockDim.x) {
+    double y = 0.0;
+    for (int j = 0; j < b.n; ++j) y = fma(entry(b.rb + i, b.cb + j), probe_value(b.cb + j), y);
+    double y64 = 0.0, y32 = 0.0;
+    for (int l = 0; l < k64; ++l) y64 = fma(U64[uo64[blockIdx.x] + (long long)l * b.m + i], t64[l], y64);
+    for (int l = 0; l < k32; ++l) y32 = fma(double(U32[uo32[blockIdx.x] + (long long)l * b.m + i]), t32[l], y32);
+    s0 += y * y;
+    s1 += (y - y64) * (y - y64);
+    s2 += (y - y32) * (y - y32);
+  }
+  s0 = cta_sum(s0, shd);
+  s1 = cta_sum(s1, shd);
+  s2 = cta_sum(s2, shd);
+  if (threadIdx.x == 0) {
+    out[3 * blockIdx.x] = s0;
+    out[3 * blockIdx.x + 1] = s1;
+    out[3 * blockIdx.x + 2] = s2;
+  }
 }
 
 // Dirichlet load from the H-matrix result: b[node] = y[pos[node]] on the boundary, 0 inside.
@@ -336,22 +455,43 @@ __global__ void k_h_dirichlet(int n, const int* __restrict__ pos, const double* 
   b[i] = (p >= 0) ? y[p] : 0.0;
 }
 
+DenseEntry dense_entry(const HSource& s) { return DenseEntry{s.B, s.ld, s.perm}; }
+MeshEntry mesh_entry(const HSource& s) { return MeshEntry{s.xp, s.tri, s.tarea, s.tnrm, s.adj_ptr, s.adj}; }
+
 }  // namespace
 
-void launch_h_near_gather(int nblk, const HBlockDev* blk, const double* B, size_t ld, const int* perm, double* d64,
-                          float* d32, cudaStream_t st) {
+void launch_h_near_gather(int nblk, const HBlockDev* blk, const HSource& src, double* d64, float* d32,
+                          cudaStream_t st) {
   if (nblk == 0) return;
+  if (!src.B) throw std::runtime_error("dense tile gather without a dense matrix");
   note_launch();
-  k_h_near_gather<<<nblk, 256, 0, st>>>(blk, B, ld, perm, d64, d32);
+  k_h_near_gather<<<nblk, 256, 0, st>>>(blk, dense_entry(src), d64, d32);
   TMB_CUDA(cudaGetLastError());
 }
 
-void launch_h_aca(int nblk, const HBlockDev* blk, const double* B, size_t ld, const int* perm, double* Us,
-                  double* Vs, unsigned char* used, int kmax, double eps_tight, double eps_loose, int* out_rank,
-                  cudaStream_t st) {
+void launch_h_aca(int nblk, const HBlockDev* blk, const HSource& src, double* Us, double* Vs, unsigned char* used,
+                  int kmax, double eps_tight, double eps_loose, int* out_rank, cudaStream_t st) {
   if (nblk == 0) return;
   note_launch();
-  k_h_aca<<<nblk, 256, 0, st>>>(blk, B, ld, perm, Us, Vs, used, kmax, eps_tight, eps_loose, out_rank);
+  if (src.B)
+    k_h_aca<<<nblk, 256, 0, st>>>(blk, dense_entry(src), Us, Vs, used, kmax, eps_tight, eps_loose, out_rank);
+  else
+    k_h_aca<<<nblk, 256, 0, st>>>(blk, mesh_entry(src), Us, Vs, used, kmax, eps_tight, eps_loose, out_rank);
+  TMB_CUDA(cudaGetLastError());
+}
+
+void launch_h_verify(int nblk, const HBlockDev* blk, const HSource& src, const int* rk64, const long long* uo64,
+                     const long long* vo64, const double* U64, const double* V64, const int* rk32,
+                     const long long* uo32, const long long* vo32, const float* U32, const float* V32, double* out,
+                     cudaStream_t st) {
+  if (nblk == 0) return;
+  note_launch();
+  if (src.B)
+    k_h_verify<<<nblk, 256, 0, st>>>(blk, dense_entry(src), rk64, uo64, vo64, U64, V64, rk32, uo32, vo32, U32, V32,
+                                     out);
+  else
+    k_h_verify<<<nblk, 256, 0, st>>>(blk, mesh_entry(src), rk64, uo64, vo64, U64, V64, rk32, uo32, vo32, U32, V32,
+                                     out);
   TMB_CUDA(cudaGetLastError());
 }
 
@@ -365,19 +505,15 @@ void launch_h_compact(int nblk, const HBlockDev* blk, const double* Us, const do
 }
 
 template <typename T>
-void launch_h_matvec(const HMatView<T>& H, const double* u, double* y, double* t, T* xp, const int* pos, int n,
-                     double* bdir, cudaStream_t st) {
+void launch_h_matvec(const HMatView<T>& H, const double* u, double* y, T* xp, const int* pos, int n, double* bdir,
+                     cudaStream_t st) {
   note_launch();
   k_h_gather<T><<<grid_for(H.nb), kBlock, 0, st>>>(H.nb, u, H.gidx, xp);
   note_launch();
   k_h_near<T><<<H.nrows, 256, 0, st>>>(H.near_rows, H.near, H.D, xp, y);
   if (H.nterms > 0) {
     note_launch();
-    k_h_far_vt<T><<<int((H.nterms * 32 + 255) / 256), 256, 0, st>>>(H.terms, H.nterms, H.far, H.voff, H.toff, H.V,
-                                                                      xp, t);
-    dim3 grid(unsigned((H.max_group_m + 255) / 256), unsigned(H.ngroups));
-    note_launch();
-    k_h_far_u<T><<<grid, 256, 0, st>>>(H.groups, H.far, H.rank, H.uoff, H.toff, H.U, t, y);
+    k_h_far<T><<<H.ngroups, 256, 0, st>>>(H.groups, H.far, H.rank, H.uoff, H.voff, H.U, H.V, xp, y);
   }
   note_launch();
   k_h_dirichlet<<<grid_for(n), kBlock, 0, st>>>(n, pos, y, bdir);
@@ -388,9 +524,9 @@ template void launch_h_compact<double>(int, const HBlockDev*, const double*, con
                                        const long long*, const int*, double*, double*, cudaStream_t);
 template void launch_h_compact<float>(int, const HBlockDev*, const double*, const double*, const long long*,
                                       const long long*, const int*, float*, float*, cudaStream_t);
-template void launch_h_matvec<double>(const HMatView<double>&, const double*, double*, double*, double*, const int*,
-                                      int, double*, cudaStream_t);
-template void launch_h_matvec<float>(const HMatView<float>&, const double*, double*, double*, float*, const int*, int,
+template void launch_h_matvec<double>(const HMatView<double>&, const double*, double*, double*, const int*, int,
+                                      double*, cudaStream_t);
+template void launch_h_matvec<float>(const HMatView<float>&, const double*, double*, float*, const int*, int,
                                      double*, cudaStream_t);
 
 }  // namespace tmb

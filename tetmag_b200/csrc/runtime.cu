@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <numeric>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -319,32 +320,62 @@ struct Ctx {
   double alpha = 1.0, gamma = kGamma0;
   int precession = 1;
   DevArray<double> js, xc, ku2, kax, dmi_s, hext, hdem, hfix;
+  // DMI form: 0 bulk (tetmag), 1 interfacial (no tetmag counterpart)
+  int dmi_kind = 0;
+  DevArray<double> idm_d, idm_a, idm_b;
+  std::vector<double> hD, hij;          // D and 1/Js per node, kept to switch the DMI form
+  void upload_dmi();
+  LocalFieldArgs local_args(const double* m, double* ydot, double* hout, unsigned long long* tq) const;
+  void launch_local(const LocalFieldArgs& a, cudaStream_t st);
   // BEM
   DevArray<double> Bd;
   DevArray<float> Bf;
   bool has_bem = false;
+  // Disjoint components (batched instances): nodes [coff[c], coff[c+1]), boundary indices
+  // [cboff[c], cboff[c+1]).  Each component has its own BEM block in Bd / Bf (row-major,
+  // leading dimension bem_ld(nb_c)); with shared_bem the components are replicas of one mesh and
+  // share one block, and the boundary matvec is one GEMM over the replicas.
+  std::vector<int> coff, cboff;
+  bool shared_bem = false;
+  int num_sms = 148;
+  DevArray<int> xpos;                   // boundary index -> padded position of its component
+  DevArray<double> xpad64;
+  DevArray<float> xpad32;
+  int xstride = 0;                      // shared: padded length of one replica's boundary
+  DevArray<GemvTile> tiles;
+  int ntiles = 0, tile_rows = 1;
+  double bem_entries = 0.0;             // matrix entries streamed by one boundary matvec
+  int ncomp() const { return int(coff.size()) - 1; }
+  void set_components(int nc, const int* off, bool shared);
+  void plan_components();
   // hierarchical BEM (tmb_bem_compress)
   struct HMat {
     bool built = false;
-    int nnear = 0, nfar = 0, nrows = 0, ngroups = 0, max_group_m = 0, failed = 0;
+    int nnear = 0, nfar = 0, nrows = 0, ngroups[2] = {0, 0}, failed = 0;
     long long terms[2] = {0, 0};          // [0] FP64 (tight), [1] FP32 (loose)
     double bytes[2] = {0, 0}, ms = 0.0;
     int max_rank = 0;
-    DevArray<int> gidx, pos;
+    DevArray<int> gidx, pos, perm;
+    std::vector<int> ranks;               // per low-rank block: tight rank, loose rank, status
     DevArray<HBlockDev> nearb, farb;
     DevArray<HNearRow> rows;
-    DevArray<HFarGroup> groups;
-    DevArray<double> D64, U64, V64, t64, y, xp64;
+    DevArray<HFarGroup> groups[2];        // per precision, largest work first
+    DevArray<double> D64, U64, V64, y, xp64;
     DevArray<float> D32, U32, V32, xp32;
     DevArray<int> rank[2];
-    DevArray<long long> uoff[2], voff[2], toff[2];
-    DevArray<int2> term[2];
-    DevArray<double> t32;
+    DevArray<long long> uoff[2], voff[2];
+    // boundary geometry in cluster order when the matrix was built from the mesh
+    bool from_mesh = false;
+    int ntri = 0;
+    DevArray<double> gx, garea, gnrm, gsolid;
+    DevArray<int> gtri, gadj_ptr;
+    DevArray<int2> gadj;
   } H;
+  HSource h_source() const;
   int bem_mode = 0;  // 0 dense, 1 hierarchical
   void h_compress(const double* bxyz, const double* bnrm, int leaf, double eta, double eps_mixed, double eps_fp64,
-                  int kmax,
-                  bool keep_dense);
+                  int kmax, bool keep_dense, const MeshHost* mesh = nullptr);
+  void h_verify(double* block_out, double* out);
   template <typename T>
   HMatView<T> h_view(int which) const;
   // demag
@@ -363,6 +394,7 @@ struct Ctx {
     TMB_CUDA(cudaSetDevice(dev));
     TMB_CUDA(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
     stream = own;
+    TMB_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
     TMB_CUDA(cudaMallocHost(&bits_h, 4 * sizeof(unsigned long long)));
     bits.alloc(4);
   }
@@ -655,7 +687,100 @@ void Ctx::set_operators(int nx, const int* ptr, const int* col, const double* K_
   bem_mode = 0;
   neu.reset();
   dir.reset();
+  coff = {0, n};
+  cboff = {0, nb};
+  shared_bem = false;
   sync();
+}
+
+// Declares the mesh a disjoint union of nc components (batched instances of tetmag's
+// single-mesh problem): the operators must not couple components; each component keeps its
+// own pinned Neumann node (node N_c / 2 of the component, DemagField.cpp:80) and its own BEM
+// block.  shared: the components are identical copies (same operators and boundary numbering,
+// checked) that share one BEM block.
+void Ctx::set_components(int nc, const int* off, bool shared) {
+  require_mesh();
+  if (nc < 1 || !off || off[0] != 0 || off[nc] != n) throw Error(TMB_ERR_ARG, "tmb_set_components: bad offsets");
+  for (int c = 0; c < nc; ++c)
+    if (off[c + 1] <= off[c]) throw Error(TMB_ERR_ARG, "tmb_set_components: offsets must increase");
+  std::vector<int> co(off, off + nc + 1), cb(nc + 1, 0);
+  for (int c = 0; c < nc; ++c) {
+    for (int i = co[c]; i < co[c + 1]; ++i)
+      for (int q = hptr[i]; q < hptr[i + 1]; ++q)
+        if (hcol[q] < co[c] || hcol[q] >= co[c + 1])
+          throw Error(TMB_ERR_ARG, "tmb_set_components: the operators couple two components");
+    cb[c] = int(std::lower_bound(hbnodes.begin(), hbnodes.end(), co[c]) - hbnodes.begin());
+  }
+  cb[nc] = nb;
+  for (int c = 0; c < nc; ++c)
+    if (cb[c + 1] - cb[c] < 3) throw Error(TMB_ERR_ARG, "tmb_set_components: a component has no boundary");
+  if (shared) {
+    const int n0 = co[1], nb0 = cb[1];
+    for (int c = 1; c < nc; ++c) {
+      if (co[c + 1] - co[c] != n0 || cb[c + 1] - cb[c] != nb0)
+        throw Error(TMB_ERR_ARG, "tmb_set_components: shared BEM needs components of equal size");
+      for (int k = 0; k < nb0; ++k)
+        if (hbnodes[cb[c] + k] - co[c] != hbnodes[k])
+          throw Error(TMB_ERR_ARG, "tmb_set_components: shared BEM needs the same boundary numbering");
+      for (int i = 0; i < n0; ++i) {
+        const int a = hptr[i], b = hptr[co[c] + i];
+        if (hptr[i + 1] - a != hptr[co[c] + i + 1] - b)
+          throw Error(TMB_ERR_ARG, "tmb_set_components: shared BEM needs identical operators");
+        for (int q = 0; q < hptr[i + 1] - a; ++q)
+          if (hcol[b + q] - co[c] != hcol[a + q] || hK[b + q] != hK[a + q])
+            throw Error(TMB_ERR_ARG, "tmb_set_components: shared BEM needs identical operators");
+      }
+    }
+  }
+  coff = co;
+  cboff = cb;
+  shared_bem = shared && nc > 1;
+  has_bem = false;
+  Bd.reset();
+  Bf.reset();
+  H = HMat{};
+  bem_mode = 0;
+  neu.reset();
+  dir.reset();
+}
+
+// Padded boundary layout and matvec plan of the components (after the blocks are assembled).
+void Ctx::plan_components() {
+  const int nc = ncomp();
+  std::vector<int> pos(nb);
+  bem_entries = 0.0;
+  if (shared_bem) {
+    const int nbc = cboff[1];
+    xstride = int(bem_ld(nbc));
+    for (int c = 0; c < nc; ++c)
+      for (int k = 0; k < nbc; ++k) pos[cboff[c] + k] = c * xstride + k;
+    xpad64.alloc(size_t(xstride) * nc);
+    xpad32.alloc(size_t(xstride) * nc);
+    bem_entries = double(nbc) * nbc;
+    ntiles = 0;
+  } else {
+    // tiles of up to 4 rows when the components are large enough to fill the GPU that way
+    tile_rows = (nb >= 16384 && double(nb) / nc >= 256.0) ? 4 : 1;
+    std::vector<GemvTile> t;
+    long long boff = 0;
+    int xo = 0;
+    for (int c = 0; c < nc; ++c) {
+      const int nbc = cboff[c + 1] - cboff[c], ld = int(bem_ld(nbc));
+      for (int k = 0; k < nbc; ++k) pos[cboff[c] + k] = xo + k;
+      for (int r = 0; r < nbc; r += tile_rows)
+        t.push_back(GemvTile{boff + (long long)r * ld, xo, cboff[c] + r, nbc, std::min(tile_rows, nbc - r), ld, 0});
+      boff += (long long)nbc * ld;
+      xo += ld;
+      bem_entries += double(nbc) * nbc;
+    }
+    ntiles = int(t.size());
+    tiles.upload(t, stream);
+    xpad64.alloc(size_t(xo));
+    xpad32.alloc(size_t(xo));
+  }
+  xpad64.zero(stream);
+  xpad32.zero(stream);
+  xpos.upload(pos, stream);
 }
 
 void Ctx::set_material(const double* Js, const double* A, const double* Ku, const double* axis, const double* D,
@@ -683,6 +808,10 @@ void Ctx::set_material(const double* Js, const double* A, const double* Ku, cons
   xc.upload(vxc, st);
   ku2.upload(vku, st);
   dmi_s.upload(vdm, st);
+  hD.assign(n, 0.0);
+  if (D) hD.assign(D, D + n);
+  hij = ij;
+  upload_dmi();
   if (axis) {
     kax.upload(axis, size_t(3) * n, st);
   } else {
@@ -702,9 +831,9 @@ void Ctx::ensure_demag() {
   if (neu && dir) return;
   // Neumann matrix: K with row N/2 replaced by the unit row (DemagField.cpp:80, 204-220)
   // Dirichlet matrix: K with boundary rows replaced by unit rows (FEMprocessing.cpp:329-369)
-  const int k = n / 2;
-  std::vector<char> isb(n, 0);
+  std::vector<char> isb(n, 0), pin(n, 0);
   for (int b : hbnodes) isb[b] = 1;
+  for (int c = 0; c < ncomp(); ++c) pin[coff[c] + (coff[c + 1] - coff[c]) / 2] = 1;  // N/2 per component
   auto build = [&](auto pinned) {
     std::vector<int> p(n + 1, 0), c;
     std::vector<double> v;
@@ -729,7 +858,7 @@ void Ctx::ensure_demag() {
     s->compute();
     return s;
   };
-  neu = build([&](int i) { return i == k; });
+  neu = build([&](int i) { return pin[i] != 0; });
   dir = build([&](int i) { return isb[i] != 0; });
   for (auto* a : {&rhs, &u1, &u2, &bdir}) a->alloc(n);
   u1b.alloc(nb);
@@ -757,9 +886,23 @@ void Ctx::demag(const double* m) {
     // hierarchical matvec in cluster order, scattered straight into the Dirichlet load
     const int w = f64 ? 0 : 1;
     prof.begin(3, st, H.bytes[w] + B * (sv + 8 + 8));
-    if (f64) launch_h_matvec<double>(h_view<double>(0), neu->x.p, H.y.p, H.t64.p, H.xp64.p, H.pos.p, n, bdir.p, st);
-    else launch_h_matvec<float>(h_view<float>(1), neu->x.p, H.y.p, H.t32.p, H.xp32.p, H.pos.p, n, bdir.p, st);
+    if (f64) launch_h_matvec<double>(h_view<double>(0), neu->x.p, H.y.p, H.xp64.p, H.pos.p, n, bdir.p, st);
+    else launch_h_matvec<float>(h_view<float>(1), neu->x.p, H.y.p, H.xp32.p, H.pos.p, n, bdir.p, st);
     prof.end(st);
+  } else if (ncomp() > 1) {
+    // batched components: padded gather, then one GEMM (shared matrix) or per-component matvecs
+    if (f64) launch_gather_pad<double>(nb, neu->x.p, bnodes.p, xpos.p, xpad64.p, st);
+    else launch_gather_pad<float>(nb, neu->x.p, bnodes.p, xpos.p, xpad32.p, st);
+    prof.begin(3, st, bem_entries * sv + B * (sv + 8));
+    if (shared_bem) {
+      if (f64) launch_bem_gemm<double>(cboff[1], ncomp(), Bd.p, xpad64.p, xstride, u2b.p, num_sms, st);
+      else launch_bem_gemm<float>(cboff[1], ncomp(), Bf.p, xpad32.p, xstride, u2b.p, num_sms, st);
+    } else {
+      if (f64) launch_bem_gemv_tiles<double>(ntiles, tiles.p, tile_rows, Bd.p, xpad64.p, u2b.p, st);
+      else launch_bem_gemv_tiles<float>(ntiles, tiles.p, tile_rows, Bf.p, xpad32.p, u2b.p, st);
+    }
+    prof.end(st);
+    launch_dirichlet_values(n, bindex.p, u2b.p, bdir.p, st);
   } else {
     if (f64) launch_gather<double>(nb, neu->x.p, bnodes.p, u1b.p, st);
     else launch_gather<float>(nb, neu->x.p, bnodes.p, u1bf.p, st);
@@ -788,8 +931,7 @@ HMatView<T> Ctx::h_view(int w) const {
   HMatView<T> v;
   v.nb = nb;
   v.nrows = H.nrows;
-  v.ngroups = H.ngroups;
-  v.max_group_m = H.max_group_m;
+  v.ngroups = H.ngroups[w];
   v.nterms = H.terms[w];
   v.gidx = H.gidx.p;
   v.near_rows = H.rows.p;
@@ -798,9 +940,7 @@ HMatView<T> Ctx::h_view(int w) const {
   v.rank = H.rank[w].p;
   v.uoff = H.uoff[w].p;
   v.voff = H.voff[w].p;
-  v.toff = H.toff[w].p;
-  v.terms = H.term[w].p;
-  v.groups = H.groups.p;
+  v.groups = H.groups[w].p;
   if constexpr (sizeof(T) == 8) {
     v.D = H.D64.p;
     v.U = H.U64.p;
@@ -815,13 +955,17 @@ HMatView<T> Ctx::h_view(int w) const {
 
 // Compresses the device-assembled dense FP64 BEM matrix into the hierarchical form:
 // dense leaf tiles plus ACA low-rank blocks, FP64 terms to eps_fp64 and FP32 terms to eps_mixed.
+// With `mesh` the entries come from the boundary mesh instead (no dense matrix needed): dense
+// tiles with the reference arithmetic, low-rank blocks from the accurate far-field weights.
 void Ctx::h_compress(const double* bxyz, const double* bnrm, int leaf, double eta, double eps_mixed,
-                     double eps_fp64, int kmax, bool keep_dense) {
+                     double eps_fp64, int kmax, bool keep_dense, const MeshHost* mesh) {
   require_mesh();
-  if (!has_bem || !Bd.p) throw Error(TMB_ERR_STATE, "tmb_bem_compress: needs the dense FP64 BEM matrix on the device");
+  if (ncomp() > 1) throw Error(TMB_ERR_STATE, "hierarchical BEM: one component per context");
+  if (!mesh && (!has_bem || !Bd.p))
+    throw Error(TMB_ERR_STATE, "tmb_bem_compress: needs the dense FP64 BEM matrix on the device");
   if (leaf < 2 || leaf > 32) throw Error(TMB_ERR_ARG, "tmb_bem_compress: leaf size must be in [2, 32]");
-  if (!(eta > 0.0) || !(eps_mixed > 0.0) || !(eps_fp64 > 0.0) || kmax < 1)
-    throw Error(TMB_ERR_ARG, "tmb_bem_compress: bad eta / tolerance / rank cap");
+  if (!(eta > 0.0) || !(eps_mixed > 0.0) || !(eps_fp64 > 0.0) || kmax < 1 || kmax > 128)
+    throw Error(TMB_ERR_ARG, "tmb_bem_compress: bad eta / tolerance / rank cap (1..128)");
   const auto t0 = std::chrono::steady_clock::now();
   cudaStream_t st = stream;
   HPartition P;
@@ -863,13 +1007,10 @@ void Ctx::h_compress(const double* bxyz, const double* bnrm, int leaf, double et
     }
     farb.push_back(b);
   }
-  if (groups.size() > 65535) throw Error(TMB_ERR_ARG, "tmb_bem_compress: too many row clusters for one launch");
   H = HMat{};
   H.nnear = int(nearb.size());
   H.nfar = int(farb.size());
   H.nrows = int(rows.size());
-  H.ngroups = int(groups.size());
-  for (const auto& g : groups) H.max_group_m = std::max(H.max_group_m, g.m);
   std::vector<int> gidx(nb), pos(n, -1);
   for (int i = 0; i < nb; ++i) {
     gidx[i] = hbnodes[P.perm[i]];
@@ -877,16 +1018,46 @@ void Ctx::h_compress(const double* bxyz, const double* bnrm, int leaf, double et
   }
   H.gidx.upload(gidx, st);
   H.pos.upload(pos, st);
-  DevArray<int> dperm;
-  dperm.upload(P.perm, st);
+  H.perm.upload(P.perm, st);
+  if (mesh) {
+    // geometry in cluster positions: coordinates, triangles, position -> touching triangles
+    const BoundaryData& Bm = mesh->bnd;
+    const int nt = int(Bm.tri_tet.size());
+    std::vector<int> at(nb);
+    for (int i = 0; i < nb; ++i) at[P.perm[i]] = i;
+    std::vector<double> gx(size_t(3) * nb), gs(nb);
+    for (int i = 0; i < nb; ++i) {
+      for (int d = 0; d < 3; ++d) gx[size_t(3) * i + d] = mesh->xyz[size_t(3) * Bm.bnodes[P.perm[i]] + d];
+      gs[i] = Bm.solid_angle[P.perm[i]];
+    }
+    std::vector<int> gt(size_t(3) * nt), aptr(nb + 1, 0);
+    for (size_t k = 0; k < gt.size(); ++k) {
+      gt[k] = at[Bm.bindex[Bm.tri[k]]];
+      ++aptr[gt[k] + 1];
+    }
+    for (int i = 0; i < nb; ++i) aptr[i + 1] += aptr[i];
+    std::vector<int2> adj(gt.size());
+    std::vector<int> fill(aptr.begin(), aptr.end() - 1);
+    for (int t = 0; t < nt; ++t)
+      for (int k = 0; k < 3; ++k) adj[fill[gt[size_t(3) * t + k]]++] = make_int2(t, k);
+    H.from_mesh = true;
+    H.ntri = nt;
+    H.gx.upload(gx, st);
+    H.gsolid.upload(gs, st);
+    H.gtri.upload(gt, st);
+    H.gadj_ptr.upload(aptr, st);
+    H.gadj.upload(adj, st);
+    H.garea.upload(Bm.tri_area, st);
+    H.gnrm.upload(Bm.tri_normal, st);
+  }
+  const HSource src = h_source();
   H.nearb.upload(nearb, st);
   H.rows.upload(rows, st);
   H.farb.upload(farb, st);
-  H.groups.upload(groups, st);
-  const size_t ld = bem_ld(nb);
   H.D64.alloc(size_t(doff));
   H.D32.alloc(size_t(doff));
-  launch_h_near_gather(H.nnear, H.nearb.p, Bd.p, ld, dperm.p, H.D64.p, H.D32.p, st);
+  if (mesh) launch_h_near_mesh(H.nnear, H.nearb.p, src, H.D64.p, H.D32.p, st);
+  else launch_h_near_gather(H.nnear, H.nearb.p, src, H.D64.p, H.D32.p, st);
   // adaptive cross approximation of every admissible block
   std::vector<int> ranks(size_t(3) * H.nfar, 0);
   if (H.nfar > 0) {
@@ -897,40 +1068,66 @@ void Ctx::h_compress(const double* bxyz, const double* bnrm, int leaf, double et
     Vs.alloc(size_t(vs));
     used.alloc(size_t(fl));
     dr.alloc(size_t(3) * H.nfar);
-    launch_h_aca(H.nfar, H.farb.p, Bd.p, ld, dperm.p, Us.p, Vs.p, used.p, kmax, eps_fp64, eps_mixed, dr.p, st);
+    launch_h_aca(H.nfar, H.farb.p, src, Us.p, Vs.p, used.p, kmax, eps_fp64, eps_mixed, dr.p, st);
     TMB_CUDA(cudaMemcpyAsync(ranks.data(), dr.p, sizeof(int) * ranks.size(), cudaMemcpyDeviceToHost, st));
     sync();
     for (int w = 0; w < 2; ++w) {
       std::vector<int> rk(H.nfar);
-      std::vector<long long> uo(H.nfar), vo(H.nfar), to(H.nfar);
-      std::vector<int2> terms;
+      std::vector<long long> uo(H.nfar), vo(H.nfar);
       long long su = 0, sv = 0, stt = 0;
       for (int q = 0; q < H.nfar; ++q) {
         rk[q] = ranks[size_t(3) * q + w];
         uo[q] = su;
         vo[q] = sv;
-        to[q] = stt;
         su += (long long)rk[q] * farb[q].m;
         sv += (long long)rk[q] * farb[q].n;
         stt += rk[q];
-        for (int l = 0; l < rk[q]; ++l) terms.push_back(make_int2(q, l));
       }
+      // matvec work items: the admissible blocks of one row cluster, cut into runs of about
+      // wmax U + V entries (about 64 items per SM), largest first
+      double total = 0.0;
+      for (int q = 0; q < H.nfar; ++q) total += double(rk[q]) * (farb[q].m + farb[q].n);
+      const double wmax = std::max(4096.0, total / (64.0 * num_sms));
+      std::vector<HFarGroup> items;
+      std::vector<double> work;
+      for (const HFarGroup& g : groups) {
+        HFarGroup it{g.rb, g.m, g.first, g.first};
+        double wk = 0.0;
+        for (int q = g.first; q < g.last; ++q) {
+          const double wq = double(rk[q]) * (farb[q].m + farb[q].n);
+          if (wk > 0.0 && wk + wq > wmax) {
+            items.push_back(it);
+            work.push_back(wk);
+            it.first = q;
+            wk = 0.0;
+          }
+          it.last = q + 1;
+          wk += wq;
+        }
+        if (wk > 0.0) {
+          items.push_back(it);
+          work.push_back(wk);
+        }
+      }
+      std::vector<int> order(items.size());
+      std::iota(order.begin(), order.end(), 0);
+      std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
+      std::vector<HFarGroup> sorted;
+      for (int g : order) sorted.push_back(items[g]);
+      H.ngroups[w] = int(sorted.size());
+      H.groups[w].upload(sorted, st);
       H.terms[w] = stt;
       H.rank[w].upload(rk, st);
       H.uoff[w].upload(uo, st);
       H.voff[w].upload(vo, st);
-      H.toff[w].upload(to, st);
-      H.term[w].upload(terms, st);
       if (w == 0) {
         H.U64.alloc(size_t(std::max(su, 1LL)));
         H.V64.alloc(size_t(std::max(sv, 1LL)));
-        H.t64.alloc(size_t(std::max(stt, 1LL)));
         launch_h_compact<double>(H.nfar, H.farb.p, Us.p, Vs.p, H.uoff[0].p, H.voff[0].p, H.rank[0].p, H.U64.p,
                                  H.V64.p, st);
       } else {
         H.U32.alloc(size_t(std::max(su, 1LL)));
         H.V32.alloc(size_t(std::max(sv, 1LL)));
-        H.t32.alloc(size_t(std::max(stt, 1LL)));
         launch_h_compact<float>(H.nfar, H.farb.p, Us.p, Vs.p, H.uoff[1].p, H.voff[1].p, H.rank[1].p, H.U32.p,
                                 H.V32.p, st);
       }
@@ -941,18 +1138,18 @@ void Ctx::h_compress(const double* bxyz, const double* bnrm, int leaf, double et
   } else {
     H.bytes[0] = double(doff) * 8;
     H.bytes[1] = double(doff) * 4;
-    H.t64.alloc(1);
-    H.t32.alloc(1);
   }
   for (int q = 0; q < H.nfar; ++q) {
     H.failed += ranks[size_t(3) * q + 2] != 0;
     H.max_rank = std::max(H.max_rank, ranks[size_t(3) * q]);
   }
+  H.ranks = ranks;
   H.y.alloc(nb);
   H.xp64.alloc(nb);
   H.xp32.alloc(nb);
   H.built = true;
   bem_mode = 1;
+  if (mesh) has_bem = true;
   if (!keep_dense) {
     Bd.reset();
     Bf.reset();
@@ -960,9 +1157,89 @@ void Ctx::h_compress(const double* bxyz, const double* bnrm, int leaf, double et
   H.ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
-void Ctx::local(const double* m, double* ydot, double* hout, unsigned long long* tq) {
-  require_mesh();
-  require_material();
+HSource Ctx::h_source() const {
+  HSource s;
+  s.nb = nb;
+  s.perm = H.perm.p;
+  if (H.from_mesh) {
+    s.ntri = H.ntri;
+    s.xp = H.gx.p;
+    s.tri = H.gtri.p;
+    s.tarea = H.garea.p;
+    s.tnrm = H.gnrm.p;
+    s.adj_ptr = H.gadj_ptr.p;
+    s.adj = H.gadj.p;
+    s.solid = H.gsolid.p;
+  } else {
+    s.B = Bd.p;
+    s.ld = bem_ld(nb);
+  }
+  return s;
+}
+
+// Accuracy of the low-rank blocks against the entries they were built from (the dense FP64
+// matrix, which must still be on the device, or the boundary mesh) for a fixed probe vector.  out = {relative error of the far part, FP64 terms; same,
+// FP32 terms; worst block relative error, FP64; same, FP32}; block_out (may be null) holds per
+// block {|A x|, |A x - U64 V64^T x|, |A x - U32 V32^T x|, tight rank, loose rank, rank-cap status}.
+void Ctx::h_verify(double* block_out, double* out) {
+  if (!H.built) throw Error(TMB_ERR_STATE, "tmb_bem_verify: no hierarchical matrix");
+  if (!H.from_mesh && !Bd.p)
+    throw Error(TMB_ERR_STATE, "tmb_bem_verify: the dense FP64 matrix was released (keep_dense = 0)");
+  for (int q = 0; q < 4; ++q) out[q] = 0.0;
+  if (H.nfar == 0) return;
+  DevArray<double> e;
+  e.alloc(size_t(3) * H.nfar);
+  launch_h_verify(H.nfar, H.farb.p, h_source(), H.rank[0].p, H.uoff[0].p, H.voff[0].p, H.U64.p,
+                  H.V64.p, H.rank[1].p, H.uoff[1].p, H.voff[1].p, H.U32.p, H.V32.p, e.p, stream);
+  std::vector<double> h(size_t(3) * H.nfar);
+  TMB_CUDA(cudaMemcpyAsync(h.data(), e.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, stream));
+  sync();
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int q = 0; q < H.nfar; ++q) {
+    const double a = h[3 * q], b = h[3 * q + 1], c = h[3 * q + 2];
+    s0 += a;
+    s1 += b;
+    s2 += c;
+    if (a > 0.0) {
+      out[2] = std::max(out[2], std::sqrt(b / a));
+      out[3] = std::max(out[3], std::sqrt(c / a));
+    }
+    if (block_out) {
+      double* o = block_out + size_t(6) * q;
+      o[0] = std::sqrt(a);
+      o[1] = std::sqrt(b);
+      o[2] = std::sqrt(c);
+      o[3] = H.ranks[size_t(3) * q];
+      o[4] = H.ranks[size_t(3) * q + 1];
+      o[5] = H.ranks[size_t(3) * q + 2];
+    }
+  }
+  if (s0 > 0.0) {
+    out[0] = std::sqrt(s1 / s0);
+    out[1] = std::sqrt(s2 / s0);
+  }
+}
+
+// Interfacial-DMI per-node factors (D_j, D_i / Js_i, 1 / (V_i Js_i)) when that form is selected.
+void Ctx::upload_dmi() {
+  if (dmi_kind != 1 || !has_dmi) {
+    idm_d.reset();
+    idm_a.reset();
+    idm_b.reset();
+    return;
+  }
+  std::vector<double> a(n), b(n);
+  for (int i = 0; i < n; ++i) {
+    a[i] = hD[i] * hij[i];
+    b[i] = hij[i] / hvol[i];
+  }
+  idm_d.upload(hD, stream);
+  idm_a.upload(a, stream);
+  idm_b.upload(b, stream);
+  sync();
+}
+
+LocalFieldArgs Ctx::local_args(const double* m, double* ydot, double* hout, unsigned long long* tq) const {
   LocalFieldArgs a;
   a.n = n;
   a.m = m;
@@ -970,22 +1247,40 @@ void Ctx::local(const double* m, double* ydot, double* hout, unsigned long long*
   a.xc = xc.p;
   a.ku2 = has_uni ? ku2.p : nullptr;
   a.kax = kax.p;
-  a.dmi_s = has_dmi ? dmi_s.p : nullptr;
+  const bool idmi = has_dmi && dmi_kind == 1;
+  a.dmi_s = (has_dmi && !idmi) ? dmi_s.p : nullptr;
   a.area = area.p;
   a.nvn = nvn.p;
+  a.idm_d = idmi ? idm_d.p : nullptr;
+  a.idm_a = idmi ? idm_a.p : nullptr;
+  a.idm_b = idmi ? idm_b.p : nullptr;
   a.alpha = alpha;
   a.precession = precession;
   a.ydot = ydot;
   a.hout = hout;
   a.torque_bits = tq;
+  return a;
+}
+
+void Ctx::launch_local(const LocalFieldArgs& a, cudaStream_t st) {
   const SellView S = pat.view();
+  if (precision == TMB_FP64)
+    launch_local_field<double>(S, K.p, tg[0].p, tg[1].p, tg[2].p, g[0].p, g[1].p, a, st);
+  else
+    launch_local_field<float>(S, Kf.p, tgf[0].p, tgf[1].p, tgf[2].p, gf[0].p, gf[1].p, a, st);
+}
+
+void Ctx::local(const double* m, double* ydot, double* hout, unsigned long long* tq) {
+  require_mesh();
+  require_material();
+  const LocalFieldArgs a = local_args(m, ydot, hout, tq);
   const double sv = precision == TMB_FP64 ? 8.0 : 4.0, z = double(hptr[n]), N = double(n);
   double bytes = z * (sv + 4) + N * 8 * (3 + 3 + 1) + (ydot ? N * 24 : 0.0) + (hout ? N * 24 : 0.0);
   if (a.ku2) bytes += N * 8 * 4;
   if (a.dmi_s) bytes += z * 3 * sv + N * 8 * 5;
+  if (a.idm_a) bytes += z * 4 * sv + N * 8 * 3;
   prof.begin(0, stream, bytes);
-  if (precision == TMB_FP64) launch_local_field<double>(S, K.p, tg[0].p, tg[1].p, tg[2].p, a, stream);
-  else launch_local_field<float>(S, Kf.p, tgf[0].p, tgf[1].p, tgf[2].p, a, stream);
+  launch_local(a, stream);
   prof.end(stream);
 }
 
@@ -1321,8 +1616,11 @@ int tmb_set_operators(tmb_ctx* ctx, int nx, int nnz, const int* rowptr, const in
   TMB_API_END
 }
 
-int tmb_bem_assemble(tmb_ctx* ctx, const tmb_mesh* mesh) {
+int tmb_bem_assemble(tmb_ctx* ctx, const tmb_mesh* mesh) { return tmb_bem_assemble_ex(ctx, mesh, 0); }
+
+int tmb_bem_assemble_ex(tmb_ctx* ctx, const tmb_mesh* mesh, int formula) {
   TMB_CHECK_ARG(ctx && mesh, "tmb_bem_assemble: null argument");
+  TMB_CHECK_ARG(formula == 0 || formula == 1, "tmb_bem_assemble_ex: formula is 0 (reference) or 1 (accurate)");
   TMB_API_BEGIN
   Ctx& c = *ctx->c;
   c.require_mesh();
@@ -1331,23 +1629,53 @@ int tmb_bem_assemble(tmb_ctx* ctx, const tmb_mesh* mesh) {
   const int nb = int(B.bnodes.size()), nt = int(B.tri_tet.size());
   if (nb != c.nb || M.nx != c.n) return fail(TMB_ERR_ARG, "tmb_bem_assemble: mesh differs from the context's");
   TMB_CUDA(cudaSetDevice(c.device));
-  std::vector<double> bxyz(size_t(3) * nb);
   for (int i = 0; i < nb; ++i)
-    for (int d = 0; d < 3; ++d) bxyz[size_t(3) * i + d] = M.xyz[size_t(3) * B.bnodes[i] + d];
-  std::vector<int> tri(size_t(3) * nt);
-  for (size_t k = 0; k < tri.size(); ++k) tri[k] = B.bindex[B.tri[k]];
-  DevArray<double> dx, da, dn, ds;
-  DevArray<int> dt;
-  dx.upload(bxyz, c.stream);
-  dt.upload(tri, c.stream);
-  da.upload(B.tri_area, c.stream);
-  dn.upload(B.tri_normal, c.stream);
-  ds.upload(B.solid_angle, c.stream);
-  const size_t ld = bem_ld(nb);
-  c.Bd.alloc(ld * nb);
-  launch_bem_assemble(nb, nt, dx.p, dt.p, da.p, dn.p, ds.p, c.Bd.p, c.stream);
-  c.Bf.alloc(ld * nb);
-  launch_to_float(c.Bd.p, c.Bf.p, ld * nb, c.stream);
+    if (B.bnodes[i] != c.hbnodes[i]) return fail(TMB_ERR_ARG, "tmb_bem_assemble: mesh differs from the context's");
+  // one block per component (one shared block for replicas), each assembled from its own
+  // boundary triangles in local boundary numbering
+  const int nc = c.ncomp(), nstore = c.shared_bem ? 1 : nc;
+  std::vector<long long> boff(nstore + 1, 0);
+  for (int k = 0; k < nstore; ++k) {
+    const int nbc = c.cboff[k + 1] - c.cboff[k];
+    boff[k + 1] = boff[k] + (long long)bem_ld(nbc) * nbc;
+  }
+  c.Bd.alloc(size_t(boff[nstore]));
+  std::vector<int> tcomp(nt);
+  for (int t = 0; t < nt; ++t) {
+    const int b0 = B.bindex[B.tri[size_t(3) * t]];
+    tcomp[t] = int(std::upper_bound(c.cboff.begin(), c.cboff.end(), b0) - c.cboff.begin()) - 1;
+  }
+  for (int k = 0; k < nstore; ++k) {
+    const int lo = c.cboff[k], nbc = c.cboff[k + 1] - lo;
+    std::vector<double> bxyz(size_t(3) * nbc), area, nrm, solid(B.solid_angle.begin() + lo,
+                                                                  B.solid_angle.begin() + lo + nbc);
+    for (int i = 0; i < nbc; ++i)
+      for (int d = 0; d < 3; ++d) bxyz[size_t(3) * i + d] = M.xyz[size_t(3) * B.bnodes[lo + i] + d];
+    std::vector<int> tri;
+    for (int t = 0; t < nt; ++t) {
+      if (tcomp[t] != k) continue;
+      for (int v = 0; v < 3; ++v) {
+        const int bi = B.bindex[B.tri[size_t(3) * t + v]] - lo;
+        if (bi < 0 || bi >= nbc) return fail(TMB_ERR_ARG, "tmb_bem_assemble: a boundary triangle spans components");
+        tri.push_back(bi);
+      }
+      area.push_back(B.tri_area[t]);
+      for (int d = 0; d < 3; ++d) nrm.push_back(B.tri_normal[size_t(3) * t + d]);
+    }
+    const int ntc = int(area.size());
+    DevArray<double> dx, da, dn, ds;
+    DevArray<int> dt;
+    dx.upload(bxyz, c.stream);
+    dt.upload(tri, c.stream);
+    da.upload(area, c.stream);
+    dn.upload(nrm, c.stream);
+    ds.upload(solid, c.stream);
+    launch_bem_assemble(nbc, ntc, dx.p, dt.p, da.p, dn.p, ds.p, c.Bd.p + boff[k], formula == 1, c.stream);
+    c.sync();
+  }
+  c.Bf.alloc(size_t(boff[nstore]));
+  launch_to_float(c.Bd.p, c.Bf.p, size_t(boff[nstore]), c.stream);
+  if (nc > 1) c.plan_components();
   c.sync();
   c.has_bem = true;
   c.H = Ctx::HMat{};
@@ -1357,12 +1685,21 @@ int tmb_bem_assemble(tmb_ctx* ctx, const tmb_mesh* mesh) {
   TMB_API_END
 }
 
+int tmb_set_components(tmb_ctx* ctx, int ncomp, const int* node_offsets, int shared_bem) {
+  TMB_CHECK_ARG(ctx && node_offsets && ncomp >= 1, "tmb_set_components: bad arguments");
+  TMB_API_BEGIN
+  TMB_CUDA(cudaSetDevice(ctx->c->device));
+  ctx->c->set_components(ncomp, node_offsets, shared_bem != 0);
+  TMB_API_END
+}
+
 int tmb_set_bem_dense(tmb_ctx* ctx, int nb, const double* B_colmajor) {
   TMB_CHECK_ARG(ctx && B_colmajor, "tmb_set_bem_dense: null argument");
   TMB_API_BEGIN
   Ctx& c = *ctx->c;
   c.require_mesh();
   if (nb != c.nb) return fail(TMB_ERR_ARG, "tmb_set_bem_dense: nb differs from the boundary node count");
+  if (c.ncomp() > 1) return fail(TMB_ERR_STATE, "tmb_set_bem_dense: the context has several components");
   TMB_CUDA(cudaSetDevice(c.device));
   const size_t ld = bem_ld(nb);
   std::vector<double> rowmajor(ld * nb, 0.0);
@@ -1384,7 +1721,8 @@ int tmb_get_bem_dense(tmb_ctx* ctx, double* B_colmajor) {
   TMB_CHECK_ARG(ctx && B_colmajor, "tmb_get_bem_dense: null argument");
   TMB_API_BEGIN
   Ctx& c = *ctx->c;
-  if (!c.has_bem) return fail(TMB_ERR_STATE, "no BEM matrix set");
+  if (!c.has_bem || !c.Bd.p) return fail(TMB_ERR_STATE, "no dense BEM matrix on the device");
+  if (c.ncomp() > 1) return fail(TMB_ERR_STATE, "tmb_get_bem_dense: the context has several components");
   const int nb = c.nb;
   const size_t ld = bem_ld(nb);
   std::vector<double> rowmajor(ld * nb);
@@ -1402,6 +1740,27 @@ int tmb_bem_compress(tmb_ctx* ctx, const double* bxyz, const double* bnormal, in
   Ctx& c = *ctx->c;
   TMB_CUDA(cudaSetDevice(c.device));
   c.h_compress(bxyz, bnormal, leaf, eta, eps_mixed, eps_fp64, kmax, keep_dense != 0);
+  TMB_API_END
+}
+
+int tmb_bem_build_h(tmb_ctx* ctx, const tmb_mesh* mesh, int leaf, double eta, double eps_mixed, double eps_fp64,
+                    int kmax) {
+  TMB_CHECK_ARG(ctx && mesh, "tmb_bem_build_h: null argument");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  c.require_mesh();
+  const MeshHost& M = mesh->m;
+  const BoundaryData& B = M.bnd;
+  const int nb = int(B.bnodes.size());
+  if (nb != c.nb || M.nx != c.n) return fail(TMB_ERR_ARG, "tmb_bem_build_h: mesh differs from the context's");
+  TMB_CUDA(cudaSetDevice(c.device));
+  std::vector<double> bxyz(size_t(3) * nb), bnrm(size_t(3) * nb);
+  for (int i = 0; i < nb; ++i)
+    for (int d = 0; d < 3; ++d) {
+      bxyz[size_t(3) * i + d] = M.xyz[size_t(3) * B.bnodes[i] + d];
+      bnrm[size_t(3) * i + d] = B.node_normal[size_t(3) * B.bnodes[i] + d];
+    }
+  c.h_compress(bxyz.data(), bnrm.data(), leaf, eta, eps_mixed, eps_fp64, kmax, true, &M);
   TMB_API_END
 }
 
@@ -1433,6 +1792,14 @@ int tmb_bem_info(tmb_ctx* ctx, double* out) {
   return TMB_OK;
 }
 
+int tmb_bem_verify(tmb_ctx* ctx, double* block_out, double* out) {
+  TMB_CHECK_ARG(ctx && out, "tmb_bem_verify: null argument");
+  TMB_API_BEGIN
+  TMB_CUDA(cudaSetDevice(ctx->c->device));
+  ctx->c->h_verify(block_out, out);
+  TMB_API_END
+}
+
 int tmb_set_material(tmb_ctx* ctx, const double* Js, const double* A, const double* Ku, const double* ku_axis,
                      const double* D, double alpha) {
   TMB_CHECK_ARG(ctx && Js && A, "tmb_set_material: Js and A are required");
@@ -1440,6 +1807,16 @@ int tmb_set_material(tmb_ctx* ctx, const double* Js, const double* A, const doub
   TMB_API_BEGIN
   TMB_CUDA(cudaSetDevice(ctx->c->device));
   ctx->c->set_material(Js, A, Ku, ku_axis, D, alpha);
+  TMB_API_END
+}
+
+int tmb_set_dmi_kind(tmb_ctx* ctx, int kind) {
+  TMB_CHECK_ARG(ctx && (kind == 0 || kind == 1), "tmb_set_dmi_kind: kind is 0 (bulk) or 1 (interfacial)");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  TMB_CUDA(cudaSetDevice(c.device));
+  c.dmi_kind = kind;
+  if (c.has_material) c.upload_dmi();
   TMB_API_END
 }
 
@@ -1614,24 +1991,7 @@ int tmb_llg_rhs_noalloc(tmb_ctx* ctx, double t, const double* y, double* ydot) {
   double* const od = stage + 3 * kNoAllocMaxNodes;   // ydot, 3N
   const size_t n3 = size_t(3) * c.n;
   TMB_CUDA(cudaMemcpyAsync(yd, y, n3 * sizeof(double), cudaMemcpyHostToDevice, c.stream));
-  LocalFieldArgs a;
-  a.n = c.n;
-  a.m = yd;
-  a.hfix = c.hfix.p;
-  a.xc = c.xc.p;
-  a.ku2 = c.has_uni ? c.ku2.p : nullptr;
-  a.kax = c.kax.p;
-  a.dmi_s = c.has_dmi ? c.dmi_s.p : nullptr;
-  a.area = c.area.p;
-  a.nvn = c.nvn.p;
-  a.alpha = c.alpha;
-  a.precession = c.precession;
-  a.ydot = od;
-  a.hout = nullptr;
-  a.torque_bits = nullptr;
-  const SellView S = c.pat.view();
-  if (c.precision == TMB_FP64) launch_local_field<double>(S, c.K.p, c.tg[0].p, c.tg[1].p, c.tg[2].p, a, c.stream);
-  else launch_local_field<float>(S, c.Kf.p, c.tgf[0].p, c.tgf[1].p, c.tgf[2].p, a, c.stream);
+  c.launch_local(c.local_args(yd, od, nullptr, nullptr), c.stream);
   TMB_CUDA(cudaMemcpyAsync(ydot, od, n3 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
   c.sync();
   TMB_API_END

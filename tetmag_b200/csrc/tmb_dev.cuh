@@ -64,6 +64,9 @@ struct LocalFieldArgs {
   const double* dmi_s;      // N  D_i / V_i / Js_i, null without bulk DMI
   const double* area;       // N  boundary node area (bulk DMI surface term)
   const double* nvn;        // 3N SoA node normal
+  const double* idm_d;      // N  D_j (interfacial DMI), null otherwise
+  const double* idm_a;      // N  D_i / Js_i (interfacial DMI), null otherwise
+  const double* idm_b;      // N  1 / (V_i Js_i) (interfacial DMI)
   double alpha;
   int precession;
   double* ydot;             // 3N out, may be null
@@ -72,8 +75,8 @@ struct LocalFieldArgs {
 };
 
 template <typename V>
-void launch_local_field(const SellView& s, const V* K, const V* tg0, const V* tg1, const V* tg2,
-                        const LocalFieldArgs& a, cudaStream_t st);
+void launch_local_field(const SellView& s, const V* K, const V* tg0, const V* tg1, const V* tg2, const V* gr0,
+                        const V* gr1, const LocalFieldArgs& a, cudaStream_t st);
 
 template <typename V>
 void launch_divergence(const SellView& s, const V* tg0, const V* tg1, const V* tg2, const double* m,
@@ -133,7 +136,7 @@ void launch_cg_dir_spmv(const SellView& s, const V* val, const double* z, const 
 
 // --- launchers (k_bem.cu) ----------------------------------------------------------------
 void launch_bem_assemble(int nb, int ntri, const double* bxyz, const int* tri, const double* area,
-                         const double* nrm, const double* solid, double* B, cudaStream_t st);
+                         const double* nrm, const double* solid, double* B, bool accurate, cudaStream_t st);
 void launch_to_float(const double* src, float* dst, size_t n, cudaStream_t st);
 template <typename V>
 void launch_bem_gemv(int nb, const V* B, const V* xb, double* u2b, cudaStream_t st);
@@ -141,6 +144,21 @@ void launch_dirichlet_values(int n, const int* bindex, const double* u2b, double
 template <typename V>
 void launch_gather(int nb, const double* u, const int* idx, V* out, cudaStream_t st);
 size_t bem_ld(int nb);  // leading dimension (elements) of the row-major device BEM matrix
+// Batched instances (disjoint components of one context): boundary values gathered to 32-element
+// aligned per-component offsets, then one matvec per component's own matrix (tiles of up to R
+// rows of one component: rows b + r * ld, columns x[0..ncols), results y[r]) or, for replicas
+// sharing one matrix, one GEMM.
+struct GemvTile {
+  long long b;
+  int x, y, ncols, nrows, ld, pad_;
+};
+template <typename V>
+void launch_gather_pad(int nb, const double* u, const int* idx, const int* pos, V* out, cudaStream_t st);
+template <typename V>
+void launch_bem_gemv_tiles(int ntiles, const GemvTile* tiles, int rows_per_tile, const V* B, const V* x, double* y,
+                           cudaStream_t st);
+template <typename V>
+void launch_bem_gemm(int nbc, int ncomp, const V* B, const V* X, int xs, double* Y, int num_sms, cudaStream_t st);
 
 // --- hierarchical BEM matrix (k_hmatrix.cu) ---------------------------------------------
 struct HBlockDev {
@@ -157,7 +175,7 @@ struct HFarGroup {
 };
 template <typename T>
 struct HMatView {
-  int nb = 0, nrows = 0, ngroups = 0, max_group_m = 0;
+  int nb = 0, nrows = 0, ngroups = 0;
   long long nterms = 0;
   const int* gidx = nullptr;             // permuted position -> boundary node (mesh numbering)
   const HNearRow* near_rows = nullptr;
@@ -167,24 +185,47 @@ struct HMatView {
   const int* rank = nullptr;
   const long long* uoff = nullptr;       // compact U offsets (column-major m x rank)
   const long long* voff = nullptr;       // compact V offsets (column-major n x rank)
-  const long long* toff = nullptr;       // offsets of t_b in the term buffer
-  const int2* terms = nullptr;           // (block, column) per low-rank term
   const T* U = nullptr;
   const T* V = nullptr;
-  const HFarGroup* groups = nullptr;
+  const HFarGroup* groups = nullptr;     // row clusters, largest work first
 };
-void launch_h_near_gather(int nblk, const HBlockDev* blk, const double* B, size_t ld, const int* perm, double* d64,
-                          float* d32, cudaStream_t st);
-void launch_h_aca(int nblk, const HBlockDev* blk, const double* B, size_t ld, const int* perm, double* Us,
-                  double* Vs, unsigned char* used, int kmax, double eps_tight, double eps_loose, int* out_rank,
-                  cudaStream_t st);
+// Where the entries of the boundary matrix (in cluster order) come from: the dense FP64
+// matrix (B != nullptr, row-major with leading dimension ld, rows/columns perm[i]) or the
+// boundary mesh itself, evaluated on the fly.
+struct HSource {
+  const double* B = nullptr;
+  size_t ld = 0;
+  const int* perm = nullptr;
+  int nb = 0, ntri = 0;
+  const double* xp = nullptr;     // 3 per cluster position: node coordinates
+  const int* tri = nullptr;       // 3 per triangle: cluster positions, mesh vertex order
+  const double* tarea = nullptr;  // triangle areas
+  const double* tnrm = nullptr;   // outward unit normals, 3 per triangle
+  const int* adj_ptr = nullptr;   // position -> [adj_ptr[p], adj_ptr[p+1]) in adj
+  const int2* adj = nullptr;      // (triangle, local vertex 0..2) touching the position
+  const double* solid = nullptr;  // interior solid angle per position
+};
+// dense tiles of the inadmissible blocks: copied from B, or assembled from the mesh with the
+// reference Lindholm formula (k_bem_assemble.cu)
+void launch_h_near_gather(int nblk, const HBlockDev* blk, const HSource& src, double* d64, float* d32,
+                          cudaStream_t st);
+void launch_h_near_mesh(int nblk, const HBlockDev* blk, const HSource& src, double* d64, float* d32,
+                        cudaStream_t st);
+void launch_h_aca(int nblk, const HBlockDev* blk, const HSource& src, double* Us, double* Vs, unsigned char* used,
+                  int kmax, double eps_tight, double eps_loose, int* out_rank, cudaStream_t st);
+// per low-rank block {|A x|^2, |A x - U64 V64^T x|^2, |A x - U32 V32^T x|^2} for a fixed probe x
+// (ranks <= 128)
+void launch_h_verify(int nblk, const HBlockDev* blk, const HSource& src, const int* rk64, const long long* uo64,
+                     const long long* vo64, const double* U64, const double* V64, const int* rk32,
+                     const long long* uo32, const long long* vo32, const float* U32, const float* V32, double* out,
+                     cudaStream_t st);
 template <typename T>
 void launch_h_compact(int nblk, const HBlockDev* blk, const double* Us, const double* Vs, const long long* du,
                       const long long* dv, const int* rank, T* U, T* V, cudaStream_t st);
 // y (cluster order, FP64) = H u[boundary]; then b[node] = y[pos[node]] (0 off the boundary)
 template <typename T>
-void launch_h_matvec(const HMatView<T>& H, const double* u, double* y, double* t, T* xp, const int* pos, int n,
-                     double* bdir, cudaStream_t st);
+void launch_h_matvec(const HMatView<T>& H, const double* u, double* y, T* xp, const int* pos, int n, double* bdir,
+                     cudaStream_t st);
 
 // Count of kernel launches issued by this library (all contexts), for benchmarking.
 long long launch_count();

@@ -110,6 +110,34 @@ def jittered_disk(diameter: float, thickness: float, h: float, seed: int,
                 scale=scale, name=name)
 
 
+def union(meshes, name: str = "union"):
+    """Disjoint union of meshes (batched instances): nodes and elements stacked in order, element
+    ids offset.  Returns the mesh and the node offsets of the components (length len(meshes)+1).
+    The components keep their own coordinates (they may overlap in space; nothing couples them)."""
+    off = np.zeros(len(meshes) + 1, dtype=np.int64)
+    for i, m in enumerate(meshes):
+        off[i + 1] = off[i] + m.nx
+    xyz = np.concatenate([m.xyz for m in meshes], axis=0)
+    tets = np.concatenate([m.tets.astype(np.int64) + off[i] for i, m in enumerate(meshes)], axis=0)
+    if off[-1] >= 2 ** 31:
+        raise ValueError("union too large for int32 node ids")
+    return Mesh(xyz=xyz, tets=np.ascontiguousarray(tets, dtype=np.int32), scale=meshes[0].scale, name=name), off
+
+
+def soa_stack(vectors) -> np.ndarray:
+    """Concatenate per-component SoA nodal vectors (3 n_c each) into the union's SoA layout."""
+    n = [v.size // 3 for v in vectors]
+    return np.ascontiguousarray(np.concatenate([np.concatenate([v[d * k:(d + 1) * k] for v, k in zip(vectors, n)])
+                                                for d in range(3)]))
+
+
+def soa_split(v: np.ndarray, offsets) -> list:
+    """Inverse of soa_stack for the union with node offsets `offsets`."""
+    N = int(offsets[-1])
+    return [np.concatenate([v[d * N + offsets[c]:d * N + offsets[c + 1]] for d in range(3)])
+            for c in range(len(offsets) - 1)]
+
+
 def random_state(n: int, seed: int) -> np.ndarray:
     """i.i.d. directions uniform on S^2 (normalised Gaussian triples), SoA (3N,)."""
     rng = np.random.default_rng(seed)

@@ -34,6 +34,8 @@ class Workload:
     duration_ps: float = 1000.0
     segment_ps: float = 0.5
     info: dict = field(default_factory=dict)
+    components: Optional[np.ndarray] = None   # node offsets of batched instances (None: one mesh)
+    shared_bem: bool = False                  # the components are replicas of one mesh
 
     @property
     def n(self) -> int:
@@ -88,21 +90,88 @@ def c4_replica(seed: int = 4, replica: int = 0) -> Workload:
                     info=dict(replica=replica, b_tesla=b))
 
 
-WORKLOADS = {"c1": c1, "c2": c2, "c4": c4_replica}
+def c4_batch(replicas: int = 64, seed: int = 4) -> Workload:
+    """The c4 cuboid as `replicas` replicas in one context (one shared BEM matrix, the boundary
+    matvec one GEMM): each replica with the m0 and applied field of c4_replica(seed, r)."""
+    reps = [c4_replica(seed=seed, replica=r) for r in range(replicas)]
+    mesh, off = meshgen.union([reps[0].mesh] * replicas, name=f"c4x{replicas}_cuboid_200x200x40nm_h4")
+    return Workload(name=mesh.name, mesh=mesh, Ms=8.0e5, A=1.3e-11, alpha=0.5,
+                    m0=meshgen.soa_stack([r.m0 for r in reps]), hext=meshgen.soa_stack([r.hext for r in reps]),
+                    duration_ps=1000.0, components=off, shared_bem=True,
+                    info=dict(replicas=replicas, b_tesla=[r.info["b_tesla"] for r in reps]))
+
+
+def c3_dots(ndots: int = 256, seed: int = 3, h_range=(2.0, 3.0)) -> Workload:
+    """Batched uneven instances: ndots cuboid nanodots, sides Lx, Ly ~ U[20, 60] nm and thickness
+    Lz ~ U[5, 20] nm at cell size h ~ U[h_range] nm (integer cell counts, at least one cell),
+    each with its own dense BEM; Ku = 5e4 J/m^3 along a random unit axis per dot, alpha = 0.1,
+    |B| ~ U[0, 100] mT in a random direction per dot, random m0; 0.5 ns."""
+    meshes, m0, hext, axes, sizes = [], [], [], [], []
+    for d in range(ndots):
+        rng = np.random.default_rng([seed, d])
+        h = rng.uniform(*h_range)
+        L = np.array([rng.uniform(20, 60), rng.uniform(20, 60), rng.uniform(5, 20)])
+        nc = np.maximum(1, np.rint(L / h).astype(int))
+        m = meshgen.kuhn_cuboid(int(nc[0]), int(nc[1]), int(nc[2]), h, name=f"dot{d}")
+        ax = rng.standard_normal(3)
+        ax /= np.linalg.norm(ax)
+        b = rng.uniform(0.0, 0.100)
+        u = rng.standard_normal(3)
+        u /= np.linalg.norm(u)
+        th, ph = np.degrees(np.arccos(u[2])), np.degrees(np.arctan2(u[1], u[0]))
+        meshes.append(m)
+        m0.append(meshgen.random_state(m.nx, int(rng.integers(1 << 31))))
+        hext.append(meshgen.field_from_angles(m.nx, b, th, ph))
+        axes.append(np.ascontiguousarray(np.repeat(ax, m.nx)))
+        sizes.append(m.nx)
+    mesh, off = meshgen.union(meshes, name=f"c3_{ndots}dots")
+    return Workload(name=mesh.name, mesh=mesh, Ms=8.0e5, A=1.3e-11, alpha=0.1, m0=meshgen.soa_stack(m0),
+                    hext=meshgen.soa_stack(hext), Ku=5e4, ku_axis=meshgen.soa_stack(axes), duration_ps=500.0,
+                    components=off, info=dict(dots=ndots, nodes_per_dot=sizes))
+
+
+def instances(w: Workload) -> int:
+    return 1 if w.components is None else len(w.components) - 1
+
+
+def component(w: Workload, c: int) -> Workload:
+    """Instance c of a batched workload as a single-mesh workload (its own mesh, m0, field)."""
+    if w.components is None:
+        return w
+    off = w.components
+    lo, hi = int(off[c]), int(off[c + 1])
+    sel = (w.mesh.tets.min(axis=1) >= lo) & (w.mesh.tets.max(axis=1) < hi)
+    mesh = meshgen.Mesh(xyz=w.mesh.xyz[lo:hi].copy(), tets=np.ascontiguousarray(w.mesh.tets[sel] - lo),
+                        scale=w.mesh.scale, name=f"{w.name}[{c}]")
+    split = lambda v: None if v is None else meshgen.soa_split(v, off)[c]  # noqa: E731
+    return Workload(name=mesh.name, mesh=mesh, Ms=w.Ms, A=w.A, alpha=w.alpha, m0=split(w.m0), hext=split(w.hext),
+                    Ku=w.Ku, ku_axis=split(w.ku_axis), D=w.D, duration_ps=w.duration_ps, segment_ps=w.segment_ps)
+
+
+WORKLOADS = {"c1": c1, "c2": c2, "c3": c3_dots, "c4": c4_replica, "c4x64": c4_batch}
 
 
 def setup_context(w: Workload, device: int = 0, mixed: bool = False, tol: float = 1e-7, maxiter: int = 100,
                   mesh_ops=None, hmatrix: bool = False, keep_dense: bool = True, eps_mixed: float = 1e-6,
                   eps_fp64: float = 1e-7, kmax: int = 64, normal_split: bool = True):
     """MeshOps + Context with operators, device-assembled BEM (dense, optionally compressed to the
-    hierarchical form with leaf 32 and eta 2), material and applied field."""
+    hierarchical form with leaf 32 and eta 2), material and applied field.  hmatrix="mesh" builds
+    the hierarchical matrix from the mesh boundary; the dense matrix is then assembled only when
+    keep_dense is set, in the far-field-accurate arithmetic the hierarchical matrix approximates."""
     from .api import Context, MeshOps
 
     mo = mesh_ops if mesh_ops is not None else MeshOps(w.mesh.xyz, w.mesh.tets)
     ctx = Context(device)
     ctx.set_mesh(mo)
-    ctx.bem_assemble(mo)
-    if hmatrix:
+    if w.components is not None:
+        ctx.set_components(w.components, shared_bem=w.shared_bem)
+    if hmatrix == "mesh":
+        if keep_dense:
+            ctx.bem_assemble(mo, accurate=True)
+        ctx.bem_build_h(mo, leaf=32, eta=2.0, eps_mixed=eps_mixed, eps_fp64=eps_fp64, kmax=kmax)
+    else:
+        ctx.bem_assemble(mo)
+    if hmatrix and hmatrix != "mesh":
         bd = mo.boundary()
         bn = bd["bnodes"]
         nrm = bd["node_normal"].reshape(3, -1).T[bn] if normal_split else None
