@@ -201,6 +201,32 @@ int tmb_normalize(tmb_ctx* ctx, double* m, int ptr_kind);
  * final max torque [T], final dt (reduced), segments, 0, 0, 0.  Synchronises. */
 int tmb_relax(tmb_ctx* ctx, double* m, double duration_ps, double segment_ps, double eps_abs, double eps_rel,
               double* stats, int ptr_kind);
+/* Time-dependent applied field: a piecewise-linear Bz(t) through ns samples [T] spaced uniformly
+ * over [t0_ps, t1_ps] (held at the end values outside), added as Bz/mu0 to the z component of the
+ * applied field during tmb_step_rk4 / tmb_adjoint_rk4.  ns = 0 removes it.  Generalises tetmag's
+ * field pulse (TheLLG::setPulseField, main/TheLLG.cpp:320-332). */
+int tmb_set_bz_pulse(tmb_ctx* ctx, int ns, const double* bz_tesla, double t0_ps, double t1_ps);
+/* Fixed-step integration: nsteps steps of dt_ps from t0_ps, each nsub classical RK4 substeps with
+ * the full effective field (demag refreshed, main/TheLLG.cpp:238-254, 670-711) at every stage,
+ * then m <- m/|m| if normalize (main/TheSimulation.cpp:404-411).  m (3N SoA) in / out.
+ * stats (may be NULL, 8): [0] right-hand-side evaluations, [3] CG iterations.  The applied field
+ * is restored afterwards.  Synchronises.  No tetmag counterpart for the fixed step (tetmag's CVODE
+ * is adaptive); this is the map that tmb_adjoint_rk4 differentiates. */
+int tmb_step_rk4(tmb_ctx* ctx, double* m, int nsteps, double dt_ps, int nsub, double t0_ps, int normalize,
+                 double* stats, int ptr_kind);
+/* Discrete adjoint of tmb_step_rk4 for the objective J = sum_k w[k] y_N[k] (w: 3N SoA, e.g. the
+ * volume weights of mean m_z): runs the forward map from m0 keeping a checkpoint every ckpt_every
+ * steps, then per checkpoint interval (last first) recomputes its steps keeping the stage states
+ * and fields, and transposes them.  Outputs: m_final (3N), J, and the gradients dJ/dm0 (3N),
+ * dJ/dKu per node (N, with the material's easy axis; Ku may be 0) and dJ/dbz (ns samples of
+ * tmb_set_bz_pulse, host memory).  grad_m0, grad_ku, grad_bz, J, stats may be NULL.
+ * stats (8): [0] forward evaluations, [1] recomputed evaluations, [2] transposed evaluations,
+ * [3] CG iterations forward, [4] CG iterations transposed, [5] checkpoints, [6] checkpoint and
+ * stage storage in bytes.  Needs the interfacial DMI form (or none), one component and the dense
+ * BEM.  Synchronises.  No tetmag counterpart (tetmag has no adjoint). */
+int tmb_adjoint_rk4(tmb_ctx* ctx, const double* m0, int nsteps, double dt_ps, int nsub, int ckpt_every, double t0_ps,
+                    int normalize, const double* w, double* m_final, double* grad_m0, double* grad_ku,
+                    double* grad_bz, double* J, double* stats, int ptr_kind);
 /* Counters of the last demag evaluation: [0] Neumann iterations, [1] Dirichlet iterations,
  * [2] Neumann relative residual, [3] Dirichlet relative residual, [4] Neumann status,
  * [5] Dirichlet status, [6] AMG levels (Neumann), [7] AMG setup ms (both). Synchronises. */

@@ -292,6 +292,46 @@ class Context:
                 "segments"]
         return {kk: st[i] for i, kk in enumerate(keys)}
 
+    def set_bz_pulse(self, bz_tesla, t0_ps: float, t1_ps: float):
+        """Piecewise-linear Bz(t) samples [T] over [t0_ps, t1_ps], added to the applied z field during
+        step_rk4 / adjoint_rk4 (an empty sequence removes it)."""
+        b = _f64(np.asarray(bz_tesla, dtype=np.float64).ravel())
+        check(lib().tmb_set_bz_pulse(self.h, int(b.size), _dptr(b) if b.size else None, float(t0_ps), float(t1_ps)))
+        return self
+
+    def step_rk4(self, m, nsteps: int, dt_ps: float, nsub: int = 1, t0_ps: float = 0.0, normalize: bool = True):
+        """Fixed-step RK4 (full field at every stage) in place on m; returns the evaluation counters."""
+        st = (C.c_double * 8)()
+        pm, k = _vec(m)
+        check(lib().tmb_step_rk4(self.h, pm, int(nsteps), float(dt_ps), int(nsub), float(t0_ps), int(normalize), st, k))
+        return {"rhs_evals": st[0], "cg_iters": st[3]}
+
+    def adjoint_rk4(self, m0, w, nsteps: int, dt_ps: float, nsub: int = 1, ckpt_every: int = 10,
+                    t0_ps: float = 0.0, normalize: bool = True, n_bz: int = 0):
+        """Discrete adjoint of step_rk4 for J = sum(w * m_final).  m0, w: 3N float64 (numpy or CUDA
+        tensors, both of one kind).  Returns dict(J, m_final, grad_m0, grad_ku, grad_bz, stats)."""
+        n3 = 3 * self.n
+        on_dev = not isinstance(m0, np.ndarray)
+        if on_dev:
+            import torch
+            mk = lambda k: torch.empty(k, dtype=torch.float64, device=m0.device)  # noqa: E731
+        else:
+            mk = lambda k: np.empty(k)  # noqa: E731
+        mf, gm, gk = mk(n3), mk(n3), mk(self.n)
+        gb = np.zeros(max(int(n_bz), 1))
+        J = C.c_double()
+        st = (C.c_double * 8)()
+        pm, k = _vec(m0)
+        pw, kw = _vec(w)
+        if kw != k:
+            raise TypeError("m0 and w must both be host or both device arrays")
+        check(lib().tmb_adjoint_rk4(self.h, pm, int(nsteps), float(dt_ps), int(nsub), int(ckpt_every), float(t0_ps),
+                                    int(normalize), pw, _vec(mf)[0], _vec(gm)[0], _vec(gk)[0], _dptr(gb), C.byref(J),
+                                    st, k))
+        keys = ["fwd_evals", "recompute_evals", "vjp_evals", "cg_fwd", "cg_adj", "checkpoints", "storage_bytes"]
+        return {"J": J.value, "m_final": mf, "grad_m0": gm, "grad_ku": gk, "grad_bz": gb[:int(n_bz)],
+                "stats": {kk: st[i] for i, kk in enumerate(keys)}}
+
     def stats(self) -> dict:
         st = (C.c_double * 8)()
         check(lib().tmb_get_stats(self.h, st))

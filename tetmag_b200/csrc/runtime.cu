@@ -254,6 +254,11 @@ struct Solver {
   int ncoarse = 0;
   DevCsr lift;
   DevArray<int> cmask;
+  // transposed solve (the adjoint): lift^T, masked load, and a warm start kept apart from the
+  // forward one
+  DevCsr liftT;
+  DevArray<double> ct, xfwd, xadj;
+  bool has_xadj = false;
   DevArray<double> x, r, z, p[2], q, bp, partials;
   CgScalars* Sd = nullptr;
   CgScalars* Sh = nullptr;
@@ -276,6 +281,9 @@ struct Solver {
   }
   void compute();
   void solve(const double* b_dev, int precision);
+  // out = A^-T c for the row-replaced matrix A = [A_FF L; 0 I] (constrained rows C are unit
+  // rows): out_F = A_FF^-1 c_F (A_FF is symmetric), out_C = c_C - (L^T out_F)_C
+  void solve_t(const double* c_dev, double* out, int precision);
   void vcycle(size_t l, const double* b, double* out, int precision, cudaStream_t st, int rz_mode);
   void precondition_rz(int precision, cudaStream_t st, bool first);
   int pcur = 0;  // which of p[0], p[1] holds the current direction
@@ -424,6 +432,23 @@ struct Ctx {
   int integrate_segment(double*& y, double*& yalt, double t0, double t1, double& dt, double eps_abs,
                         double eps_rel, double* stats);
   int relax(double* m_dev, double duration_ps, double segment_ps, double eps_abs, double eps_rel, double* stats);
+  // Fixed-step integration with the full field at every stage, and its discrete adjoint.
+  std::vector<double> bz;               // Bz(t) samples [T], uniformly spaced over [bz_t0, bz_t1] ps
+  double bz_t0 = 0.0, bz_t1 = 0.0;
+  struct AdjBuf {
+    DevArray<double> hbase, ck, segY, segH, segZ, segYend, lam, g[4], abar, mu, w, v, vb, z, a1, q, bpart, zpart,
+        dku, ninvvol, zn, io[5];
+  } ab;
+  double cnt[8] = {};                   // stage evals, recomputed evals, VJPs, CG its fwd / transposed, ...
+  double pulse_hz(double t_ps) const;
+  void begin_timed_field();
+  void end_timed_field();
+  void stage_eval(const double* Y, double t_ps, double* k, double* H);
+  void rk4_substep(double* y, double t_ps, double ds_ps, double* Ys, double* Hs);
+  void vjp(const double* Y, const double* H, const double* abar, double* gout, double* zpart);
+  void step_rk4(double* m_dev, int nsteps, double dt_ps, int nsub, double t0_ps, bool normalize);
+  void adjoint_rk4(const double* m0, int nsteps, double dt_ps, int nsub, int ckpt, double t0_ps, bool normalize,
+                   const double* w, double* m_final, double* grad_m0, double* grad_ku, double* grad_bz);
   double time_scale() const { return gamma / (1.0 + alpha * alpha) * 1e-12; }
   void sync() { TMB_CUDA(cudaStreamSynchronize(stream)); }
 };
@@ -504,6 +529,22 @@ void Solver::compute() {
     Ap.ptr[i + 1] = int(Ap.col.size());
     L.ptr[i + 1] = int(L.col.size());
   }
+  Csr LT;
+  LT.nrows = LT.ncols = n;
+  LT.ptr.assign(n + 1, 0);
+  for (int j : L.col) LT.ptr[j + 1]++;
+  for (int i = 0; i < n; ++i) LT.ptr[i + 1] += LT.ptr[i];
+  LT.col.resize(L.col.size());
+  LT.val.resize(L.col.size());
+  {
+    std::vector<int> fill(LT.ptr.begin(), LT.ptr.end() - 1);
+    for (int i = 0; i < n; ++i)
+      for (int k = L.ptr[i]; k < L.ptr[i + 1]; ++k) {
+        const int q = fill[L.col[k]]++;
+        LT.col[q] = i;
+        LT.val[q] = L.val[k];
+      }
+  }
   drop_graphs();  // captured graphs hold the previous buffers
   amg_build(Ap, prm, H);
   nnz_fine = double(Ap.nnz());
@@ -532,6 +573,8 @@ void Solver::compute() {
   ncoarse = H.ncoarse;
   cinv.upload(H.coarse_inv, st);
   lift.upload(L, st);
+  liftT.upload(LT, st);
+  has_xadj = false;
   cmask.upload(cm, st);
   x.alloc(n);
   x.zero(st);
@@ -642,6 +685,25 @@ void Solver::solve(const double* b_dev, int precision) {
   last_status = Sh->status == 2 ? 0 : Sh->status;
   last_relres = (Sh->bb > 0.0) ? std::sqrt(Sh->rr / Sh->bb) : 0.0;
   has_x = true;
+}
+
+void Solver::solve_t(const double* c, double* out, int precision) {
+  cudaStream_t st = ctx->stream;
+  ct.alloc(n);
+  xfwd.alloc(n);
+  if (!has_xadj) {
+    xadj.alloc(n);
+    xadj.zero(st);
+    has_xadj = true;
+  }
+  launch_mask_constrained(n, cmask.p, c, ct.p, st);
+  TMB_CUDA(cudaMemcpyAsync(xfwd.p, x.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  TMB_CUDA(cudaMemcpyAsync(x.p, xadj.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  solve(ct.p, precision);
+  if (precision == TMB_FP64) launch_lift_t<double>(n, liftT.view(), liftT.v.p, cmask.p, c, x.p, out, st);
+  else launch_lift_t<float>(n, liftT.view(), liftT.vf.p, cmask.p, c, x.p, out, st);
+  TMB_CUDA(cudaMemcpyAsync(xadj.p, x.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  TMB_CUDA(cudaMemcpyAsync(x.p, xfwd.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1402,6 +1464,272 @@ int Ctx::relax(double* m, double duration_ps, double segment_ps, double eps_abs,
   return TMB_OK;
 }
 
+// ------------------------------------------------------------------------------------------
+// Fixed-step RK4 with the full effective field at every stage, and its discrete adjoint
+// (no tetmag counterpart; the right-hand side is tetmag's, main/TheLLG.cpp:238-254, 670-711).
+// ------------------------------------------------------------------------------------------
+double Ctx::pulse_hz(double t_ps) const {
+  const int ns = int(bz.size());
+  if (ns == 0) return 0.0;
+  double b;
+  if (ns == 1 || t_ps <= bz_t0) b = bz[0];
+  else if (t_ps >= bz_t1) b = bz[ns - 1];
+  else {
+    const double u = (t_ps - bz_t0) / (bz_t1 - bz_t0) * (ns - 1);
+    const int k = std::min(int(std::floor(u)), ns - 2);
+    const double f = u - k;
+    b = (1.0 - f) * bz[k] + f * bz[k + 1];
+  }
+  return b / kMu0;
+}
+
+// The applied field in effect before a fixed-step run is kept and restored afterwards.
+void Ctx::begin_timed_field() {
+  const size_t n3 = size_t(3) * n;
+  ab.hbase.alloc(n3);
+  TMB_CUDA(cudaMemcpyAsync(ab.hbase.p, hext.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+}
+
+void Ctx::end_timed_field() {
+  const size_t n3 = size_t(3) * n;
+  TMB_CUDA(cudaMemcpyAsync(hext.p, ab.hbase.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+  launch_add(int(n3), hext.p, hdem.p, hfix.p, stream);
+}
+
+// One right-hand-side evaluation with the demag field refreshed: k = f(Y, t), H = total field.
+void Ctx::stage_eval(const double* Y, double t_ps, double* k, double* H) {
+  if (!bz.empty()) launch_set_hz(n, ab.hbase.p, pulse_hz(t_ps), hext.p, stream);
+  if (has_bem) {
+    demag(Y);
+    cnt[3] += neu->last_iters + dir->last_iters;
+  } else {
+    launch_add(3 * n, hext.p, hdem.p, hfix.p, stream);
+  }
+  local(Y, k, H, nullptr);
+}
+
+// y <- y + h/6 (k1 + 2 k2 + 2 k3 + k4); with Ys / Hs (4 x 3N each) the stage states and fields
+// are kept for the adjoint.
+void Ctx::rk4_substep(double* y, double t_ps, double ds_ps, double* Ys, double* Hs) {
+  const int n3 = 3 * n;
+  const double h = ds_ps * time_scale();
+  double* K[4] = {kst[0].p, kst[1].p, kst[2].p, kst[3].p};
+  if (Ys) TMB_CUDA(cudaMemcpyAsync(Ys, y, sizeof(double) * n3, cudaMemcpyDeviceToDevice, stream));
+  stage_eval(y, t_ps, K[0], Hs);
+  const double c[3] = {0.5 * h, 0.5 * h, h};
+  const double tt[3] = {t_ps + 0.5 * ds_ps, t_ps + 0.5 * ds_ps, t_ps + ds_ps};
+  for (int i = 0; i < 3; ++i) {
+    double* Yi = Ys ? Ys + size_t(i + 1) * n3 : ytmp.p;
+    launch_lincomb(n3, Yi, 1.0, y, c[i], K[i], 0.0, nullptr, stream);
+    stage_eval(Yi, tt[i], K[i + 1], Hs ? Hs + size_t(i + 1) * n3 : nullptr);
+  }
+  launch_rk4_final(n3, y, K[0], K[1], K[2], K[3], h, stream);
+}
+
+// gout = (df/dm)(Y)^T abar at one stage; dku accumulates (df/dKu)^T abar, zpart gets the block
+// partial sums of mu_z (the Bz gradient).  The demag part runs the chain backwards:
+// w = -grad^T mu, v = A_D^-T w, a = w + (B^T v_b scattered), a1 = A_N^-T a, div^T a1.
+void Ctx::vjp(const double* Y, const double* H, const double* abar, double* gout, double* zpart) {
+  const bool f64 = precision == TMB_FP64;
+  const SellView S = pat.view();
+  AdjPreArgs pa{};
+  pa.n = n;
+  pa.m = Y;
+  pa.H = H;
+  pa.abar = abar;
+  pa.alpha = alpha;
+  pa.precession = precession;
+  pa.js = js.p;
+  pa.kax = kax.p;
+  pa.mu = ab.mu.p;
+  pa.g = gout;
+  pa.dku = ab.dku.p;
+  pa.zpart = zpart;
+  launch_adj_pre(pa, stream);
+  const double* q = nullptr;
+  if (has_bem) {
+    if (f64) launch_divergence<double>(S, tg[0].p, tg[1].p, tg[2].p, ab.mu.p, ab.ninvvol.p, 1.0, ab.w.p, stream);
+    else launch_divergence<float>(S, tgf[0].p, tgf[1].p, tgf[2].p, ab.mu.p, ab.ninvvol.p, 1.0, ab.w.p, stream);
+    dir->solve_t(ab.w.p, ab.v.p, precision);
+    launch_gather<double>(nb, ab.v.p, bnodes.p, ab.vb.p, stream);
+    const int nch = bem_gemv_t_chunks(nb, num_sms);
+    if (f64) launch_bem_gemv_t<double>(nb, Bd.p, ab.vb.p, ab.bpart.p, nch, ab.z.p, stream);
+    else launch_bem_gemv_t<float>(nb, Bf.p, ab.vb.p, ab.bpart.p, nch, ab.z.p, stream);
+    launch_scatter_add(nb, bnodes.p, ab.z.p, ab.w.p, stream);
+    neu->solve_t(ab.w.p, ab.a1.p, precision);
+    cnt[4] += neu->last_iters + dir->last_iters;
+    if (f64) launch_gradient<double>(S, g[0].p, g[1].p, g[2].p, ab.a1.p, nullptr, nullptr, ab.q.p, nullptr, stream);
+    else launch_gradient<float>(S, gf[0].p, gf[1].p, gf[2].p, ab.a1.p, nullptr, nullptr, ab.q.p, nullptr, stream);
+    q = ab.q.p;
+  }
+  const bool idmi = has_dmi && dmi_kind == 1;
+  AdjLocalArgs la{};
+  la.n = n;
+  la.mu = ab.mu.p;
+  la.xc = xc.p;
+  la.ku2 = has_uni ? ku2.p : nullptr;
+  la.kax = kax.p;
+  la.idm_d = idmi ? idm_d.p : nullptr;
+  la.idm_b = idmi ? idm_b.p : nullptr;
+  la.vol = node_vol.p;
+  la.js = js.p;
+  la.q = q;
+  la.inv_mu0 = 1.0 / kMu0;
+  la.g = gout;
+  if (f64) launch_adj_local<double>(S, K.p, tg[0].p, tg[1].p, g[0].p, g[1].p, la, stream);
+  else launch_adj_local<float>(S, Kf.p, tgf[0].p, tgf[1].p, gf[0].p, gf[1].p, la, stream);
+  cnt[2] += 1;
+}
+
+void Ctx::step_rk4(double* m, int nsteps, double dt_ps, int nsub, double t0_ps, bool normalize) {
+  require_mesh();
+  require_material();
+  const int n3 = 3 * n;
+  for (int j = 0; j < 4; ++j) kst[j].alloc(n3);
+  ytmp.alloc(n3);
+  ab.zn.alloc(n);
+  begin_timed_field();
+  const double ds = dt_ps / nsub;
+  for (int k = 0; k < nsteps; ++k) {
+    for (int s = 0; s < nsub; ++s) {
+      rk4_substep(m, t0_ps + k * dt_ps + s * ds, ds, nullptr, nullptr);
+      cnt[0] += 4;
+    }
+    if (normalize) launch_normalize_keep(n, m, ab.zn.p, stream);
+  }
+  end_timed_field();
+  sync();
+}
+
+void Ctx::adjoint_rk4(const double* m0, int nsteps, double dt_ps, int nsub, int ckpt, double t0_ps, bool normalize,
+                      const double* w, double* m_final, double* grad_m0, double* grad_ku, double* grad_bz) {
+  require_mesh();
+  require_material();
+  if (has_dmi && dmi_kind != 1)
+    throw Error(TMB_ERR_STATE, "adjoint: the bulk DMI form has no transpose here (interfacial or none)");
+  if (has_bem && (ncomp() != 1 || bem_mode != 0))
+    throw Error(TMB_ERR_STATE, "adjoint: needs one component and the dense BEM matrix");
+  if (has_bem) ensure_demag();
+  cudaStream_t st = stream;
+  const size_t n3 = size_t(3) * n;
+  const int nck = (nsteps + ckpt - 1) / ckpt;
+  const size_t per_seg = size_t(ckpt) * nsub * 4 * n3;
+  for (int j = 0; j < 4; ++j) kst[j].alloc(n3);
+  ytmp.alloc(n3);
+  ybuf[0].alloc(n3);
+  ab.ck.alloc(std::max(1, nck) * n3);
+  ab.segY.alloc(per_seg);
+  ab.segH.alloc(per_seg);
+  ab.segZ.alloc(size_t(ckpt) * n);
+  ab.segYend.alloc(size_t(ckpt) * n3);
+  ab.zn.alloc(n);
+  ab.lam.alloc(n3);
+  for (auto& gg : ab.g) gg.alloc(n3);
+  ab.abar.alloc(n3);
+  ab.mu.alloc(n3);
+  ab.w.alloc(n);
+  ab.v.alloc(n);
+  ab.a1.alloc(n);
+  ab.q.alloc(n3);
+  ab.vb.alloc(std::max(nb, 1));
+  ab.z.alloc(std::max(nb, 1));
+  ab.bpart.alloc(size_t(bem_gemv_t_chunks(std::max(nb, 1), num_sms)) * std::max(nb, 1));
+  const int nblk = adj_pre_blocks(n);
+  const long long nstage = 4LL * nsteps * nsub;
+  ab.zpart.alloc(size_t(std::max(1LL, nstage)) * nblk);
+  ab.dku.alloc(n);
+  ab.dku.zero(st);
+  {
+    std::vector<double> niv(n);
+    for (int i = 0; i < n; ++i) niv[i] = -1.0 / hvol[i];
+    ab.ninvvol.upload(niv, st);
+  }
+  begin_timed_field();
+  const double ds = dt_ps / nsub;
+  const double h = ds * time_scale();
+  double* y = ybuf[0].p;
+  TMB_CUDA(cudaMemcpyAsync(y, m0, sizeof(double) * n3, cudaMemcpyDeviceToDevice, st));
+  // forward sweep, keeping a checkpoint every `ckpt` steps
+  for (int k = 0; k < nsteps; ++k) {
+    if (k % ckpt == 0)
+      TMB_CUDA(cudaMemcpyAsync(ab.ck.p + size_t(k / ckpt) * n3, y, sizeof(double) * n3, cudaMemcpyDeviceToDevice, st));
+    for (int s = 0; s < nsub; ++s) {
+      rk4_substep(y, t0_ps + k * dt_ps + s * ds, ds, nullptr, nullptr);
+      cnt[0] += 4;
+    }
+    if (normalize) launch_normalize_keep(n, y, ab.zn.p, st);
+  }
+  TMB_CUDA(cudaMemcpyAsync(m_final, y, sizeof(double) * n3, cudaMemcpyDeviceToDevice, st));
+  // backward sweep: recompute each checkpoint interval keeping its stages, then transpose it
+  TMB_CUDA(cudaMemcpyAsync(ab.lam.p, w, sizeof(double) * n3, cudaMemcpyDeviceToDevice, st));
+  for (int seg = nck - 1; seg >= 0; --seg) {
+    const int k0 = seg * ckpt, k1 = std::min(nsteps, k0 + ckpt);
+    TMB_CUDA(cudaMemcpyAsync(y, ab.ck.p + size_t(seg) * n3, sizeof(double) * n3, cudaMemcpyDeviceToDevice, st));
+    for (int k = k0; k < k1; ++k) {
+      for (int s = 0; s < nsub; ++s) {
+        const size_t off = (size_t(k - k0) * nsub + s) * 4 * n3;
+        rk4_substep(y, t0_ps + k * dt_ps + s * ds, ds, ab.segY.p + off, ab.segH.p + off);
+        cnt[1] += 4;
+      }
+      if (normalize) launch_normalize_keep(n, y, ab.segZ.p + size_t(k - k0) * n, st);
+      TMB_CUDA(cudaMemcpyAsync(ab.segYend.p + size_t(k - k0) * n3, y, sizeof(double) * n3, cudaMemcpyDeviceToDevice,
+                               st));
+    }
+    for (int k = k1 - 1; k >= k0; --k) {
+      if (normalize) launch_adj_normalize(n, ab.segYend.p + size_t(k - k0) * n3, ab.segZ.p + size_t(k - k0) * n,
+                                          ab.lam.p, st);
+      for (int s = nsub - 1; s >= 0; --s) {
+        const size_t off = (size_t(k - k0) * nsub + s) * 4 * n3;
+        const double* Y = ab.segY.p + off;
+        const double* Hs = ab.segH.p + off;
+        double* zp = ab.zpart.p + size_t((long long)(k * nsub + s) * 4) * nblk;
+        double* G[4] = {ab.g[0].p, ab.g[1].p, ab.g[2].p, ab.g[3].p};
+        double* lam = ab.lam.p;
+        double* a = ab.abar.p;
+        launch_lincomb(int(n3), a, h / 6.0, lam, 0.0, nullptr, 0.0, nullptr, st);
+        vjp(Y + 3 * n3, Hs + 3 * n3, a, G[3], zp + 3 * nblk);
+        launch_lincomb(int(n3), a, h / 3.0, lam, h, G[3], 0.0, nullptr, st);
+        vjp(Y + 2 * n3, Hs + 2 * n3, a, G[2], zp + 2 * nblk);
+        launch_lincomb(int(n3), a, h / 3.0, lam, 0.5 * h, G[2], 0.0, nullptr, st);
+        vjp(Y + n3, Hs + n3, a, G[1], zp + nblk);
+        launch_lincomb(int(n3), a, h / 6.0, lam, 0.5 * h, G[1], 0.0, nullptr, st);
+        vjp(Y, Hs, a, G[0], zp);
+        launch_lincomb(int(n3), lam, 1.0, lam, 1.0, G[0], 1.0, G[1], st);
+        launch_lincomb(int(n3), lam, 1.0, lam, 1.0, G[2], 1.0, G[3], st);
+      }
+    }
+  }
+  if (grad_m0) TMB_CUDA(cudaMemcpyAsync(grad_m0, ab.lam.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, st));
+  if (grad_ku) TMB_CUDA(cudaMemcpyAsync(grad_ku, ab.dku.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  const int ns = int(bz.size());
+  if (grad_bz && ns > 0) {
+    std::vector<double> zp(size_t(nstage) * nblk);
+    TMB_CUDA(cudaMemcpyAsync(zp.data(), ab.zpart.p, zp.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    sync();
+    std::fill(grad_bz, grad_bz + ns, 0.0);
+    const double cst[4] = {0.0, 0.5, 0.5, 1.0};
+    for (long long q = 0; q < nstage; ++q) {
+      double sz = 0.0;
+      for (int b = 0; b < nblk; ++b) sz += zp[size_t(q) * nblk + b];
+      const long long ks = q / 4;
+      const int k = int(ks / nsub), sub = int(ks % nsub), i = int(q % 4);
+      const double t = t0_ps + k * dt_ps + (sub + cst[i]) * ds;
+      // hat weights of the samples at t
+      if (ns == 1 || t <= bz_t0) grad_bz[0] += sz / kMu0;
+      else if (t >= bz_t1) grad_bz[ns - 1] += sz / kMu0;
+      else {
+        const double u = (t - bz_t0) / (bz_t1 - bz_t0) * (ns - 1);
+        const int j = std::min(int(std::floor(u)), ns - 2);
+        const double f = u - j;
+        grad_bz[j] += (1.0 - f) * sz / kMu0;
+        grad_bz[j + 1] += f * sz / kMu0;
+      }
+    }
+  }
+  end_timed_field();
+  sync();
+}
+
 }  // namespace tmb
 
 // ==========================================================================================
@@ -2044,6 +2372,99 @@ int tmb_relax(tmb_ctx* ctx, double* m, double duration_ps, double segment_ps, do
     TMB_CUDA(cudaMemcpyAsync(m, c.in3.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     c.sync();
   }
+  TMB_API_END
+}
+
+int tmb_set_bz_pulse(tmb_ctx* ctx, int ns, const double* bz_tesla, double t0_ps, double t1_ps) {
+  TMB_CHECK_ARG(ctx && ns >= 0 && (ns == 0 || bz_tesla), "tmb_set_bz_pulse: null argument or ns < 0");
+  TMB_CHECK_ARG(ns <= 1 || t1_ps > t0_ps, "tmb_set_bz_pulse: t1_ps must exceed t0_ps");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  c.bz.assign(bz_tesla, bz_tesla + ns);
+  for (double b : c.bz)
+    if (!std::isfinite(b)) throw Error(TMB_ERR_ARG, "tmb_set_bz_pulse: samples must be finite");
+  c.bz_t0 = t0_ps;
+  c.bz_t1 = t1_ps;
+  TMB_API_END
+}
+
+int tmb_step_rk4(tmb_ctx* ctx, double* m, int nsteps, double dt_ps, int nsub, double t0_ps, int normalize,
+                 double* stats, int ptr_kind) {
+  TMB_CHECK_ARG(ctx && m, "tmb_step_rk4: null argument");
+  TMB_CHECK_ARG(nsteps >= 0 && nsub >= 1 && dt_ps > 0.0 && std::isfinite(dt_ps), "tmb_step_rk4: bad step arguments");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  c.require_mesh();
+  TMB_CUDA(cudaSetDevice(c.device));
+  const size_t n3 = size_t(3) * c.n;
+  for (double& v : c.cnt) v = 0.0;
+  double* md = m;
+  if (ptr_kind != TMB_PTR_DEVICE) {
+    c.ab.io[0].alloc(n3);
+    TMB_CUDA(cudaMemcpyAsync(c.ab.io[0].p, m, n3 * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+    md = c.ab.io[0].p;
+  }
+  c.step_rk4(md, nsteps, dt_ps, nsub, t0_ps, normalize != 0);
+  if (ptr_kind != TMB_PTR_DEVICE) {
+    TMB_CUDA(cudaMemcpyAsync(m, md, n3 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+  }
+  if (stats)
+    for (int i = 0; i < 8; ++i) stats[i] = c.cnt[i];
+  TMB_API_END
+}
+
+int tmb_adjoint_rk4(tmb_ctx* ctx, const double* m0, int nsteps, double dt_ps, int nsub, int ckpt_every, double t0_ps,
+                    int normalize, const double* w, double* m_final, double* grad_m0, double* grad_ku,
+                    double* grad_bz, double* J, double* stats, int ptr_kind) {
+  TMB_CHECK_ARG(ctx && m0 && w && m_final, "tmb_adjoint_rk4: null argument");
+  TMB_CHECK_ARG(nsteps >= 1 && nsub >= 1 && ckpt_every >= 1 && dt_ps > 0.0 && std::isfinite(dt_ps),
+                "tmb_adjoint_rk4: bad step arguments");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  c.require_mesh();
+  TMB_CUDA(cudaSetDevice(c.device));
+  const size_t n3 = size_t(3) * c.n, n = size_t(c.n);
+  for (double& v : c.cnt) v = 0.0;
+  const bool dev = ptr_kind == TMB_PTR_DEVICE;
+  const double* m0d = stage_in(c, c.ab.io[0], m0, n3, ptr_kind);
+  const double* wd = stage_in(c, c.ab.io[1], w, n3, ptr_kind);
+  double* mfd = m_final;
+  double* gmd = grad_m0;
+  double* gkd = grad_ku;
+  if (!dev) {
+    c.ab.io[2].alloc(n3);
+    mfd = c.ab.io[2].p;
+    if (grad_m0) {
+      c.ab.io[3].alloc(n3);
+      gmd = c.ab.io[3].p;
+    }
+    if (grad_ku) {
+      c.ab.io[4].alloc(n);
+      gkd = c.ab.io[4].p;
+    }
+  }
+  c.adjoint_rk4(m0d, nsteps, dt_ps, nsub, ckpt_every, t0_ps, normalize != 0, wd, mfd, gmd, gkd, grad_bz);
+  std::vector<double> hm(n3), hw(n3);
+  TMB_CUDA(cudaMemcpyAsync(hm.data(), mfd, n3 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  TMB_CUDA(cudaMemcpyAsync(hw.data(), wd, n3 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  if (!dev) {
+    TMB_CUDA(cudaMemcpyAsync(m_final, mfd, n3 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    if (grad_m0) TMB_CUDA(cudaMemcpyAsync(grad_m0, gmd, n3 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    if (grad_ku) TMB_CUDA(cudaMemcpyAsync(grad_ku, gkd, n * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  }
+  c.sync();
+  if (J) {
+    double s = 0.0;
+    for (size_t i = 0; i < n3; ++i) s += hw[i] * hm[i];
+    *J = s;
+  }
+  if (stats) {
+    for (int i = 0; i < 8; ++i) stats[i] = c.cnt[i];
+    stats[5] = (nsteps + ckpt_every - 1) / ckpt_every;
+    stats[6] = double(c.ab.segY.n + c.ab.segH.n + c.ab.ck.n) * sizeof(double);
+  }
+  if (!std::isfinite(J ? *J : 0.0)) throw Error(TMB_ERR_NAN, "adjoint: objective is not finite");
   TMB_API_END
 }
 

@@ -227,6 +227,56 @@ template <typename T>
 void launch_h_matvec(const HMatView<T>& H, const double* u, double* y, T* xp, const int* pos, int n, double* bdir,
                      cudaStream_t st);
 
+// --- discrete adjoint of the fixed-step integration (k_adjoint.cu) -------------------------
+struct AdjPreArgs {
+  int n;
+  const double* m;       // 3N stage state
+  const double* H;       // 3N total field at the stage
+  const double* abar;    // 3N adjoint weight of the stage's right-hand side
+  double alpha;
+  int precession;
+  const double* js;      // N  Js (uniaxial gradient), with kax
+  const double* kax;     // 3N easy axis
+  double* mu;            // 3N out: (df/dH)^T abar
+  double* g;             // 3N out: (df/dm at fixed H)^T abar
+  double* dku;           // N  accumulated dJ/dKu, may be null
+  double* zpart;         // one partial sum of mu_z per block, may be null
+};
+struct AdjLocalArgs {
+  int n;
+  const double* mu;      // 3N
+  const double* xc;      // N  exchange row scale
+  const double* ku2;     // N  2 Ku / Js, null without uniaxial anisotropy
+  const double* kax;     // 3N
+  const double* idm_d;   // N  D (interfacial DMI), null otherwise
+  const double* idm_b;   // N  1 / (V Js), null without interfacial DMI
+  const double* vol;     // N  node volumes
+  const double* js;      // N
+  const double* q;       // 3N -grad a1 of the transposed demag chain, null without demag
+  double inv_mu0;
+  double* g;             // 3N in/out
+};
+void launch_set_hz(int n, const double* hbase, double hz, double* hext, cudaStream_t st);
+void launch_lincomb(int n3, double* out, double c0, const double* v0, double c1, const double* v1, double c2,
+                    const double* v2, cudaStream_t st);
+void launch_rk4_final(int n3, double* y, const double* k1, const double* k2, const double* k3, const double* k4,
+                      double h, cudaStream_t st);
+void launch_normalize_keep(int n, double* y, double* zn, cudaStream_t st);
+void launch_adj_normalize(int n, const double* y, const double* zn, double* lam, cudaStream_t st);
+int adj_pre_blocks(int n);
+void launch_adj_pre(const AdjPreArgs& a, cudaStream_t st);
+template <typename V>
+void launch_adj_local(const SellView& s, const V* K, const V* tg0, const V* tg1, const V* gr0, const V* gr1,
+                      const AdjLocalArgs& a, cudaStream_t st);
+int bem_gemv_t_chunks(int nb, int num_sms);
+template <typename V>
+void launch_bem_gemv_t(int nb, const V* B, const double* x, double* part, int nchunk, double* out, cudaStream_t st);
+void launch_mask_constrained(int n, const int* cmask, const double* c, double* out, cudaStream_t st);
+template <typename V>
+void launch_lift_t(int n, const CsrView& lt, const V* lval, const int* cmask, const double* c, const double* x,
+                   double* out, cudaStream_t st);
+void launch_scatter_add(int nb, const int* idx, const double* z, double* a, cudaStream_t st);
+
 // Count of kernel launches issued by this library (all contexts), for benchmarking.
 long long launch_count();
 void note_launch();

@@ -9,8 +9,8 @@ specs/InitMag.cpp:44-247.  The workloads here are generated instead:
   cells use the same split, so the mesh is conforming.  Coordinates are in
   mesh units (nm for ``scale = 1e-9``), centred on the origin like the
   vortex initial state of specs/InitMag.cpp:203-225 expects.
-* ``jittered_disk`` -- an unstructured disk from a seeded Delaunay
-  tetrahedralisation of a jittered lattice (the interfacial-DMI workload).
+* ``jittered_disk`` -- an unstructured disk from a seeded Delaunay triangulation of a
+  jittered lattice, extruded in layers (the interfacial-DMI workload).
 * initial states: uniform random on the unit sphere, and a vortex with a
   seeded core position.
 
@@ -69,45 +69,52 @@ def kuhn_cuboid(ncx: int, ncy: int, ncz: int, h: float, scale: float = 1e-9,
 
 def jittered_disk(diameter: float, thickness: float, h: float, seed: int,
                   jitter: float = 0.3, scale: float = 1e-9, name: str = "disk") -> Mesh:
-    """Seeded Delaunay disk: jittered lattice points inside a cylinder.
+    """Seeded disk: Delaunay triangulation of a jittered square lattice of spacing h inside the
+    circle (plus a rim ring of about 2 pi R / h points), extruded through round(t / h) layers.
 
-    Boundary points (rim circle rings and the two faces) are placed without
-    jitter in the normal direction so the surface stays a clean cylinder.
-    Slivers (tets with |volume| < 1e-3 h^3) are removed.
+    Lattice points are jittered by up to +-jitter*h in x and y and kept if they lie more than
+    h/2 inside the rim.  Each prism (triangle x layer) is split into three tetrahedra by the
+    vertex-order rule (the diagonal of every side quad runs from the lower-numbered vertex's
+    bottom node to the higher-numbered vertex's top node), so neighbouring prisms share their
+    split faces and the mesh is conforming.  The 2D Delaunay step keeps every triangle well
+    shaped, so the mesh has no slivers (a 3D Delaunay of a jittered lattice has many, and their
+    stiffness sets the explicit time step).  All tetrahedra are positively oriented.
     """
     from scipy.spatial import Delaunay
 
     rng = np.random.default_rng(seed)
     R = 0.5 * diameter
+    g = np.arange(-R, R + 1e-9, h)
+    X, Y = np.meshgrid(g, g, indexing="ij")
+    X = X.ravel() + jitter * h * rng.uniform(-1, 1, X.size)
+    Y = Y.ravel() + jitter * h * rng.uniform(-1, 1, Y.size)
+    keep = X * X + Y * Y < (R - 0.5 * h) ** 2
+    n_ring = max(8, int(round(2 * np.pi * R / h)))
+    phi = 2 * np.pi * np.arange(n_ring) / n_ring
+    p2 = np.concatenate([np.stack([X[keep], Y[keep]], axis=1),
+                         np.stack([R * np.cos(phi), R * np.sin(phi)], axis=1)], axis=0)
+    tri = np.sort(Delaunay(p2).simplices.astype(np.int64), axis=1)
+    e1, e2 = p2[tri[:, 1]] - p2[tri[:, 0]], p2[tri[:, 2]] - p2[tri[:, 0]]
+    a2 = np.abs(e1[:, 0] * e2[:, 1] - e1[:, 1] * e2[:, 0]) * 0.5
+    tri = tri[a2 > 1e-6 * h * h]
     nz = max(1, int(round(thickness / h)))
     zs = np.linspace(-0.5 * thickness, 0.5 * thickness, nz + 1)
-    pts = []
-    n_ring = max(8, int(round(2 * np.pi * R / h)))
-    for iz, z in enumerate(zs):
-        # interior lattice points of this layer
-        g = np.arange(-R, R + 1e-9, h)
-        X, Y = np.meshgrid(g, g, indexing="ij")
-        X = X.ravel(); Y = Y.ravel()
-        X = X + jitter * h * rng.uniform(-1, 1, X.size)
-        Y = Y + jitter * h * rng.uniform(-1, 1, Y.size)
-        keep = X * X + Y * Y < (R - 0.5 * h) ** 2
-        zz = np.full(int(keep.sum()), z)
-        if 0 < iz < nz:
-            zz = zz + jitter * h * rng.uniform(-1, 1, zz.size) * 0.5
-        pts.append(np.stack([X[keep], Y[keep], zz], axis=1))
-        phi = 2 * np.pi * (np.arange(n_ring) + 0.5 * (iz % 2)) / n_ring
-        pts.append(np.stack([R * np.cos(phi), R * np.sin(phi), np.full(n_ring, z)], axis=1))
-    xyz = np.concatenate(pts, axis=0)
-    tri = Delaunay(xyz)
-    tets = tri.simplices.astype(np.int32)
+    n2 = p2.shape[0]
+    xyz = np.concatenate([np.concatenate([p2, np.full((n2, 1), z)], axis=1) for z in zs], axis=0)
+    tets = []
+    for k in range(nz):
+        i, j, l = tri[:, 0], tri[:, 1], tri[:, 2]
+        b, t = k * n2, (k + 1) * n2
+        tets.append(np.stack([i + b, j + b, l + b, l + t], axis=1))
+        tets.append(np.stack([i + b, j + b, j + t, l + t], axis=1))
+        tets.append(np.stack([i + b, i + t, j + t, l + t], axis=1))
+    tets = np.concatenate(tets, axis=0)
     p = xyz[tets]
-    vol = np.einsum("ij,ij->i", np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0]), p[:, 3] - p[:, 0]) / 6.0
-    tets = tets[np.abs(vol) > 1e-3 * h ** 3]
-    used = np.unique(tets)
-    remap = -np.ones(xyz.shape[0], dtype=np.int64)
-    remap[used] = np.arange(used.size)
-    return Mesh(xyz=np.ascontiguousarray(xyz[used]), tets=remap[tets].astype(np.int32),
-                scale=scale, name=name)
+    vol = np.einsum("ij,ij->i", np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0]), p[:, 3] - p[:, 0])
+    neg = vol < 0
+    tets[neg, 2], tets[neg, 3] = tets[neg, 3].copy(), tets[neg, 2].copy()
+    return Mesh(xyz=np.ascontiguousarray(xyz), tets=np.ascontiguousarray(tets, dtype=np.int32), scale=scale,
+                name=name)
 
 
 def union(meshes, name: str = "union"):
@@ -167,6 +174,29 @@ def vortex_state(xyz: np.ndarray, seed: int, core_radius: float = 10.0,
     m = np.stack([mx, my, mz], axis=1)
     m /= np.linalg.norm(m, axis=1, keepdims=True)
     return np.ascontiguousarray(m.T.ravel()), centre
+
+
+def skyrmion_state(xyz: np.ndarray, seed: int, radius: float = 20.0, wall: float = 5.0,
+                   core_shift: float = 2.0, polarity: float = -1.0, helicity: float = 0.0) -> np.ndarray:
+    """Neel skyrmion (helicity 0: radial in-plane rotation, the interfacial-DMI chirality) with a
+    seeded core offset of at most ``core_shift`` from the xy centre of the mesh.
+
+    theta(r) = 2 atan(exp((radius - r) / wall)) measured from the background direction
+    -polarity * z, so the core points along polarity * z.  SoA (3N,), unit length.
+    """
+    rng = np.random.default_rng(seed)
+    lo, hi = xyz[:, :2].min(axis=0), xyz[:, :2].max(axis=0)
+    centre = 0.5 * (lo + hi) + core_shift * rng.uniform(-1, 1, 2)
+    d = xyz[:, :2] - centre
+    r = np.linalg.norm(d, axis=1)
+    th = 2.0 * np.arctan(np.exp((radius - r) / wall))
+    ph = np.arctan2(d[:, 1], d[:, 0]) + helicity
+    mz = -polarity * np.cos(th)
+    mx = np.sin(th) * np.cos(ph)
+    my = np.sin(th) * np.sin(ph)
+    m = np.stack([mx, my, mz], axis=1)
+    m /= np.linalg.norm(m, axis=1, keepdims=True)
+    return np.ascontiguousarray(m.T.ravel())
 
 
 def uniform_state(n: int, direction=(1.0, 0.0, 0.0)) -> np.ndarray:
