@@ -2,15 +2,18 @@
 """Benchmark of tetmag's full field evaluation (demag chain + local field + LLG
 right-hand side) on B200.
 
-A step is one full field evaluation of the 363,609-node permalloy film
-(500x500x20 nm at 2.5 nm, seeded vortex, 20 mT in-plane): divergence, Neumann
-PCG+AMG, dense double-layer BEM matvec, Dirichlet PCG+AMG, gradient, fused
-local field + LLG right-hand side.  The headline path is the mixed one (FP32
-operator values, FP64 vectors / reductions / coarse solve); the plain FP64 path
-is measured in the same run as the speed bar, with the relative error between
-the two.
+Default (c2): a step is one full field evaluation of the 363,609-node permalloy
+film (500x500x20 nm at 2.5 nm, seeded vortex, 20 mT in-plane): divergence,
+Neumann PCG+AMG, hierarchical (leaf 32, eta 2) double-layer BEM matvec,
+Dirichlet PCG+AMG, gradient, fused local field + LLG right-hand side.  The
+headline path is the mixed one (FP32 operator values, FP64 vectors /
+reductions / coarse solve); the plain FP64 paths (hierarchical and dense BEM)
+are measured in the same run as the speed bar, with the relative error between
+them.  Other workloads: c1, c3 (256 uneven dots in one batched context), c4 /
+c4x64 (replicas sharing one dense BEM, the boundary product a GEMM), c5 (the
+interfacial-DMI disk: fixed-step RK4 and its discrete adjoint).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload c2]
 
 Under torchrun each rank evaluates its own replica (independent seed): no
 data-path collective; value = all ranks' evaluations / max-over-ranks time.
@@ -47,9 +50,15 @@ def parse():
     p.add_argument("--tol", type=float, default=1e-7)
     p.add_argument("--sim-ps", type=float, default=2.0, help="simulated ps for the ns/hour figure")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--bem", default="dense", choices=["hmatrix", "hmatrix-dense", "dense"],
-                   help="BEM form of the timed paths (the dense FP64 path is always measured too)")
-    return p.parse_args()
+    p.add_argument("--c5-steps", type=int, default=500, help="time steps of the adjoint workload (c5)")
+    p.add_argument("--bem", default="auto", choices=["auto", "hmatrix", "hmatrix-dense", "dense"],
+                   help="BEM form of the timed paths (the dense FP64 path is always measured too); auto: the "
+                        "hierarchical matrix built from the mesh for c2 (its configuration names the "
+                        "H2-compressed BEM), the dense matrix otherwise")
+    a = p.parse_args()
+    if a.bem == "auto":
+        a.bem = "hmatrix" if a.workload == "c2" else "dense"
+    return a
 
 
 def peak_hbm():
@@ -410,10 +419,125 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
+def run_adjoint(args):
+    """c5: the interfacial-DMI disk integrated with fixed-step RK4 (full field at every stage) and
+    the discrete adjoint of that map.  value = field evaluations / s of the mixed forward run;
+    the adjoint's cost is reported as (forward + backward sweep time) / forward time."""
+    import torch
+    from tetmag_b200 import api, workloads
+    from tetmag_b200.autograd import LLGObjective
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    nsteps = args.c5_steps
+    w = workloads.c5_disk(nsteps=nsteps)
+    info = w.info
+    t0 = time.perf_counter()
+    mo, ctx = workloads.setup_context(w, device=local, mixed=True, tol=args.tol, maxiter=200)
+    nsub = workloads.stable_substeps(w, mo, info["dt_ps"])
+    setup_s = time.perf_counter() - t0
+    n = w.n
+    node_vol = mo.operators()["node_vol"]
+    wv = np.zeros(3 * n)
+    wv[2 * n:] = node_vol / node_vol.sum()                  # J = volume-weighted mean m_z
+    Js, A_, _, axis, D = w.material_arrays()
+    ku0 = np.zeros(n)
+    bz0 = np.asarray(info["bz"])
+    ckpt = info["ckpt_every"]
+    prob = LLGObjective(ctx, Js, A_, axis, D, w.alpha, w.m0, wv, nsteps, info["dt_ps"], nsub=nsub, ckpt_every=ckpt,
+                        bz_t0=info["bz_t0"], bz_t1=info["bz_t1"])
+
+    def sync():
+        torch.cuda.synchronize()
+
+    def timed_forward():
+        sync()
+        t = time.perf_counter()
+        J = prob.forward_only(ku0, bz0)
+        sync()
+        return J, time.perf_counter() - t
+
+    def timed_adjoint():
+        sync()
+        t = time.perf_counter()
+        r = prob.run(ku0, bz0)
+        sync()
+        return r, time.perf_counter() - t
+
+    out = {}
+    clocks = Clocks(local)
+    for mixed in (True, False):
+        ctx.set_precision(mixed)
+        ctx.set_solver_params(args.tol if mixed else 1e-12, 200)
+        if args.warmup > 0:
+            prob.forward_only(ku0, bz0)
+        if mixed:
+            clocks.start()
+        l0 = api.kernel_launches()
+        Jf, tf = timed_forward()
+        launches = api.kernel_launches() - l0
+        r, ta = timed_adjoint()
+        if mixed:
+            clk = clocks.stop()
+        out[mixed] = dict(J=Jf, forward_s=tf, adjoint_s=ta, r=r, launches=launches)
+    mx, f64 = out[True], out[False]
+    evals = 4.0 * nsteps * nsub
+    # directional central differences of the mixed forward map
+    rng = np.random.default_rng(17)
+    ctx.set_precision(True)
+    ctx.set_solver_params(args.tol, 200)
+    fd = {}
+    v = rng.standard_normal(n)
+    eps = 200.0
+    d_ku = (prob.forward_only(ku0 + eps * v, bz0) - prob.forward_only(ku0 - eps * v, bz0)) / (2 * eps)
+    g = float(mx["r"]["grad_ku"] @ v)
+    fd["ku"] = {"fd": d_ku, "adjoint": g, "rel_err": abs(d_ku - g) / abs(g)}
+    v = rng.standard_normal(bz0.size)
+    eps = 1e-3
+    d_bz = (prob.forward_only(ku0, bz0 + eps * v) - prob.forward_only(ku0, bz0 - eps * v)) / (2 * eps)
+    g = float(mx["r"]["grad_bz"] @ v)
+    fd["bz"] = {"fd": d_bz, "adjoint": g, "rel_err": abs(d_bz - g) / abs(g)}
+
+    def rel(a, b):
+        return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(b))
+
+    value = evals / mx["forward_s"]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": 1, "warmup": args.warmup,
+        "ms_per_step": 1e3 * mx["forward_s"] / evals, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 operators / f64 vectors+reductions", "data": "synthetic",
+        "config": {"workload": w.name, "nodes": n, "boundary_nodes": mo.nb, "nnz": mo.nnz, "dmi": "interfacial",
+                   "steps": nsteps, "dt_ps": info["dt_ps"], "rk4_substeps": nsub, "checkpoint_every": ckpt,
+                   "bz_samples": int(bz0.size), "objective": "volume-weighted mean m_z after the run",
+                   "parameters": "per-node Ku (FP32 tensor, baseline 0, easy axis z) and the Bz(t) samples",
+                   "cg_tol": args.tol, "parallelism": "single",
+                   "timing": "host wall clock around synchronous library calls (one stream)"},
+        "gpu_launches": mx["launches"],
+        "clocks": clk,
+        "fp64_value": evals / f64["forward_s"],
+        "sim_ns_per_hour": nsteps * info["dt_ps"] * 1e-3 / (mx["forward_s"] / 3600.0),
+        "adjoint": {
+            "forward_s": mx["forward_s"], "forward_plus_adjoint_s": mx["adjoint_s"],
+            "cost_ratio": mx["adjoint_s"] / mx["forward_s"],
+            "cost_ratio_fp64": f64["adjoint_s"] / f64["forward_s"],
+            "fd_check_mixed": fd,
+            "grad_rel_err_mixed_vs_fp64": {"ku": rel(mx["r"]["grad_ku"], f64["r"]["grad_ku"]),
+                                           "bz": rel(mx["r"]["grad_bz"], f64["r"]["grad_bz"])},
+            "J": {"mixed": mx["J"], "fp64": f64["J"]},
+            "mean_m_diff_mixed_vs_fp64": abs(mx["J"] - f64["J"]),
+            "stats_mixed": mx["r"]["stats"], "stats_fp64": f64["r"]["stats"]},
+        "setup_s": setup_s,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "c5":
+        run_adjoint(args)
     else:
         run_gpu(args)
 
