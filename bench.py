@@ -349,6 +349,37 @@ def run_gpu(args):
     sim_s = max_over_ranks(time.perf_counter() - t)
     ns_per_hour = ninst * (args.sim_ps * 1e-3) / (sim_s / 3600.0)
 
+    # batched workloads: the plain FP64 path one instance at a time (one single-mesh context per
+    # instance, as the reference runs one mesh per process) on a sample of the instances
+    unbatched = None
+    if ninst > 1:
+        sizes = np.diff(w.components)
+        sample = sorted(set(int(i) for i in np.argsort(sizes)[np.linspace(0, ninst - 1, min(ninst, 8)).astype(int)]))
+        if w.shared_bem:
+            sample = sample[:1]
+        t_tot, n_ev = 0.0, 0
+        for c in sample:
+            wc = workloads.component(w, c)
+            _, cx = workloads.setup_context(wc, device=local, mixed=False, tol=args.tol, maxiter=100)
+            cx.set_stream(stream.cuda_stream)
+            mc = torch.from_numpy(np.ascontiguousarray(wc.m0)).to(dev)
+            yc = torch.empty_like(mc)
+            for _ in range(W):
+                cx.field_eval(mc, yc)
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(K):
+                cx.field_eval(mc, yc)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            t_tot += e0.elapsed_time(e1) / 1e3
+            n_ev += K
+            del cx
+        per_inst_s = t_tot / n_ev          # mean time of one instance evaluation
+        unbatched = {"value": 1.0 / per_inst_s, "unit": "instance field evals/s", "instances_sampled": len(sample),
+                     "path": "plain FP64, one single-mesh context per instance, dense BEM, same CG tolerance"}
+
     value = world * ninst * K / (ms_mx / 1e3)
     fp64_value = world * ninst * K / (ms_64 / 1e3)
     peak, peak_kind = peak_hbm()
@@ -389,10 +420,13 @@ def run_gpu(args):
                      "bytes_per_launch": d["bytes_per_launch"], "avg_ms": avg_ms},
         "clocks": clk,
         "fp64_value": fp64_value, "speedup_vs_fp64": value / fp64_value,
+        "plain_fp64_unbatched": unbatched,
+        "speedup_vs_plain_fp64_unbatched": (value / world / unbatched["value"]) if unbatched else None,
         "fp64_dense_value": world * ninst * K / (ms_64d / 1e3), "speedup_vs_fp64_dense": ms_64d / ms_mx,
         "rel_err_vs_fp64": {"hdem": err_h, "ydot": err_y, "reference": "FP64, dense BEM, CG to 1e-12"},
         "rel_err_fp64_hier_vs_dense": {"hdem": err_h64, "ydot": err_y64},
         "bem_info": bem_info,
+        "bem_gemm": ctx.bem_gemm_info() if w.shared_bem else None,
         "local_rhs_evals_per_s": world * local_per_s,
         "sim_ns_per_hour": world * ns_per_hour,
         "relax": {"sim_ps": args.sim_ps, "wall_s": sim_s, "steps": rs["accepted"], "rejected": rs["rejected"],

@@ -413,3 +413,28 @@ def test_interfacial_dmi_local_field(golden):
         ctx.set_precision(False)
         ctx.set_dmi_kind(False)
     assert rel(ctx.effective_field(m), O.rows_to_soa(g["H"])) <= 1e-12
+
+
+@pytest.mark.parametrize("replicas", [64, 70])
+def test_tensor_core_replica_gemm_matches_cuda_cores(replicas):
+    # the 3xTF32 tcgen05 boundary GEMM against the CUDA-core GEMM on the mixed path: one full
+    # 64-replica tile, and 70 replicas (a second, mostly empty tile); plus the FP64 reference
+    base = meshgen.kuhn_cuboid(14, 12, 3, 3.0)
+    m0s = [meshgen.random_state(base.nx, 300 + r) for r in range(replicas)]
+    mesh, off = meshgen.union([base] * replicas)
+    w = workloads.Workload(name="reps", mesh=mesh, Ms=8.0e5, A=1.3e-11, alpha=0.5, m0=meshgen.soa_stack(m0s),
+                           hext=np.zeros(3 * mesh.nx), components=off, shared_bem=True)
+    mo, ctx = workloads.setup_context(w, tol=1e-12, maxiter=300)
+    H64 = ctx.demag_field(w.m0)
+    ctx.set_precision(True)
+    ctx.set_solver_params(1e-11, 300)
+    ctx.set_bem_gemm_kind(False)
+    Hcc = ctx.demag_field(w.m0)
+    ctx.set_bem_gemm_kind(True)
+    Htc = ctx.demag_field(w.m0)
+    info = ctx.bem_gemm_info()
+    assert info["tensor_cores"] and info["split"] >= 1 and info["tuned_ms"]
+    assert rel(Htc, Hcc) <= 2e-6
+    assert rel(Htc, H64) <= MIXED_TOL
+    Htc2 = ctx.demag_field(w.m0)           # second call: tuned split, warm solves
+    assert rel(Htc2, Htc) <= 1e-8

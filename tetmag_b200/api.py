@@ -145,6 +145,17 @@ class Context:
         check(lib().tmb_set_components(self.h, off.size - 1, _iptr(off), 1 if shared_bem else 0))
         return self
 
+    def set_bem_gemm_kind(self, tensor_cores: bool):
+        """Replicas' boundary GEMM on the mixed path: 3xTF32 tensor cores (default) or CUDA cores."""
+        check(lib().tmb_set_bem_gemm_kind(self.h, 1 if tensor_cores else 0))
+        return self
+
+    def bem_gemm_info(self) -> dict:
+        out = (C.c_double * 10)()
+        check(lib().tmb_bem_gemm_info(self.h, out))
+        return {"tensor_cores": bool(out[0]), "split": int(out[1]),
+                "tuned_ms": {k + 1: out[2 + k] for k in range(8) if out[2 + k] > 0}}
+
     def set_bem_dense(self, B: np.ndarray):
         Bc = np.asfortranarray(B, dtype=np.float64)
         check(lib().tmb_set_bem_dense(self.h, Bc.shape[0], Bc.ctypes.data_as(C.POINTER(C.c_double))))

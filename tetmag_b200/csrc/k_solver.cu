@@ -64,6 +64,11 @@ __device__ __forceinline__ bool grid_reduce(const double (&v)[K], double* partia
   return true;
 }
 
+// Entries of a SELL-32 row are visited in chunks of kChunk: the chunk's column indices and
+// values are loaded first (coalesced across the warp), then its kChunk gathers are issued
+// together, so that a thread keeps kChunk gathers in flight (FEM rows hold 10-15 entries).
+constexpr int kChunk = 8;
+
 template <typename V>
 __device__ __forceinline__ double sell_row_dot(const SellView& s, const V* __restrict__ val,
                                                const double* __restrict__ x, int row) {
@@ -71,8 +76,19 @@ __device__ __forceinline__ double sell_row_dot(const SellView& s, const V* __res
   const int beg = __ldg(s.soff + sl) + (row & 31);
   const int end = __ldg(s.soff + sl + 1);
   double acc = 0.0;
-#pragma unroll 4
-  for (int k = beg; k < end; k += kSlice) acc = fma(static_cast<double>(__ldg(val + k)), __ldg(x + __ldg(s.col + k)), acc);
+  for (int k0 = beg; k0 < end; k0 += kChunk * kSlice) {
+    int j[kChunk];
+    double v[kChunk];
+#pragma unroll
+    for (int u = 0; u < kChunk; ++u) {
+      const int k = k0 + u * kSlice;
+      const bool ok = k < end;
+      j[u] = ok ? __ldg(s.col + k) : row;
+      v[u] = ok ? static_cast<double>(__ldg(val + k)) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kChunk; ++u) acc = fma(v[u], __ldg(x + j[u]), acc);
+  }
   return acc;
 }
 
@@ -124,32 +140,90 @@ __global__ void __launch_bounds__(kBlock) k_jacobi0_residual(SellView s, const V
   const int beg = __ldg(s.soff + sl) + (row & 31);
   const int end = __ldg(s.soff + sl + 1);
   double acc = 0.0;
-#pragma unroll 4
-  for (int k = beg; k < end; k += kSlice) {
-    const int j = __ldg(s.col + k);
-    acc = fma(static_cast<double>(__ldg(val + k)), __ldg(dinv + j) * __ldg(b + j), acc);
+  for (int k0 = beg; k0 < end; k0 += kChunk * kSlice) {
+    int j[kChunk];
+    double v[kChunk];
+#pragma unroll
+    for (int u = 0; u < kChunk; ++u) {
+      const int k = k0 + u * kSlice;
+      const bool ok = k < end;
+      j[u] = ok ? __ldg(s.col + k) : row;
+      v[u] = ok ? static_cast<double>(__ldg(val + k)) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kChunk; ++u) acc = fma(v[u], __ldg(dinv + j[u]) * __ldg(b + j[u]), acc);
   }
   const double bi = b[row];
   x[row] = dinv[row] * bi;
   r[row] = bi - acc;
 }
 
-// CSR product for the transfer operators; 4 threads cooperate on a row.
-template <typename V>
+// Sum over the T consecutive lanes that share a row (T a power of two dividing 32).
+template <int T>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+  for (int o = T / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Partial dot of a CSR row over the entries k = beg + sub, beg + sub + T, ... (x premultiplied by
+// w when w is not null).
+template <typename V, int T>
+__device__ __forceinline__ double csr_row_part(const CsrView& c, const V* __restrict__ val, const double* __restrict__ x,
+                                               const double* __restrict__ w, int row, int sub) {
+  double acc = 0.0;
+  if (row < c.n) {
+    const int beg = __ldg(c.ptr + row), end = __ldg(c.ptr + row + 1);
+    for (int k = beg + sub; k < end; k += T) {
+      const int j = __ldg(c.col + k);
+      const double xj = w ? __ldg(w + j) * __ldg(x + j) : __ldg(x + j);
+      acc = fma(static_cast<double>(__ldg(val + k)), xj, acc);
+    }
+  }
+  return acc;
+}
+
+// CSR product (transfer operators, coarse levels); T threads cooperate on a row.
+template <typename V, int T>
 __global__ void __launch_bounds__(kBlock) k_csr_spmv(CsrView c, const V* __restrict__ val,
                                                      const double* __restrict__ x, double* __restrict__ y,
                                                      int accumulate, const int* done) {
   if (done && *done) return;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int row = t >> 2, sub = t & 3;
-  double acc = 0.0;
-  if (row < c.n) {
-    const int beg = __ldg(c.ptr + row), end = __ldg(c.ptr + row + 1);
-    for (int k = beg + sub; k < end; k += 4) acc = fma(static_cast<double>(__ldg(val + k)), __ldg(x + __ldg(c.col + k)), acc);
-  }
-  acc += __shfl_xor_sync(0xffffffffu, acc, 1);
-  acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+  const int row = t / T, sub = t & (T - 1);
+  const double acc = group_sum<T>(csr_row_part<V, T>(c, val, x, nullptr, row, sub));
   if (row < c.n && sub == 0) y[row] = accumulate ? y[row] + acc : acc;
+}
+
+// Coarse levels (rows of 20-60 entries): the first Jacobi sweep from zero fused with the
+// residual, x = D_w^-1 b, r = b - A x, T threads per row.
+template <typename V, int T>
+__global__ void __launch_bounds__(kBlock) k_csr_jacobi0_residual(CsrView c, const V* __restrict__ val,
+                                                                 const double* __restrict__ dinv,
+                                                                 const double* __restrict__ b, double* __restrict__ x,
+                                                                 double* __restrict__ r, const int* done) {
+  if (done && *done) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int row = t / T, sub = t & (T - 1);
+  const double acc = group_sum<T>(csr_row_part<V, T>(c, val, b, dinv, row, sub));
+  if (row < c.n && sub == 0) {
+    const double bi = b[row];
+    x[row] = dinv[row] * bi;
+    r[row] = bi - acc;
+  }
+}
+
+// Coarse levels: xout = xin + D_w^-1 (b - A xin), T threads per row.
+template <typename V, int T>
+__global__ void __launch_bounds__(kBlock) k_csr_jacobi(CsrView c, const V* __restrict__ val,
+                                                       const double* __restrict__ dinv, const double* __restrict__ b,
+                                                       const double* __restrict__ xin, double* __restrict__ xout,
+                                                       const int* done) {
+  if (done && *done) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int row = t / T, sub = t & (T - 1);
+  const double acc = group_sum<T>(csr_row_part<V, T>(c, val, xin, nullptr, row, sub));
+  if (row < c.n && sub == 0) xout[row] = xin[row] + dinv[row] * (b[row] - acc);
 }
 
 // x = A_c^-1 b on the coarsest level: one warp per row of the dense FP64 inverse.
@@ -184,13 +258,12 @@ template <typename V>
 __global__ void __launch_bounds__(kBlock) k_cg_residual(SellView s, const V* __restrict__ val,
                                                         const double* __restrict__ bp, const double* __restrict__ x,
                                                         double* __restrict__ r, CgScalars* S, double* partials) {
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
   double v[2] = {0.0, 0.0};
-  if (row < s.n) {
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < s.n; row += gridDim.x * blockDim.x) {
     const double ri = bp[row] - sell_row_dot(s, val, x, row);
     r[row] = ri;
-    v[0] = ri * ri;
-    v[1] = bp[row] * bp[row];
+    v[0] = fma(ri, ri, v[0]);
+    v[1] = fma(bp[row], bp[row], v[1]);
   }
   double tot[2];
   if (grid_reduce<2>(v, partials, &S->ticket[0], tot) && threadIdx.x == 0) {
@@ -210,8 +283,8 @@ __global__ void __launch_bounds__(kBlock) k_cg_residual(SellView s, const V* __r
 __global__ void __launch_bounds__(kBlock) k_cg_rz(int n, const double* __restrict__ r, const double* __restrict__ z,
                                                   CgScalars* S, double* partials, int first) {
   if (S->done) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double v[1] = {i < n ? r[i] * z[i] : 0.0};
+  double v[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[0] = fma(r[i], z[i], v[0]);
   double tot[1];
   if (grid_reduce<1>(v, partials, &S->ticket[1], tot) && threadIdx.x == 0) {
     if (first) {
@@ -231,13 +304,12 @@ __global__ void __launch_bounds__(kBlock) k_jacobi_rz(SellView s, const V* __res
                                                       const double* __restrict__ xin, double* __restrict__ z,
                                                       CgScalars* S, double* partials, int first) {
   if (S->done) return;
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
   double v[1] = {0.0};
-  if (row < s.n) {
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < s.n; row += gridDim.x * blockDim.x) {
     const double ri = r[row];
     const double zi = xin[row] + dinv[row] * (ri - sell_row_dot(s, val, xin, row));
     z[row] = zi;
-    v[0] = ri * zi;
+    v[0] = fma(ri, zi, v[0]);
   }
   double tot[1];
   if (grid_reduce<1>(v, partials, &S->ticket[1], tot) && threadIdx.x == 0) {
@@ -255,28 +327,34 @@ __global__ void __launch_bounds__(kBlock) k_cg_dir_spmv(SellView s, const V* __r
                                                         double* __restrict__ q, CgScalars* S, double* partials) {
   if (S->done) return;
   const double beta = S->beta;
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
   double v[1] = {0.0};
-  if (row < s.n) {
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < s.n; row += gridDim.x * blockDim.x) {
     const int sl = row >> 5;
     const int beg = __ldg(s.soff + sl) + (row & 31);
     const int end = __ldg(s.soff + sl + 1);
     double acc = 0.0;
-    if (beta == 0.0) {
-#pragma unroll 4
-      for (int k = beg; k < end; k += kSlice)
-        acc = fma(static_cast<double>(__ldg(val + k)), __ldg(z + __ldg(s.col + k)), acc);
-    } else {
-#pragma unroll 4
-      for (int k = beg; k < end; k += kSlice) {
-        const int j = __ldg(s.col + k);
-        acc = fma(static_cast<double>(__ldg(val + k)), fma(beta, __ldg(p_old + j), __ldg(z + j)), acc);
+    for (int k0 = beg; k0 < end; k0 += kChunk * kSlice) {
+      int j[kChunk];
+      double v[kChunk];
+#pragma unroll
+      for (int u = 0; u < kChunk; ++u) {
+        const int k = k0 + u * kSlice;
+        const bool ok = k < end;
+        j[u] = ok ? __ldg(s.col + k) : row;
+        v[u] = ok ? static_cast<double>(__ldg(val + k)) : 0.0;
+      }
+      if (beta == 0.0) {
+#pragma unroll
+        for (int u = 0; u < kChunk; ++u) acc = fma(v[u], __ldg(z + j[u]), acc);
+      } else {
+#pragma unroll
+        for (int u = 0; u < kChunk; ++u) acc = fma(v[u], fma(beta, __ldg(p_old + j[u]), __ldg(z + j[u])), acc);
       }
     }
     const double pi = (beta == 0.0) ? z[row] : fma(beta, p_old[row], z[row]);
     p_new[row] = pi;
     q[row] = acc;
-    v[0] = pi * acc;
+    v[0] = fma(pi, acc, v[0]);
   }
   double tot[1];
   if (grid_reduce<1>(v, partials, &S->ticket[2], tot) && threadIdx.x == 0) {
@@ -298,12 +376,11 @@ __global__ void __launch_bounds__(kBlock) k_cg_spmv_pq(SellView s, const V* __re
                                                        const double* __restrict__ p, double* __restrict__ q,
                                                        CgScalars* S, double* partials) {
   if (S->done) return;
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
   double v[1] = {0.0};
-  if (row < s.n) {
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < s.n; row += gridDim.x * blockDim.x) {
     const double qi = sell_row_dot(s, val, p, row);
     q[row] = qi;
-    v[0] = p[row] * qi;
+    v[0] = fma(p[row], qi, v[0]);
   }
   double tot[1];
   if (grid_reduce<1>(v, partials, &S->ticket[2], tot) && threadIdx.x == 0) {
@@ -316,14 +393,13 @@ __global__ void __launch_bounds__(kBlock) k_cg_update(int n, const double* __res
                                                       const double* __restrict__ q, double* __restrict__ x,
                                                       double* __restrict__ r, CgScalars* S, double* partials) {
   if (S->done) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const double alpha = S->alpha;
   double v[1] = {0.0};
-  if (i < n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     x[i] = fma(alpha, p[i], x[i]);
     const double ri = fma(-alpha, q[i], r[i]);
     r[i] = ri;
-    v[0] = ri * ri;
+    v[0] = fma(ri, ri, v[0]);
   }
   double tot[1];
   if (grid_reduce<1>(v, partials, &S->ticket[3], tot) && threadIdx.x == 0) {
@@ -342,6 +418,19 @@ __global__ void __launch_bounds__(kBlock) k_cg_update(int n, const double* __res
 }
 
 }  // namespace
+
+// Grid of the reduction kernels: at most eight 256-thread blocks per SM (a full SM); the rows
+// beyond are covered by a grid-stride loop, so that the blocks' publish-and-count tails are few.
+int reduce_grid(long long n) {
+  static int cap = 0;
+  if (cap == 0) {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cap = 8 * sms;
+  }
+  const int g = grid_for(n);
+  return g < cap ? g : cap;
+}
 
 template <typename V>
 void launch_spmv(const SellView& s, const V* val, const double* x, double* y, const int* done, cudaStream_t st) {
@@ -364,12 +453,42 @@ void launch_jacobi(const SellView& s, const V* val, const double* dinv, const do
   note_launch();
   k_jacobi<V><<<grid_for(s.n), kBlock, 0, st>>>(s, val, dinv, b, xin, xout, done);
 }
+int csr_threads_per_row(long long nrows, long long nnz) {
+  const double avg = nrows > 0 ? double(nnz) / double(nrows) : 0.0;
+  int t = 1;
+  while (t < 32 && t * 6 < avg) t *= 2;  // about six entries per thread
+  return t;
+}
+
+#define TMB_CSR_DISPATCH(T, KERNEL, NROWS, ...)                                                            \
+  switch (T) {                                                                                            \
+    case 1: KERNEL<V, 1><<<grid_for(1LL * (NROWS)), kBlock, 0, st>>>(__VA_ARGS__); break;                 \
+    case 2: KERNEL<V, 2><<<grid_for(2LL * (NROWS)), kBlock, 0, st>>>(__VA_ARGS__); break;                 \
+    case 4: KERNEL<V, 4><<<grid_for(4LL * (NROWS)), kBlock, 0, st>>>(__VA_ARGS__); break;                 \
+    case 8: KERNEL<V, 8><<<grid_for(8LL * (NROWS)), kBlock, 0, st>>>(__VA_ARGS__); break;                 \
+    case 16: KERNEL<V, 16><<<grid_for(16LL * (NROWS)), kBlock, 0, st>>>(__VA_ARGS__); break;              \
+    default: KERNEL<V, 32><<<grid_for(32LL * (NROWS)), kBlock, 0, st>>>(__VA_ARGS__); break;              \
+  }
+
 template <typename V>
 void launch_csr_spmv(const CsrView& c, const V* val, const double* x, double* y, bool accumulate,
-                     const int* done, cudaStream_t st) {
+                     const int* done, cudaStream_t st, int tpr) {
   note_launch();
-  k_csr_spmv<V><<<grid_for(4LL * c.n), kBlock, 0, st>>>(c, val, x, y, accumulate ? 1 : 0, done);
+  TMB_CSR_DISPATCH(tpr, k_csr_spmv, c.n, c, val, x, y, accumulate ? 1 : 0, done)
 }
+template <typename V>
+void launch_csr_jacobi0_residual(const CsrView& c, const V* val, const double* dinv, const double* b, double* x,
+                                 double* r, const int* done, cudaStream_t st, int tpr) {
+  note_launch();
+  TMB_CSR_DISPATCH(tpr, k_csr_jacobi0_residual, c.n, c, val, dinv, b, x, r, done)
+}
+template <typename V>
+void launch_csr_jacobi(const CsrView& c, const V* val, const double* dinv, const double* b, const double* xin,
+                       double* xout, const int* done, cudaStream_t st, int tpr) {
+  note_launch();
+  TMB_CSR_DISPATCH(tpr, k_csr_jacobi, c.n, c, val, dinv, b, xin, xout, done)
+}
+#undef TMB_CSR_DISPATCH
 void launch_coarse_solve(int n, const double* inv, const double* b, double* x, const int* done, cudaStream_t st) {
   note_launch();
   k_coarse_solve<<<grid_for(32LL * n), kBlock, 0, st>>>(n, inv, b, x, done);
@@ -384,12 +503,12 @@ template <typename V>
 void launch_cg_residual(const SellView& s, const V* val, const double* bp, const double* x, double* r,
                         CgScalars* S, double* partials, cudaStream_t st) {
   note_launch();
-  k_cg_residual<V><<<grid_for(s.n), kBlock, 0, st>>>(s, val, bp, x, r, S, partials);
+  k_cg_residual<V><<<reduce_grid(s.n), kBlock, 0, st>>>(s, val, bp, x, r, S, partials);
 }
 void launch_cg_rz(int n, const double* r, const double* z, CgScalars* S, double* partials, bool first,
                   cudaStream_t st) {
   note_launch();
-  k_cg_rz<<<grid_for(n), kBlock, 0, st>>>(n, r, z, S, partials, first ? 1 : 0);
+  k_cg_rz<<<reduce_grid(n), kBlock, 0, st>>>(n, r, z, S, partials, first ? 1 : 0);
 }
 void launch_cg_pupdate(int n, const double* z, double* p, CgScalars* S, cudaStream_t st) {
   note_launch();
@@ -399,7 +518,7 @@ template <typename V>
 void launch_cg_spmv_pq(const SellView& s, const V* val, const double* p, double* q, CgScalars* S,
                        double* partials, cudaStream_t st) {
   note_launch();
-  k_cg_spmv_pq<V><<<grid_for(s.n), kBlock, 0, st>>>(s, val, p, q, S, partials);
+  k_cg_spmv_pq<V><<<reduce_grid(s.n), kBlock, 0, st>>>(s, val, p, q, S, partials);
 }
 template <typename V>
 void launch_jacobi0_residual(const SellView& s, const V* val, const double* dinv, const double* b, double* x,
@@ -411,19 +530,19 @@ template <typename V>
 void launch_jacobi_rz(const SellView& s, const V* val, const double* dinv, const double* r, const double* xin,
                       double* z, CgScalars* S, double* partials, bool first, cudaStream_t st) {
   note_launch();
-  k_jacobi_rz<V><<<grid_for(s.n), kBlock, 0, st>>>(s, val, dinv, r, xin, z, S, partials, first ? 1 : 0);
+  k_jacobi_rz<V><<<reduce_grid(s.n), kBlock, 0, st>>>(s, val, dinv, r, xin, z, S, partials, first ? 1 : 0);
 }
 template <typename V>
 void launch_cg_dir_spmv(const SellView& s, const V* val, const double* z, const double* p_old, double* p_new,
                         double* q, CgScalars* S, double* partials, cudaStream_t st) {
   note_launch();
-  k_cg_dir_spmv<V><<<grid_for(s.n), kBlock, 0, st>>>(s, val, z, p_old, p_new, q, S, partials);
+  k_cg_dir_spmv<V><<<reduce_grid(s.n), kBlock, 0, st>>>(s, val, z, p_old, p_new, q, S, partials);
 }
 
 void launch_cg_update(int n, const double* p, const double* q, double* x, double* r, CgScalars* S,
                       double* partials, cudaStream_t st) {
   note_launch();
-  k_cg_update<<<grid_for(n), kBlock, 0, st>>>(n, p, q, x, r, S, partials);
+  k_cg_update<<<reduce_grid(n), kBlock, 0, st>>>(n, p, q, x, r, S, partials);
 }
 
 #define TMB_INST(V)                                                                                          \
@@ -433,7 +552,11 @@ void launch_cg_update(int n, const double* p, const double* q, double* x, double
   template void launch_jacobi<V>(const SellView&, const V*, const double*, const double*, const double*,    \
                                  double*, const int*, cudaStream_t);                                        \
   template void launch_csr_spmv<V>(const CsrView&, const V*, const double*, double*, bool, const int*,      \
-                                   cudaStream_t);                                                           \
+                                   cudaStream_t, int);                                                      \
+  template void launch_csr_jacobi0_residual<V>(const CsrView&, const V*, const double*, const double*,      \
+                                               double*, double*, const int*, cudaStream_t, int);            \
+  template void launch_csr_jacobi<V>(const CsrView&, const V*, const double*, const double*, const double*, \
+                                     double*, const int*, cudaStream_t, int);                               \
   template void launch_cg_init<V>(int, const CsrView&, const V*, const int*, const double*, double*,        \
                                   double*, cudaStream_t);                                                   \
   template void launch_cg_residual<V>(const SellView&, const V*, const double*, const double*, double*,     \

@@ -233,7 +233,9 @@ struct Prof {
 // ------------------------------------------------------------------------------------------
 struct DevLevel {
   int n = 0;
-  DevSell A;
+  DevSell A;                 // fine level: SELL-32, one thread per row (about 14 entries per row)
+  DevCsr Ac;                 // coarser levels: CSR, tA threads per row (Galerkin rows of 20-60 entries)
+  int tA = 1, tP = 1, tR = 1;
   DevArray<double> Ad, dinv, X, R, b, out;
   DevArray<float> Af;
   DevCsr P, Rop;
@@ -257,8 +259,9 @@ struct Solver {
   // transposed solve (the adjoint): lift^T, masked load, and a warm start kept apart from the
   // forward one
   DevCsr liftT;
-  DevArray<double> ct, xfwd, xadj;
-  bool has_xadj = false;
+  static constexpr int kAdjSlots = 4;   // one warm start per RK stage
+  DevArray<double> ct, xfwd, xadj[kAdjSlots];
+  bool has_xadj[kAdjSlots] = {false, false, false, false};
   DevArray<double> x, r, z, p[2], q, bp, partials;
   CgScalars* Sd = nullptr;
   CgScalars* Sh = nullptr;
@@ -283,7 +286,9 @@ struct Solver {
   void solve(const double* b_dev, int precision);
   // out = A^-T c for the row-replaced matrix A = [A_FF L; 0 I] (constrained rows C are unit
   // rows): out_F = A_FF^-1 c_F (A_FF is symmetric), out_C = c_C - (L^T out_F)_C
-  void solve_t(const double* c_dev, double* out, int precision);
+  // slot: which of kAdjSlots warm-start vectors to use (the adjoint keeps one per RK stage, since
+  // the same stage's load changes little from one substep to the next)
+  void solve_t(const double* c_dev, double* out, int precision, int slot = 0);
   void vcycle(size_t l, const double* b, double* out, int precision, cudaStream_t st, int rz_mode);
   void precondition_rz(int precision, cudaStream_t st, bool first);
   int pcur = 0;  // which of p[0], p[1] holds the current direction
@@ -348,8 +353,16 @@ struct Ctx {
   int num_sms = 148;
   DevArray<int> xpos;                   // boundary index -> padded position of its component
   DevArray<double> xpad64;
-  DevArray<float> xpad32;
+  DevArray<float> xpad32, xhi32, xlo32;
   int xstride = 0;                      // shared: padded length of one replica's boundary
+  // tensor-core (3xTF32) boundary GEMM of the mixed path: on by default, split-K picked by
+  // tune_gemm_tc on first use; tc_err is the kernel's time-out word
+  bool gemm_tc = true;
+  int tc_split = 0;
+  DevArray<int> tc_err;
+  std::vector<double> tc_tune_ms;       // per candidate split 1..8 (0: not tried)
+  void tune_gemm_tc();
+  void bem_gemm(bool f64, cudaStream_t st);
   DevArray<GemvTile> tiles;
   int ntiles = 0, tile_rows = 1;
   double bem_entries = 0.0;             // matrix entries streamed by one boundary matvec
@@ -404,6 +417,7 @@ struct Ctx {
     stream = own;
     TMB_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
     TMB_CUDA(cudaMallocHost(&bits_h, 4 * sizeof(unsigned long long)));
+    std::memset(bits_h, 0, 4 * sizeof(unsigned long long));
     bits.alloc(4);
   }
   ~Ctx() {
@@ -445,7 +459,7 @@ struct Ctx {
   void end_timed_field();
   void stage_eval(const double* Y, double t_ps, double* k, double* H);
   void rk4_substep(double* y, double t_ps, double ds_ps, double* Ys, double* Hs);
-  void vjp(const double* Y, const double* H, const double* abar, double* gout, double* zpart);
+  void vjp(const double* Y, const double* H, const double* abar, double* gout, double* zpart, int stage);
   void step_rk4(double* m_dev, int nsteps, double dt_ps, int nsub, double t0_ps, bool normalize);
   void adjoint_rk4(const double* m0, int nsteps, double dt_ps, int nsub, int ckpt, double t0_ps, bool normalize,
                    const double* w, double* m_final, double* grad_m0, double* grad_ku, double* grad_bz);
@@ -554,10 +568,15 @@ void Solver::compute() {
     const AmgLevel& hl = H.levels[l];
     DevLevel& d = lev[l];
     d.n = hl.A.nrows;
-    SellHost S = build_sell(d.n, hl.A.ptr.data(), hl.A.col.data());
-    d.A.upload(S, st);
-    d.Ad.upload(sell_values<double>(S, hl.A.val.data()), st);
-    d.Af.upload(sell_values<float>(S, hl.A.val.data()), st);
+    if (l == 0) {
+      SellHost S = build_sell(d.n, hl.A.ptr.data(), hl.A.col.data());
+      d.A.upload(S, st);
+      d.Ad.upload(sell_values<double>(S, hl.A.val.data()), st);
+      d.Af.upload(sell_values<float>(S, hl.A.val.data()), st);
+    } else {
+      d.Ac.upload(hl.A, st);
+      d.tA = csr_threads_per_row(hl.A.nrows, hl.A.nnz());
+    }
     d.dinv.upload(hl.dinv, st);
     d.X.alloc(d.n);
     d.R.alloc(d.n);
@@ -568,13 +587,15 @@ void Solver::compute() {
     if (l + 1 < H.levels.size()) {
       d.P.upload(hl.P, st);
       d.Rop.upload(hl.R, st);
+      d.tP = csr_threads_per_row(hl.P.nrows, hl.P.nnz());
+      d.tR = csr_threads_per_row(hl.R.nrows, hl.R.nnz());
     }
   }
   ncoarse = H.ncoarse;
   cinv.upload(H.coarse_inv, st);
   lift.upload(L, st);
   liftT.upload(LT, st);
-  has_xadj = false;
+  for (bool& h : has_xadj) h = false;
   cmask.upload(cm, st);
   x.alloc(n);
   x.zero(st);
@@ -602,22 +623,35 @@ void Solver::vcycle(size_t l, const double* b, double* out, int precision, cudaS
     return;
   }
   DevLevel& C = lev[l + 1];
-  const SellView A = L.A.view();
   const bool f64 = precision == TMB_FP64;
-  if (f64) launch_jacobi0_residual<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, L.R.p, done, st);
-  else launch_jacobi0_residual<float>(A, L.Af.p, L.dinv.p, b, L.X.p, L.R.p, done, st);
-  if (f64) launch_csr_spmv<double>(L.Rop.view(), L.Rop.v.p, L.R.p, C.b.p, false, done, st);
-  else launch_csr_spmv<float>(L.Rop.view(), L.Rop.vf.p, L.R.p, C.b.p, false, done, st);
-  vcycle(l + 1, C.b.p, C.out.p, precision, st, -1);
-  if (f64) launch_csr_spmv<double>(L.P.view(), L.P.v.p, C.out.p, L.X.p, true, done, st);
-  else launch_csr_spmv<float>(L.P.view(), L.P.vf.p, C.out.p, L.X.p, true, done, st);
-  if (l == 0 && rz_mode >= 0) {
-    // finest level: the post-smoothing sweep also reduces r.z for the next CG direction
-    if (f64) launch_jacobi_rz<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, out, Sd, partials.p, rz_mode == 1, st);
-    else launch_jacobi_rz<float>(A, L.Af.p, L.dinv.p, b, L.X.p, out, Sd, partials.p, rz_mode == 1, st);
+  if (l == 0) {
+    const SellView A = L.A.view();
+    if (f64) launch_jacobi0_residual<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, L.R.p, done, st);
+    else launch_jacobi0_residual<float>(A, L.Af.p, L.dinv.p, b, L.X.p, L.R.p, done, st);
   } else {
-    if (f64) launch_jacobi<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, out, done, st);
-    else launch_jacobi<float>(A, L.Af.p, L.dinv.p, b, L.X.p, out, done, st);
+    const CsrView A = L.Ac.view();
+    if (f64) launch_csr_jacobi0_residual<double>(A, L.Ac.v.p, L.dinv.p, b, L.X.p, L.R.p, done, st, L.tA);
+    else launch_csr_jacobi0_residual<float>(A, L.Ac.vf.p, L.dinv.p, b, L.X.p, L.R.p, done, st, L.tA);
+  }
+  if (f64) launch_csr_spmv<double>(L.Rop.view(), L.Rop.v.p, L.R.p, C.b.p, false, done, st, L.tR);
+  else launch_csr_spmv<float>(L.Rop.view(), L.Rop.vf.p, L.R.p, C.b.p, false, done, st, L.tR);
+  vcycle(l + 1, C.b.p, C.out.p, precision, st, -1);
+  if (f64) launch_csr_spmv<double>(L.P.view(), L.P.v.p, C.out.p, L.X.p, true, done, st, L.tP);
+  else launch_csr_spmv<float>(L.P.view(), L.P.vf.p, C.out.p, L.X.p, true, done, st, L.tP);
+  if (l == 0) {
+    const SellView A = L.A.view();
+    if (rz_mode >= 0) {
+      // finest level: the post-smoothing sweep also reduces r.z for the next CG direction
+      if (f64) launch_jacobi_rz<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, out, Sd, partials.p, rz_mode == 1, st);
+      else launch_jacobi_rz<float>(A, L.Af.p, L.dinv.p, b, L.X.p, out, Sd, partials.p, rz_mode == 1, st);
+    } else {
+      if (f64) launch_jacobi<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, out, done, st);
+      else launch_jacobi<float>(A, L.Af.p, L.dinv.p, b, L.X.p, out, done, st);
+    }
+  } else {
+    const CsrView A = L.Ac.view();
+    if (f64) launch_csr_jacobi<double>(A, L.Ac.v.p, L.dinv.p, b, L.X.p, out, done, st, L.tA);
+    else launch_csr_jacobi<float>(A, L.Ac.vf.p, L.dinv.p, b, L.X.p, out, done, st, L.tA);
   }
 }
 
@@ -687,22 +721,24 @@ void Solver::solve(const double* b_dev, int precision) {
   has_x = true;
 }
 
-void Solver::solve_t(const double* c, double* out, int precision) {
+void Solver::solve_t(const double* c, double* out, int precision, int slot) {
   cudaStream_t st = ctx->stream;
+  slot = (slot < 0 || slot >= kAdjSlots) ? 0 : slot;
   ct.alloc(n);
   xfwd.alloc(n);
-  if (!has_xadj) {
-    xadj.alloc(n);
-    xadj.zero(st);
-    has_xadj = true;
+  DevArray<double>& xa = xadj[slot];
+  if (!has_xadj[slot]) {
+    xa.alloc(n);
+    xa.zero(st);
+    has_xadj[slot] = true;
   }
   launch_mask_constrained(n, cmask.p, c, ct.p, st);
   TMB_CUDA(cudaMemcpyAsync(xfwd.p, x.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-  TMB_CUDA(cudaMemcpyAsync(x.p, xadj.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  TMB_CUDA(cudaMemcpyAsync(x.p, xa.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
   solve(ct.p, precision);
   if (precision == TMB_FP64) launch_lift_t<double>(n, liftT.view(), liftT.v.p, cmask.p, c, x.p, out, st);
   else launch_lift_t<float>(n, liftT.view(), liftT.vf.p, cmask.p, c, x.p, out, st);
-  TMB_CUDA(cudaMemcpyAsync(xadj.p, x.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  TMB_CUDA(cudaMemcpyAsync(xa.p, x.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
   TMB_CUDA(cudaMemcpyAsync(x.p, xfwd.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
 }
 
@@ -818,6 +854,8 @@ void Ctx::plan_components() {
       for (int k = 0; k < nbc; ++k) pos[cboff[c] + k] = c * xstride + k;
     xpad64.alloc(size_t(xstride) * nc);
     xpad32.alloc(size_t(xstride) * nc);
+    xhi32.alloc(size_t(xstride) * nc);
+    xlo32.alloc(size_t(xstride) * nc);
     bem_entries = double(nbc) * nbc;
     ntiles = 0;
   } else {
@@ -957,8 +995,7 @@ void Ctx::demag(const double* m) {
     else launch_gather_pad<float>(nb, neu->x.p, bnodes.p, xpos.p, xpad32.p, st);
     prof.begin(3, st, bem_entries * sv + B * (sv + 8));
     if (shared_bem) {
-      if (f64) launch_bem_gemm<double>(cboff[1], ncomp(), Bd.p, xpad64.p, xstride, u2b.p, num_sms, st);
-      else launch_bem_gemm<float>(cboff[1], ncomp(), Bf.p, xpad32.p, xstride, u2b.p, num_sms, st);
+      bem_gemm(f64, st);
     } else {
       if (f64) launch_bem_gemv_tiles<double>(ntiles, tiles.p, tile_rows, Bd.p, xpad64.p, u2b.p, st);
       else launch_bem_gemv_tiles<float>(ntiles, tiles.p, tile_rows, Bf.p, xpad32.p, u2b.p, st);
@@ -975,7 +1012,9 @@ void Ctx::demag(const double* m) {
     launch_dirichlet_values(n, bindex.p, u2b.p, bdir.p, st);
   }
   prof.begin(5, st, 0.0);
-  dir->solve(bdir.p, precision);
+  dir->solve(bdir.p, precision);  // synchronises: the GEMM's time-out word is readable below
+  if (shared_bem && !f64 && gemm_tc && bits_h[2] != 0)
+    throw Error(TMB_ERR_CUDA, "tensor-core boundary GEMM timed out waiting on a barrier");
   prof.end(st);
   prof.begin(2, st, z * (3 * sv + 4) + N * 8 * 11);
   if (f64) launch_gradient<double>(S, g[0].p, g[1].p, g[2].p, neu->x.p, dir->x.p, hext.p, hdem.p, hfix.p, st);
@@ -986,6 +1025,59 @@ void Ctx::demag(const double* m) {
   if (neu->last_status == 5 || dir->last_status == 5) throw Error(TMB_ERR_NAN, "demag solve broke down (NaN)");
   if (neu->last_status == 3 || dir->last_status == 3)
     throw Error(TMB_ERR_NOCONVERGE, "demag solve did not converge within maxiter");
+}
+
+// Replicas' boundary product.  Mixed path: the 3xTF32 tensor-core GEMM (its time-out word is
+// copied to the pinned bits_h[2] behind it); FP64 path: the CUDA-core GEMM.
+void Ctx::bem_gemm(bool f64, cudaStream_t st) {
+  const int nbc = cboff[1], nc = ncomp();
+  if (f64 || !gemm_tc || !bem_gemm_tc_supported(nbc, bem_ld(nbc), xstride)) {
+    if (f64) launch_bem_gemm<double>(nbc, nc, Bd.p, xpad64.p, xstride, u2b.p, num_sms, st);
+    else launch_bem_gemm<float>(nbc, nc, Bf.p, xpad32.p, xstride, u2b.p, num_sms, st);
+    return;
+  }
+  if (tc_split == 0) tune_gemm_tc();
+  launch_bem_gemm_tc(nbc, nc, bem_ld(nbc), Bf.p, xpad32.p, xstride, xhi32.p, xlo32.p, u2b.p, tc_split, tc_err.p, st);
+  TMB_CUDA(cudaMemcpyAsync(bits_h + 2, tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+}
+
+// Autotuner of the tensor-core GEMM's K split: every candidate that gives at least one CTA per
+// SM is timed (CUDA events, three launches after one warm-up) on the current panel, the fastest
+// is kept for the context.
+void Ctx::tune_gemm_tc() {
+  const int nbc = cboff[1], nc = ncomp();
+  cudaStream_t st = stream;
+  tc_err.alloc(1);
+  tc_err.zero(st);
+  const int mt = (nbc + 127) / 128 * ((nc + 63) / 64), nks = (nbc + 31) / 32;
+  cudaEvent_t e0, e1;
+  TMB_CUDA(cudaEventCreate(&e0));
+  TMB_CUDA(cudaEventCreate(&e1));
+  tc_tune_ms.assign(9, 0.0);
+  double best = 1e300;
+  int best_split = 1;
+  for (int sp = 1; sp <= 8; ++sp) {
+    if (sp > nks || (sp > 1 && mt * (sp - 1) >= 2 * num_sms)) break;
+    launch_bem_gemm_tc(nbc, nc, bem_ld(nbc), Bf.p, xpad32.p, xstride, xhi32.p, xlo32.p, u2b.p, sp, tc_err.p, st);
+    TMB_CUDA(cudaEventRecord(e0, st));
+    for (int r = 0; r < 3; ++r)
+      launch_bem_gemm_tc(nbc, nc, bem_ld(nbc), Bf.p, xpad32.p, xstride, xhi32.p, xlo32.p, u2b.p, sp, tc_err.p, st);
+    TMB_CUDA(cudaEventRecord(e1, st));
+    TMB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    TMB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    tc_tune_ms[sp] = ms / 3.0;
+    if (ms < best) {
+      best = ms;
+      best_split = sp;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  int err = 0;
+  TMB_CUDA(cudaMemcpy(&err, tc_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) throw Error(TMB_ERR_CUDA, "tensor-core boundary GEMM timed out waiting on a barrier");
+  tc_split = best_split;
 }
 
 template <typename T>
@@ -1529,7 +1621,7 @@ void Ctx::rk4_substep(double* y, double t_ps, double ds_ps, double* Ys, double* 
 // gout = (df/dm)(Y)^T abar at one stage; dku accumulates (df/dKu)^T abar, zpart gets the block
 // partial sums of mu_z (the Bz gradient).  The demag part runs the chain backwards:
 // w = -grad^T mu, v = A_D^-T w, a = w + (B^T v_b scattered), a1 = A_N^-T a, div^T a1.
-void Ctx::vjp(const double* Y, const double* H, const double* abar, double* gout, double* zpart) {
+void Ctx::vjp(const double* Y, const double* H, const double* abar, double* gout, double* zpart, int stage) {
   const bool f64 = precision == TMB_FP64;
   const SellView S = pat.view();
   AdjPreArgs pa{};
@@ -1550,13 +1642,13 @@ void Ctx::vjp(const double* Y, const double* H, const double* abar, double* gout
   if (has_bem) {
     if (f64) launch_divergence<double>(S, tg[0].p, tg[1].p, tg[2].p, ab.mu.p, ab.ninvvol.p, 1.0, ab.w.p, stream);
     else launch_divergence<float>(S, tgf[0].p, tgf[1].p, tgf[2].p, ab.mu.p, ab.ninvvol.p, 1.0, ab.w.p, stream);
-    dir->solve_t(ab.w.p, ab.v.p, precision);
+    dir->solve_t(ab.w.p, ab.v.p, precision, stage);
     launch_gather<double>(nb, ab.v.p, bnodes.p, ab.vb.p, stream);
     const int nch = bem_gemv_t_chunks(nb, num_sms);
     if (f64) launch_bem_gemv_t<double>(nb, Bd.p, ab.vb.p, ab.bpart.p, nch, ab.z.p, stream);
     else launch_bem_gemv_t<float>(nb, Bf.p, ab.vb.p, ab.bpart.p, nch, ab.z.p, stream);
     launch_scatter_add(nb, bnodes.p, ab.z.p, ab.w.p, stream);
-    neu->solve_t(ab.w.p, ab.a1.p, precision);
+    neu->solve_t(ab.w.p, ab.a1.p, precision, stage);
     cnt[4] += neu->last_iters + dir->last_iters;
     if (f64) launch_gradient<double>(S, g[0].p, g[1].p, g[2].p, ab.a1.p, nullptr, nullptr, ab.q.p, nullptr, stream);
     else launch_gradient<float>(S, gf[0].p, gf[1].p, gf[2].p, ab.a1.p, nullptr, nullptr, ab.q.p, nullptr, stream);
@@ -1687,13 +1779,13 @@ void Ctx::adjoint_rk4(const double* m0, int nsteps, double dt_ps, int nsub, int 
         double* lam = ab.lam.p;
         double* a = ab.abar.p;
         launch_lincomb(int(n3), a, h / 6.0, lam, 0.0, nullptr, 0.0, nullptr, st);
-        vjp(Y + 3 * n3, Hs + 3 * n3, a, G[3], zp + 3 * nblk);
+        vjp(Y + 3 * n3, Hs + 3 * n3, a, G[3], zp + 3 * nblk, 3);
         launch_lincomb(int(n3), a, h / 3.0, lam, h, G[3], 0.0, nullptr, st);
-        vjp(Y + 2 * n3, Hs + 2 * n3, a, G[2], zp + 2 * nblk);
+        vjp(Y + 2 * n3, Hs + 2 * n3, a, G[2], zp + 2 * nblk, 2);
         launch_lincomb(int(n3), a, h / 3.0, lam, 0.5 * h, G[2], 0.0, nullptr, st);
-        vjp(Y + n3, Hs + n3, a, G[1], zp + nblk);
+        vjp(Y + n3, Hs + n3, a, G[1], zp + nblk, 1);
         launch_lincomb(int(n3), a, h / 6.0, lam, 0.5 * h, G[1], 0.0, nullptr, st);
-        vjp(Y, Hs, a, G[0], zp);
+        vjp(Y, Hs, a, G[0], zp, 0);
         launch_lincomb(int(n3), lam, 1.0, lam, 1.0, G[0], 1.0, G[1], st);
         launch_lincomb(int(n3), lam, 1.0, lam, 1.0, G[2], 1.0, G[3], st);
       }
@@ -2372,6 +2464,24 @@ int tmb_relax(tmb_ctx* ctx, double* m, double duration_ps, double segment_ps, do
     TMB_CUDA(cudaMemcpyAsync(m, c.in3.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     c.sync();
   }
+  TMB_API_END
+}
+
+int tmb_set_bem_gemm_kind(tmb_ctx* ctx, int tensor_cores) {
+  TMB_CHECK_ARG(ctx && (tensor_cores == 0 || tensor_cores == 1), "tmb_set_bem_gemm_kind: kind is 0 or 1");
+  TMB_API_BEGIN
+  ctx->c->gemm_tc = tensor_cores != 0;
+  TMB_API_END
+}
+
+int tmb_bem_gemm_info(tmb_ctx* ctx, double* out) {
+  TMB_CHECK_ARG(ctx && out, "tmb_bem_gemm_info: null argument");
+  TMB_API_BEGIN
+  const Ctx& c = *ctx->c;
+  for (int i = 0; i < 10; ++i) out[i] = 0.0;
+  out[0] = c.gemm_tc ? 1.0 : 0.0;
+  out[1] = c.tc_split;
+  for (size_t i = 1; i < c.tc_tune_ms.size() && i <= 8; ++i) out[1 + i] = c.tc_tune_ms[i];
   TMB_API_END
 }
 

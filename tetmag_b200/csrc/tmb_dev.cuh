@@ -104,9 +104,18 @@ void launch_jacobi0(int n, const double* dinv, const double* b, double* x, const
 template <typename V>
 void launch_jacobi(const SellView& s, const V* val, const double* dinv, const double* b, const double* xin,
                    double* xout, const int* done, cudaStream_t st);
+// CSR kernels with tpr (1, 2, 4, 8, 16, 32) threads per row; csr_threads_per_row picks it from
+// the average row length (about six entries per thread)
+int csr_threads_per_row(long long nrows, long long nnz);
 template <typename V>
 void launch_csr_spmv(const CsrView& c, const V* val, const double* x, double* y, bool accumulate,
-                     const int* done, cudaStream_t st);
+                     const int* done, cudaStream_t st, int tpr = 4);
+template <typename V>
+void launch_csr_jacobi0_residual(const CsrView& c, const V* val, const double* dinv, const double* b, double* x,
+                                 double* r, const int* done, cudaStream_t st, int tpr);
+template <typename V>
+void launch_csr_jacobi(const CsrView& c, const V* val, const double* dinv, const double* b, const double* xin,
+                       double* xout, const int* done, cudaStream_t st, int tpr);
 void launch_coarse_solve(int n, const double* inv, const double* b, double* x, const int* done, cudaStream_t st);
 
 template <typename V>
@@ -159,6 +168,14 @@ void launch_bem_gemv_tiles(int ntiles, const GemvTile* tiles, int rows_per_tile,
                            cudaStream_t st);
 template <typename V>
 void launch_bem_gemm(int nbc, int ncomp, const V* B, const V* X, int xs, double* Y, int num_sms, cudaStream_t st);
+
+// 3xTF32 tensor-core GEMM of shared-mesh replicas (k_bem_tc.cu): Y = B X on FP32 B and X,
+// FP64 Y ([replica][row]); Xhi / Xlo receive the TF32 split of X (same layout); split = K
+// splits (partial sums added atomically into a zeroed Y);
+// err is set when a barrier wait timed out.
+bool bem_gemm_tc_supported(int nbc, size_t ld, int xs);
+void launch_bem_gemm_tc(int nbc, int ncomp, size_t ld, const float* B, const float* X, int xs, float* Xhi,
+                        float* Xlo, double* Y, int split, int* err, cudaStream_t st);
 
 // --- hierarchical BEM matrix (k_hmatrix.cu) ---------------------------------------------
 struct HBlockDev {
