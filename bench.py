@@ -484,18 +484,22 @@ def run_adjoint(args):
     def sync():
         torch.cuda.synchronize()
 
-    def timed_forward():
+    def timed_forward(tag):
         sync()
+        torch.cuda.nvtx.range_push(f"timed_forward_{tag}")
         t = time.perf_counter()
         J = prob.forward_only(ku0, bz0)
         sync()
+        torch.cuda.nvtx.range_pop()
         return J, time.perf_counter() - t
 
-    def timed_adjoint():
+    def timed_adjoint(tag):
         sync()
+        torch.cuda.nvtx.range_push(f"timed_adjoint_{tag}")
         t = time.perf_counter()
         r = prob.run(ku0, bz0)
         sync()
+        torch.cuda.nvtx.range_pop()
         return r, time.perf_counter() - t
 
     out = {}
@@ -508,9 +512,10 @@ def run_adjoint(args):
         if mixed:
             clocks.start()
         l0 = api.kernel_launches()
-        Jf, tf = timed_forward()
+        tag = "mixed" if mixed else "fp64"
+        Jf, tf = timed_forward(tag)
         launches = api.kernel_launches() - l0
-        r, ta = timed_adjoint()
+        r, ta = timed_adjoint(tag)
         if mixed:
             clk = clocks.stop()
         out[mixed] = dict(J=Jf, forward_s=tf, adjoint_s=ta, r=r, launches=launches)
