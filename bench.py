@@ -149,7 +149,9 @@ def cpu_baseline_sample(w, samples: int = 1):
     from oracle import cpu_baseline, tetmag_oracle as O
     from tetmag_b200 import workloads
 
-    if w.components is not None:
+    if w.replicas > 1:
+        w = workloads.component(w, 0)
+    elif w.components is not None:
         sizes = np.diff(w.components)
         w = workloads.component(w, int(np.argsort(sizes)[len(sizes) // 2]))
     axis = None if w.ku_axis is None else O.soa_to_rows(w.ku_axis)
@@ -223,7 +225,7 @@ def run_gpu(args):
     stream = torch.cuda.Stream(dev)
     ctx.set_stream(stream.cuda_stream)
     torch.cuda.set_stream(stream)
-    n = w.n
+    n = w.m0.size // 3          # state nodes (all instances)
     K, W = args.steps, args.warmup
 
     # W + K distinct states: the seeded initial state with seeded perturbations
@@ -353,10 +355,12 @@ def run_gpu(args):
     # instance, as the reference runs one mesh per process) on a sample of the instances
     unbatched = None
     if ninst > 1:
-        sizes = np.diff(w.components)
-        sample = sorted(set(int(i) for i in np.argsort(sizes)[np.linspace(0, ninst - 1, min(ninst, 8)).astype(int)]))
-        if w.shared_bem:
-            sample = sample[:1]
+        if w.replicas > 1 or w.shared_bem:
+            sample = [0]                 # identical meshes: one instance's rate
+        else:
+            sizes = np.diff(w.components)
+            sample = sorted(set(int(i) for i in
+                                np.argsort(sizes)[np.linspace(0, ninst - 1, min(ninst, 8)).astype(int)]))
         t_tot, n_ev = 0.0, 0
         for c in sample:
             wc = workloads.component(w, c)
@@ -400,7 +404,10 @@ def run_gpu(args):
         "dtype": "f32 operators / f64 vectors+reductions", "data": "synthetic",
         "config": {"workload": w.name, "nodes": n, "boundary_nodes": mo.nb, "nnz": mo.nnz, "instances": ninst,
                    "batched": (None if ninst == 1 else
-                               ("replicas of one mesh sharing one BEM matrix (boundary matvec = one GEMM)"
+                               ("interleaved replicas of one mesh: every operator row applied to all replicas "
+                                "at once, the boundary product one GEMM (3xTF32 tensor cores on the mixed path)"
+                                if w.replicas > 1 else
+                                "replicas of one mesh sharing one BEM matrix (boundary matvec = one GEMM)"
                                 if w.shared_bem else "uneven meshes, one BEM block each, one batched matvec")
                                + "; one CG and one step size for the batch; value counts instance evals"),
                    "bem": ("hierarchical (leaf 32, eta 2, ACA: FP32 terms to 1e-6 on the mixed path, FP64 "
@@ -426,7 +433,7 @@ def run_gpu(args):
         "rel_err_vs_fp64": {"hdem": err_h, "ydot": err_y, "reference": "FP64, dense BEM, CG to 1e-12"},
         "rel_err_fp64_hier_vs_dense": {"hdem": err_h64, "ydot": err_y64},
         "bem_info": bem_info,
-        "bem_gemm": ctx.bem_gemm_info() if w.shared_bem else None,
+        "bem_gemm": ctx.bem_gemm_info() if (w.shared_bem or w.replicas > 1) else None,
         "local_rhs_evals_per_s": world * local_per_s,
         "sim_ns_per_hour": world * ns_per_hour,
         "relax": {"sim_ps": args.sim_ps, "wall_s": sim_s, "steps": rs["accepted"], "rejected": rs["rejected"],

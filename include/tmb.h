@@ -109,6 +109,16 @@ int tmb_set_bem_dense(tmb_ctx* ctx, int nb, const double* B_colmajor);
  * No tetmag counterpart (tetmag runs one mesh per process).  Call before tmb_bem_assemble; the
  * hierarchical BEM and tmb_set_bem_dense / tmb_get_bem_dense need ncomp = 1. */
 int tmb_set_components(tmb_ctx* ctx, int ncomp, const int* node_offsets, int shared_bem);
+/* R interleaved replicas of the context's single mesh (same operators, material and BEM matrix;
+ * own state and applied field each): every state vector (m, ydot, fields, tmb_set_applied_field)
+ * then holds 3 * N * R doubles, component d of node i of replica r at d * N * R + i * R + r.
+ * Every operator row is applied to the R replicas at once (a warp reads the row's indices and
+ * values once for 32 replicas), the two solves are one CG over the replicas, and the boundary
+ * product is one GEMM (tmb_set_bem_gemm_kind).  Call after tmb_set_mesh and before
+ * tmb_bem_assemble / tmb_set_bem_dense; material arrays stay per node (N).  Not with
+ * tmb_set_components, the hierarchical BEM or the adjoint.  No tetmag counterpart (tetmag runs
+ * one magnetisation per process). */
+int tmb_set_replicas(tmb_ctx* ctx, int nrep);
 /* Boundary GEMM of shared-mesh replicas on the mixed path: 1 (default) the 3xTF32 tensor-core
  * kernel (tcgen05, FP32 accumulation per K split, FP64 sum of the splits), 0 the CUDA-core kernel
  * (FP32 products, FP64 accumulation).  The FP64 path always uses the CUDA-core kernel.  The K

@@ -438,3 +438,35 @@ def test_tensor_core_replica_gemm_matches_cuda_cores(replicas):
     assert rel(Htc, H64) <= MIXED_TOL
     Htc2 = ctx.demag_field(w.m0)           # second call: tuned split, warm solves
     assert rel(Htc2, Htc) <= 1e-8
+
+
+@pytest.mark.parametrize("R", [5, 40])
+def test_interleaved_replicas_match_separate_contexts(R):
+    # R interleaved replicas of one cuboid (operators applied to all replicas at once, the boundary
+    # product one GEMM) against R single-mesh contexts: FP64 to 1e-10, mixed to 1e-5; R = 5 mixes
+    # operator rows inside a warp, R = 40 gives warps of one row and warps that straddle two rows
+    base = meshgen.kuhn_cuboid(10, 9, 3, 3.0)
+    m0s = [meshgen.random_state(base.nx, 500 + r) for r in range(R)]
+    hx = [meshgen.field_from_angles(base.nx, 0.002 * r, 13.0 * r, 7.0 * r) for r in range(R)]
+    w = workloads.Workload(name="irep", mesh=base, Ms=8.0e5, A=1.3e-11, alpha=0.5, m0=meshgen.interleave(m0s),
+                           hext=meshgen.interleave(hx), replicas=R)
+    mo, ctx = workloads.setup_context(w, tol=1e-13, maxiter=300)
+    H = meshgen.deinterleave(ctx.demag_field(w.m0), R)
+    Y = meshgen.deinterleave(ctx.llg_rhs(0.0, w.m0), R)
+    torque = ctx.max_torque(w.m0)
+    ref = _separate([base] * R, m0s, hx, [None] * R, 0.0, 0.5)
+    for r in range(R):
+        assert rel(H[r], ref[r][0]) <= 1e-10
+        assert rel(Y[r], ref[r][1]) <= 1e-10
+    assert torque > 0.0
+    ctx.set_precision(True)
+    ctx.set_solver_params(1e-10, 300)
+    Hm = meshgen.deinterleave(ctx.demag_field(w.m0), R)
+    for r in range(R):
+        assert rel(Hm[r], ref[r][0]) <= MIXED_TOL
+    # a short relaxation of the batch stays normalised and finite
+    m = w.m0.copy()
+    st = ctx.relax(m, duration_ps=0.5, segment_ps=0.25)
+    assert np.isfinite(st["max_torque"])
+    nrm = np.linalg.norm(m.reshape(3, -1), axis=0)
+    assert np.max(np.abs(nrm - 1.0)) < 1e-12

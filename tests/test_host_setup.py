@@ -94,3 +94,13 @@ def test_union_and_soa_round_trip():
     assert mu.nb == ma.nb + MeshOps(b.xyz, b.tets).nb
     Ku, Ka = mu.operators(), ma.operators()
     assert np.allclose(Ku["stiff"][:Ka["rowptr"][-1]], Ka["stiff"], rtol=0, atol=0)
+
+
+def test_interleave_roundtrip():
+    rng = np.random.default_rng(0)
+    vs = [rng.standard_normal(3 * 7) for _ in range(4)]
+    v = meshgen.interleave(vs)
+    assert v.shape == (3 * 7 * 4,)
+    assert v[1 * 7 * 4 + 2 * 4 + 3] == vs[3][1 * 7 + 2]      # y of node 2, replica 3
+    for a, b in zip(meshgen.deinterleave(v, 4), vs):
+        assert np.array_equal(a, b)

@@ -39,6 +39,7 @@ SIGNATURES = {
     "tmb_bem_assemble_ex": [_P, _P, _int],
     "tmb_set_bem_dense": [_P, _int, _D],
     "tmb_set_components": [_P, _int, _I, _int],
+    "tmb_set_replicas": [_P, _int],
     "tmb_set_bem_gemm_kind": [_P, _int],
     "tmb_bem_gemm_info": [_P, _D],
     "tmb_get_bem_dense": [_P, _D],

@@ -110,6 +110,7 @@ class Context:
         self.h = h
         self.n = 0
         self.nb = 0
+        self.rep = 1
 
     def __del__(self):
         h = getattr(self, "h", None)
@@ -143,6 +144,13 @@ class Context:
         """The mesh is a disjoint union of components (batched instances); see tmb_set_components."""
         off = _i32(node_offsets)
         check(lib().tmb_set_components(self.h, off.size - 1, _iptr(off), 1 if shared_bem else 0))
+        return self
+
+    def set_replicas(self, nrep: int):
+        """nrep interleaved replicas of the mesh (tmb_set_replicas): state vectors become 3 N nrep long,
+        node i of replica r at i * nrep + r in each component."""
+        check(lib().tmb_set_replicas(self.h, int(nrep)))
+        self.rep = int(nrep)
         return self
 
     def set_bem_gemm_kind(self, tensor_cores: bool):
@@ -245,9 +253,9 @@ class Context:
     # --- evaluation ----------------------------------------------------------------------
     def _out_like(self, m):
         if isinstance(m, np.ndarray):
-            return np.empty(3 * self.n)
+            return np.empty(3 * self.n * self.rep)
         import torch
-        return torch.empty(3 * self.n, dtype=torch.float64, device=m.device)
+        return torch.empty(3 * self.n * self.rep, dtype=torch.float64, device=m.device)
 
     def demag_field(self, m, out=None):
         out = self._out_like(m) if out is None else out

@@ -198,6 +198,27 @@ __global__ void __launch_bounds__(256) k_bem_gemm(int nbc, int ncomp, size_t ld,
     }
 }
 
+// Interleaved replicas: X[r * xs + b] = u[bnodes[b] * R + r] (t over nb * R, coalesced reads).
+template <typename V>
+__global__ void k_gather_rep(int nb, int R, const double* __restrict__ u, const int* __restrict__ idx, int xs,
+                             V* __restrict__ X) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nb * R) return;
+  const int b = int(t / R), r = int(t - (long long)b * R);
+  X[size_t(r) * xs + b] = static_cast<V>(u[size_t(__ldg(idx + b)) * R + r]);
+}
+
+// Interleaved replicas: Dirichlet load of state row g = i * R + r from the GEMM output
+// Y[r * nb + bindex[i]] (0 inside).
+__global__ void k_dirichlet_rep(int n, int R, const int* __restrict__ bindex, const double* __restrict__ Y, int nb,
+                                double* __restrict__ b) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (long long)n * R) return;
+  const int i = int(g / R), r = int(g - (long long)i * R);
+  const int k = bindex[i];
+  b[g] = (k >= 0) ? Y[size_t(r) * nb + k] : 0.0;
+}
+
 __global__ void k_dirichlet_values(int n, const int* __restrict__ bindex, const double* __restrict__ u2b,
                                    double* __restrict__ b) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -263,6 +284,19 @@ void launch_bem_gemm(int nbc, int ncomp, const V* B, const V* X, int xs, double*
   TMB_CUDA(cudaGetLastError());
 }
 
+template <typename V>
+void launch_gather_rep(int nb, int R, const double* u, const int* idx, int xs, V* X, cudaStream_t st) {
+  note_launch();
+  k_gather_rep<V><<<grid_for(1LL * nb * R), kBlock, 0, st>>>(nb, R, u, idx, xs, X);
+  TMB_CUDA(cudaGetLastError());
+}
+
+void launch_dirichlet_rep(int n, int R, const int* bindex, const double* Y, int nb, double* b, cudaStream_t st) {
+  note_launch();
+  k_dirichlet_rep<<<grid_for(1LL * n * R), kBlock, 0, st>>>(n, R, bindex, Y, nb, b);
+  TMB_CUDA(cudaGetLastError());
+}
+
 void launch_dirichlet_values(int n, const int* bindex, const double* u2b, double* b, cudaStream_t st) {
   note_launch();
   k_dirichlet_values<<<grid_for(n), kBlock, 0, st>>>(n, bindex, u2b, b);
@@ -281,5 +315,7 @@ template void launch_bem_gemv_tiles<float>(int, const GemvTile*, int, const floa
 template void launch_bem_gemm<double>(int, int, const double*, const double*, int, double*, int, cudaStream_t);
 template void launch_bem_gemm<float>(int, int, const float*, const float*, int, double*, int, cudaStream_t);
 template void launch_gather<float>(int, const double*, const int*, float*, cudaStream_t);
+template void launch_gather_rep<double>(int, int, const double*, const int*, int, double*, cudaStream_t);
+template void launch_gather_rep<float>(int, int, const double*, const int*, int, float*, cudaStream_t);
 
 }  // namespace tmb

@@ -42,10 +42,13 @@ __global__ void __launch_bounds__(kBlock) k_local_field(SellView s, const V* __r
                                                         const V* __restrict__ tg0, const V* __restrict__ tg1,
                                                         const V* __restrict__ tg2, const V* __restrict__ gr0,
                                                         const V* __restrict__ gr1, LocalFieldArgs a) {
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  const int R = s.rep;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;  // state row (node row of replica r)
   double torque = 0.0;
-  if (row < a.n) {
-    const int n = a.n;
+  if (g < a.n * R) {
+    const int nn = a.n;          // operator rows: stride of the per-node arrays
+    const int n = nn * R;        // stride of the state components
+    const int row = g / R, r = g - row * R;
     const double* __restrict__ mx = a.m;
     const double* __restrict__ my = a.m + n;
     const double* __restrict__ mz = a.m + 2 * n;
@@ -57,8 +60,9 @@ __global__ void __launch_bounds__(kBlock) k_local_field(SellView s, const V* __r
 #pragma unroll 4
     for (int k = beg; k < end; k += kSlice) {
       const int j = __ldg(s.col + k);
+      const int jj = j * R + r;
       const double v = ld(K, k);
-      const double ax = __ldg(mx + j), ay = __ldg(my + j), az = __ldg(mz + j);
+      const double ax = __ldg(mx + jj), ay = __ldg(my + jj), az = __ldg(mz + jj);
       kx = fma(v, ax, kx);
       ky = fma(v, ay, ky);
       kz = fma(v, az, kz);
@@ -84,11 +88,11 @@ __global__ void __launch_bounds__(kBlock) k_local_field(SellView s, const V* __r
         czy = fma(t0, dj * ax, fma(t1, dj * ay, czy));
       }
     }
-    const double m0 = mx[row], m1 = my[row], m2 = mz[row];
+    const double m0 = mx[g], m1 = my[g], m2 = mz[g];
     const double xc = a.xc[row];
     double H0 = xc * kx, H1 = xc * ky, H2 = xc * kz;
     if (UNI) {
-      const double e0 = a.kax[row], e1 = a.kax[row + n], e2 = a.kax[row + 2 * n];
+      const double e0 = a.kax[row], e1 = a.kax[row + nn], e2 = a.kax[row + 2 * nn];
       const double f = a.ku2[row] * (e0 * m0 + e1 * m1 + e2 * m2);
       H0 = fma(f, e0, H0);
       H1 = fma(f, e1, H1);
@@ -106,7 +110,7 @@ __global__ void __launch_bounds__(kBlock) k_local_field(SellView s, const V* __r
       // curl m with tGrad' = -tGrad (main/EffFieldCalc.cpp:43, 280-298)
       const double c0 = -(cyz - czy), c1 = -(czx - cxz), c2 = -(cxy - cyx);
       const double ar = a.area[row];
-      const double n0 = a.nvn[row], n1 = a.nvn[row + n], n2 = a.nvn[row + 2 * n];
+      const double n0 = a.nvn[row], n1 = a.nvn[row + nn], n2 = a.nvn[row + 2 * nn];
       const double s0 = ar * (m1 * n2 - m2 * n1), s1 = ar * (m2 * n0 - m0 * n2), s2 = ar * (m0 * n1 - m1 * n0);
       const double ds = a.dmi_s[row];
       H0 += ds * (s0 - 2.0 * c0);
@@ -114,14 +118,14 @@ __global__ void __launch_bounds__(kBlock) k_local_field(SellView s, const V* __r
       H2 += ds * (s2 - 2.0 * c2);
     }
     if (a.hfix) {
-      H0 += a.hfix[row];
-      H1 += a.hfix[row + n];
-      H2 += a.hfix[row + 2 * n];
+      H0 += a.hfix[g];
+      H1 += a.hfix[g + n];
+      H2 += a.hfix[g + 2 * n];
     }
     if (a.hout) {
-      a.hout[row] = H0;
-      a.hout[row + n] = H1;
-      a.hout[row + 2 * n] = H2;
+      a.hout[g] = H0;
+      a.hout[g + n] = H1;
+      a.hout[g + 2 * n] = H2;
     }
     const double x0 = m1 * H2 - m2 * H1, x1 = m2 * H0 - m0 * H2, x2 = m0 * H1 - m1 * H0;  // m x H
     torque = sqrt(x0 * x0 + x1 * x1 + x2 * x2);
@@ -129,13 +133,13 @@ __global__ void __launch_bounds__(kBlock) k_local_field(SellView s, const V* __r
       const double d0 = m1 * x2 - m2 * x1, d1 = m2 * x0 - m0 * x2, d2 = m0 * x1 - m1 * x0;  // m x (m x H)
       const double al = a.alpha;
       if (a.precession) {
-        a.ydot[row] = -x0 - al * d0;
-        a.ydot[row + n] = -x1 - al * d1;
-        a.ydot[row + 2 * n] = -x2 - al * d2;
+        a.ydot[g] = -x0 - al * d0;
+        a.ydot[g + n] = -x1 - al * d1;
+        a.ydot[g + 2 * n] = -x2 - al * d2;
       } else {
-        a.ydot[row] = -al * d0;
-        a.ydot[row + n] = -al * d1;
-        a.ydot[row + 2 * n] = -al * d2;
+        a.ydot[g] = -al * d0;
+        a.ydot[g + n] = -al * d1;
+        a.ydot[g + 2 * n] = -al * d2;
       }
     }
   }
@@ -150,9 +154,11 @@ __global__ void __launch_bounds__(kBlock) k_divergence(SellView s, const V* __re
                                                        const V* __restrict__ tg1, const V* __restrict__ tg2,
                                                        const double* __restrict__ m, const double* __restrict__ js,
                                                        double inv_mu0, double* __restrict__ rhs) {
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= s.n) return;
-  const int n = s.n;
+  const int R = s.rep;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= s.n * R) return;
+  const int n = s.n * R;
+  const int row = g / R, r = g - row * R;
   const int sl = row >> 5;
   const int beg = __ldg(s.soff + sl) + (row & 31);
   const int end = __ldg(s.soff + sl + 1);
@@ -160,11 +166,12 @@ __global__ void __launch_bounds__(kBlock) k_divergence(SellView s, const V* __re
 #pragma unroll 4
   for (int k = beg; k < end; k += kSlice) {
     const int j = __ldg(s.col + k);
+    const int jj = j * R + r;
     const double J = __ldg(js + j);
-    const double t = ld(tg0, k) * __ldg(m + j) + ld(tg1, k) * __ldg(m + n + j) + ld(tg2, k) * __ldg(m + 2 * n + j);
+    const double t = ld(tg0, k) * __ldg(m + jj) + ld(tg1, k) * __ldg(m + n + jj) + ld(tg2, k) * __ldg(m + 2 * n + jj);
     acc = fma(t, J, acc);
   }
-  rhs[row] = acc * inv_mu0;
+  rhs[g] = acc * inv_mu0;
 }
 
 template <typename V>
@@ -172,31 +179,33 @@ __global__ void __launch_bounds__(kBlock) k_gradient(SellView s, const V* __rest
                                                      const V* __restrict__ g2, const double* __restrict__ u1,
                                                      const double* __restrict__ u2, const double* __restrict__ hext,
                                                      double* __restrict__ hdem, double* __restrict__ hfix) {
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= s.n) return;
-  const int n = s.n;
+  const int R = s.rep;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= s.n * R) return;
+  const int n = s.n * R;
+  const int row = g / R, r = g - row * R;
   const int sl = row >> 5;
   const int beg = __ldg(s.soff + sl) + (row & 31);
   const int end = __ldg(s.soff + sl + 1);
   double a0 = 0.0, a1 = 0.0, a2 = 0.0;
 #pragma unroll 4
   for (int k = beg; k < end; k += kSlice) {
-    const int j = __ldg(s.col + k);
+    const int j = __ldg(s.col + k) * R + r;
     const double u = u2 ? __ldg(u1 + j) + __ldg(u2 + j) : __ldg(u1 + j);
     a0 = fma(ld(g0, k), u, a0);
     a1 = fma(ld(g1, k), u, a1);
     a2 = fma(ld(g2, k), u, a2);
   }
   if (hdem) {
-    hdem[row] = -a0;
-    hdem[row + n] = -a1;
-    hdem[row + 2 * n] = -a2;
+    hdem[g] = -a0;
+    hdem[g + n] = -a1;
+    hdem[g + 2 * n] = -a2;
   }
   if (hfix) {
-    const double e0 = hext ? hext[row] : 0.0, e1 = hext ? hext[row + n] : 0.0, e2 = hext ? hext[row + 2 * n] : 0.0;
-    hfix[row] = e0 - a0;
-    hfix[row + n] = e1 - a1;
-    hfix[row + 2 * n] = e2 - a2;
+    const double e0 = hext ? hext[g] : 0.0, e1 = hext ? hext[g + n] : 0.0, e2 = hext ? hext[g + 2 * n] : 0.0;
+    hfix[g] = e0 - a0;
+    hfix[g + n] = e1 - a1;
+    hfix[g + 2 * n] = e2 - a2;
   }
 }
 
@@ -261,7 +270,7 @@ template <typename V>
 void launch_local_field(const SellView& s, const V* K, const V* tg0, const V* tg1, const V* tg2, const V* gr0,
                         const V* gr1, const LocalFieldArgs& a, cudaStream_t st) {
   note_launch();
-  const int g = grid_for(a.n);
+  const int g = grid_for(1LL * a.n * s.rep);
   const bool uni = a.ku2 != nullptr;
   const int dmi = a.idm_a ? 2 : (a.dmi_s ? 1 : 0);
 #define TMB_LF(U, D) k_local_field<V, U, D><<<g, kBlock, 0, st>>>(s, K, tg0, tg1, tg2, gr0, gr1, a)
@@ -282,7 +291,7 @@ template <typename V>
 void launch_divergence(const SellView& s, const V* tg0, const V* tg1, const V* tg2, const double* m,
                        const double* js, double inv_mu0, double* rhs, cudaStream_t st) {
   note_launch();
-  k_divergence<V><<<grid_for(s.n), kBlock, 0, st>>>(s, tg0, tg1, tg2, m, js, inv_mu0, rhs);
+  k_divergence<V><<<grid_for(1LL * s.n * s.rep), kBlock, 0, st>>>(s, tg0, tg1, tg2, m, js, inv_mu0, rhs);
   TMB_CUDA(cudaGetLastError());
 }
 
@@ -290,7 +299,7 @@ template <typename V>
 void launch_gradient(const SellView& s, const V* g0, const V* g1, const V* g2, const double* u1,
                      const double* u2, const double* hext, double* hdem, double* hfix, cudaStream_t st) {
   note_launch();
-  k_gradient<V><<<grid_for(s.n), kBlock, 0, st>>>(s, g0, g1, g2, u1, u2, hext, hdem, hfix);
+  k_gradient<V><<<grid_for(1LL * s.n * s.rep), kBlock, 0, st>>>(s, g0, g1, g2, u1, u2, hext, hdem, hfix);
   TMB_CUDA(cudaGetLastError());
 }
 

@@ -69,9 +69,12 @@ __device__ __forceinline__ bool grid_reduce(const double (&v)[K], double* partia
 // together, so that a thread keeps kChunk gathers in flight (FEM rows hold 10-15 entries).
 constexpr int kChunk = 8;
 
+// Dot of operator row g / rep with replica g % rep of x (state row g).
 template <typename V>
 __device__ __forceinline__ double sell_row_dot(const SellView& s, const V* __restrict__ val,
-                                               const double* __restrict__ x, int row) {
+                                               const double* __restrict__ x, int g) {
+  const int R = s.rep;
+  const int row = g / R, r = g - row * R;
   const int sl = row >> 5;
   const int beg = __ldg(s.soff + sl) + (row & 31);
   const int end = __ldg(s.soff + sl + 1);
@@ -83,7 +86,7 @@ __device__ __forceinline__ double sell_row_dot(const SellView& s, const V* __res
     for (int u = 0; u < kChunk; ++u) {
       const int k = k0 + u * kSlice;
       const bool ok = k < end;
-      j[u] = ok ? __ldg(s.col + k) : row;
+      j[u] = ok ? __ldg(s.col + k) * R + r : g;
       v[u] = ok ? static_cast<double>(__ldg(val + k)) : 0.0;
     }
 #pragma unroll
@@ -96,8 +99,8 @@ template <typename V>
 __global__ void __launch_bounds__(kBlock) k_spmv(SellView s, const V* __restrict__ val, const double* __restrict__ x,
                                                  double* __restrict__ y, const int* done) {
   if (done && *done) return;
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row < s.n) y[row] = sell_row_dot(s, val, x, row);
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < s.n * s.rep) y[g] = sell_row_dot(s, val, x, g);
 }
 
 template <typename V>
@@ -105,15 +108,15 @@ __global__ void __launch_bounds__(kBlock) k_residual(SellView s, const V* __rest
                                                      const double* __restrict__ b, const double* __restrict__ x,
                                                      double* __restrict__ r, const int* done) {
   if (done && *done) return;
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row < s.n) r[row] = b[row] - sell_row_dot(s, val, x, row);
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < s.n * s.rep) r[g] = b[g] - sell_row_dot(s, val, x, g);
 }
 
-__global__ void k_jacobi0(int n, const double* __restrict__ dinv, const double* __restrict__ b,
+__global__ void k_jacobi0(int n, int R, const double* __restrict__ dinv, const double* __restrict__ b,
                           double* __restrict__ x, const int* done) {
   if (done && *done) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) x[i] = dinv[i] * b[i];
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < n * R) x[g] = dinv[g / R] * b[g];
 }
 
 template <typename V>
@@ -122,8 +125,8 @@ __global__ void __launch_bounds__(kBlock) k_jacobi(SellView s, const V* __restri
                                                    const double* __restrict__ xin, double* __restrict__ xout,
                                                    const int* done) {
   if (done && *done) return;
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row < s.n) xout[row] = xin[row] + dinv[row] * (b[row] - sell_row_dot(s, val, xin, row));
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < s.n * s.rep) xout[g] = xin[g] + dinv[g / s.rep] * (b[g] - sell_row_dot(s, val, xin, g));
 }
 
 // First smoothing sweep from zero fused with the residual: x = D_w^-1 b, r = b - A x,
@@ -134,8 +137,10 @@ __global__ void __launch_bounds__(kBlock) k_jacobi0_residual(SellView s, const V
                                                              const double* __restrict__ b, double* __restrict__ x,
                                                              double* __restrict__ r, const int* done) {
   if (done && *done) return;
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= s.n) return;
+  const int R = s.rep;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= s.n * R) return;
+  const int row = g / R, rr = g - row * R;
   const int sl = row >> 5;
   const int beg = __ldg(s.soff + sl) + (row & 31);
   const int end = __ldg(s.soff + sl + 1);
@@ -151,11 +156,11 @@ __global__ void __launch_bounds__(kBlock) k_jacobi0_residual(SellView s, const V
       v[u] = ok ? static_cast<double>(__ldg(val + k)) : 0.0;
     }
 #pragma unroll
-    for (int u = 0; u < kChunk; ++u) acc = fma(v[u], __ldg(dinv + j[u]) * __ldg(b + j[u]), acc);
+    for (int u = 0; u < kChunk; ++u) acc = fma(v[u], __ldg(dinv + j[u]) * __ldg(b + j[u] * R + rr), acc);
   }
-  const double bi = b[row];
-  x[row] = dinv[row] * bi;
-  r[row] = bi - acc;
+  const double bi = b[g];
+  x[g] = dinv[row] * bi;
+  r[g] = bi - acc;
 }
 
 // Sum over the T consecutive lanes that share a row (T a power of two dividing 32).
@@ -170,13 +175,15 @@ __device__ __forceinline__ double group_sum(double v) {
 // w when w is not null).
 template <typename V, int T>
 __device__ __forceinline__ double csr_row_part(const CsrView& c, const V* __restrict__ val, const double* __restrict__ x,
-                                               const double* __restrict__ w, int row, int sub) {
+                                               const double* __restrict__ w, int g, int sub) {
   double acc = 0.0;
-  if (row < c.n) {
+  const int R = c.rep;
+  if (g < c.n * R) {
+    const int row = g / R, r = g - row * R;
     const int beg = __ldg(c.ptr + row), end = __ldg(c.ptr + row + 1);
     for (int k = beg + sub; k < end; k += T) {
       const int j = __ldg(c.col + k);
-      const double xj = w ? __ldg(w + j) * __ldg(x + j) : __ldg(x + j);
+      const double xj = w ? __ldg(w + j) * __ldg(x + j * R + r) : __ldg(x + j * R + r);
       acc = fma(static_cast<double>(__ldg(val + k)), xj, acc);
     }
   }
@@ -192,7 +199,7 @@ __global__ void __launch_bounds__(kBlock) k_csr_spmv(CsrView c, const V* __restr
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int row = t / T, sub = t & (T - 1);
   const double acc = group_sum<T>(csr_row_part<V, T>(c, val, x, nullptr, row, sub));
-  if (row < c.n && sub == 0) y[row] = accumulate ? y[row] + acc : acc;
+  if (row < c.n * c.rep && sub == 0) y[row] = accumulate ? y[row] + acc : acc;
 }
 
 // Coarse levels (rows of 20-60 entries): the first Jacobi sweep from zero fused with the
@@ -206,9 +213,9 @@ __global__ void __launch_bounds__(kBlock) k_csr_jacobi0_residual(CsrView c, cons
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int row = t / T, sub = t & (T - 1);
   const double acc = group_sum<T>(csr_row_part<V, T>(c, val, b, dinv, row, sub));
-  if (row < c.n && sub == 0) {
+  if (row < c.n * c.rep && sub == 0) {
     const double bi = b[row];
-    x[row] = dinv[row] * bi;
+    x[row] = dinv[row / c.rep] * bi;
     r[row] = bi - acc;
   }
 }
@@ -223,34 +230,37 @@ __global__ void __launch_bounds__(kBlock) k_csr_jacobi(CsrView c, const V* __res
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int row = t / T, sub = t & (T - 1);
   const double acc = group_sum<T>(csr_row_part<V, T>(c, val, xin, nullptr, row, sub));
-  if (row < c.n && sub == 0) xout[row] = xin[row] + dinv[row] * (b[row] - acc);
+  if (row < c.n * c.rep && sub == 0) xout[row] = xin[row] + dinv[row / c.rep] * (b[row] - acc);
 }
 
 // x = A_c^-1 b on the coarsest level: one warp per row of the dense FP64 inverse.
-__global__ void k_coarse_solve(int n, const double* __restrict__ inv, const double* __restrict__ b,
+__global__ void k_coarse_solve(int n, int R, const double* __restrict__ inv, const double* __restrict__ b,
                                double* __restrict__ x, const int* done) {
   if (done && *done) return;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (warp >= n) return;
-  const double* row = inv + size_t(warp) * n;
+  const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (g >= n * R) return;
+  const int i = g / R, r = g - i * R;
+  const double* row = inv + size_t(i) * n;
   double acc = 0.0;
-  for (int j = lane; j < n; j += 32) acc = fma(row[j], b[j], acc);
+  for (int j = lane; j < n; j += 32) acc = fma(row[j], b[j * R + r], acc);
   acc = warp_sum(acc);
-  if (lane == 0) x[warp] = acc;
+  if (lane == 0) x[g] = acc;
 }
 
 template <typename V>
 __global__ void k_cg_init(int n, CsrView lift, const V* __restrict__ lval, const int* __restrict__ cmask,
                           const double* __restrict__ b, double* __restrict__ bprime, double* __restrict__ x) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  const int R = lift.rep;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n * R) return;
+  const int i = g / R, r = g - i * R;
   if (cmask[i]) {
-    bprime[i] = b[i];
-    x[i] = b[i];
+    bprime[g] = b[g];
+    x[g] = b[g];
   } else {
-    double acc = b[i];
-    for (int k = lift.ptr[i]; k < lift.ptr[i + 1]; ++k) acc -= static_cast<double>(lval[k]) * b[lift.col[k]];
-    bprime[i] = acc;
+    double acc = b[g];
+    for (int k = lift.ptr[i]; k < lift.ptr[i + 1]; ++k) acc -= static_cast<double>(lval[k]) * b[lift.col[k] * R + r];
+    bprime[g] = acc;
   }
 }
 
@@ -259,11 +269,11 @@ __global__ void __launch_bounds__(kBlock) k_cg_residual(SellView s, const V* __r
                                                         const double* __restrict__ bp, const double* __restrict__ x,
                                                         double* __restrict__ r, CgScalars* S, double* partials) {
   double v[2] = {0.0, 0.0};
-  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < s.n; row += gridDim.x * blockDim.x) {
-    const double ri = bp[row] - sell_row_dot(s, val, x, row);
-    r[row] = ri;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < s.n * s.rep; g += gridDim.x * blockDim.x) {
+    const double ri = bp[g] - sell_row_dot(s, val, x, g);
+    r[g] = ri;
     v[0] = fma(ri, ri, v[0]);
-    v[1] = fma(bp[row], bp[row], v[1]);
+    v[1] = fma(bp[g], bp[g], v[1]);
   }
   double tot[2];
   if (grid_reduce<2>(v, partials, &S->ticket[0], tot) && threadIdx.x == 0) {
@@ -305,10 +315,10 @@ __global__ void __launch_bounds__(kBlock) k_jacobi_rz(SellView s, const V* __res
                                                       CgScalars* S, double* partials, int first) {
   if (S->done) return;
   double v[1] = {0.0};
-  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < s.n; row += gridDim.x * blockDim.x) {
-    const double ri = r[row];
-    const double zi = xin[row] + dinv[row] * (ri - sell_row_dot(s, val, xin, row));
-    z[row] = zi;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < s.n * s.rep; g += gridDim.x * blockDim.x) {
+    const double ri = r[g];
+    const double zi = xin[g] + dinv[g / s.rep] * (ri - sell_row_dot(s, val, xin, g));
+    z[g] = zi;
     v[0] = fma(ri, zi, v[0]);
   }
   double tot[1];
@@ -328,7 +338,9 @@ __global__ void __launch_bounds__(kBlock) k_cg_dir_spmv(SellView s, const V* __r
   if (S->done) return;
   const double beta = S->beta;
   double v[1] = {0.0};
-  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < s.n; row += gridDim.x * blockDim.x) {
+  const int R = s.rep;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < s.n * R; g += gridDim.x * blockDim.x) {
+    const int row = g / R, rr = g - row * R;
     const int sl = row >> 5;
     const int beg = __ldg(s.soff + sl) + (row & 31);
     const int end = __ldg(s.soff + sl + 1);
@@ -340,7 +352,7 @@ __global__ void __launch_bounds__(kBlock) k_cg_dir_spmv(SellView s, const V* __r
       for (int u = 0; u < kChunk; ++u) {
         const int k = k0 + u * kSlice;
         const bool ok = k < end;
-        j[u] = ok ? __ldg(s.col + k) : row;
+        j[u] = ok ? __ldg(s.col + k) * R + rr : g;
         v[u] = ok ? static_cast<double>(__ldg(val + k)) : 0.0;
       }
       if (beta == 0.0) {
@@ -351,9 +363,9 @@ __global__ void __launch_bounds__(kBlock) k_cg_dir_spmv(SellView s, const V* __r
         for (int u = 0; u < kChunk; ++u) acc = fma(v[u], fma(beta, __ldg(p_old + j[u]), __ldg(z + j[u])), acc);
       }
     }
-    const double pi = (beta == 0.0) ? z[row] : fma(beta, p_old[row], z[row]);
-    p_new[row] = pi;
-    q[row] = acc;
+    const double pi = (beta == 0.0) ? z[g] : fma(beta, p_old[g], z[g]);
+    p_new[g] = pi;
+    q[g] = acc;
     v[0] = fma(pi, acc, v[0]);
   }
   double tot[1];
@@ -377,10 +389,10 @@ __global__ void __launch_bounds__(kBlock) k_cg_spmv_pq(SellView s, const V* __re
                                                        CgScalars* S, double* partials) {
   if (S->done) return;
   double v[1] = {0.0};
-  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < s.n; row += gridDim.x * blockDim.x) {
-    const double qi = sell_row_dot(s, val, p, row);
-    q[row] = qi;
-    v[0] = fma(p[row], qi, v[0]);
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < s.n * s.rep; g += gridDim.x * blockDim.x) {
+    const double qi = sell_row_dot(s, val, p, g);
+    q[g] = qi;
+    v[0] = fma(p[g], qi, v[0]);
   }
   double tot[1];
   if (grid_reduce<1>(v, partials, &S->ticket[2], tot) && threadIdx.x == 0) {
@@ -435,23 +447,23 @@ int reduce_grid(long long n) {
 template <typename V>
 void launch_spmv(const SellView& s, const V* val, const double* x, double* y, const int* done, cudaStream_t st) {
   note_launch();
-  k_spmv<V><<<grid_for(s.n), kBlock, 0, st>>>(s, val, x, y, done);
+  k_spmv<V><<<grid_for(1LL * s.n * s.rep), kBlock, 0, st>>>(s, val, x, y, done);
 }
 template <typename V>
 void launch_residual(const SellView& s, const V* val, const double* b, const double* x, double* r,
                      const int* done, cudaStream_t st) {
   note_launch();
-  k_residual<V><<<grid_for(s.n), kBlock, 0, st>>>(s, val, b, x, r, done);
+  k_residual<V><<<grid_for(1LL * s.n * s.rep), kBlock, 0, st>>>(s, val, b, x, r, done);
 }
-void launch_jacobi0(int n, const double* dinv, const double* b, double* x, const int* done, cudaStream_t st) {
+void launch_jacobi0(int n, int rep, const double* dinv, const double* b, double* x, const int* done, cudaStream_t st) {
   note_launch();
-  k_jacobi0<<<grid_for(n), kBlock, 0, st>>>(n, dinv, b, x, done);
+  k_jacobi0<<<grid_for(1LL * n * rep), kBlock, 0, st>>>(n, rep, dinv, b, x, done);
 }
 template <typename V>
 void launch_jacobi(const SellView& s, const V* val, const double* dinv, const double* b, const double* xin,
                    double* xout, const int* done, cudaStream_t st) {
   note_launch();
-  k_jacobi<V><<<grid_for(s.n), kBlock, 0, st>>>(s, val, dinv, b, xin, xout, done);
+  k_jacobi<V><<<grid_for(1LL * s.n * s.rep), kBlock, 0, st>>>(s, val, dinv, b, xin, xout, done);
 }
 int csr_threads_per_row(long long nrows, long long nnz) {
   const double avg = nrows > 0 ? double(nnz) / double(nrows) : 0.0;
@@ -474,36 +486,37 @@ template <typename V>
 void launch_csr_spmv(const CsrView& c, const V* val, const double* x, double* y, bool accumulate,
                      const int* done, cudaStream_t st, int tpr) {
   note_launch();
-  TMB_CSR_DISPATCH(tpr, k_csr_spmv, c.n, c, val, x, y, accumulate ? 1 : 0, done)
+  TMB_CSR_DISPATCH(tpr, k_csr_spmv, 1LL * c.n * c.rep, c, val, x, y, accumulate ? 1 : 0, done)
 }
 template <typename V>
 void launch_csr_jacobi0_residual(const CsrView& c, const V* val, const double* dinv, const double* b, double* x,
                                  double* r, const int* done, cudaStream_t st, int tpr) {
   note_launch();
-  TMB_CSR_DISPATCH(tpr, k_csr_jacobi0_residual, c.n, c, val, dinv, b, x, r, done)
+  TMB_CSR_DISPATCH(tpr, k_csr_jacobi0_residual, 1LL * c.n * c.rep, c, val, dinv, b, x, r, done)
 }
 template <typename V>
 void launch_csr_jacobi(const CsrView& c, const V* val, const double* dinv, const double* b, const double* xin,
                        double* xout, const int* done, cudaStream_t st, int tpr) {
   note_launch();
-  TMB_CSR_DISPATCH(tpr, k_csr_jacobi, c.n, c, val, dinv, b, xin, xout, done)
+  TMB_CSR_DISPATCH(tpr, k_csr_jacobi, 1LL * c.n * c.rep, c, val, dinv, b, xin, xout, done)
 }
 #undef TMB_CSR_DISPATCH
-void launch_coarse_solve(int n, const double* inv, const double* b, double* x, const int* done, cudaStream_t st) {
+void launch_coarse_solve(int n, int rep, const double* inv, const double* b, double* x, const int* done,
+                         cudaStream_t st) {
   note_launch();
-  k_coarse_solve<<<grid_for(32LL * n), kBlock, 0, st>>>(n, inv, b, x, done);
+  k_coarse_solve<<<grid_for(32LL * n * rep), kBlock, 0, st>>>(n, rep, inv, b, x, done);
 }
 template <typename V>
 void launch_cg_init(int n, const CsrView& lift, const V* lval, const int* cmask, const double* b,
                     double* bprime, double* x, cudaStream_t st) {
   note_launch();
-  k_cg_init<V><<<grid_for(n), kBlock, 0, st>>>(n, lift, lval, cmask, b, bprime, x);
+  k_cg_init<V><<<grid_for(1LL * n * lift.rep), kBlock, 0, st>>>(n, lift, lval, cmask, b, bprime, x);
 }
 template <typename V>
 void launch_cg_residual(const SellView& s, const V* val, const double* bp, const double* x, double* r,
                         CgScalars* S, double* partials, cudaStream_t st) {
   note_launch();
-  k_cg_residual<V><<<reduce_grid(s.n), kBlock, 0, st>>>(s, val, bp, x, r, S, partials);
+  k_cg_residual<V><<<reduce_grid(1LL * s.n * s.rep), kBlock, 0, st>>>(s, val, bp, x, r, S, partials);
 }
 void launch_cg_rz(int n, const double* r, const double* z, CgScalars* S, double* partials, bool first,
                   cudaStream_t st) {
@@ -518,25 +531,25 @@ template <typename V>
 void launch_cg_spmv_pq(const SellView& s, const V* val, const double* p, double* q, CgScalars* S,
                        double* partials, cudaStream_t st) {
   note_launch();
-  k_cg_spmv_pq<V><<<reduce_grid(s.n), kBlock, 0, st>>>(s, val, p, q, S, partials);
+  k_cg_spmv_pq<V><<<reduce_grid(1LL * s.n * s.rep), kBlock, 0, st>>>(s, val, p, q, S, partials);
 }
 template <typename V>
 void launch_jacobi0_residual(const SellView& s, const V* val, const double* dinv, const double* b, double* x,
                              double* r, const int* done, cudaStream_t st) {
   note_launch();
-  k_jacobi0_residual<V><<<grid_for(s.n), kBlock, 0, st>>>(s, val, dinv, b, x, r, done);
+  k_jacobi0_residual<V><<<grid_for(1LL * s.n * s.rep), kBlock, 0, st>>>(s, val, dinv, b, x, r, done);
 }
 template <typename V>
 void launch_jacobi_rz(const SellView& s, const V* val, const double* dinv, const double* r, const double* xin,
                       double* z, CgScalars* S, double* partials, bool first, cudaStream_t st) {
   note_launch();
-  k_jacobi_rz<V><<<reduce_grid(s.n), kBlock, 0, st>>>(s, val, dinv, r, xin, z, S, partials, first ? 1 : 0);
+  k_jacobi_rz<V><<<reduce_grid(1LL * s.n * s.rep), kBlock, 0, st>>>(s, val, dinv, r, xin, z, S, partials, first ? 1 : 0);
 }
 template <typename V>
 void launch_cg_dir_spmv(const SellView& s, const V* val, const double* z, const double* p_old, double* p_new,
                         double* q, CgScalars* S, double* partials, cudaStream_t st) {
   note_launch();
-  k_cg_dir_spmv<V><<<reduce_grid(s.n), kBlock, 0, st>>>(s, val, z, p_old, p_new, q, S, partials);
+  k_cg_dir_spmv<V><<<reduce_grid(1LL * s.n * s.rep), kBlock, 0, st>>>(s, val, z, p_old, p_new, q, S, partials);
 }
 
 void launch_cg_update(int n, const double* p, const double* q, double* x, double* r, CgScalars* S,

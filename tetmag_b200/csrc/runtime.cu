@@ -138,7 +138,7 @@ static std::vector<V> sell_values(const SellHost& S, const double* v) {
 struct DevSell {
   int n = 0, nslice = 0;
   DevArray<int> soff, col;
-  SellView view() const { return SellView{n, nslice, soff.p, col.p}; }
+  SellView view(int rep = 1) const { return SellView{n, nslice, soff.p, col.p, rep}; }
   void upload(const SellHost& S, cudaStream_t st) {
     n = S.n;
     nslice = S.nslice;
@@ -152,7 +152,7 @@ struct DevCsr {
   DevArray<int> ptr, col;
   DevArray<double> v;
   DevArray<float> vf;
-  CsrView view() const { return CsrView{n, ptr.p, col.p}; }
+  CsrView view(int rep = 1) const { return CsrView{n, ptr.p, col.p, rep}; }
   void upload(const Csr& A, cudaStream_t st) {
     n = A.nrows;
     ptr.upload(A.ptr, st);
@@ -249,6 +249,8 @@ struct Solver {
   int check_every = 2;
   bool computed = false;
   int n = 0;
+  int rep = 1;                // interleaved replicas: every vector holds n * rep entries
+  int want_rep = -1;          // >= 1: fixed by the owner (the solver plugin); else the context's
   AmgParams prm;
   AmgHierarchy H;
   std::vector<DevLevel> lev;
@@ -320,6 +322,11 @@ struct Ctx {
   cudaStream_t own = nullptr, stream = nullptr;
   int precision = TMB_FP64;
   int n = 0, nb = 0;
+  // Interleaved replicas of one mesh (tmb_set_replicas): every state vector holds rep copies,
+  // node i of replica r at i * rep + r; operators, material and the BEM matrix are stored once.
+  int rep = 1;
+  int nr() const { return n * rep; }
+  void set_replicas(int R);
   // operators
   DevSell pat;
   DevArray<double> K, g[3], tg[3];
@@ -472,17 +479,17 @@ void Solver::ctx_prof_end(cudaStream_t st) { ctx->prof.end(st); }
 bool Solver::ctx_prof_on() const { return ctx->prof.on; }
 
 void Solver::iteration_body(int precision, cudaStream_t st, bool profile) {
-  const SellView A0 = lev[0].A.view();
+  const SellView A0 = lev[0].A.view(rep);
   const bool f64 = precision == TMB_FP64;
   double* pold = p[pcur].p;
   double* pnew = p[pcur ^ 1].p;
   pcur ^= 1;
   // direction update fused into A p: gathers z and p_old (two 8-byte gathers per entry)
-  if (profile) ctx_prof_begin(6, st, nnz_fine * ((f64 ? 8.0 : 4.0) + 4.0) + 5.0 * 8.0 * n);
+  if (profile) ctx_prof_begin(6, st, nnz_fine * ((f64 ? 8.0 : 4.0) + 4.0) + 5.0 * 8.0 * n * rep);
   if (f64) launch_cg_dir_spmv<double>(A0, lev[0].Ad.p, z.p, pold, pnew, q.p, Sd, partials.p, st);
   else launch_cg_dir_spmv<float>(A0, lev[0].Af.p, z.p, pold, pnew, q.p, Sd, partials.p, st);
   if (profile) ctx_prof_end(st);
-  launch_cg_update(n, pnew, q.p, x.p, r.p, Sd, partials.p, st);
+  launch_cg_update(n * rep, pnew, q.p, x.p, r.p, Sd, partials.p, st);
   precondition_rz(precision, st, false);
 }
 
@@ -514,6 +521,7 @@ cudaGraphExec_t Solver::graph_for(int precision) {
 void Solver::compute() {
   cudaStream_t st = ctx->stream;
   n = A.nrows;
+  rep = want_rep >= 1 ? want_rep : ctx->rep;
   if (n <= 0) throw Error(TMB_ERR_ARG, "solver: empty matrix");
   // constraints: rows whose only entry is a unit diagonal
   std::vector<int> cm(n, 0);
@@ -575,20 +583,21 @@ void Solver::compute() {
       d.Af.upload(sell_values<float>(S, hl.A.val.data()), st);
     } else {
       d.Ac.upload(hl.A, st);
-      d.tA = csr_threads_per_row(hl.A.nrows, hl.A.nnz());
+      d.tA = rep >= 8 ? 1 : csr_threads_per_row(hl.A.nrows, hl.A.nnz());
     }
     d.dinv.upload(hl.dinv, st);
-    d.X.alloc(d.n);
-    d.R.alloc(d.n);
+    d.X.alloc(size_t(d.n) * rep);
+    d.R.alloc(size_t(d.n) * rep);
     if (l > 0) {
-      d.b.alloc(d.n);
-      d.out.alloc(d.n);
+      d.b.alloc(size_t(d.n) * rep);
+      d.out.alloc(size_t(d.n) * rep);
     }
     if (l + 1 < H.levels.size()) {
       d.P.upload(hl.P, st);
       d.Rop.upload(hl.R, st);
-      d.tP = csr_threads_per_row(hl.P.nrows, hl.P.nnz());
-      d.tR = csr_threads_per_row(hl.R.nrows, hl.R.nnz());
+      // with 8 or more interleaved replicas a warp already covers replicas of one row
+      d.tP = rep >= 8 ? 1 : csr_threads_per_row(hl.P.nrows, hl.P.nnz());
+      d.tR = rep >= 8 ? 1 : csr_threads_per_row(hl.R.nrows, hl.R.nnz());
     }
   }
   ncoarse = H.ncoarse;
@@ -597,15 +606,16 @@ void Solver::compute() {
   liftT.upload(LT, st);
   for (bool& h : has_xadj) h = false;
   cmask.upload(cm, st);
-  x.alloc(n);
+  const size_t nr = size_t(n) * rep;
+  x.alloc(nr);
   x.zero(st);
-  r.alloc(n);
-  z.alloc(n);
-  p[0].alloc(n);
-  p[1].alloc(n);
-  q.alloc(n);
-  bp.alloc(n);
-  partials.alloc(size_t(2) * grid_for(n) + 64);
+  r.alloc(nr);
+  z.alloc(nr);
+  p[0].alloc(nr);
+  p[1].alloc(nr);
+  q.alloc(nr);
+  bp.alloc(nr);
+  partials.alloc(size_t(2) * grid_for((long long)nr) + 64);
   if (!Sd) TMB_CUDA(cudaMalloc(&Sd, sizeof(CgScalars)));
   if (!Sh) TMB_CUDA(cudaMallocHost(&Sh, sizeof(CgScalars)));
   std::memset(Sh, 0, sizeof(CgScalars));
@@ -619,27 +629,27 @@ void Solver::vcycle(size_t l, const double* b, double* out, int precision, cudaS
   DevLevel& L = lev[l];
   const int* done = &Sd->done;
   if (l + 1 == lev.size()) {
-    launch_coarse_solve(ncoarse, cinv.p, b, out, done, st);
+    launch_coarse_solve(ncoarse, rep, cinv.p, b, out, done, st);
     return;
   }
   DevLevel& C = lev[l + 1];
   const bool f64 = precision == TMB_FP64;
   if (l == 0) {
-    const SellView A = L.A.view();
+    const SellView A = L.A.view(rep);
     if (f64) launch_jacobi0_residual<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, L.R.p, done, st);
     else launch_jacobi0_residual<float>(A, L.Af.p, L.dinv.p, b, L.X.p, L.R.p, done, st);
   } else {
-    const CsrView A = L.Ac.view();
+    const CsrView A = L.Ac.view(rep);
     if (f64) launch_csr_jacobi0_residual<double>(A, L.Ac.v.p, L.dinv.p, b, L.X.p, L.R.p, done, st, L.tA);
     else launch_csr_jacobi0_residual<float>(A, L.Ac.vf.p, L.dinv.p, b, L.X.p, L.R.p, done, st, L.tA);
   }
-  if (f64) launch_csr_spmv<double>(L.Rop.view(), L.Rop.v.p, L.R.p, C.b.p, false, done, st, L.tR);
-  else launch_csr_spmv<float>(L.Rop.view(), L.Rop.vf.p, L.R.p, C.b.p, false, done, st, L.tR);
+  if (f64) launch_csr_spmv<double>(L.Rop.view(rep), L.Rop.v.p, L.R.p, C.b.p, false, done, st, L.tR);
+  else launch_csr_spmv<float>(L.Rop.view(rep), L.Rop.vf.p, L.R.p, C.b.p, false, done, st, L.tR);
   vcycle(l + 1, C.b.p, C.out.p, precision, st, -1);
-  if (f64) launch_csr_spmv<double>(L.P.view(), L.P.v.p, C.out.p, L.X.p, true, done, st, L.tP);
-  else launch_csr_spmv<float>(L.P.view(), L.P.vf.p, C.out.p, L.X.p, true, done, st, L.tP);
+  if (f64) launch_csr_spmv<double>(L.P.view(rep), L.P.v.p, C.out.p, L.X.p, true, done, st, L.tP);
+  else launch_csr_spmv<float>(L.P.view(rep), L.P.vf.p, C.out.p, L.X.p, true, done, st, L.tP);
   if (l == 0) {
-    const SellView A = L.A.view();
+    const SellView A = L.A.view(rep);
     if (rz_mode >= 0) {
       // finest level: the post-smoothing sweep also reduces r.z for the next CG direction
       if (f64) launch_jacobi_rz<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, out, Sd, partials.p, rz_mode == 1, st);
@@ -649,7 +659,7 @@ void Solver::vcycle(size_t l, const double* b, double* out, int precision, cudaS
       else launch_jacobi<float>(A, L.Af.p, L.dinv.p, b, L.X.p, out, done, st);
     }
   } else {
-    const CsrView A = L.Ac.view();
+    const CsrView A = L.Ac.view(rep);
     if (f64) launch_csr_jacobi<double>(A, L.Ac.v.p, L.dinv.p, b, L.X.p, out, done, st, L.tA);
     else launch_csr_jacobi<float>(A, L.Ac.vf.p, L.dinv.p, b, L.X.p, out, done, st, L.tA);
   }
@@ -661,7 +671,7 @@ void Solver::precondition_rz(int precision, cudaStream_t st, bool first) {
     vcycle(0, r.p, z.p, precision, st, first ? 1 : 0);
   } else {
     vcycle(0, r.p, z.p, precision, st, -1);
-    launch_cg_rz(n, r.p, z.p, Sd, partials.p, first, st);
+    launch_cg_rz(n * rep, r.p, z.p, Sd, partials.p, first, st);
   }
 }
 
@@ -674,10 +684,10 @@ void Solver::solve(const double* b_dev, int precision) {
   Sh->status = 0;
   Sh->iter = 0;
   TMB_CUDA(cudaMemcpyAsync(Sd, Sh, sizeof(CgScalars), cudaMemcpyHostToDevice, st));
-  const SellView A0 = lev[0].A.view();
+  const SellView A0 = lev[0].A.view(rep);
   const bool f64 = precision == TMB_FP64;
-  if (f64) launch_cg_init<double>(n, lift.view(), lift.v.p, cmask.p, b_dev, bp.p, x.p, st);
-  else launch_cg_init<float>(n, lift.view(), lift.vf.p, cmask.p, b_dev, bp.p, x.p, st);
+  if (f64) launch_cg_init<double>(n, lift.view(rep), lift.v.p, cmask.p, b_dev, bp.p, x.p, st);
+  else launch_cg_init<float>(n, lift.view(rep), lift.vf.p, cmask.p, b_dev, bp.p, x.p, st);
   if (f64) launch_cg_residual<double>(A0, lev[0].Ad.p, bp.p, x.p, r.p, Sd, partials.p, st);
   else launch_cg_residual<float>(A0, lev[0].Af.p, bp.p, x.p, r.p, Sd, partials.p, st);
   precondition_rz(precision, st, true);
@@ -775,6 +785,7 @@ void Ctx::set_operators(int nx, const int* ptr, const int* col, const double* K_
   std::vector<int> bi(nx, -1);
   for (int i = 0; i < nb_; ++i) bi[bn[i]] = i;
   bindex.upload(bi, st);
+  rep = 1;
   for (auto* a : {&hext, &hdem, &hfix}) {
     a->alloc(size_t(3) * nx);
     a->zero(st);
@@ -842,11 +853,45 @@ void Ctx::set_components(int nc, const int* off, bool shared) {
   dir.reset();
 }
 
+// Declares rep interleaved replicas of the (single) mesh: state vectors grow to 3 * n * R, the
+// operators, material and BEM matrix stay those of one mesh; the boundary product becomes one
+// GEMM over the replicas.  Resets the solvers and the BEM (assembled afterwards).
+void Ctx::set_replicas(int R) {
+  require_mesh();
+  if (R < 1) throw Error(TMB_ERR_ARG, "tmb_set_replicas: R must be >= 1");
+  if (ncomp() != 1) throw Error(TMB_ERR_STATE, "tmb_set_replicas: not with tmb_set_components");
+  if (size_t(n) * R * 3 >= size_t(1) << 31) throw Error(TMB_ERR_ARG, "tmb_set_replicas: n * R too large");
+  cudaStream_t st = stream;
+  rep = R;
+  for (auto* a : {&hext, &hdem, &hfix}) {
+    a->alloc(size_t(3) * nr());
+    a->zero(st);
+  }
+  has_bem = false;
+  H = HMat{};
+  bem_mode = 0;
+  neu.reset();
+  dir.reset();
+  tc_split = 0;
+  sync();
+}
+
 // Padded boundary layout and matvec plan of the components (after the blocks are assembled).
 void Ctx::plan_components() {
   const int nc = ncomp();
   std::vector<int> pos(nb);
   bem_entries = 0.0;
+  if (rep > 1) {
+    // replicas: the boundary values of all replicas as a [replica][ld] panel
+    xstride = int(bem_ld(nb));
+    xpad64.alloc(size_t(xstride) * rep);
+    xpad32.alloc(size_t(xstride) * rep);
+    xhi32.alloc(size_t(xstride) * rep);
+    xlo32.alloc(size_t(xstride) * rep);
+    bem_entries = double(nb) * nb;
+    ntiles = 0;
+    return;
+  }
   if (shared_bem) {
     const int nbc = cboff[1];
     xstride = int(bem_ld(nbc));
@@ -960,10 +1005,10 @@ void Ctx::ensure_demag() {
   };
   neu = build([&](int i) { return pin[i] != 0; });
   dir = build([&](int i) { return isb[i] != 0; });
-  for (auto* a : {&rhs, &u1, &u2, &bdir}) a->alloc(n);
+  for (auto* a : {&rhs, &u1, &u2, &bdir}) a->alloc(size_t(nr()));
   u1b.alloc(nb);
   u1bf.alloc(nb);
-  u2b.alloc(nb);
+  u2b.alloc(size_t(nb) * rep);
 }
 
 void Ctx::demag(const double* m) {
@@ -971,9 +1016,9 @@ void Ctx::demag(const double* m) {
   cudaStream_t st = stream;
   neu->tol = dir->tol = tol;
   neu->maxit = dir->maxit = maxit;
-  const SellView S = pat.view();
+  const SellView S = pat.view(rep);
   const bool f64 = precision == TMB_FP64;
-  const double sv = f64 ? 8.0 : 4.0, z = double(hptr[n]), N = double(n), B = double(nb);
+  const double sv = f64 ? 8.0 : 4.0, z = double(hptr[n]), N = double(nr()), B = double(nb) * rep;
   prof.begin(7, st, 0.0);
   prof.begin(1, st, z * (3 * sv + 4) + N * 8 * 5);
   if (f64) launch_divergence<double>(S, tg[0].p, tg[1].p, tg[2].p, m, js.p, 1.0 / kMu0, rhs.p, st);
@@ -989,6 +1034,15 @@ void Ctx::demag(const double* m) {
     if (f64) launch_h_matvec<double>(h_view<double>(0), neu->x.p, H.y.p, H.xp64.p, H.pos.p, n, bdir.p, st);
     else launch_h_matvec<float>(h_view<float>(1), neu->x.p, H.y.p, H.xp32.p, H.pos.p, n, bdir.p, st);
     prof.end(st);
+  } else if (rep > 1) {
+    // interleaved replicas: the replicas' boundary values as a panel, one GEMM, then the
+    // Dirichlet load of every replica from the GEMM's [replica][row] output
+    if (f64) launch_gather_rep<double>(nb, rep, neu->x.p, bnodes.p, xstride, xpad64.p, st);
+    else launch_gather_rep<float>(nb, rep, neu->x.p, bnodes.p, xstride, xpad32.p, st);
+    prof.begin(3, st, bem_entries * sv + B * (sv + 8));
+    bem_gemm(f64, st);
+    prof.end(st);
+    launch_dirichlet_rep(n, rep, bindex.p, u2b.p, nb, bdir.p, st);
   } else if (ncomp() > 1) {
     // batched components: padded gather, then one GEMM (shared matrix) or per-component matvecs
     if (f64) launch_gather_pad<double>(nb, neu->x.p, bnodes.p, xpos.p, xpad64.p, st);
@@ -1013,7 +1067,7 @@ void Ctx::demag(const double* m) {
   }
   prof.begin(5, st, 0.0);
   dir->solve(bdir.p, precision);  // synchronises: the GEMM's time-out word is readable below
-  if (shared_bem && !f64 && gemm_tc && bits_h[2] != 0)
+  if ((shared_bem || rep > 1) && !f64 && gemm_tc && bits_h[2] != 0)
     throw Error(TMB_ERR_CUDA, "tensor-core boundary GEMM timed out waiting on a barrier");
   prof.end(st);
   prof.begin(2, st, z * (3 * sv + 4) + N * 8 * 11);
@@ -1030,7 +1084,7 @@ void Ctx::demag(const double* m) {
 // Replicas' boundary product.  Mixed path: the 3xTF32 tensor-core GEMM (its time-out word is
 // copied to the pinned bits_h[2] behind it); FP64 path: the CUDA-core GEMM.
 void Ctx::bem_gemm(bool f64, cudaStream_t st) {
-  const int nbc = cboff[1], nc = ncomp();
+  const int nbc = rep > 1 ? nb : cboff[1], nc = rep > 1 ? rep : ncomp();
   if (f64 || !gemm_tc || !bem_gemm_tc_supported(nbc, bem_ld(nbc), xstride)) {
     if (f64) launch_bem_gemm<double>(nbc, nc, Bd.p, xpad64.p, xstride, u2b.p, num_sms, st);
     else launch_bem_gemm<float>(nbc, nc, Bf.p, xpad32.p, xstride, u2b.p, num_sms, st);
@@ -1045,7 +1099,7 @@ void Ctx::bem_gemm(bool f64, cudaStream_t st) {
 // SM is timed (CUDA events, three launches after one warm-up) on the current panel, the fastest
 // is kept for the context.
 void Ctx::tune_gemm_tc() {
-  const int nbc = cboff[1], nc = ncomp();
+  const int nbc = rep > 1 ? nb : cboff[1], nc = rep > 1 ? rep : ncomp();
   cudaStream_t st = stream;
   tc_err.alloc(1);
   tc_err.zero(st);
@@ -1417,7 +1471,7 @@ LocalFieldArgs Ctx::local_args(const double* m, double* ydot, double* hout, unsi
 }
 
 void Ctx::launch_local(const LocalFieldArgs& a, cudaStream_t st) {
-  const SellView S = pat.view();
+  const SellView S = pat.view(rep);
   if (precision == TMB_FP64)
     launch_local_field<double>(S, K.p, tg[0].p, tg[1].p, tg[2].p, g[0].p, g[1].p, a, st);
   else
@@ -1428,7 +1482,7 @@ void Ctx::local(const double* m, double* ydot, double* hout, unsigned long long*
   require_mesh();
   require_material();
   const LocalFieldArgs a = local_args(m, ydot, hout, tq);
-  const double sv = precision == TMB_FP64 ? 8.0 : 4.0, z = double(hptr[n]), N = double(n);
+  const double sv = precision == TMB_FP64 ? 8.0 : 4.0, z = double(hptr[n]), N = double(nr());
   double bytes = z * (sv + 4) + N * 8 * (3 + 3 + 1) + (ydot ? N * 24 : 0.0) + (hout ? N * 24 : 0.0);
   if (a.ku2) bytes += N * 8 * 4;
   if (a.dmi_s) bytes += z * 3 * sv + N * 8 * 5;
@@ -1468,7 +1522,7 @@ static const double kDpE[7] = {35.0 / 384 - 5179.0 / 57600, 0.0, 500.0 / 1113 - 
 // Adaptive segment with odeint's controlled_runge_kutta error control and step adjustment.
 int Ctx::integrate_segment(double*& y, double*& yalt, double t0, double t1, double& dt, double eps_abs,
                            double eps_rel, double* stats) {
-  const int n3 = 3 * n;
+  const int n3 = 3 * nr();
   cudaStream_t st = stream;
   double t = t0;
   local(y, kst[0].p, nullptr, nullptr);
@@ -1517,7 +1571,7 @@ int Ctx::integrate_segment(double*& y, double*& yalt, double t0, double t1, doub
 int Ctx::relax(double* m, double duration_ps, double segment_ps, double eps_abs, double eps_rel, double* stats) {
   require_mesh();
   require_material();
-  const int n3 = 3 * n;
+  const int n3 = 3 * nr();
   cudaStream_t st = stream;
   for (auto& b : ybuf) b.alloc(n3);
   for (auto& k : kst) k.alloc(n3);
@@ -1525,7 +1579,7 @@ int Ctx::relax(double* m, double duration_ps, double segment_ps, double eps_abs,
   TMB_CUDA(cudaMemcpyAsync(ybuf[0].p, m, sizeof(double) * n3, cudaMemcpyDeviceToDevice, st));
   double* y = ybuf[0].p;
   double* yalt = ybuf[1].p;
-  launch_normalize(n, y, st);
+  launch_normalize(nr(), y, st);
   const double ts = time_scale();
   double dt = std::min(segment_ps * ts, ts);
   for (int i = 0; i < 12; ++i) stats[i] = 0.0;
@@ -1540,7 +1594,7 @@ int Ctx::relax(double* m, double duration_ps, double segment_ps, double eps_abs,
     }
     const double seg = std::min(segment_ps, duration_ps - t_ps);
     integrate_segment(y, yalt, t_ps * ts, (t_ps + seg) * ts, dt, eps_abs, eps_rel, stats);
-    launch_normalize(n, y, st);
+    launch_normalize(nr(), y, st);
     t_ps += seg;
     stats[8] += 1;
   }
@@ -1577,25 +1631,25 @@ double Ctx::pulse_hz(double t_ps) const {
 
 // The applied field in effect before a fixed-step run is kept and restored afterwards.
 void Ctx::begin_timed_field() {
-  const size_t n3 = size_t(3) * n;
+  const size_t n3 = size_t(3) * nr();
   ab.hbase.alloc(n3);
   TMB_CUDA(cudaMemcpyAsync(ab.hbase.p, hext.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
 }
 
 void Ctx::end_timed_field() {
-  const size_t n3 = size_t(3) * n;
+  const size_t n3 = size_t(3) * nr();
   TMB_CUDA(cudaMemcpyAsync(hext.p, ab.hbase.p, n3 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
   launch_add(int(n3), hext.p, hdem.p, hfix.p, stream);
 }
 
 // One right-hand-side evaluation with the demag field refreshed: k = f(Y, t), H = total field.
 void Ctx::stage_eval(const double* Y, double t_ps, double* k, double* H) {
-  if (!bz.empty()) launch_set_hz(n, ab.hbase.p, pulse_hz(t_ps), hext.p, stream);
+  if (!bz.empty()) launch_set_hz(nr(), ab.hbase.p, pulse_hz(t_ps), hext.p, stream);
   if (has_bem) {
     demag(Y);
     cnt[3] += neu->last_iters + dir->last_iters;
   } else {
-    launch_add(3 * n, hext.p, hdem.p, hfix.p, stream);
+    launch_add(3 * nr(), hext.p, hdem.p, hfix.p, stream);
   }
   local(Y, k, H, nullptr);
 }
@@ -1603,7 +1657,7 @@ void Ctx::stage_eval(const double* Y, double t_ps, double* k, double* H) {
 // y <- y + h/6 (k1 + 2 k2 + 2 k3 + k4); with Ys / Hs (4 x 3N each) the stage states and fields
 // are kept for the adjoint.
 void Ctx::rk4_substep(double* y, double t_ps, double ds_ps, double* Ys, double* Hs) {
-  const int n3 = 3 * n;
+  const int n3 = 3 * nr();
   const double h = ds_ps * time_scale();
   double* K[4] = {kst[0].p, kst[1].p, kst[2].p, kst[3].p};
   if (Ys) TMB_CUDA(cudaMemcpyAsync(Ys, y, sizeof(double) * n3, cudaMemcpyDeviceToDevice, stream));
@@ -1676,10 +1730,10 @@ void Ctx::vjp(const double* Y, const double* H, const double* abar, double* gout
 void Ctx::step_rk4(double* m, int nsteps, double dt_ps, int nsub, double t0_ps, bool normalize) {
   require_mesh();
   require_material();
-  const int n3 = 3 * n;
+  const int n3 = 3 * nr();
   for (int j = 0; j < 4; ++j) kst[j].alloc(n3);
   ytmp.alloc(n3);
-  ab.zn.alloc(n);
+  ab.zn.alloc(size_t(nr()));
   begin_timed_field();
   const double ds = dt_ps / nsub;
   for (int k = 0; k < nsteps; ++k) {
@@ -1687,7 +1741,7 @@ void Ctx::step_rk4(double* m, int nsteps, double dt_ps, int nsub, double t0_ps, 
       rk4_substep(m, t0_ps + k * dt_ps + s * ds, ds, nullptr, nullptr);
       cnt[0] += 4;
     }
-    if (normalize) launch_normalize_keep(n, m, ab.zn.p, stream);
+    if (normalize) launch_normalize_keep(nr(), m, ab.zn.p, stream);
   }
   end_timed_field();
   sync();
@@ -1701,6 +1755,7 @@ void Ctx::adjoint_rk4(const double* m0, int nsteps, double dt_ps, int nsub, int 
     throw Error(TMB_ERR_STATE, "adjoint: the bulk DMI form has no transpose here (interfacial or none)");
   if (has_bem && (ncomp() != 1 || bem_mode != 0))
     throw Error(TMB_ERR_STATE, "adjoint: needs one component and the dense BEM matrix");
+  if (rep != 1) throw Error(TMB_ERR_STATE, "adjoint: not for interleaved replicas");
   if (has_bem) ensure_demag();
   cudaStream_t st = stream;
   const size_t n3 = size_t(3) * n;
@@ -2095,7 +2150,7 @@ int tmb_bem_assemble_ex(tmb_ctx* ctx, const tmb_mesh* mesh, int formula) {
   }
   c.Bf.alloc(size_t(boff[nstore]));
   launch_to_float(c.Bd.p, c.Bf.p, size_t(boff[nstore]), c.stream);
-  if (nc > 1) c.plan_components();
+  if (nc > 1 || c.rep > 1) c.plan_components();
   c.sync();
   c.has_bem = true;
   c.H = Ctx::HMat{};
@@ -2108,8 +2163,17 @@ int tmb_bem_assemble_ex(tmb_ctx* ctx, const tmb_mesh* mesh, int formula) {
 int tmb_set_components(tmb_ctx* ctx, int ncomp, const int* node_offsets, int shared_bem) {
   TMB_CHECK_ARG(ctx && node_offsets && ncomp >= 1, "tmb_set_components: bad arguments");
   TMB_API_BEGIN
+  if (ctx->c->rep > 1) return fail(TMB_ERR_STATE, "tmb_set_components: the context has interleaved replicas");
   TMB_CUDA(cudaSetDevice(ctx->c->device));
   ctx->c->set_components(ncomp, node_offsets, shared_bem != 0);
+  TMB_API_END
+}
+
+int tmb_set_replicas(tmb_ctx* ctx, int nrep) {
+  TMB_CHECK_ARG(ctx && nrep >= 1, "tmb_set_replicas: nrep must be >= 1");
+  TMB_API_BEGIN
+  TMB_CUDA(cudaSetDevice(ctx->c->device));
+  ctx->c->set_replicas(nrep);
   TMB_API_END
 }
 
@@ -2128,6 +2192,7 @@ int tmb_set_bem_dense(tmb_ctx* ctx, int nb, const double* B_colmajor) {
   c.Bd.upload(rowmajor, c.stream);
   c.Bf.alloc(ld * nb);
   launch_to_float(c.Bd.p, c.Bf.p, ld * nb, c.stream);
+  if (c.rep > 1) c.plan_components();
   c.sync();
   c.has_bem = true;
   c.H = Ctx::HMat{};
@@ -2158,6 +2223,7 @@ int tmb_bem_compress(tmb_ctx* ctx, const double* bxyz, const double* bnormal, in
   TMB_CHECK_ARG(ctx && bxyz, "tmb_bem_compress: null argument");
   TMB_API_BEGIN
   Ctx& c = *ctx->c;
+  if (c.rep > 1) return fail(TMB_ERR_STATE, "tmb_bem_compress: not for interleaved replicas (dense GEMM)");
   TMB_CUDA(cudaSetDevice(c.device));
   c.h_compress(bxyz, bnormal, leaf, eta, eps_mixed, eps_fp64, kmax, keep_dense != 0);
   TMB_API_END
@@ -2173,6 +2239,7 @@ int tmb_bem_build_h(tmb_ctx* ctx, const tmb_mesh* mesh, int leaf, double eta, do
   const BoundaryData& B = M.bnd;
   const int nb = int(B.bnodes.size());
   if (nb != c.nb || M.nx != c.n) return fail(TMB_ERR_ARG, "tmb_bem_build_h: mesh differs from the context's");
+  if (c.rep > 1) return fail(TMB_ERR_STATE, "tmb_bem_build_h: not for interleaved replicas (dense GEMM)");
   TMB_CUDA(cudaSetDevice(c.device));
   std::vector<double> bxyz(size_t(3) * nb), bnrm(size_t(3) * nb);
   for (int i = 0; i < nb; ++i)
@@ -2245,7 +2312,7 @@ int tmb_set_applied_field(tmb_ctx* ctx, const double* hext, int ptr_kind) {
   TMB_API_BEGIN
   Ctx& c = *ctx->c;
   c.require_mesh();
-  const size_t n3 = size_t(3) * c.n;
+  const size_t n3 = size_t(3) * c.nr();
   TMB_CUDA(cudaMemcpyAsync(c.hext.p, hext, n3 * sizeof(double),
                            ptr_kind == TMB_PTR_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c.stream));
   launch_add(int(n3), c.hext.p, c.hdem.p, c.hfix.p, c.stream);
@@ -2272,7 +2339,7 @@ int tmb_demag_field(tmb_ctx* ctx, const double* m, double* hdem, int ptr_kind) {
   TMB_API_BEGIN
   Ctx& c = *ctx->c;
   c.require_mesh();
-  const size_t n3 = size_t(3) * c.n;
+  const size_t n3 = size_t(3) * c.nr();
   const double* md = stage_in(c, c.in3, m, n3, ptr_kind);
   c.demag(md);
   if (hdem)
@@ -2288,7 +2355,7 @@ int tmb_field_eval(tmb_ctx* ctx, const double* m, double* ydot, double* hdem, in
   TMB_API_BEGIN
   Ctx& c = *ctx->c;
   c.require_mesh();
-  const size_t n3 = size_t(3) * c.n;
+  const size_t n3 = size_t(3) * c.nr();
   const double* md = stage_in(c, c.in3, m, n3, ptr_kind);
   c.demag(md);
   if (ptr_kind == TMB_PTR_DEVICE) {
@@ -2309,7 +2376,7 @@ int tmb_set_demag_frozen(tmb_ctx* ctx, const double* hdem, int ptr_kind) {
   TMB_API_BEGIN
   Ctx& c = *ctx->c;
   c.require_mesh();
-  const size_t n3 = size_t(3) * c.n;
+  const size_t n3 = size_t(3) * c.nr();
   TMB_CUDA(cudaMemcpyAsync(c.hdem.p, hdem, n3 * sizeof(double),
                            ptr_kind == TMB_PTR_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c.stream));
   launch_add(int(n3), c.hext.p, c.hdem.p, c.hfix.p, c.stream);
@@ -2322,7 +2389,7 @@ int tmb_effective_field(tmb_ctx* ctx, const double* m, double* h, int ptr_kind) 
   TMB_API_BEGIN
   Ctx& c = *ctx->c;
   c.require_mesh();
-  const size_t n3 = size_t(3) * c.n;
+  const size_t n3 = size_t(3) * c.nr();
   const double* md = stage_in(c, c.in3, m, n3, ptr_kind);
   if (ptr_kind == TMB_PTR_DEVICE) {
     c.local(md, nullptr, h, nullptr);
@@ -2341,7 +2408,7 @@ int tmb_llg_rhs(tmb_ctx* ctx, double t, const double* y, double* ydot, int ptr_k
   TMB_API_BEGIN
   Ctx& c = *ctx->c;
   c.require_mesh();
-  const size_t n3 = size_t(3) * c.n;
+  const size_t n3 = size_t(3) * c.nr();
   const double* yd = stage_in(c, c.in3, y, n3, ptr_kind);
   if (ptr_kind == TMB_PTR_DEVICE) {
     c.local(yd, ydot, nullptr, nullptr);
@@ -2399,8 +2466,8 @@ int tmb_llg_rhs_noalloc(tmb_ctx* ctx, double t, const double* y, double* ydot) {
   Ctx& c = *ctx->c;
   c.require_mesh();
   c.require_material();
-  if (c.n > kNoAllocMaxNodes)
-    return fail(TMB_ERR_ARG, "tmb_llg_rhs_noalloc: the mesh has " + std::to_string(c.n) +
+  if (c.nr() > kNoAllocMaxNodes)
+    return fail(TMB_ERR_ARG, "tmb_llg_rhs_noalloc: the mesh has " + std::to_string(c.nr()) +
                                  " nodes; its static staging array holds at most " +
                                  std::to_string(kNoAllocMaxNodes) + " (use tmb_llg_rhs)");
   if (c.device < 0 || c.device >= kNoAllocMaxDevices)
@@ -2409,7 +2476,7 @@ int tmb_llg_rhs_noalloc(tmb_ctx* ctx, double t, const double* y, double* ydot) {
   double* const stage = staging_address(c.device);
   double* const yd = stage;                          // y, 3N
   double* const od = stage + 3 * kNoAllocMaxNodes;   // ydot, 3N
-  const size_t n3 = size_t(3) * c.n;
+  const size_t n3 = size_t(3) * c.nr();
   TMB_CUDA(cudaMemcpyAsync(yd, y, n3 * sizeof(double), cudaMemcpyHostToDevice, c.stream));
   c.launch_local(c.local_args(yd, od, nullptr, nullptr), c.stream);
   TMB_CUDA(cudaMemcpyAsync(ydot, od, n3 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
@@ -2422,7 +2489,7 @@ int tmb_max_torque(tmb_ctx* ctx, const double* m, double* out, int ptr_kind) {
   TMB_API_BEGIN
   Ctx& c = *ctx->c;
   c.require_mesh();
-  const double* md = stage_in(c, c.in3, m, size_t(3) * c.n, ptr_kind);
+  const double* md = stage_in(c, c.in3, m, size_t(3) * c.nr(), ptr_kind);
   *out = c.max_torque(md);
   if (!std::isfinite(*out)) return fail(TMB_ERR_NAN, "tmb_max_torque: torque is not finite");
   TMB_API_END
@@ -2433,13 +2500,13 @@ int tmb_normalize(tmb_ctx* ctx, double* m, int ptr_kind) {
   TMB_API_BEGIN
   Ctx& c = *ctx->c;
   c.require_mesh();
-  const size_t n3 = size_t(3) * c.n;
+  const size_t n3 = size_t(3) * c.nr();
   if (ptr_kind == TMB_PTR_DEVICE) {
-    launch_normalize(c.n, m, c.stream);
+    launch_normalize(c.nr(), m, c.stream);
   } else {
     c.in3.alloc(n3);
     TMB_CUDA(cudaMemcpyAsync(c.in3.p, m, n3 * sizeof(double), cudaMemcpyHostToDevice, c.stream));
-    launch_normalize(c.n, c.in3.p, c.stream);
+    launch_normalize(c.nr(), c.in3.p, c.stream);
     TMB_CUDA(cudaMemcpyAsync(m, c.in3.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     c.sync();
   }
@@ -2454,7 +2521,7 @@ int tmb_relax(tmb_ctx* ctx, double* m, double duration_ps, double segment_ps, do
   TMB_API_BEGIN
   Ctx& c = *ctx->c;
   c.require_mesh();
-  const size_t n3 = size_t(3) * c.n;
+  const size_t n3 = size_t(3) * c.nr();
   if (ptr_kind == TMB_PTR_DEVICE) {
     c.relax(m, duration_ps, segment_ps, eps_abs, eps_rel, stats);
   } else {
@@ -2506,7 +2573,7 @@ int tmb_step_rk4(tmb_ctx* ctx, double* m, int nsteps, double dt_ps, int nsub, do
   Ctx& c = *ctx->c;
   c.require_mesh();
   TMB_CUDA(cudaSetDevice(c.device));
-  const size_t n3 = size_t(3) * c.n;
+  const size_t n3 = size_t(3) * c.nr();
   for (double& v : c.cnt) v = 0.0;
   double* md = m;
   if (ptr_kind != TMB_PTR_DEVICE) {
@@ -2534,7 +2601,7 @@ int tmb_adjoint_rk4(tmb_ctx* ctx, const double* m0, int nsteps, double dt_ps, in
   Ctx& c = *ctx->c;
   c.require_mesh();
   TMB_CUDA(cudaSetDevice(c.device));
-  const size_t n3 = size_t(3) * c.n, n = size_t(c.n);
+  const size_t n3 = size_t(3) * c.nr(), n = size_t(c.n);
   for (double& v : c.cnt) v = 0.0;
   const bool dev = ptr_kind == TMB_PTR_DEVICE;
   const double* m0d = stage_in(c, c.ab.io[0], m0, n3, ptr_kind);
@@ -2622,6 +2689,7 @@ int tmb_solver_create(tmb_ctx* ctx, tmb_solver** out) {
   auto* s = new tmb_solver();
   s->ctx = ctx->c.get();
   s->s = std::make_unique<Solver>(s->ctx);
+  s->s->want_rep = 1;  // the plugin solves one right-hand side
   *out = s;
   TMB_API_END
 }

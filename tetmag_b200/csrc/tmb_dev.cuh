@@ -32,17 +32,23 @@ namespace tmb {
 constexpr int kSlice = 32;
 constexpr int kBlock = 256;
 
+// rep > 1: the operator acts on rep interleaved copies of its vectors (shared-mesh replicas):
+// state row g = i * rep + r is row i of the operator for replica r, and column j of row i
+// gathers entry j * rep + r.  A warp then covers 32 replicas of one operator row, so the row's
+// indices and values are loaded once for all of them (broadcast) and the gathers are contiguous.
 struct SellView {
-  int n;             // rows
+  int n;             // operator rows
   int nslice;
   const int* soff;   // nslice + 1 element offsets (multiples of 32)
   const int* col;    // padded column indices
+  int rep;           // interleaved replicas (1: plain vectors)
 };
 
 struct CsrView {
   int n;
   const int* ptr;
   const int* col;
+  int rep;
 };
 
 // Scalars of one PCG solve, resident on the device so that no kernel needs
@@ -100,7 +106,7 @@ void launch_spmv(const SellView& s, const V* val, const double* x, double* y, co
 template <typename V>
 void launch_residual(const SellView& s, const V* val, const double* b, const double* x, double* r,
                      const int* done, cudaStream_t st);
-void launch_jacobi0(int n, const double* dinv, const double* b, double* x, const int* done, cudaStream_t st);
+void launch_jacobi0(int n, int rep, const double* dinv, const double* b, double* x, const int* done, cudaStream_t st);
 template <typename V>
 void launch_jacobi(const SellView& s, const V* val, const double* dinv, const double* b, const double* xin,
                    double* xout, const int* done, cudaStream_t st);
@@ -116,7 +122,8 @@ void launch_csr_jacobi0_residual(const CsrView& c, const V* val, const double* d
 template <typename V>
 void launch_csr_jacobi(const CsrView& c, const V* val, const double* dinv, const double* b, const double* xin,
                        double* xout, const int* done, cudaStream_t st, int tpr);
-void launch_coarse_solve(int n, const double* inv, const double* b, double* x, const int* done, cudaStream_t st);
+void launch_coarse_solve(int n, int rep, const double* inv, const double* b, double* x, const int* done,
+                         cudaStream_t st);
 
 template <typename V>
 void launch_cg_init(int n, const CsrView& lift, const V* lval, const int* cmask, const double* b,
@@ -150,6 +157,10 @@ void launch_to_float(const double* src, float* dst, size_t n, cudaStream_t st);
 template <typename V>
 void launch_bem_gemv(int nb, const V* B, const V* xb, double* u2b, cudaStream_t st);
 void launch_dirichlet_values(int n, const int* bindex, const double* u2b, double* b, cudaStream_t st);
+// interleaved replicas (state row i * R + r): boundary panel X[r * xs + b], Dirichlet load from Y[r * nb + b]
+template <typename V>
+void launch_gather_rep(int nb, int R, const double* u, const int* idx, int xs, V* X, cudaStream_t st);
+void launch_dirichlet_rep(int n, int R, const int* bindex, const double* Y, int nb, double* b, cudaStream_t st);
 template <typename V>
 void launch_gather(int nb, const double* u, const int* idx, V* out, cudaStream_t st);
 size_t bem_ld(int nb);  // leading dimension (elements) of the row-major device BEM matrix

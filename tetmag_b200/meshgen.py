@@ -145,6 +145,21 @@ def soa_split(v: np.ndarray, offsets) -> list:
             for c in range(len(offsets) - 1)]
 
 
+def interleave(vectors) -> np.ndarray:
+    """R per-replica SoA vectors (3N each, one mesh) -> the interleaved replica layout of
+    tmb_set_replicas: component d of node i of replica r at d * N * R + i * R + r."""
+    R = len(vectors)
+    n = vectors[0].size // 3
+    a = np.stack([np.asarray(v, dtype=np.float64).reshape(3, n) for v in vectors], axis=2)  # (3, N, R)
+    return np.ascontiguousarray(a.ravel())
+
+
+def deinterleave(v: np.ndarray, R: int) -> list:
+    """Inverse of interleave."""
+    a = np.asarray(v).reshape(3, -1, R)
+    return [np.ascontiguousarray(a[:, :, r].ravel()) for r in range(R)]
+
+
 def random_state(n: int, seed: int) -> np.ndarray:
     """i.i.d. directions uniform on S^2 (normalised Gaussian triples), SoA (3N,)."""
     rng = np.random.default_rng(seed)

@@ -37,6 +37,7 @@ class Workload:
     components: Optional[np.ndarray] = None   # node offsets of batched instances (None: one mesh)
     shared_bem: bool = False                  # the components are replicas of one mesh
     dmi_kind: str = "bulk"                    # "bulk" (tetmag's) or "interfacial"
+    replicas: int = 1                         # interleaved replicas of `mesh` (tmb_set_replicas)
 
     @property
     def n(self) -> int:
@@ -91,15 +92,24 @@ def c4_replica(seed: int = 4, replica: int = 0) -> Workload:
                     info=dict(replica=replica, b_tesla=b))
 
 
-def c4_batch(replicas: int = 64, seed: int = 4) -> Workload:
-    """The c4 cuboid as `replicas` replicas in one context (one shared BEM matrix, the boundary
-    matvec one GEMM): each replica with the m0 and applied field of c4_replica(seed, r)."""
+def c4_batch(replicas: int = 64, seed: int = 4, interleaved: bool = True) -> Workload:
+    """The c4 cuboid as `replicas` replicas in one context, each with the m0 and applied field of
+    c4_replica(seed, r).  interleaved: one mesh with interleaved replica vectors (tmb_set_replicas:
+    every operator row applied to all replicas at once, the boundary product one GEMM); else the
+    disjoint union of copies declared as shared-BEM components (tmb_set_components)."""
     reps = [c4_replica(seed=seed, replica=r) for r in range(replicas)]
-    mesh, off = meshgen.union([reps[0].mesh] * replicas, name=f"c4x{replicas}_cuboid_200x200x40nm_h4")
+    info = dict(replicas=replicas, b_tesla=[r.info["b_tesla"] for r in reps])
+    if interleaved:
+        base = reps[0].mesh
+        mesh = meshgen.Mesh(xyz=base.xyz, tets=base.tets, scale=base.scale,
+                            name=f"c4x{replicas}_cuboid_200x200x40nm_h4")
+        return Workload(name=mesh.name, mesh=mesh, Ms=8.0e5, A=1.3e-11, alpha=0.5,
+                        m0=meshgen.interleave([r.m0 for r in reps]), hext=meshgen.interleave([r.hext for r in reps]),
+                        duration_ps=1000.0, replicas=replicas, info=info)
+    mesh, off = meshgen.union([reps[0].mesh] * replicas, name=f"c4x{replicas}_union_cuboid_200x200x40nm_h4")
     return Workload(name=mesh.name, mesh=mesh, Ms=8.0e5, A=1.3e-11, alpha=0.5,
                     m0=meshgen.soa_stack([r.m0 for r in reps]), hext=meshgen.soa_stack([r.hext for r in reps]),
-                    duration_ps=1000.0, components=off, shared_bem=True,
-                    info=dict(replicas=replicas, b_tesla=[r.info["b_tesla"] for r in reps]))
+                    duration_ps=1000.0, components=off, shared_bem=True, info=info)
 
 
 def c3_dots(ndots: int = 256, seed: int = 3, h_range=(2.0, 3.0)) -> Workload:
@@ -132,11 +142,18 @@ def c3_dots(ndots: int = 256, seed: int = 3, h_range=(2.0, 3.0)) -> Workload:
 
 
 def instances(w: Workload) -> int:
+    if w.replicas > 1:
+        return w.replicas
     return 1 if w.components is None else len(w.components) - 1
 
 
 def component(w: Workload, c: int) -> Workload:
     """Instance c of a batched workload as a single-mesh workload (its own mesh, m0, field)."""
+    if w.replicas > 1:
+        pick = lambda v: None if v is None else meshgen.deinterleave(v, w.replicas)[c]  # noqa: E731
+        return Workload(name=f"{w.name}[{c}]", mesh=w.mesh, Ms=w.Ms, A=w.A, alpha=w.alpha, m0=pick(w.m0),
+                        hext=pick(w.hext), Ku=w.Ku, ku_axis=w.ku_axis, D=w.D, duration_ps=w.duration_ps,
+                        segment_ps=w.segment_ps, dmi_kind=w.dmi_kind)
     if w.components is None:
         return w
     off = w.components
@@ -204,6 +221,8 @@ def setup_context(w: Workload, device: int = 0, mixed: bool = False, tol: float 
     mo = mesh_ops if mesh_ops is not None else MeshOps(w.mesh.xyz, w.mesh.tets)
     ctx = Context(device)
     ctx.set_mesh(mo)
+    if w.replicas > 1:
+        ctx.set_replicas(w.replicas)
     if w.components is not None:
         ctx.set_components(w.components, shared_bem=w.shared_bem)
     if hmatrix == "mesh":
