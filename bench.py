@@ -395,7 +395,8 @@ def run_gpu(args):
     traffic = None
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():
-        traffic = json.loads(tf.read_text()).get(w.name, {}).get(dom)
+        key = w.name + ("/" + args.bem if hier else "")
+        traffic = json.loads(tf.read_text()).get(key, {}).get(dom)
     kshare = {k: round(prof[k]["total_ms"] / ms_mx, 4) for k in prof if k != "demag_chain"}
 
     line = {

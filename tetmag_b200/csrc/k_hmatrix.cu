@@ -335,7 +335,14 @@ __global__ void __launch_bounds__(256) k_h_far(const HFarGroup* __restrict__ grp
                                                const long long* __restrict__ voff, const T* __restrict__ U,
                                                const T* __restrict__ V, const T* __restrict__ xp,
                                                double* __restrict__ y) {
-  __shared__ double ts[128];
+  // The row cluster's low-rank blocks are taken in chunks (at most kBlkCap blocks and kTermCap
+  // terms): first every term t = V_b^T x_sigma of the chunk (one warp per term), then every row
+  // accumulates U_b t over the chunk's blocks, so the CTA synchronises twice per chunk instead of
+  // twice per block.
+  constexpr int kTermCap = 1024, kBlkCap = 128;
+  __shared__ double ts[kTermCap];
+  __shared__ int tb[kBlkCap + 1];   // term offsets of the chunk's blocks
+  __shared__ int nq_s;
   __shared__ double red[256];
   const HFarGroup g = grp[blockIdx.x];
   const int m = g.m;
@@ -345,35 +352,58 @@ __global__ void __launch_bounds__(256) k_h_far(const HFarGroup* __restrict__ grp
   const int row = m >= 256 ? threadIdx.x : threadIdx.x % m;
   const int slice = m >= 256 ? 0 : threadIdx.x / m;
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int q = g.first; q < g.last; ++q) {
-    const int k = rank[q];
-    if (k == 0) continue;
-    const int n = blk[q].n, cb = blk[q].cb;
-    const T* v = V + voff[q];
-    for (int l = warp; l < k; l += 8) {
-      const T* vl = v + (long long)l * n;
+  for (int q0 = g.first; q0 < g.last;) {
+    if (threadIdx.x == 0) {
+      int t = 0, c = 0;
+      tb[0] = 0;
+      while (q0 + c < g.last && c < kBlkCap) {
+        const int k = rank[q0 + c];
+        if (c > 0 && t + k > kTermCap) break;
+        t += k;
+        ++c;
+        tb[c] = t;
+      }
+      nq_s = c;
+    }
+    __syncthreads();
+    const int nq = nq_s, nt = tb[nq];
+    for (int p = warp; p < nt; p += 8) {
+      int lo = 0, hi = nq - 1;  // block c of term p: tb[c] <= p < tb[c + 1]
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tb[mid] <= p) lo = mid;
+        else hi = mid - 1;
+      }
+      const int q = q0 + lo, l = p - tb[lo];
+      const int n = blk[q].n, cb = blk[q].cb;
+      const T* vl = V + voff[q] + (long long)l * n;
       double a = 0.0;
 #pragma unroll 4
       for (int j = lane; j < n; j += 32) a = fma(double(vl[j]), double(xp[cb + j]), a);
       a = warp_sum_d(a);
-      if (lane == 0) ts[l] = a;
+      if (lane == 0) ts[p] = a;
     }
     __syncthreads();
-    const T* u = U + uoff[q];
-    if (m >= 256) {
+    for (int c = 0; c < nq; ++c) {
+      const int q = q0 + c, k = tb[c + 1] - tb[c];
+      const T* u = U + uoff[q];
+      const double* tq = ts + tb[c];
+      if (m >= 256) {
 #pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int i = row + 256 * r;
-        if (i < m) {
+        for (int r = 0; r < 4; ++r) {
+          const int i = row + 256 * r;
+          if (i < m) {
 #pragma unroll 4
-          for (int l = 0; l < k; ++l) acc[r] = fma(double(u[(long long)l * m + i]), ts[l], acc[r]);
+            for (int l = 0; l < k; ++l) acc[r] = fma(double(u[(long long)l * m + i]), tq[l], acc[r]);
+          }
         }
-      }
-    } else if (slice < slices) {
+      } else if (slice < slices) {
 #pragma unroll 4
-      for (int l = slice; l < k; l += slices) acc[0] = fma(double(u[(long long)l * m + row]), ts[l], acc[0]);
+        for (int l = slice; l < k; l += slices) acc[0] = fma(double(u[(long long)l * m + row]), tq[l], acc[0]);
+      }
     }
     __syncthreads();
+    q0 += nq;
   }
   if (m >= 256) {
 #pragma unroll
