@@ -172,6 +172,24 @@ int tmb_set_material(tmb_ctx* ctx, const double* Js, const double* A, const doub
  * counterpart): H = -(1/V) dE/dm of E = sum_i V_i D_i [m_z div m - (m . grad) m_z]_i with
  * tetmag's nodal gradient operators, divided by Js. */
 int tmb_set_dmi_kind(tmb_ctx* ctx, int kind);
+/* Cubic anisotropy (EffFieldCalc::cubicAnisotropyField, main/EffFieldCalc.cpp:249-272): Kc1, Kc2
+ * [J/m^3] per node, axes 9 per node (node i: the three cubic axes c1, c2, c3, each x, y, z, as
+ * SimulationData::cubicAxes' columns).  H += C dE/dalpha / Js with alpha = C^T m.  Kc1 = NULL
+ * removes the term.  Call after tmb_set_mesh; the 1/Js scaling follows tmb_set_material. */
+int tmb_set_cubic_anisotropy(tmb_ctx* ctx, const double* Kc1, const double* Kc2, const double* axes);
+/* Surface anisotropy (EffFieldCalc::surfaceAnisotropyField, main/EffFieldCalc.cpp:128-149): Ks per
+ * node [J/m^2, already divided by scale as specs/SimulationData.cpp:47], multiplied by the node's
+ * boundary area; H += -2 Ks a nm (nm m - n) / (V Js) with n the node normal, nm = m . n.  NULL
+ * removes the term. */
+int tmb_set_surface_anisotropy(tmb_ctx* ctx, const double* Ks);
+/* Zhang-Li spin-transfer torque (TheLLG::sttDynamics, main/TheLLG.cpp:201-220; u term
+ * calcUtermSTT, :402-415): eta = 3N SoA per node (tetmag's eta_jx, eta_jy, eta_jz: current
+ * density times the spin-polarisation factor, specs/ProgramSpecs.cpp:395-420), beta the
+ * non-adiabaticity, scale the current-pulse value (1 for a constant current; the caller updates
+ * it for a pulse).  Adds s [-(beta - alpha) m x U - (1 + alpha beta) m x (m x U)] with
+ * U = sum_d eta_d (grad_d m) to every right-hand side; the max-torque value excludes it (as
+ * main/TheLLG.cpp:437).  eta = NULL removes it. */
+int tmb_set_stt(tmb_ctx* ctx, const double* eta, double beta, double scale);
 /* Applied field, 3N SoA in A/m (TheLLG::setZeemanField, main/TheLLG.cpp:477-483). */
 int tmb_set_applied_field(tmb_ctx* ctx, const double* hext, int ptr_kind);
 /* precession = 0 selects the "remove precession" dynamics (TheLLG::noPrecession, main/TheLLG.cpp:180-199). */
@@ -219,6 +237,15 @@ int tmb_normalize(tmb_ctx* ctx, double* m, int ptr_kind);
  * final max torque [T], final dt (reduced), segments, 0, 0, 0.  Synchronises. */
 int tmb_relax(tmb_ctx* ctx, double* m, double duration_ps, double segment_ps, double eps_abs, double eps_rel,
               double* stats, int ptr_kind);
+/* Energy densities [J/m^3] of TheSimulation::calculateEnergies (main/TheSimulation.cpp:385-396):
+ * out[0..7] = total, demag (DemagField::getDemagEnergy, main/DemagField.cpp:97-99), exchange
+ * (EffFieldCalc::calcExchangeEnergy, main/EffFieldCalc.cpp:65-69), uniaxial with tetmag's offset
+ * sum V Ku (:86-95), Zeeman (TheLLG::getZeemanEnergy, main/TheLLG.cpp:345-348), cubic
+ * (cubicAnisotropyEnergy, :232-247), surface (surfaceAnisotropyEnergy, :108-126), DMI
+ * (-1/2 sum V Js H_dmi . m, bulk or interfacial), each divided by the total node volume.  The
+ * demag field is evaluated for m when a BEM matrix is set (the frozen one otherwise).  With
+ * components or replicas the sums run over the whole batch.  Synchronises. */
+int tmb_energies(tmb_ctx* ctx, const double* m, double* out, int ptr_kind);
 /* Time-dependent applied field: a piecewise-linear Bz(t) through ns samples [T] spaced uniformly
  * over [t0_ps, t1_ps] (held at the end values outside), added as Bz/mu0 to the z component of the
  * applied field during tmb_step_rk4 / tmb_adjoint_rk4.  ns = 0 removes it.  Generalises tetmag's

@@ -430,6 +430,29 @@ def uniaxial_field(pb: Problem, m):
     return (2.0 * pb.Ku * km)[:, None] * pb.ku_axis
 
 
+def cubic_field(pb: Problem, m):
+    """EffFieldCalc::cubicAnisotropyField (:249-272): alpha = C^T m (axes as columns of C),
+    dE_j = -2 a_j (Kc1 (a_j+1^2 + a_j+2^2) + Kc2 a_j+1^2 a_j+2^2), H = C dE.
+    pb.extra: Kc1, Kc2 (N,), cax (N, 3, 3) with the axes as rows."""
+    cax = pb.extra["cax"]
+    al = np.einsum("nkd,nd->nk", cax, m)
+    k1, k2 = pb.extra["Kc1"], pb.extra["Kc2"]
+    de = np.empty_like(al)
+    for j in range(3):
+        b1, b2 = al[:, (j + 1) % 3] ** 2, al[:, (j + 2) % 3] ** 2
+        de[:, j] = -2.0 * al[:, j] * (k1 * (b1 + b2) + k2 * b1 * b2)
+    return np.einsum("nkd,nk->nd", cax, de)
+
+
+def surface_field(pb: Problem, m):
+    """EffFieldCalc::surfaceAnisotropyField (:128-149) with Ksn = Ks * node area (:102-106):
+    -2 Ksn nm (nm m - n) / V, nm = m . n.  pb.extra: Ks (N,)."""
+    ksn = pb.extra["Ks"] * pb.bnd.node_area
+    nv = pb.bnd.node_normal
+    nm = np.sum(m * nv, axis=1)
+    return (-2.0 * ksn * nm / pb.fem.node_vol)[:, None] * (nm[:, None] * m - nv)
+
+
 def curl_m(pb: Problem, m):
     """EffFieldCalc::curlM (:280-298) with tGrad = -msh.tGrad (:43)."""
     tx, ty, tz = [-t for t in pb.fem.tgrad]
@@ -555,15 +578,28 @@ def local_field(pb: Problem, m, hdem):
         h = h + uniaxial_field(pb, m)
     if np.any(pb.D != 0.0):
         h = h + (dmi_field(pb, m) if pb.dmi_kind == "bulk" else interfacial_dmi_field(pb, m))
+    if "Kc1" in pb.extra:
+        h = h + cubic_field(pb, m)
+    if "Ks" in pb.extra:
+        h = h + surface_field(pb, m)
     return h * inv_js(pb)[:, None] + pb.hext + hdem
 
 
 def llg_rhs(pb: Problem, m, H, precession=True):
-    """classicVersion / noPrecession (:150-199): -m x H - alpha m x (m x H)."""
+    """classicVersion / noPrecession (:150-199): -m x H - alpha m x (m x H); with pb.extra["eta"]
+    ((N, 3): eta_jx, eta_jy, eta_jz) the spin-transfer term of sttDynamics (:201-220, U term
+    calcUtermSTT :402-415): s [-(beta - alpha) m x U - (1 + alpha beta) m x (m x U)]."""
     mxh = np.cross(m, H)
     out = -pb.alpha * np.cross(m, mxh)
     if precession:
         out = out - mxh
+    extra = getattr(pb, "extra", {})
+    if "eta" in extra:
+        eta, beta, s = extra["eta"], extra.get("beta", 0.0), extra.get("stt_scale", 1.0)
+        g = pb.fem.grad
+        U = sum(eta[:, d][:, None] * np.stack([g[d] @ m[:, c] for c in range(3)], axis=1) for d in range(3))
+        mxu = np.cross(m, U)
+        out = out + s * (-(beta - pb.alpha) * mxu - (1.0 + pb.alpha * beta) * np.cross(m, mxu))
     return out
 
 
@@ -679,6 +715,40 @@ def relax(pb: Problem, m0_soa, duration_ps, segment_ps=0.5, demag: Optional[Dema
     H = local_field(pb, m, hdem)
     stats["max_torque"] = max_torque(m, H)
     return m, stats
+
+
+def energies(pb: Problem, m, hdem):
+    """TheSimulation::calculateEnergies (main/TheSimulation.cpp:385-396), energy densities:
+    demag -1/2 sum Js V H_dem.m (DemagField.cpp:97-99), exchange -1/2 sum V H_ex.m with
+    H_ex = -2 (A/V) K m (EffFieldCalc.cpp:65-69), uniaxial sum V Ku - sum V Ku (k.m)^2 (:86-95),
+    Zeeman -sum Js V H_ext.m (TheLLG.cpp:345-348), cubic (EffFieldCalc.cpp:232-247), surface
+    (:108-126), DMI -1/2 sum V H_dmi.m (the interfacial form: its own discrete energy), all divided
+    by the total volume."""
+    V = pb.fem.node_vol
+    vt = V.sum()
+    e_dem = -0.5 * np.sum(pb.Js * V * np.sum(hdem * m, axis=1)) / vt
+    e_ex = -0.5 * np.sum(V * np.sum(exchange_field(pb, m) * m, axis=1)) / vt
+    km = np.sum(pb.ku_axis * m, axis=1)
+    e_uni = (np.sum(V * pb.Ku) - np.sum(V * pb.Ku * km * km)) / vt
+    e_zee = -np.sum(pb.Js * V * np.sum(pb.hext * m, axis=1)) / vt
+    if not np.any(pb.D != 0.0):
+        e_dmi = 0.0
+    elif pb.dmi_kind == "bulk":
+        e_dmi = -0.5 * np.sum(V * np.sum(dmi_field(pb, m) * m, axis=1)) / vt
+    else:
+        e_dmi = interfacial_dmi_energy(pb, m) / vt
+    e_cub = e_srf = 0.0
+    if "Kc1" in pb.extra:
+        al2 = np.einsum("nkd,nd->nk", pb.extra["cax"], m) ** 2
+        e_cub = np.sum(V * (pb.extra["Kc1"] * (al2[:, 0] * al2[:, 1] + al2[:, 1] * al2[:, 2] + al2[:, 0] * al2[:, 2])
+                            + pb.extra["Kc2"] * al2[:, 0] * al2[:, 1] * al2[:, 2])) / vt
+    if "Ks" in pb.extra:
+        ksn = pb.extra["Ks"] * pb.bnd.node_area
+        nm = np.sum(m * pb.bnd.node_normal, axis=1)
+        e_srf = (np.sum(ksn) - np.sum(ksn * nm * nm)) / vt
+    tot = e_dem + e_ex + e_uni + e_zee + e_dmi + e_cub + e_srf
+    return dict(total=tot, demag=e_dem, exchange=e_ex, uniaxial=e_uni, zeeman=e_zee, cubic=e_cub, surface=e_srf,
+                dmi=e_dmi)
 
 
 def mean_m(pb: Problem, m):

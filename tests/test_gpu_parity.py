@@ -470,3 +470,127 @@ def test_interleaved_replicas_match_separate_contexts(R):
     assert np.isfinite(st["max_torque"])
     nrm = np.linalg.norm(m.reshape(3, -1), axis=0)
     assert np.max(np.abs(nrm - 1.0)) < 1e-12
+
+
+def _golden_problem(g, dmi_kind="bulk"):
+    return O.make_problem(g["xyz"], g["tets"], 1e-9, Ms=8e5, A=1.3e-11, alpha=0.3, Ku=5e4, ku_axis=g["axis"],
+                          D=3e-3, hext=np.ascontiguousarray(g["hext"]), with_bem=False, dmi_kind=dmi_kind)
+
+
+def _check_energies(e, eo, tol):
+    scale = max(abs(v) for v in eo.values())
+    for k, v in eo.items():
+        assert abs(e[k] - v) <= tol * scale, (k, e[k], v)
+
+
+def test_energies_match_oracle(golden):
+    # the energy densities of TheSimulation::calculateEnergies (demag evaluated for m through the
+    # solves) against the oracle's sums, bulk and interfacial DMI, FP64 and mixed
+    g, mo, ctx = golden
+    m = O.rows_to_soa(g["m"])
+    try:
+        for kind in ("bulk", "interfacial"):
+            ctx.set_dmi_kind(kind == "interfacial")
+            eo = O.energies(_golden_problem(g, kind), g["m"], g["hdem"])
+            assert eo["dmi"] != 0.0 and eo["uniaxial"] > 0.0
+            ctx.set_solver_params(1e-13, 300)
+            _check_energies(ctx.energies(m), eo, 1e-10)
+            ctx.set_precision(True)
+            ctx.set_solver_params(1e-10, 300)
+            _check_energies(ctx.energies(m), eo, MIXED_TOL)
+            ctx.set_precision(False)
+    finally:
+        ctx.set_precision(False)
+        ctx.set_dmi_kind(False)
+        ctx.set_solver_params(1e-13, 300)
+
+
+def test_energies_uniform_state_and_replicas():
+    # a uniform state along the easy axis has no exchange, anisotropy or DMI energy and a positive
+    # demag energy below (1/2) Js Ms; R interleaved replicas give the mean of R single contexts
+    base = meshgen.kuhn_cuboid(10, 9, 3, 3.0)
+    R = 3
+    axis = np.concatenate([np.zeros(2 * base.nx), np.ones(base.nx)])
+    up = np.concatenate([np.zeros(2 * base.nx), np.ones(base.nx)])
+    w = workloads.Workload(name="up", mesh=base, Ms=8.0e5, A=1.3e-11, alpha=0.5, m0=up, hext=np.zeros(3 * base.nx),
+                           Ku=5e4, ku_axis=axis, D=2e-3)
+    ctx = workloads.setup_context(w, tol=1e-13, maxiter=300)[1]
+    e = ctx.energies(up)
+    ed = 0.5 * O.MU0 * 8.0e5 ** 2
+    assert 0.0 < e["demag"] < ed
+    for k in ("exchange", "uniaxial", "dmi", "zeeman", "cubic", "surface"):
+        assert abs(e[k]) <= 1e-9 * ed, (k, e[k])
+    m0s = [meshgen.random_state(base.nx, 900 + r) for r in range(R)]
+    hx = [meshgen.field_from_angles(base.nx, 0.01 * (r + 1), 20.0 * r, 5.0 * r) for r in range(R)]
+    singles = []
+    for r in range(R):
+        wr = workloads.Workload(name="one", mesh=base, Ms=8.0e5, A=1.3e-11, alpha=0.5, m0=m0s[r], hext=hx[r],
+                                Ku=5e4, ku_axis=axis, D=2e-3)
+        singles.append(workloads.setup_context(wr, tol=1e-13, maxiter=300)[1].energies(m0s[r]))
+    wR = workloads.Workload(name="rep", mesh=base, Ms=8.0e5, A=1.3e-11, alpha=0.5, m0=meshgen.interleave(m0s),
+                            hext=meshgen.interleave(hx), Ku=5e4, ku_axis=axis, D=2e-3, replicas=R)
+    eR = workloads.setup_context(wR, tol=1e-13, maxiter=300)[1].energies(wR.m0)
+    mean = {k: np.mean([s[k] for s in singles]) for k in singles[0]}
+    _check_energies(eR, mean, 1e-10)
+
+
+def _random_cubic_axes(n, seed):
+    q, _ = np.linalg.qr(np.random.default_rng(seed).standard_normal((n, 3, 3)))
+    return np.ascontiguousarray(np.transpose(q, (0, 2, 1)))   # rows: the three cubic axes
+
+
+def test_cubic_and_surface_anisotropy_match_oracle(golden):
+    # cubic anisotropy with per-node axes (EffFieldCalc::cubicAnisotropyField) and surface
+    # anisotropy (surfaceAnisotropyField): field, right-hand side and energies against the oracle
+    # in both precisions; removing them gives back the golden field
+    g, mo, ctx = golden
+    m = O.rows_to_soa(g["m"])
+    n = mo.nx
+    cax = _random_cubic_axes(n, 21)
+    k1 = np.random.default_rng(5).uniform(2e4, 6e4, n)
+    pb = _golden_problem(g)
+    pb.extra.update(Kc1=k1, Kc2=np.full(n, -1.5e4), cax=cax, Ks=np.full(n, 8e-4 / 1e-9))
+    Ho = O.local_field(pb, g["m"], g["hdem"])
+    ctx.set_cubic_anisotropy(k1, -1.5e4, cax)
+    ctx.set_surface_anisotropy(8e-4 / 1e-9)
+    try:
+        ctx.set_demag_frozen(O.rows_to_soa(g["hdem"]))
+        assert rel(ctx.effective_field(m), O.rows_to_soa(Ho)) <= 1e-12
+        assert rel(TheLLG(ctx)(m, 0.0), O.rows_to_soa(O.llg_rhs(pb, g["m"], Ho))) <= 1e-12
+        ctx.set_solver_params(1e-13, 300)
+        eo = O.energies(pb, g["m"], g["hdem"])
+        assert eo["cubic"] != 0.0 and eo["surface"] != 0.0
+        _check_energies(ctx.energies(m), eo, 1e-10)
+        ctx.set_precision(True)
+        ctx.set_demag_frozen(O.rows_to_soa(g["hdem"]))
+        assert rel(ctx.effective_field(m), O.rows_to_soa(Ho)) <= MIXED_TOL
+    finally:
+        ctx.set_precision(False)
+        ctx.set_cubic_anisotropy(None)
+        ctx.set_surface_anisotropy(None)
+    ctx.set_demag_frozen(O.rows_to_soa(g["hdem"]))
+    assert rel(ctx.effective_field(m), O.rows_to_soa(g["H"])) <= 1e-12
+
+
+def test_spin_transfer_torque_rhs_matches_oracle(golden):
+    # Zhang-Li term of TheLLG::sttDynamics with per-node eta, beta and a pulse scale, against the
+    # oracle; the max torque ignores it (TheLLG::getMaxTorque); removing it gives the golden rhs
+    g, mo, ctx = golden
+    m = O.rows_to_soa(g["m"])
+    eta = np.random.default_rng(8).standard_normal((mo.nx, 3)) * 4e6
+    pb = _golden_problem(g)
+    pb.extra.update(eta=eta, beta=0.05, stt_scale=0.7)
+    Ho = O.local_field(pb, g["m"], g["hdem"])
+    ref = O.rows_to_soa(O.llg_rhs(pb, g["m"], Ho))
+    assert rel(ref, O.rows_to_soa(g["ydot"])) > 1e-2          # the term matters at this size
+    ctx.set_demag_frozen(O.rows_to_soa(g["hdem"]))
+    ctx.set_stt(O.rows_to_soa(eta), beta=0.05, scale=0.7)
+    try:
+        assert rel(TheLLG(ctx)(m, 0.0), ref) <= 1e-12
+        assert abs(ctx.max_torque(m) - float(g["torque"])) <= 1e-12 * float(g["torque"])
+        ctx.set_precision(True)
+        assert rel(TheLLG(ctx)(m, 0.0), ref) <= MIXED_TOL
+    finally:
+        ctx.set_precision(False)
+        ctx.set_stt(None)
+    assert rel(TheLLG(ctx)(m, 0.0), O.rows_to_soa(g["ydot"])) <= 1e-12

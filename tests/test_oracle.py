@@ -195,3 +195,64 @@ def test_interfacial_dmi_field_is_energy_gradient():
         mm[i, d] -= eps
         dE = (O.interfacial_dmi_energy(pb, mp) - O.interfacial_dmi_energy(pb, mm)) / (2 * eps)
         assert abs(-dE / V[i] - H[i, d]) <= 1e-7 * np.max(np.abs(H))
+
+
+def _anisotropy_problem():
+    from tetmag_b200 import meshgen
+    mesh = meshgen.kuhn_cuboid(4, 3, 2, 3.0)
+    rng = np.random.default_rng(11)
+    k = rng.standard_normal(3)
+    pb = O.make_problem(mesh.xyz, mesh.tets, 1e-9, Ms=8e5, A=1.3e-11, alpha=0.3, Ku=4e4,
+                        ku_axis=k / np.linalg.norm(k), with_bem=False,
+                        hext=rng.standard_normal((mesh.nx, 3)) * 1e4)
+    q, _ = np.linalg.qr(rng.standard_normal((3, 3)))
+    pb.extra.update(Kc1=np.full(mesh.nx, 4.5e4), Kc2=np.full(mesh.nx, -1.2e4),
+                    cax=np.broadcast_to(q.T, (mesh.nx, 3, 3)).copy(), Ks=np.full(mesh.nx, 1e-3 / 1e-9))
+    m = O.soa_to_rows(meshgen.random_state(mesh.nx, 7))
+    return mesh, pb, m
+
+
+def test_energy_terms_consistent_with_fields():
+    # each energy density (TheSimulation::calculateEnergies) times the total volume is the discrete
+    # energy whose gradient is -V_i Js H_i of its field term: exchange, uniaxial, Zeeman, cubic by
+    # central differences; surface up to a component along m (tetmag's surface field drops the
+    # constant part, main/EffFieldCalc.cpp:137-139); the parts add up to the total
+    mesh, pb, m = _anisotropy_problem()
+    V, vt = pb.fem.node_vol, pb.fem.node_vol.sum()
+    hz = np.zeros_like(m)
+    e0 = O.energies(pb, m, hz)
+    assert np.isclose(e0["total"], sum(v for k, v in e0.items() if k != "total"), rtol=1e-14, atol=0)
+    fields = dict(exchange=O.exchange_field(pb, m), uniaxial=O.uniaxial_field(pb, m),
+                  zeeman=pb.Js[:, None] * pb.hext, cubic=O.cubic_field(pb, m), surface=O.surface_field(pb, m))
+    rng = np.random.default_rng(3)
+    for term, H in fields.items():
+        scale = np.max(np.abs(H))
+        for _ in range(8):
+            i, d = int(rng.integers(mesh.nx)), int(rng.integers(3))
+            eps = 1e-6
+            mp, mm = m.copy(), m.copy()
+            mp[i, d] += eps
+            mm[i, d] -= eps
+            dE = (O.energies(pb, mp, hz)[term] - O.energies(pb, mm, hz)[term]) * vt / (2 * eps)
+            g = np.zeros(3)
+            g[d] = -dE / V[i]
+            if term == "surface":
+                # compare only what is perpendicular to m: the rest of the gradient lies along the normal
+                nv = pb.bnd.node_normal[i]
+                nm = m[i] @ nv
+                full = 2.0 * pb.extra["Ks"][i] * pb.bnd.node_area[i] * nm * nv / V[i]
+                assert abs(full[d] - g[d]) <= 1e-6 * max(scale, 1.0)
+                assert np.allclose(np.cross(m[i], H[i] - full), 0.0, atol=1e-9 * max(scale, 1.0))
+            else:
+                assert abs(H[i, d] - g[d]) <= 1e-6 * max(scale, 1.0)
+
+
+def test_stt_term_of_a_uniform_state_vanishes():
+    # U = sum_d eta_d grad_d m is zero for a uniform m (gradient operators annihilate constants)
+    mesh, pb, _ = _anisotropy_problem()
+    pb.extra.update(eta=np.tile([3.0, -1.0, 0.5], (mesh.nx, 1)), beta=0.04)
+    m = np.tile([0.6, 0.0, 0.8], (mesh.nx, 1))
+    H = O.local_field(pb, m, np.zeros_like(m))
+    ref = O.llg_rhs(pb, m, H)
+    del pb.extra["eta"]
+    assert np.max(np.abs(ref - O.llg_rhs(pb, m, H))) <= 1e-10 * np.max(np.abs(ref))

@@ -62,6 +62,10 @@ SIGNATURES = {
     "tmb_max_torque": [_P, _P, _D, _int],
     "tmb_normalize": [_P, _P, _int],
     "tmb_relax": [_P, _P, _dbl, _dbl, _dbl, _dbl, _D, _int],
+    "tmb_energies": [_P, _P, _D, _int],
+    "tmb_set_cubic_anisotropy": [_P, _D, _D, _D],
+    "tmb_set_surface_anisotropy": [_P, _D],
+    "tmb_set_stt": [_P, _D, _dbl, _dbl],
     "tmb_set_bz_pulse": [_P, _int, _D, _dbl, _dbl],
     "tmb_step_rk4": [_P, _P, _int, _dbl, _int, _dbl, _int, _D, _int],
     "tmb_adjoint_rk4": [_P, _P, _int, _dbl, _int, _int, _dbl, _int, _P, _P, _P, _P, _D, _D, _D, _int],

@@ -311,6 +311,47 @@ class Context:
                 "segments"]
         return {kk: st[i] for i, kk in enumerate(keys)}
 
+    def set_cubic_anisotropy(self, Kc1=None, Kc2=None, axes=None):
+        """Cubic anisotropy: Kc1, Kc2 per node [J/m^3] (scalars broadcast), axes (N, 3, 3) or (3, 3) with
+        the cubic axes as rows c1, c2, c3.  Kc1=None removes it."""
+        if Kc1 is None:
+            check(lib().tmb_set_cubic_anisotropy(self.h, None, None, None))
+            return self
+        n = self.n
+        k1, k2 = _f64(np.broadcast_to(Kc1, (n,))), _f64(np.broadcast_to(0.0 if Kc2 is None else Kc2, (n,)))
+        ax = _f64(np.broadcast_to(np.asarray(axes, np.float64), (n, 3, 3)).reshape(n, 9))
+        check(lib().tmb_set_cubic_anisotropy(self.h, _dptr(k1), _dptr(k2), _dptr(ax)))
+        return self
+
+    def set_surface_anisotropy(self, Ks=None):
+        """Surface anisotropy Ks per node [J/m^2, divided by the length scale]; None removes it."""
+        if Ks is None:
+            check(lib().tmb_set_surface_anisotropy(self.h, None))
+            return self
+        ks = _f64(np.broadcast_to(Ks, (self.n,)))
+        check(lib().tmb_set_surface_anisotropy(self.h, _dptr(ks)))
+        return self
+
+    def set_stt(self, eta=None, beta: float = 0.0, scale: float = 1.0):
+        """Zhang-Li spin-transfer torque: eta 3N SoA per node (or a 3-vector for all nodes), beta, pulse scale."""
+        if eta is None:
+            check(lib().tmb_set_stt(self.h, None, 0.0, 1.0))
+            return self
+        e = np.asarray(eta, np.float64)
+        if e.size == 3:
+            e = np.repeat(e, self.n)
+        e = _f64(e)
+        check(lib().tmb_set_stt(self.h, _dptr(e), float(beta), float(scale)))
+        return self
+
+    def energies(self, m) -> dict:
+        """Energy densities [J/m^3] (tmb_energies): total, demag, exchange, uniaxial, zeeman, cubic, surface, dmi."""
+        out = (C.c_double * 8)()
+        pm, k = _vec(m)
+        check(lib().tmb_energies(self.h, pm, out, k))
+        keys = ["total", "demag", "exchange", "uniaxial", "zeeman", "cubic", "surface", "dmi"]
+        return {kk: out[i] for i, kk in enumerate(keys)}
+
     def set_bz_pulse(self, bz_tesla, t0_ps: float, t1_ps: float):
         """Piecewise-linear Bz(t) samples [T] over [t0_ps, t1_ps], added to the applied z field during
         step_rk4 / adjoint_rk4 (an empty sequence removes it)."""

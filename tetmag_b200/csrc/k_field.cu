@@ -98,6 +98,35 @@ __global__ void __launch_bounds__(kBlock) k_local_field(SellView s, const V* __r
       H1 = fma(f, e1, H1);
       H2 = fma(f, e2, H2);
     }
+    if (a.cub_k1) {
+      // cubic anisotropy (EffFieldCalc::cubicAnisotropyField, main/EffFieldCalc.cpp:249-272):
+      // alpha = C^T m, dE/dalpha_j = -2 alpha_j (Kc1 (a_j+1^2 + a_j+2^2) + Kc2 a_j+1^2 a_j+2^2), H = C dE
+      double c[3][3], al[3];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) c[j][d] = a.cub_ax[(3 * j + d) * nn + row];
+        al[j] = c[j][0] * m0 + c[j][1] * m1 + c[j][2] * m2;
+      }
+      const double k1 = a.cub_k1[row], k2 = a.cub_k2[row];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const double b1 = al[(j + 1) % 3] * al[(j + 1) % 3], b2 = al[(j + 2) % 3] * al[(j + 2) % 3];
+        const double de = -2.0 * al[j] * (k1 * (b1 + b2) + k2 * b1 * b2);
+        H0 = fma(de, c[j][0], H0);
+        H1 = fma(de, c[j][1], H1);
+        H2 = fma(de, c[j][2], H2);
+      }
+    }
+    if (a.srf_k) {
+      // surface anisotropy (EffFieldCalc::surfaceAnisotropyField, main/EffFieldCalc.cpp:128-149):
+      // -2 Ks nm (nm m - n) / V with nm = m . n
+      const double q0 = a.nvn[row], q1 = a.nvn[row + nn], q2 = a.nvn[row + 2 * nn];
+      const double nm = m0 * q0 + m1 * q1 + m2 * q2, f = -2.0 * a.srf_k[row] * nm;
+      H0 = fma(f, nm * m0 - q0, H0);
+      H1 = fma(f, nm * m1 - q1, H1);
+      H2 = fma(f, nm * m2 - q2, H2);
+    }
     if (DMI == 2) {
       // interfacial DMI, E = sum_i V_i D_i [m_z div m - (m . grad) m_z]_i with the nodal gradient
       // operators; H = -(1/V) dE/dm (exact gradient of the discrete energy), divided by Js
@@ -261,6 +290,133 @@ __global__ void k_add(int n, const double* a, const double* b, double* out) {
 std::atomic<long long> g_launches{0};
 
 }  // namespace
+
+// Zhang-Li spin-transfer torque added to the right-hand side (TheLLG::sttDynamics,
+// main/TheLLG.cpp:201-220; u term TheLLG::calcUtermSTT, :402-415; GPU form gpu/EffFieldGPU.cu:
+// 107-148, 434-475): U = sum_d eta_d (grad_d m) per component, ydot += s [-(beta - alpha) m x U
+// - (1 + alpha beta) m x (m x U)], s the current pulse value.  R interleaved replicas.
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_stt_add(SellView sv, const V* __restrict__ g0, const V* __restrict__ g1,
+                                                    const V* __restrict__ g2, const double* __restrict__ m,
+                                                    const double* __restrict__ eta, double alpha, double beta,
+                                                    double scale, double* __restrict__ ydot) {
+  const int R = sv.rep;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= sv.n * R) return;
+  const int nn = sv.n, n = nn * R;
+  const int row = g / R, r = g - row * R;
+  const int sl = row >> 5;
+  const int beg = __ldg(sv.soff + sl) + (row & 31);
+  const int end = __ldg(sv.soff + sl + 1);
+  double d[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};  // d[c][k] = (grad_k m_c)
+#pragma unroll 4
+  for (int k = beg; k < end; k += kSlice) {
+    const int jj = __ldg(sv.col + k) * R + r;
+    const double w0 = ld(g0, k), w1 = ld(g1, k), w2 = ld(g2, k);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const double mc = __ldg(m + c * n + jj);
+      d[c][0] = fma(w0, mc, d[c][0]);
+      d[c][1] = fma(w1, mc, d[c][1]);
+      d[c][2] = fma(w2, mc, d[c][2]);
+    }
+  }
+  const double ex = eta[row], ey = eta[row + nn], ez = eta[row + 2 * nn];
+  double u[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) u[c] = ex * d[c][0] + ey * d[c][1] + ez * d[c][2];
+  const double m0 = m[g], m1 = m[g + n], m2 = m[g + 2 * n];
+  const double x0 = m1 * u[2] - m2 * u[1], x1 = m2 * u[0] - m0 * u[2], x2 = m0 * u[1] - m1 * u[0];  // m x U
+  const double y0 = m1 * x2 - m2 * x1, y1 = m2 * x0 - m0 * x2, y2 = m0 * x1 - m1 * x0;            // m x (m x U)
+  const double a = -(beta - alpha) * scale, b = -(1.0 + alpha * beta) * scale;
+  ydot[g] += a * x0 + b * y0;
+  ydot[g + n] += a * x1 + b * y1;
+  ydot[g + 2 * n] += a * x2 + b * y2;
+}
+
+template <typename V>
+void launch_stt_add(const SellView& s, const V* g0, const V* g1, const V* g2, const double* m, const double* eta,
+                    double alpha, double beta, double scale, double* ydot, cudaStream_t st) {
+  note_launch();
+  k_stt_add<V><<<grid_for(1LL * s.n * s.rep), kBlock, 0, st>>>(s, g0, g1, g2, m, eta, alpha, beta, scale, ydot);
+  TMB_CUDA(cudaGetLastError());
+}
+template void launch_stt_add<double>(const SellView&, const double*, const double*, const double*, const double*,
+                                     const double*, double, double, double, double*, cudaStream_t);
+template void launch_stt_add<float>(const SellView&, const float*, const float*, const float*, const double*,
+                                    const double*, double, double, double, double*, cudaStream_t);
+
+// Per-block partial sums of the energy terms (TheSimulation::calculateEnergies,
+// main/TheSimulation.cpp:385-396), state row g = i * R + r:
+//   [0] sum V Js (H_ex . m)      exchange (E = -1/2 of it)
+//   [1] sum V Js (H_dmi . m)     DMI      (E = -1/2 of it)
+//   [2] sum V Ku (k . m)^2       uniaxial (E = sum V Ku - it)
+//   [3] sum V Js (H_ext . m)     Zeeman   (E = -it)
+//   [4] sum V Js (H_dem . m)     demag    (E = -1/2 of it)
+//   [5] sum V (Kc1 (a0^2 a1^2 + a1^2 a2^2 + a0^2 a2^2) + Kc2 a0^2 a1^2 a2^2), a = C^T m   cubic
+//   [6] sum Ks a (n . m)^2       surface  (E = sum Ks a - it)
+// Fields here are the library's per-Js fields (A/m); Ku = ku2 Js / 2.
+__global__ void __launch_bounds__(kBlock) k_energy_terms(int n, int R, const double* __restrict__ m,
+                                                         const double* __restrict__ hex, const double* __restrict__ hdmi,
+                                                         const double* __restrict__ hext, const double* __restrict__ hdem,
+                                                         const double* __restrict__ js, const double* __restrict__ vol,
+                                                         const double* __restrict__ ku2, const double* __restrict__ kax,
+                                                         EnergyExtra x, double* __restrict__ part) {
+  __shared__ double sh[kEnergyTerms][kBlock / 32];
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int N = n * R;
+  double e[kEnergyTerms] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  if (g < N) {
+    const int i = g / R;
+    const double m0 = m[g], m1 = m[g + N], m2 = m[g + 2 * N];
+    const double w = vol[i] * js[i];
+    auto dot = [&](const double* h) { return h[g] * m0 + h[g + N] * m1 + h[g + 2 * N] * m2; };
+    e[0] = w * dot(hex);
+    if (hdmi) e[1] = w * dot(hdmi);
+    if (ku2) {
+      const double km = kax[i] * m0 + kax[i + n] * m1 + kax[i + 2 * n] * m2;
+      e[2] = vol[i] * 0.5 * ku2[i] * js[i] * km * km;
+    }
+    if (hext) e[3] = w * dot(hext);
+    if (hdem) e[4] = w * dot(hdem);
+    if (x.kc1) {
+      double al[3];
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        al[j] = x.cax[(3 * j) * n + i] * m0 + x.cax[(3 * j + 1) * n + i] * m1 + x.cax[(3 * j + 2) * n + i] * m2;
+      const double s0 = al[0] * al[0], s1 = al[1] * al[1], s2 = al[2] * al[2];
+      e[5] = vol[i] * (x.kc1[i] * (s0 * s1 + s1 * s2 + s0 * s2) + x.kc2[i] * s0 * s1 * s2);
+    }
+    if (x.ksa) {
+      const double nm = x.nvn[i] * m0 + x.nvn[i + n] * m1 + x.nvn[i + 2 * n] * m2;
+      e[6] = x.ksa[i] * nm * nm;
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < kEnergyTerms; ++q) {
+    double v = e[q];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[q][warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < kEnergyTerms) {
+    double s = 0.0;
+    for (int w = 0; w < kBlock / 32; ++w) s += sh[threadIdx.x][w];
+    part[size_t(blockIdx.x) * kEnergyTerms + threadIdx.x] = s;
+  }
+}
+
+int energy_blocks(int n, int R) { return grid_for(1LL * n * R); }
+
+void launch_energy_terms(int n, int R, const double* m, const double* hex, const double* hdmi, const double* hext,
+                         const double* hdem, const double* js, const double* vol, const double* ku2, const double* kax,
+                         const EnergyExtra& x, double* part, cudaStream_t st) {
+  note_launch();
+  k_energy_terms<<<grid_for(1LL * n * R), kBlock, 0, st>>>(n, R, m, hex, hdmi, hext, hdem, js, vol, ku2, kax, x,
+                                                          part);
+  TMB_CUDA(cudaGetLastError());
+}
 
 long long launch_count() { return g_launches.load(); }
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }

@@ -345,6 +345,16 @@ struct Ctx {
   DevArray<double> idm_d, idm_a, idm_b;
   std::vector<double> hD, hij;          // D and 1/Js per node, kept to switch the DMI form
   void upload_dmi();
+  // cubic and surface anisotropy (EffFieldCalc.cpp:128-149, 249-272): raw per-node constants on the
+  // host, device copies scaled by 1/Js (fields) and raw (energies)
+  std::vector<double> hKc1, hKc2, hcax, hKs, harea;
+  DevArray<double> cub_k1, cub_k2, cub_ax, srf_k, kc1_raw, kc2_raw, ksa_raw;
+  bool has_cub = false, has_srf = false;
+  void upload_extra();
+  // Zhang-Li spin-transfer torque (TheLLG::sttDynamics, main/TheLLG.cpp:201-220)
+  bool has_stt = false;
+  double stt_beta = 0.0, stt_scale = 1.0;
+  DevArray<double> stt_eta;
   LocalFieldArgs local_args(const double* m, double* ydot, double* hout, unsigned long long* tq) const;
   void launch_local(const LocalFieldArgs& a, cudaStream_t st);
   // BEM
@@ -450,6 +460,8 @@ struct Ctx {
   void demag(const double* m_dev);
   void local(const double* m, double* ydot, double* hout, unsigned long long* torque_bits);
   double max_torque(const double* m_dev);
+  void energies(const double* m_dev, double* out8);
+  DevArray<double> ebuf[2], epart;
   int integrate_segment(double*& y, double*& yalt, double t0, double t1, double& dt, double eps_abs,
                         double eps_rel, double* stats);
   int relax(double* m_dev, double duration_ps, double segment_ps, double eps_abs, double eps_rel, double* stats);
@@ -780,6 +792,10 @@ void Ctx::set_operators(int nx, const int* ptr, const int* col, const double* K_
   }
   node_vol.upload(vol, nx, st);
   area.upload(area_, nx, st);
+  harea.assign(area_, area_ + nx);
+  hKc1.clear();
+  hKs.clear();
+  has_cub = has_srf = has_stt = false;
   nvn.upload(nvn_soa, size_t(3) * nx, st);
   bnodes.upload(bn, nb_, st);
   std::vector<int> bi(nx, -1);
@@ -957,6 +973,7 @@ void Ctx::set_material(const double* Js, const double* A, const double* Ku, cons
   if (D) hD.assign(D, D + n);
   hij = ij;
   upload_dmi();
+  upload_extra();
   if (axis) {
     kax.upload(axis, size_t(3) * n, st);
   } else {
@@ -1447,6 +1464,38 @@ void Ctx::upload_dmi() {
   sync();
 }
 
+// Device arrays of the cubic / surface anisotropy for the current material (Js).
+void Ctx::upload_extra() {
+  cudaStream_t st = stream;
+  has_cub = !hKc1.empty();
+  has_srf = !hKs.empty();
+  if (has_cub) {
+    std::vector<double> k1(n), k2(n), ax(size_t(9) * n);
+    for (int i = 0; i < n; ++i) {
+      const double ij = hij.empty() ? 0.0 : hij[i];
+      k1[i] = hKc1[i] * ij;
+      k2[i] = hKc2[i] * ij;
+      for (int q = 0; q < 9; ++q) ax[size_t(q) * n + i] = hcax[size_t(9) * i + q];
+    }
+    cub_k1.upload(k1, st);
+    cub_k2.upload(k2, st);
+    cub_ax.upload(ax, st);
+    kc1_raw.upload(hKc1, st);
+    kc2_raw.upload(hKc2, st);
+  }
+  if (has_srf) {
+    std::vector<double> ks(n), ksa(n);
+    for (int i = 0; i < n; ++i) {
+      const double ij = hij.empty() ? 0.0 : hij[i];
+      ksa[i] = hKs[i] * harea[i];
+      ks[i] = ksa[i] / hvol[i] * ij;
+    }
+    srf_k.upload(ks, st);
+    ksa_raw.upload(ksa, st);
+  }
+  sync();
+}
+
 LocalFieldArgs Ctx::local_args(const double* m, double* ydot, double* hout, unsigned long long* tq) const {
   LocalFieldArgs a;
   a.n = n;
@@ -1462,6 +1511,10 @@ LocalFieldArgs Ctx::local_args(const double* m, double* ydot, double* hout, unsi
   a.idm_d = idmi ? idm_d.p : nullptr;
   a.idm_a = idmi ? idm_a.p : nullptr;
   a.idm_b = idmi ? idm_b.p : nullptr;
+  a.cub_k1 = has_cub ? cub_k1.p : nullptr;
+  a.cub_k2 = cub_k2.p;
+  a.cub_ax = cub_ax.p;
+  a.srf_k = has_srf ? srf_k.p : nullptr;
   a.alpha = alpha;
   a.precession = precession;
   a.ydot = ydot;
@@ -1476,6 +1529,12 @@ void Ctx::launch_local(const LocalFieldArgs& a, cudaStream_t st) {
     launch_local_field<double>(S, K.p, tg[0].p, tg[1].p, tg[2].p, g[0].p, g[1].p, a, st);
   else
     launch_local_field<float>(S, Kf.p, tgf[0].p, tgf[1].p, tgf[2].p, gf[0].p, gf[1].p, a, st);
+  if (has_stt && a.ydot) {
+    if (precision == TMB_FP64)
+      launch_stt_add<double>(S, g[0].p, g[1].p, g[2].p, a.m, stt_eta.p, alpha, stt_beta, stt_scale, a.ydot, st);
+    else
+      launch_stt_add<float>(S, gf[0].p, gf[1].p, gf[2].p, a.m, stt_eta.p, alpha, stt_beta, stt_scale, a.ydot, st);
+  }
 }
 
 void Ctx::local(const double* m, double* ydot, double* hout, unsigned long long* tq) {
@@ -1490,6 +1549,86 @@ void Ctx::local(const double* m, double* ydot, double* hout, unsigned long long*
   prof.begin(0, stream, bytes);
   launch_local(a, stream);
   prof.end(stream);
+}
+
+// Energy densities of TheSimulation::calculateEnergies (main/TheSimulation.cpp:385-396): demag
+// (DemagField::getDemagEnergy, main/DemagField.cpp:97-99), exchange (calcExchangeEnergy,
+// main/EffFieldCalc.cpp:65-69), uniaxial with its offset (uniaxialEnergy, :86-95), Zeeman
+// (TheLLG::getZeemanEnergy, main/TheLLG.cpp:345-348), cubic (cubicAnisotropyEnergy, :232-247),
+// surface with its offset (surfaceAnisotropyEnergy, :108-126), DMI (-1/2 sum V H_dmi . m), each
+// divided by the total volume.  out = {total, demag, exchange, uniaxial, Zeeman, cubic, surface,
+// DMI}.  The demag field is evaluated for m when a BEM matrix is set (else the frozen one is
+// used).  With components or replicas the sums run over the whole batch.
+void Ctx::energies(const double* m, double* out) {
+  require_mesh();
+  require_material();
+  cudaStream_t st = stream;
+  const size_t n3 = size_t(3) * nr();
+  if (has_bem) demag(m);
+  for (auto& b : ebuf) b.alloc(n3);
+  // exchange alone, then exchange + DMI: the DMI field is the difference
+  LocalFieldArgs a = local_args(m, nullptr, ebuf[0].p, nullptr);
+  a.hfix = nullptr;
+  a.ku2 = nullptr;
+  a.dmi_s = nullptr;
+  a.idm_a = a.idm_b = a.idm_d = nullptr;
+  a.cub_k1 = nullptr;
+  a.srf_k = nullptr;
+  launch_local(a, st);
+  const double* hdmi = nullptr;
+  if (has_dmi) {
+    LocalFieldArgs b = local_args(m, nullptr, ebuf[1].p, nullptr);
+    b.hfix = nullptr;
+    b.ku2 = nullptr;
+    b.cub_k1 = nullptr;
+    b.srf_k = nullptr;
+    launch_local(b, st);
+    launch_lincomb(int(n3), ebuf[1].p, 1.0, ebuf[1].p, -1.0, ebuf[0].p, 0.0, nullptr, st);
+    hdmi = ebuf[1].p;
+  }
+  const int nblk = energy_blocks(n, rep);
+  epart.alloc(size_t(kEnergyTerms) * nblk);
+  EnergyExtra ex;
+  if (has_cub) {
+    ex.kc1 = kc1_raw.p;
+    ex.kc2 = kc2_raw.p;
+    ex.cax = cub_ax.p;
+  }
+  if (has_srf) {
+    ex.ksa = ksa_raw.p;
+    ex.nvn = nvn.p;
+  }
+  launch_energy_terms(n, rep, m, ebuf[0].p, hdmi, hext.p, hdem.p, js.p, node_vol.p, has_uni ? ku2.p : nullptr,
+                      kax.p, ex, epart.p, st);
+  std::vector<double> h(size_t(kEnergyTerms) * nblk);
+  TMB_CUDA(cudaMemcpyAsync(h.data(), epart.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  sync();
+  double sum[kEnergyTerms] = {0, 0, 0, 0, 0, 0, 0};
+  for (int b = 0; b < nblk; ++b)
+    for (int q = 0; q < kEnergyTerms; ++q) sum[q] += h[size_t(kEnergyTerms) * b + q];
+  double vtot = 0.0, ku_vol = 0.0, ks_off = 0.0;
+  for (int i = 0; i < n; ++i) vtot += hvol[i];
+  if (has_uni) {
+    std::vector<double> k2(n);
+    TMB_CUDA(cudaMemcpy(k2.data(), ku2.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; ++i) ku_vol += hvol[i] * 0.5 * k2[i] / (hij[i] != 0.0 ? hij[i] : 1.0);
+  }
+  if (has_srf)
+    for (int i = 0; i < n; ++i) ks_off += hKs[i] * harea[i];  // EffFieldCalc::setSurfaceAnisotropy
+  vtot *= rep;
+  ku_vol *= rep;
+  ks_off *= rep;
+  const double e_dem = -0.5 * sum[4] / vtot, e_ex = -0.5 * sum[0] / vtot, e_uni = (ku_vol - sum[2]) / vtot;
+  const double e_zee = -sum[3] / vtot, e_dmi = -0.5 * sum[1] / vtot;
+  const double e_cub = sum[5] / vtot, e_srf = has_srf ? (ks_off - sum[6]) / vtot : 0.0;
+  out[0] = e_dem + e_ex + e_uni + e_zee + e_dmi + e_cub + e_srf;
+  out[1] = e_dem;
+  out[2] = e_ex;
+  out[3] = e_uni;
+  out[4] = e_zee;
+  out[5] = e_cub;
+  out[6] = e_srf;
+  out[7] = e_dmi;
 }
 
 static double bits_to_double(unsigned long long b) {
@@ -1756,6 +1895,8 @@ void Ctx::adjoint_rk4(const double* m0, int nsteps, double dt_ps, int nsub, int 
   if (has_bem && (ncomp() != 1 || bem_mode != 0))
     throw Error(TMB_ERR_STATE, "adjoint: needs one component and the dense BEM matrix");
   if (rep != 1) throw Error(TMB_ERR_STATE, "adjoint: not for interleaved replicas");
+  if (has_cub || has_srf || has_stt)
+    throw Error(TMB_ERR_STATE, "adjoint: cubic / surface anisotropy and spin-transfer torque have no transpose here");
   if (has_bem) ensure_demag();
   cudaStream_t st = stream;
   const size_t n3 = size_t(3) * n;
@@ -2531,6 +2672,69 @@ int tmb_relax(tmb_ctx* ctx, double* m, double duration_ps, double segment_ps, do
     TMB_CUDA(cudaMemcpyAsync(m, c.in3.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
     c.sync();
   }
+  TMB_API_END
+}
+
+int tmb_set_cubic_anisotropy(tmb_ctx* ctx, const double* Kc1, const double* Kc2, const double* axes) {
+  TMB_CHECK_ARG(ctx, "tmb_set_cubic_anisotropy: null context");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  c.require_mesh();
+  TMB_CUDA(cudaSetDevice(c.device));
+  if (!Kc1) {
+    c.hKc1.clear();
+  } else {
+    if (!Kc2 || !axes) return fail(TMB_ERR_ARG, "tmb_set_cubic_anisotropy: Kc2 and axes are required with Kc1");
+    c.hKc1.assign(Kc1, Kc1 + c.n);
+    c.hKc2.assign(Kc2, Kc2 + c.n);
+    c.hcax.assign(axes, axes + size_t(9) * c.n);
+  }
+  c.upload_extra();
+  TMB_API_END
+}
+
+int tmb_set_surface_anisotropy(tmb_ctx* ctx, const double* Ks) {
+  TMB_CHECK_ARG(ctx, "tmb_set_surface_anisotropy: null context");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  c.require_mesh();
+  TMB_CUDA(cudaSetDevice(c.device));
+  if (!Ks) c.hKs.clear();
+  else c.hKs.assign(Ks, Ks + c.n);
+  c.upload_extra();
+  TMB_API_END
+}
+
+int tmb_set_stt(tmb_ctx* ctx, const double* eta, double beta, double scale) {
+  TMB_CHECK_ARG(ctx, "tmb_set_stt: null context");
+  TMB_CHECK_ARG(std::isfinite(beta) && std::isfinite(scale), "tmb_set_stt: beta and scale must be finite");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  c.require_mesh();
+  TMB_CUDA(cudaSetDevice(c.device));
+  if (!eta) {
+    c.has_stt = false;
+    c.stt_eta.reset();
+  } else {
+    c.stt_eta.upload(eta, size_t(3) * c.n, c.stream);
+    c.stt_beta = beta;
+    c.stt_scale = scale;
+    c.has_stt = true;
+    c.sync();
+  }
+  TMB_API_END
+}
+
+int tmb_energies(tmb_ctx* ctx, const double* m, double* out, int ptr_kind) {
+  TMB_CHECK_ARG(ctx && m && out, "tmb_energies: null argument");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  c.require_mesh();
+  TMB_CUDA(cudaSetDevice(c.device));
+  const double* md = stage_in(c, c.in3, m, size_t(3) * c.nr(), ptr_kind);
+  c.energies(md, out);
+  for (int i = 0; i < 8; ++i)
+    if (!std::isfinite(out[i])) return fail(TMB_ERR_NAN, "tmb_energies: an energy is not finite");
   TMB_API_END
 }
 

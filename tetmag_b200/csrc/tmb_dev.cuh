@@ -73,6 +73,10 @@ struct LocalFieldArgs {
   const double* idm_d;      // N  D_j (interfacial DMI), null otherwise
   const double* idm_a;      // N  D_i / Js_i (interfacial DMI), null otherwise
   const double* idm_b;      // N  1 / (V_i Js_i) (interfacial DMI)
+  const double* cub_k1;     // N  Kc1 / Js (cubic anisotropy), null without it
+  const double* cub_k2;     // N  Kc2 / Js
+  const double* cub_ax;     // 9N SoA cubic axes: c1 (x, y, z), c2, c3, each N long
+  const double* srf_k;      // N  Ks * node area / (V Js) (surface anisotropy), null without it
   double alpha;
   int precession;
   double* ydot;             // 3N out, may be null
@@ -93,6 +97,24 @@ void launch_gradient(const SellView& s, const V* g0, const V* g1, const V* g2, c
                      const double* u2, const double* hext, double* hdem, double* hfix, cudaStream_t st);
 
 void launch_normalize(int n, double* m, cudaStream_t st);
+// Zhang-Li spin-transfer torque added to ydot (eta: 3N SoA per node)
+template <typename V>
+void launch_stt_add(const SellView& s, const V* g0, const V* g1, const V* g2, const double* m, const double* eta,
+                    double alpha, double beta, double scale, double* ydot, cudaStream_t st);
+// energy terms, R interleaved replicas: kEnergyTerms partial sums per block (see k_field.cu);
+// extra: cubic (raw Kc1, Kc2 [J/m^3], axes SoA 9N) and surface anisotropy (Ks * node area [J])
+struct EnergyExtra {
+  const double* kc1 = nullptr;
+  const double* kc2 = nullptr;
+  const double* cax = nullptr;
+  const double* ksa = nullptr;
+  const double* nvn = nullptr;
+};
+constexpr int kEnergyTerms = 7;
+int energy_blocks(int n, int R);
+void launch_energy_terms(int n, int R, const double* m, const double* hex, const double* hdmi, const double* hext,
+                         const double* hdem, const double* js, const double* vol, const double* ku2, const double* kax,
+                         const EnergyExtra& x, double* part, cudaStream_t st);
 void launch_rk_combine(int n3, const double* y, const double* const* k, const double* a, int nk, double h,
                        double* out, cudaStream_t st);
 void launch_rk_error(int n3, const double* y, const double* k1, const double* const* k, const double* e, int nk,
