@@ -302,6 +302,38 @@ int tmb_solver_solve(tmb_solver* s, const double* b, double* x, int ptr_kind);  
 /* info[0] iterations, [1] relative residual, [2] status (0 ok, 3 not converged, 5 breakdown) */
 int tmb_solver_info(tmb_solver* s, double* info);
 
+/* ---------------------------------------------------------------------------------------
+ * Run artefacts (host only, no device work except where stated).
+ * ------------------------------------------------------------------------------------- */
+/* MeshWriter::outputVTK (io/MeshWriter.cpp:174-239; grid of defineUnstructuredVTKGrid, :69-86):
+ * a VTK XML unstructured grid of tetrahedra with point vectors "Magnetization" (m, 3N SoA), point
+ * scalars "Material" (material, N ints; NULL writes zeros), an optional second point vector field
+ * (field, 3N SoA, named field_name; NULL: none; tetmag's final file carries "Demag",
+ * main/TheSimulation.cpp:321) and the field-data value "timeInPs" (io/MeshWriter.h:60).
+ * xyz: N x 3 row-major, tets: E x 4.  binary = 0 writes ASCII arrays, 1 appended raw binary. */
+int tmb_write_vtu(const char* path, int nx, const double* xyz, int ntet, const int* tets, const double* m,
+                  const int* material, double time_ps, const double* field, const char* field_name, int binary);
+/* VTKReader::readMag + getTime (io/VTKReader.cpp:83-181): the point array "Magnetization" of a .vtu
+ * (ASCII, inline base64 or appended raw / base64 arrays, optionally zlib-compressed, UInt32 or UInt64
+ * headers: what VTK's XML writer produces) or of a legacy ASCII .vtk file, into m (3N SoA), and the
+ * field-data value "timeInPs" into time_ps (0 when absent).  A point count other than nx is an
+ * error (VTKReader::checkNodeNumber, :72-81). */
+int tmb_read_magnetization(const char* path, int nx, double* m, double* time_ps);
+/* writeLogFileHeader (main/TheSimulation.cpp:85-93): the header lines of tetmag's .log file, with
+ * the start time as ctime() gives it (ending in a newline), host and user; NUL-terminated in buf. */
+int tmb_log_header(const char* start_time, const char* host, const char* user, char* buf, int cap);
+/* TheSimulation::writeLogStream (main/TheSimulation.cpp:367-372) after calculateEnergies (:385-396):
+ * one .log row for state m at elapsed_ps, character for character as tetmag writes it: time,
+ * the eight energy densities of tmb_energies, the max torque (computed when max_torque < 0), the
+ * volume-weighted mean m and mean applied field in T (applied field plus the Bz pulse at
+ * elapsed_ps).  Evaluates the demag field for m like tmb_energies; synchronises. */
+int tmb_log_row(tmb_ctx* ctx, const double* m, int ptr_kind, double elapsed_ps, double max_torque, char* buf,
+                int cap);
+/* The formatting step of tmb_log_row alone (writeLogStream, main/TheSimulation.cpp:367-372):
+ * energies[8] in tmb_energies order, mean_m[3], mean_h_tesla[3]. */
+int tmb_log_format(double elapsed_ps, const double* energies, double max_torque, const double* mean_m,
+                   const double* mean_h_tesla, char* buf, int cap);
+
 #ifdef __cplusplus
 }
 #endif

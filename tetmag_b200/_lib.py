@@ -63,6 +63,11 @@ SIGNATURES = {
     "tmb_normalize": [_P, _P, _int],
     "tmb_relax": [_P, _P, _dbl, _dbl, _dbl, _dbl, _D, _int],
     "tmb_energies": [_P, _P, _D, _int],
+    "tmb_write_vtu": [C.c_char_p, _int, _D, _int, _I, _D, _I, _dbl, _D, C.c_char_p, _int],
+    "tmb_read_magnetization": [C.c_char_p, _int, _D, _D],
+    "tmb_log_header": [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, _int],
+    "tmb_log_row": [_P, _P, _int, _dbl, _dbl, C.c_char_p, _int],
+    "tmb_log_format": [_dbl, _D, _dbl, _D, _D, C.c_char_p, _int],
     "tmb_set_cubic_anisotropy": [_P, _D, _D, _D],
     "tmb_set_surface_anisotropy": [_P, _D],
     "tmb_set_stt": [_P, _D, _dbl, _dbl],

@@ -352,6 +352,13 @@ class Context:
         keys = ["total", "demag", "exchange", "uniaxial", "zeeman", "cubic", "surface", "dmi"]
         return {kk: out[i] for i, kk in enumerate(keys)}
 
+    def log_row(self, m, elapsed_ps: float, max_torque: float = -1.0) -> str:
+        """One row of tetmag's .log file for state m (tmb_log_row)."""
+        buf = C.create_string_buffer(1024)
+        pm, k = _vec(m)
+        check(lib().tmb_log_row(self.h, pm, k, float(elapsed_ps), float(max_torque), buf, len(buf)))
+        return buf.value.decode()
+
     def set_bz_pulse(self, bz_tesla, t0_ps: float, t1_ps: float):
         """Piecewise-linear Bz(t) samples [T] over [t0_ps, t1_ps], added to the applied z field during
         step_rk4 / adjoint_rk4 (an empty sequence removes it)."""
@@ -398,6 +405,43 @@ class Context:
         keys = ["it_neumann", "it_dirichlet", "res_neumann", "res_dirichlet", "status_neumann",
                 "status_dirichlet", "amg_levels", "amg_setup_ms"]
         return {kk: st[i] for i, kk in enumerate(keys)}
+
+
+def write_vtu(path, xyz, tets, m, material=None, time_ps: float = 0.0, field=None, field_name: str = "Demag",
+              binary: bool = True):
+    """tetmag's .vtu output (tmb_write_vtu): xyz (N, 3), tets (E, 4), m and field 3N SoA."""
+    x, t, mm = _f64(xyz).reshape(-1, 3), _i32(tets).reshape(-1, 4), _f64(m)
+    n = x.shape[0]
+    mat = None if material is None else _i32(np.broadcast_to(material, (n,)))
+    f = None if field is None else _f64(field)
+    check(lib().tmb_write_vtu(str(path).encode(), n, _dptr(x), t.shape[0], _iptr(t), _dptr(mm),
+                              None if mat is None else _iptr(mat), float(time_ps),
+                              None if f is None else _dptr(f), field_name.encode(), 1 if binary else 0))
+
+
+def read_magnetization(path, nx: int):
+    """VTKReader::readMag + getTime (tmb_read_magnetization): (m as 3N SoA, time in ps)."""
+    m = np.empty(3 * nx)
+    t = C.c_double(0.0)
+    check(lib().tmb_read_magnetization(str(path).encode(), int(nx), _dptr(m), C.byref(t)))
+    return m, t.value
+
+
+def log_header(start_time: str, host: str, user: str) -> str:
+    """The header of tetmag's .log file (tmb_log_header)."""
+    buf = C.create_string_buffer(2048)
+    check(lib().tmb_log_header(start_time.encode(), host.encode(), user.encode(), buf, len(buf)))
+    return buf.value.decode()
+
+
+def log_format(elapsed_ps: float, energies, max_torque: float, mean_m, mean_h_tesla) -> str:
+    """A .log row from its values (tmb_log_format); energies in tmb_energies order (dict or 8 values)."""
+    keys = ["total", "demag", "exchange", "uniaxial", "zeeman", "cubic", "surface", "dmi"]
+    e = _f64([energies[k] for k in keys] if isinstance(energies, dict) else energies)
+    mm, hh = _f64(mean_m), _f64(mean_h_tesla)
+    buf = C.create_string_buffer(1024)
+    check(lib().tmb_log_format(float(elapsed_ps), _dptr(e), float(max_torque), _dptr(mm), _dptr(hh), buf, len(buf)))
+    return buf.value.decode()
 
 
 def kernel_launches() -> int:

@@ -2738,6 +2738,90 @@ int tmb_energies(tmb_ctx* ctx, const double* m, double* out, int ptr_kind) {
   TMB_API_END
 }
 
+int tmb_write_vtu(const char* path, int nx, const double* xyz, int ntet, const int* tets, const double* m,
+                  const int* material, double time_ps, const double* field, const char* field_name, int binary) {
+  TMB_CHECK_ARG(path && nx > 0 && ntet >= 0 && xyz && m && (ntet == 0 || tets) && (binary == 0 || binary == 1),
+                "tmb_write_vtu: null argument or bad size");
+  TMB_API_BEGIN
+  for (long long k = 0; k < 4LL * ntet; ++k)
+    if (tets[k] < 0 || tets[k] >= nx) return fail(TMB_ERR_ARG, "tmb_write_vtu: node index out of range");
+  std::string err;
+  if (int rc = write_vtu(path, nx, xyz, ntet, tets, m, material, time_ps, "timeInPs", field, field_name, binary,
+                         err))
+    return fail(rc, err);
+  TMB_API_END
+}
+
+int tmb_read_magnetization(const char* path, int nx, double* m, double* time_ps) {
+  TMB_CHECK_ARG(path && nx > 0 && m && time_ps, "tmb_read_magnetization: null argument or nx <= 0");
+  TMB_API_BEGIN
+  std::string err;
+  if (int rc = read_magnetization(path, nx, m, time_ps, err)) return fail(rc, err);
+  TMB_API_END
+}
+
+static int copy_text(const std::string& t, char* buf, int cap, const char* who) {
+  if (int(t.size()) + 1 > cap)
+    return fail(TMB_ERR_ARG, std::string(who) + ": buffer too small (" + std::to_string(t.size() + 1) + " bytes needed)");
+  std::memcpy(buf, t.c_str(), t.size() + 1);
+  return TMB_OK;
+}
+
+int tmb_log_header(const char* start_time, const char* host, const char* user, char* buf, int cap) {
+  TMB_CHECK_ARG(buf && cap > 0, "tmb_log_header: null buffer");
+  TMB_API_BEGIN
+  return copy_text(log_header(start_time, host, user), buf, cap, "tmb_log_header");
+  TMB_API_END
+}
+
+int tmb_log_format(double elapsed_ps, const double* energies, double max_torque, const double* mean_m,
+                   const double* mean_h_tesla, char* buf, int cap) {
+  TMB_CHECK_ARG(energies && mean_m && mean_h_tesla && buf && cap > 0, "tmb_log_format: null argument");
+  TMB_API_BEGIN
+  return copy_text(log_row(elapsed_ps, energies, max_torque, mean_m, mean_h_tesla), buf, cap, "tmb_log_format");
+  TMB_API_END
+}
+
+int tmb_log_row(tmb_ctx* ctx, const double* m, int ptr_kind, double elapsed_ps, double max_torque, char* buf,
+                int cap) {
+  TMB_CHECK_ARG(ctx && m && buf && cap > 0, "tmb_log_row: null argument");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  c.require_mesh();
+  c.require_material();
+  TMB_CUDA(cudaSetDevice(c.device));
+  const size_t n3 = size_t(3) * c.nr();
+  const double* md = stage_in(c, c.in3, m, n3, ptr_kind);
+  double e[8];
+  c.energies(md, e);
+  if (max_torque < 0.0) max_torque = c.max_torque(md);
+  // volume-weighted means (TheSimulation::getMeanM, main/TheSimulation.cpp:100-102; TheLLG::getMeanH,
+  // main/TheLLG.cpp:421-423) over every node of every replica, the field in Tesla
+  std::vector<double> hm(n3), hh(n3);
+  TMB_CUDA(cudaMemcpyAsync(hm.data(), md, n3 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  TMB_CUDA(cudaMemcpyAsync(hh.data(), c.hext.p, n3 * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  c.sync();
+  const int nrr = c.nr(), R = c.rep;
+  double mm[3] = {0, 0, 0}, mh[3] = {0, 0, 0}, vt = 0.0;
+  for (int g = 0; g < nrr; ++g) {
+    const double v = c.hvol[g / R];
+    vt += v;
+    for (int d = 0; d < 3; ++d) {
+      mm[d] += v * hm[size_t(d) * nrr + g];
+      mh[d] += v * hh[size_t(d) * nrr + g];
+    }
+  }
+  for (int d = 0; d < 3; ++d) {
+    mm[d] /= vt;
+    mh[d] = mh[d] / vt * kMu0;
+  }
+  mh[2] += c.pulse_hz(elapsed_ps) * kMu0;
+  for (double x : e)
+    if (!std::isfinite(x)) return fail(TMB_ERR_NAN, "tmb_log_row: an energy is not finite");
+  return copy_text(log_row(elapsed_ps, e, max_torque, mm, mh), buf, cap, "tmb_log_row");
+  TMB_API_END
+}
+
 int tmb_set_bem_gemm_kind(tmb_ctx* ctx, int tensor_cores) {
   TMB_CHECK_ARG(ctx && (tensor_cores == 0 || tensor_cores == 1), "tmb_set_bem_gemm_kind: kind is 0 or 1");
   TMB_API_BEGIN

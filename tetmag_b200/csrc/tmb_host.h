@@ -111,3 +111,15 @@ void csr_transpose(const Csr& A, Csr& T);
 void csr_multiply(const Csr& A, const Csr& B, Csr& C);
 
 }  // namespace tmb
+
+namespace tmb {
+
+// output.cpp -- run artefacts: VTU files, magnetisation restart files, .log columns.
+int write_vtu(const std::string& path, int nx, const double* xyz, int ntet, const int* tets, const double* m,
+              const int* material, double time_ps, const char* time_name, const double* field,
+              const char* field_name, int binary, std::string& err);
+int read_magnetization(const std::string& path, int nx, double* m, double* time_ps, std::string& err);
+std::string log_header(const char* start_time, const char* host, const char* user);
+std::string log_row(double t_ps, const double e[8], double torque, const double mean_m[3], const double mean_h_t[3]);
+
+}  // namespace tmb
