@@ -125,7 +125,7 @@ def test_log_row_of_a_context_matches_oracle():
     m = O.rows_to_soa(g["m"])
     row = ctx.log_row(m, 250.0)
     cols = row.rstrip("\n").split("\t")
-    assert len(cols) == 13 and cols[0] == "250.0000"
+    assert len(cols) == 12 and cols[0] == "250.0000"
     pb = O.make_problem(g["xyz"], g["tets"], 1e-9, Ms=8e5, A=1.3e-11, alpha=0.3, Ku=5e4, ku_axis=g["axis"],
                         D=3e-3, hext=np.ascontiguousarray(g["hext"]), with_bem=False)
     eo = O.energies(pb, g["m"], g["hdem"])

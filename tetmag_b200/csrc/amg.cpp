@@ -154,6 +154,7 @@ void dense_inverse(std::vector<double>& a, int n) {
       }
     const double d = 1.0 / a[size_t(c) * n + c];
     for (int k = 0; k < n; ++k) { a[size_t(c) * n + k] *= d; inv[size_t(c) * n + k] *= d; }
+#pragma omp parallel for schedule(static) if (n >= 256)
     for (int r = 0; r < n; ++r) {
       if (r == c) continue;
       const double f = a[size_t(r) * n + c];

@@ -287,9 +287,16 @@ __global__ void k_h_compact(const HBlockDev* __restrict__ blk, const double* __r
                             T* __restrict__ V) {
   const HBlockDev b = blk[blockIdx.x];
   const int k = rank[blockIdx.x];
-  const long long nu = (long long)k * b.m, nv = (long long)k * b.n;
-  for (long long t = threadIdx.x; t < nu; t += blockDim.x) U[dst_u[blockIdx.x] + t] = static_cast<T>(Us[b.uoff + t]);
-  for (long long t = threadIdx.x; t < nv; t += blockDim.x) V[dst_v[blockIdx.x] + t] = static_cast<T>(Vs[b.voff + t]);
+  const int mp = pad4(b.m), np = pad4(b.n);
+  const long long nu = (long long)k * mp, nv = (long long)k * np;
+  for (long long t = threadIdx.x; t < nu; t += blockDim.x) {
+    const int l = int(t / mp), i = int(t - (long long)l * mp);
+    U[dst_u[blockIdx.x] + t] = i < b.m ? static_cast<T>(Us[b.uoff + (long long)l * b.m + i]) : T(0);
+  }
+  for (long long t = threadIdx.x; t < nv; t += blockDim.x) {
+    const int l = int(t / np), j = int(t - (long long)l * np);
+    V[dst_v[blockIdx.x] + t] = j < b.n ? static_cast<T>(Vs[b.voff + (long long)l * b.n + j]) : T(0);
+  }
 }
 
 // x in cluster order: xp[i] = u[gidx[i]] (gidx = boundary node of permuted position i).
@@ -324,104 +331,6 @@ __global__ void __launch_bounds__(256) k_h_near(const HNearRow* __restrict__ row
   }
 }
 
-// Low-rank part, one CTA per work item (a run of admissible blocks b = (tau, sigma) of one row
-// cluster tau, bounded in size so the CTAs are balanced): for each block t = V_b^T x_sigma (a
-// warp per term, t in shared memory), then y_tau += U_b t accumulated in registers, each thread
-// owning a row and a slice of the terms; one atomic add per row at the end.  Every U and V entry
-// is read once per matvec.
-template <typename T>
-__global__ void __launch_bounds__(256) k_h_far(const HFarGroup* __restrict__ grp, const HBlockDev* __restrict__ blk,
-                                               const int* __restrict__ rank, const long long* __restrict__ uoff,
-                                               const long long* __restrict__ voff, const T* __restrict__ U,
-                                               const T* __restrict__ V, const T* __restrict__ xp,
-                                               double* __restrict__ y) {
-  // The row cluster's low-rank blocks are taken in chunks (at most kBlkCap blocks and kTermCap
-  // terms): first every term t = V_b^T x_sigma of the chunk (one warp per term), then every row
-  // accumulates U_b t over the chunk's blocks, so the CTA synchronises twice per chunk instead of
-  // twice per block.
-  constexpr int kTermCap = 1024, kBlkCap = 128;
-  __shared__ double ts[kTermCap];
-  __shared__ int tb[kBlkCap + 1];   // term offsets of the chunk's blocks
-  __shared__ int nq_s;
-  __shared__ double red[256];
-  const HFarGroup g = grp[blockIdx.x];
-  const int m = g.m;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  // m <= 256: thread -> (row, term slice); m > 256: thread -> rows threadIdx.x + 256 r
-  const int slices = m >= 256 ? 1 : 256 / m;
-  const int row = m >= 256 ? threadIdx.x : threadIdx.x % m;
-  const int slice = m >= 256 ? 0 : threadIdx.x / m;
-  double acc[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int q0 = g.first; q0 < g.last;) {
-    if (threadIdx.x == 0) {
-      int t = 0, c = 0;
-      tb[0] = 0;
-      while (q0 + c < g.last && c < kBlkCap) {
-        const int k = rank[q0 + c];
-        if (c > 0 && t + k > kTermCap) break;
-        t += k;
-        ++c;
-        tb[c] = t;
-      }
-      nq_s = c;
-    }
-    __syncthreads();
-    const int nq = nq_s, nt = tb[nq];
-    for (int p = warp; p < nt; p += 8) {
-      int lo = 0, hi = nq - 1;  // block c of term p: tb[c] <= p < tb[c + 1]
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (tb[mid] <= p) lo = mid;
-        else hi = mid - 1;
-      }
-      const int q = q0 + lo, l = p - tb[lo];
-      const int n = blk[q].n, cb = blk[q].cb;
-      const T* vl = V + voff[q] + (long long)l * n;
-      double a = 0.0;
-#pragma unroll 4
-      for (int j = lane; j < n; j += 32) a = fma(double(vl[j]), double(xp[cb + j]), a);
-      a = warp_sum_d(a);
-      if (lane == 0) ts[p] = a;
-    }
-    __syncthreads();
-    for (int c = 0; c < nq; ++c) {
-      const int q = q0 + c, k = tb[c + 1] - tb[c];
-      const T* u = U + uoff[q];
-      const double* tq = ts + tb[c];
-      if (m >= 256) {
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          const int i = row + 256 * r;
-          if (i < m) {
-#pragma unroll 4
-            for (int l = 0; l < k; ++l) acc[r] = fma(double(u[(long long)l * m + i]), tq[l], acc[r]);
-          }
-        }
-      } else if (slice < slices) {
-#pragma unroll 4
-        for (int l = slice; l < k; l += slices) acc[0] = fma(double(u[(long long)l * m + row]), tq[l], acc[0]);
-      }
-    }
-    __syncthreads();
-    q0 += nq;
-  }
-  if (m >= 256) {
-#pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int i = row + 256 * r;
-      if (i < m) atomicAdd(&y[g.rb + i], acc[r]);
-    }
-  } else {
-    red[threadIdx.x] = acc[0];
-    __syncthreads();
-    if (threadIdx.x < m) {
-      double s = 0.0;
-      for (int sl = 0; sl < slices; ++sl) s += red[sl * m + threadIdx.x];
-      atomicAdd(&y[g.rb + threadIdx.x], s);
-    }
-  }
-}
-
 // Deterministic probe value in [-1, 1) for position j (cluster order): splitmix64 of j.
 __device__ __forceinline__ double probe_value(long long j) {
   unsigned long long z = static_cast<unsigned long long>(j) + 0x9e3779b97f4a7c15ull;
@@ -449,7 +358,8 @@ __global__ void __launch_bounds__(256) k_h_verify(const HBlockDev* __restrict__ 
     const int q = f ? l : l - k64;
     double a = 0.0;
     for (int j = lane; j < b.n; j += 32) {
-      const double v = f ? V64[vo64[blockIdx.x] + (long long)q * b.n + j] : double(V32[vo32[blockIdx.x] + (long long)q * b.n + j]);
+      const long long o = (long long)q * pad4(b.n) + j;
+      const double v = f ? V64[vo64[blockIdx.x] + o] : double(V32[vo32[blockIdx.x] + o]);
       a = fma(v, probe_value(b.cb + j), a);
     }
     a = warp_sum_d(a);
@@ -461,8 +371,9 @@ __global__ void __launch_bounds__(256) k_h_verify(const HBlockDev* __restrict__ 
     double y = 0.0;
     for (int j = 0; j < b.n; ++j) y = fma(entry(b.rb + i, b.cb + j), probe_value(b.cb + j), y);
     double y64 = 0.0, y32 = 0.0;
-    for (int l = 0; l < k64; ++l) y64 = fma(U64[uo64[blockIdx.x] + (long long)l * b.m + i], t64[l], y64);
-    for (int l = 0; l < k32; ++l) y32 = fma(double(U32[uo32[blockIdx.x] + (long long)l * b.m + i]), t32[l], y32);
+    const int mp = pad4(b.m);
+    for (int l = 0; l < k64; ++l) y64 = fma(U64[uo64[blockIdx.x] + (long long)l * mp + i], t64[l], y64);
+    for (int l = 0; l < k32; ++l) y32 = fma(double(U32[uo32[blockIdx.x] + (long long)l * mp + i]), t32[l], y32);
     s0 += y * y;
     s1 += (y - y64) * (y - y64);
     s2 += (y - y32) * (y - y32);
@@ -474,6 +385,129 @@ __global__ void __launch_bounds__(256) k_h_verify(const HBlockDev* __restrict__ 
     out[3 * blockIdx.x] = s0;
     out[3 * blockIdx.x + 1] = s1;
     out[3 * blockIdx.x + 2] = s2;
+  }
+}
+
+// 16-byte vectors of the factor type: 4 floats or 2 doubles.
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+  using type = float4;
+  static constexpr int n = 4;
+  __device__ static void add(double* a, const float4& u, double t) {
+    a[0] = fma(double(u.x), t, a[0]);
+    a[1] = fma(double(u.y), t, a[1]);
+    a[2] = fma(double(u.z), t, a[2]);
+    a[3] = fma(double(u.w), t, a[3]);
+  }
+  __device__ static double dot(const float4& v, const float* x) {
+    return double(v.x) * double(x[0]) + double(v.y) * double(x[1]) + double(v.z) * double(x[2]) +
+           double(v.w) * double(x[3]);
+  }
+};
+template <>
+struct Vec16<double> {
+  using type = double2;
+  static constexpr int n = 2;
+  __device__ static void add(double* a, const double2& u, double t) {
+    a[0] = fma(u.x, t, a[0]);
+    a[1] = fma(u.y, t, a[1]);
+  }
+  __device__ static double dot(const double2& v, const double* x) { return fma(v.x, x[0], v.y * x[1]); }
+};
+
+// Far field, first pass: t_p = V_p^T x_sigma for every term p of every admissible block, one warp
+// per term, 16-byte streaming loads of V (each entry read once), x from cache.  The padded tail
+// of V is zero and x has four zero entries past its end.
+template <typename T>
+__global__ void __launch_bounds__(256) k_h_vt(long long nterms, const HTerm* __restrict__ terms,
+                                              const T* __restrict__ V, const T* __restrict__ xp,
+                                              double* __restrict__ t) {
+  using W = Vec16<T>;
+  using VT = typename W::type;
+  const long long p = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (p >= nterms) return;
+  const int lane = threadIdx.x & 31;
+  const HTerm h = terms[p];
+  const VT* v = reinterpret_cast<const VT*>(V + h.v);
+  const T* x = xp + h.cb;
+  const int nv = h.n4 / W::n;
+  double a0 = 0.0, a1 = 0.0;
+  int j = lane;
+  for (; j + 32 < nv; j += 64) {
+    const VT v0 = __ldcs(v + j), v1 = __ldcs(v + j + 32);
+    a0 += W::dot(v0, x + W::n * j);
+    a1 += W::dot(v1, x + W::n * (j + 32));
+  }
+  if (j < nv) a0 += W::dot(__ldcs(v + j), x + W::n * j);
+  double a = warp_sum_d(a0 + a1);
+  if (lane == 0) t[p] = a;
+}
+
+// Far field, second pass: y_tau += sum_b U_b t_b over the admissible blocks of one work item (a
+// run of blocks of one row cluster tau), one CTA per item.  Thread -> (16-byte row vector, term
+// slice); U is streamed with 16-byte loads, each entry read once; one atomic add per row.
+template <typename T>
+__global__ void __launch_bounds__(256) k_h_ut(const HFarGroup* __restrict__ grp, const int* __restrict__ rank,
+                                              const long long* __restrict__ uoff, const long long* __restrict__ toff,
+                                              const T* __restrict__ U, const double* __restrict__ t,
+                                              double* __restrict__ y) {
+  using W = Vec16<T>;
+  using VT = typename W::type;
+  constexpr int E = W::n;
+  __shared__ double red[256 * E];
+  const HFarGroup g = grp[blockIdx.x];
+  const int mp = pad4(g.m), nvec = mp / E;
+  // nvec <= 256 (floats, m <= 1024): thread -> (vec, slice); doubles with nvec > 256: two vecs
+  const int per = (nvec + 255) / 256;
+  const int slices = nvec >= 256 ? 1 : 256 / nvec;
+  const int vec = nvec >= 256 ? threadIdx.x : threadIdx.x % nvec;
+  const int slice = nvec >= 256 ? 0 : threadIdx.x / nvec;
+  double acc[2][E];
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+#pragma unroll
+    for (int e = 0; e < E; ++e) acc[r][e] = 0.0;
+  if (slice < slices) {
+    for (int q = g.first; q < g.last; ++q) {
+      const int k = rank[q];
+      const VT* u = reinterpret_cast<const VT*>(U + uoff[q]);
+      const double* tq = t + toff[q];
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const int vv = vec + 256 * r;
+        if (r < per && vv < nvec) {
+          int l = slice;
+          for (; l + slices < k; l += 2 * slices) {
+            const VT u0 = __ldcs(u + (long long)l * nvec + vv), u1 = __ldcs(u + (long long)(l + slices) * nvec + vv);
+            const double t0 = __ldg(tq + l), t1 = __ldg(tq + l + slices);
+            W::add(acc[r], u0, t0);
+            W::add(acc[r], u1, t1);
+          }
+          if (l < k) W::add(acc[r], __ldcs(u + (long long)l * nvec + vv), __ldg(tq + l));
+        }
+      }
+    }
+  }
+  if (nvec >= 256) {
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int i = E * (vec + 256 * r) + e;
+        if (r < per && i < g.m) atomicAdd(&y[g.rb + i], acc[r][e]);
+      }
+  } else {
+#pragma unroll
+    for (int e = 0; e < E; ++e) red[threadIdx.x * E + e] = acc[0][e];
+    __syncthreads();
+    for (int i = threadIdx.x; i < g.m; i += 256) {
+      const int v = i / E, e = i - v * E;
+      double s = 0.0;
+      for (int sl = 0; sl < slices; ++sl) s += red[(sl * nvec + v) * E + e];
+      atomicAdd(&y[g.rb + i], s);
+    }
   }
 }
 
@@ -543,7 +577,9 @@ void launch_h_matvec(const HMatView<T>& H, const double* u, double* y, T* xp, co
   k_h_near<T><<<H.nrows, 256, 0, st>>>(H.near_rows, H.near, H.D, xp, y);
   if (H.nterms > 0) {
     note_launch();
-    k_h_far<T><<<H.ngroups, 256, 0, st>>>(H.groups, H.far, H.rank, H.uoff, H.voff, H.U, H.V, xp, y);
+    k_h_vt<T><<<unsigned((H.nterms + 7) / 8), 256, 0, st>>>(H.nterms, H.terms, H.V, xp, H.t);
+    note_launch();
+    k_h_ut<T><<<H.ngroups, 256, 0, st>>>(H.groups, H.rank, H.uoff, H.toff, H.U, H.t, y);
   }
   note_launch();
   k_h_dirichlet<<<grid_for(n), kBlock, 0, st>>>(n, pos, y, bdir);

@@ -233,18 +233,41 @@ __global__ void __launch_bounds__(kBlock) k_csr_jacobi(CsrView c, const V* __res
   if (row < c.n * c.rep && sub == 0) xout[row] = xin[row] + dinv[row / c.rep] * (b[row] - acc);
 }
 
-// x = A_c^-1 b on the coarsest level: one warp per row of the dense FP64 inverse.
-__global__ void k_coarse_solve(int n, int R, const double* __restrict__ inv, const double* __restrict__ b,
+// x = A_c^-1 b on the coarsest level (dense FP64 inverse, row-major, even leading dimension ld):
+// one warp per row and replica.
+__global__ void k_coarse_solve(int n, int ld, int R, const double* __restrict__ inv, const double* __restrict__ b,
                                double* __restrict__ x, const int* done) {
   if (done && *done) return;
   const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (g >= n * R) return;
   const int i = g / R, r = g - i * R;
-  const double* row = inv + size_t(i) * n;
+  const double* row = inv + size_t(i) * ld;
   double acc = 0.0;
   for (int j = lane; j < n; j += 32) acc = fma(row[j], b[j * R + r], acc);
   acc = warp_sum(acc);
   if (lane == 0) x[g] = acc;
+}
+
+// The same product for one replica and a larger coarsest level: one 128-thread CTA per row, all
+// of a thread's 16-byte loads of the row issued together.
+__global__ void __launch_bounds__(128) k_coarse_solve_rows(int n, int ld, const double* __restrict__ inv,
+                                                           const double* __restrict__ b, double* __restrict__ x,
+                                                           const int* done) {
+  if (done && *done) return;
+  __shared__ double red[4];
+  const double2* row = reinterpret_cast<const double2*>(inv + size_t(blockIdx.x) * ld);
+  const int np = ld / 2;
+  double a0 = 0.0, a1 = 0.0;
+  for (int j = threadIdx.x; j < np; j += 128) {
+    const double2 v = __ldg(row + j);
+    const int c = 2 * j;
+    a0 = fma(v.x, __ldg(b + c), a0);
+    if (c + 1 < n) a1 = fma(v.y, __ldg(b + c + 1), a1);
+  }
+  double a = warp_sum(a0 + a1);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
+  __syncthreads();
+  if (threadIdx.x == 0) x[blockIdx.x] = (red[0] + red[1]) + (red[2] + red[3]);
 }
 
 template <typename V>
@@ -501,10 +524,11 @@ void launch_csr_jacobi(const CsrView& c, const V* val, const double* dinv, const
   TMB_CSR_DISPATCH(tpr, k_csr_jacobi, 1LL * c.n * c.rep, c, val, dinv, b, xin, xout, done)
 }
 #undef TMB_CSR_DISPATCH
-void launch_coarse_solve(int n, int rep, const double* inv, const double* b, double* x, const int* done,
+void launch_coarse_solve(int n, int ld, int rep, const double* inv, const double* b, double* x, const int* done,
                          cudaStream_t st) {
   note_launch();
-  k_coarse_solve<<<grid_for(32LL * n * rep), kBlock, 0, st>>>(n, rep, inv, b, x, done);
+  if (rep == 1 && n >= 256) k_coarse_solve_rows<<<n, 128, 0, st>>>(n, ld, inv, b, x, done);
+  else k_coarse_solve<<<grid_for(32LL * n * rep), kBlock, 0, st>>>(n, ld, rep, inv, b, x, done);
 }
 template <typename V>
 void launch_cg_init(int n, const CsrView& lift, const V* lval, const int* cmask, const double* b,

@@ -255,7 +255,7 @@ struct Solver {
   AmgHierarchy H;
   std::vector<DevLevel> lev;
   DevArray<double> cinv;
-  int ncoarse = 0;
+  int ncoarse = 0, cld = 0;
   DevCsr lift;
   DevArray<int> cmask;
   // transposed solve (the adjoint): lift^T, masked load, and a warm start kept apart from the
@@ -401,7 +401,9 @@ struct Ctx {
     DevArray<double> D64, U64, V64, y, xp64;
     DevArray<float> D32, U32, V32, xp32;
     DevArray<int> rank[2];
-    DevArray<long long> uoff[2], voff[2];
+    DevArray<long long> uoff[2], voff[2], toff[2];
+    DevArray<HTerm> termd[2];             // per-term descriptors of the far-field product
+    DevArray<double> tval;                // the terms' values, one matvec at a time
     // boundary geometry in cluster order when the matrix was built from the mesh
     bool from_mesh = false;
     int ntri = 0;
@@ -613,7 +615,14 @@ void Solver::compute() {
     }
   }
   ncoarse = H.ncoarse;
-  cinv.upload(H.coarse_inv, st);
+  cld = ncoarse + (ncoarse & 1);  // even rows: 16-byte loads
+  {
+    std::vector<double> ci(size_t(ncoarse) * cld, 0.0);
+    for (int i = 0; i < ncoarse; ++i)
+      std::copy(H.coarse_inv.begin() + size_t(i) * ncoarse, H.coarse_inv.begin() + size_t(i + 1) * ncoarse,
+                ci.begin() + size_t(i) * cld);
+    cinv.upload(ci, st);
+  }
   lift.upload(L, st);
   liftT.upload(LT, st);
   for (bool& h : has_xadj) h = false;
@@ -641,7 +650,7 @@ void Solver::vcycle(size_t l, const double* b, double* out, int precision, cudaS
   DevLevel& L = lev[l];
   const int* done = &Sd->done;
   if (l + 1 == lev.size()) {
-    launch_coarse_solve(ncoarse, rep, cinv.p, b, out, done, st);
+    launch_coarse_solve(ncoarse, cld, rep, cinv.p, b, out, done, st);
     return;
   }
   DevLevel& C = lev[l + 1];
@@ -1166,6 +1175,9 @@ HMatView<T> Ctx::h_view(int w) const {
   v.uoff = H.uoff[w].p;
   v.voff = H.voff[w].p;
   v.groups = H.groups[w].p;
+  v.terms = H.termd[w].p;
+  v.toff = H.toff[w].p;
+  v.t = H.tval.p;
   if constexpr (sizeof(T) == 8) {
     v.D = H.D64.p;
     v.U = H.U64.p;
@@ -1300,14 +1312,21 @@ void Ctx::h_compress(const double* bxyz, const double* bnrm, int leaf, double et
       std::vector<int> rk(H.nfar);
       std::vector<long long> uo(H.nfar), vo(H.nfar);
       long long su = 0, sv = 0, stt = 0;
+      std::vector<long long> to(H.nfar);
+      std::vector<HTerm> td;
       for (int q = 0; q < H.nfar; ++q) {
         rk[q] = ranks[size_t(3) * q + w];
         uo[q] = su;
         vo[q] = sv;
-        su += (long long)rk[q] * farb[q].m;
-        sv += (long long)rk[q] * farb[q].n;
+        to[q] = stt;
+        const int np = pad4(farb[q].n);
+        for (int l = 0; l < rk[q]; ++l) td.push_back(HTerm{sv + (long long)l * np, np, farb[q].cb});
+        su += (long long)rk[q] * pad4(farb[q].m);
+        sv += (long long)rk[q] * np;
         stt += rk[q];
       }
+      H.toff[w].upload(to, st);
+      H.termd[w].upload(td, st);
       // matvec work items: the admissible blocks of one row cluster, cut into runs of about
       // wmax U + V entries (about 64 items per SM), largest first
       double total = 0.0;
@@ -1370,8 +1389,12 @@ void Ctx::h_compress(const double* bxyz, const double* bnrm, int leaf, double et
   }
   H.ranks = ranks;
   H.y.alloc(nb);
-  H.xp64.alloc(nb);
-  H.xp32.alloc(nb);
+  // four zero entries past the end: the padded tail of a V row meets them
+  H.xp64.alloc(size_t(nb) + 4);
+  H.xp32.alloc(size_t(nb) + 4);
+  H.xp64.zero(st);
+  H.xp32.zero(st);
+  H.tval.alloc(size_t(std::max(std::max(H.terms[0], H.terms[1]), 1LL)));
   H.built = true;
   bem_mode = 1;
   if (mesh) has_bem = true;

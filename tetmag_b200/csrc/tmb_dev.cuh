@@ -144,7 +144,7 @@ void launch_csr_jacobi0_residual(const CsrView& c, const V* val, const double* d
 template <typename V>
 void launch_csr_jacobi(const CsrView& c, const V* val, const double* dinv, const double* b, const double* xin,
                        double* xout, const int* done, cudaStream_t st, int tpr);
-void launch_coarse_solve(int n, int rep, const double* inv, const double* b, double* x, const int* done,
+void launch_coarse_solve(int n, int ld, int rep, const double* inv, const double* b, double* x, const int* done,
                          cudaStream_t st);
 
 template <typename V>
@@ -223,6 +223,14 @@ struct HNearRow {
 struct HFarGroup {
   int rb, m, first, last;  // row cluster and its admissible blocks [first, last)
 };
+// Low-rank factors are stored with leading dimensions padded to a multiple of 4 entries (zero
+// padding), so that every column of U and every row of V^T starts on a 16-byte boundary.
+__host__ __device__ inline int pad4(int x) { return (x + 3) & ~3; }
+// One term of the far-field product: t = V_l^T x[cb .. cb + n4) (n4 = pad4(n)), V_l at offset v.
+struct HTerm {
+  long long v;
+  int n4, cb;
+};
 template <typename T>
 struct HMatView {
   int nb = 0, nrows = 0, ngroups = 0;
@@ -233,11 +241,14 @@ struct HMatView {
   const T* D = nullptr;                  // dense tiles
   const HBlockDev* far = nullptr;
   const int* rank = nullptr;
-  const long long* uoff = nullptr;       // compact U offsets (column-major m x rank)
-  const long long* voff = nullptr;       // compact V offsets (column-major n x rank)
+  const long long* uoff = nullptr;       // compact U offsets (column-major pad4(m) x rank)
+  const long long* voff = nullptr;       // compact V offsets (column-major pad4(n) x rank)
   const T* U = nullptr;
   const T* V = nullptr;
   const HFarGroup* groups = nullptr;     // row clusters, largest work first
+  const HTerm* terms = nullptr;          // every term of every admissible block, block by block
+  const long long* toff = nullptr;       // first term of each admissible block
+  double* t = nullptr;                   // the terms' values V^T x (nterms)
 };
 // Where the entries of the boundary matrix (in cluster order) come from: the dense FP64
 // matrix (B != nullptr, row-major with leading dimension ld, rows/columns perm[i]) or the

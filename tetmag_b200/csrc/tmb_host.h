@@ -75,7 +75,10 @@ struct AmgParams {
   // on the 363,609-node film to 1e-7)
   double eps_strong = 0.02;
   double relax = 0.75;                     // prolongation-smoother factor (main/AMGCLSolver.cpp:40)
-  int coarse_enough = 200;                 // dense FP64 solve below this size
+  // dense FP64 solve at or below this size: on the 363,609-node film the hierarchy then stops at
+  // the 1,676-unknown level (one dense product instead of five latency-bound launches for the two
+  // smallest levels per V-cycle)
+  int coarse_enough = 2000;
   int max_levels = 12;
   double jacobi_omega = 0.9;               // smoother damping (times 4 / (3 rho(D^-1 A)))
   bool singular = false;                   // operator annihilates constants (pure Neumann)
