@@ -417,46 +417,73 @@ struct Vec16<double> {
   __device__ static double dot(const double2& v, const double* x) { return fma(v.x, x[0], v.y * x[1]); }
 };
 
-// Far field, first pass: t_p = V_p^T x_sigma for every term p of every admissible block, one warp
-// per term, 16-byte streaming loads of V (each entry read once), x from cache.  The padded tail
+// Far field, first pass: t_p = V_p^T x_sigma for every term p of every admissible block.  A warp
+// takes four consecutive terms and issues the 16-byte streaming loads of all four rows of V before
+// it uses them (each entry read once; x from cache), then reduces the four dots.  The padded tail
 // of V is zero and x has four zero entries past its end.
+constexpr int kTermsPerWarp = 4;
 template <typename T>
 __global__ void __launch_bounds__(256) k_h_vt(long long nterms, const HTerm* __restrict__ terms,
                                               const T* __restrict__ V, const T* __restrict__ xp,
                                               double* __restrict__ t) {
   using W = Vec16<T>;
   using VT = typename W::type;
-  const long long p = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
-  if (p >= nterms) return;
+  constexpr int P = kTermsPerWarp;
+  const long long p0 = ((long long)blockIdx.x * 8 + (threadIdx.x >> 5)) * P;
+  if (p0 >= nterms) return;
   const int lane = threadIdx.x & 31;
-  const HTerm h = terms[p];
-  const VT* v = reinterpret_cast<const VT*>(V + h.v);
-  const T* x = xp + h.cb;
-  const int nv = h.n4 / W::n;
-  double a0 = 0.0, a1 = 0.0;
-  int j = lane;
-  for (; j + 32 < nv; j += 64) {
-    const VT v0 = __ldcs(v + j), v1 = __ldcs(v + j + 32);
-    a0 += W::dot(v0, x + W::n * j);
-    a1 += W::dot(v1, x + W::n * (j + 32));
+  const VT* v[P];
+  const T* x[P];
+  int nv[P];
+  int most = 0;
+#pragma unroll
+  for (int i = 0; i < P; ++i) {
+    const bool ok = p0 + i < nterms;
+    const HTerm h = terms[ok ? p0 + i : p0];
+    v[i] = reinterpret_cast<const VT*>(V + h.v);
+    x[i] = xp + h.cb;
+    nv[i] = ok ? h.n4 / W::n : 0;
+    most = max(most, nv[i]);
   }
-  if (j < nv) a0 += W::dot(__ldcs(v + j), x + W::n * j);
-  double a = warp_sum_d(a0 + a1);
-  if (lane == 0) t[p] = a;
+  double acc[P];
+#pragma unroll
+  for (int i = 0; i < P; ++i) acc[i] = 0.0;
+  for (int j = lane; j < most; j += 64) {
+    VT a[P], b[P];
+#pragma unroll
+    for (int i = 0; i < P; ++i) {
+      if (j < nv[i]) a[i] = __ldcs(v[i] + j);
+      if (j + 32 < nv[i]) b[i] = __ldcs(v[i] + j + 32);
+    }
+#pragma unroll
+    for (int i = 0; i < P; ++i) {
+      if (j < nv[i]) acc[i] += W::dot(a[i], x[i] + W::n * j);
+      if (j + 32 < nv[i]) acc[i] += W::dot(b[i], x[i] + W::n * (j + 32));
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < P; ++i) {
+    const double s = warp_sum_d(acc[i]);
+    if (lane == 0 && p0 + i < nterms) t[p0 + i] = s;
+  }
 }
 
 // Far field, second pass: y_tau += sum_b U_b t_b over the admissible blocks of one work item (a
-// run of blocks of one row cluster tau), one CTA per item.  Thread -> (16-byte row vector, term
-// slice); U is streamed with 16-byte loads, each entry read once; one atomic add per row.
+// run of blocks of one row cluster tau, hence a contiguous range of terms), one CTA per item.
+// The item's term offsets and values are staged in shared memory (up to kStage at a time), then
+// thread -> (16-byte row vector, term slice) streams its U entries with independent 16-byte loads
+// (each entry read once); one atomic add per row at the end.
+constexpr int kStage = 512;
 template <typename T>
-__global__ void __launch_bounds__(256) k_h_ut(const HFarGroup* __restrict__ grp, const int* __restrict__ rank,
-                                              const long long* __restrict__ uoff, const long long* __restrict__ toff,
-                                              const T* __restrict__ U, const double* __restrict__ t,
-                                              double* __restrict__ y) {
+__global__ void __launch_bounds__(256) k_h_ut(const HFarGroup* __restrict__ grp, const long long* __restrict__ toff,
+                                              const HTerm* __restrict__ terms, const T* __restrict__ U,
+                                              const double* __restrict__ t, double* __restrict__ y) {
   using W = Vec16<T>;
   using VT = typename W::type;
   constexpr int E = W::n;
   __shared__ double red[256 * E];
+  __shared__ long long su[kStage];
+  __shared__ double st[kStage];
   const HFarGroup g = grp[blockIdx.x];
   const int mp = pad4(g.m), nvec = mp / E;
   // nvec <= 256 (floats, m <= 1024): thread -> (vec, slice); doubles with nvec > 256: two vecs
@@ -464,28 +491,34 @@ __global__ void __launch_bounds__(256) k_h_ut(const HFarGroup* __restrict__ grp,
   const int slices = nvec >= 256 ? 1 : 256 / nvec;
   const int vec = nvec >= 256 ? threadIdx.x : threadIdx.x % nvec;
   const int slice = nvec >= 256 ? 0 : threadIdx.x / nvec;
+  const long long pbeg = toff[g.first], pend = toff[g.last];  // toff has an entry past the last block
   double acc[2][E];
 #pragma unroll
   for (int r = 0; r < 2; ++r)
 #pragma unroll
     for (int e = 0; e < E; ++e) acc[r][e] = 0.0;
-  if (slice < slices) {
-    for (int q = g.first; q < g.last; ++q) {
-      const int k = rank[q];
-      const VT* u = reinterpret_cast<const VT*>(U + uoff[q]);
-      const double* tq = t + toff[q];
+  for (long long c0 = pbeg; c0 < pend; c0 += kStage) {
+    const int nc = int(min((long long)kStage, pend - c0));
+    __syncthreads();  // the previous stage is consumed
+    for (int i = threadIdx.x; i < nc; i += 256) {
+      su[i] = terms[c0 + i].u;
+      st[i] = t[c0 + i];
+    }
+    __syncthreads();
+    if (slice < slices) {
 #pragma unroll
       for (int r = 0; r < 2; ++r) {
         const int vv = vec + 256 * r;
         if (r < per && vv < nvec) {
-          int l = slice;
-          for (; l + slices < k; l += 2 * slices) {
-            const VT u0 = __ldcs(u + (long long)l * nvec + vv), u1 = __ldcs(u + (long long)(l + slices) * nvec + vv);
-            const double t0 = __ldg(tq + l), t1 = __ldg(tq + l + slices);
-            W::add(acc[r], u0, t0);
-            W::add(acc[r], u1, t1);
+          int i = slice;
+          for (; i + 3 * slices < nc; i += 4 * slices) {
+            VT uv[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) uv[c] = __ldcs(reinterpret_cast<const VT*>(U + su[i + c * slices]) + vv);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) W::add(acc[r], uv[c], st[i + c * slices]);
           }
-          if (l < k) W::add(acc[r], __ldcs(u + (long long)l * nvec + vv), __ldg(tq + l));
+          for (; i < nc; i += slices) W::add(acc[r], __ldcs(reinterpret_cast<const VT*>(U + su[i]) + vv), st[i]);
         }
       }
     }
@@ -499,6 +532,7 @@ __global__ void __launch_bounds__(256) k_h_ut(const HFarGroup* __restrict__ grp,
         if (r < per && i < g.m) atomicAdd(&y[g.rb + i], acc[r][e]);
       }
   } else {
+    __syncthreads();
 #pragma unroll
     for (int e = 0; e < E; ++e) red[threadIdx.x * E + e] = acc[0][e];
     __syncthreads();
@@ -577,9 +611,10 @@ void launch_h_matvec(const HMatView<T>& H, const double* u, double* y, T* xp, co
   k_h_near<T><<<H.nrows, 256, 0, st>>>(H.near_rows, H.near, H.D, xp, y);
   if (H.nterms > 0) {
     note_launch();
-    k_h_vt<T><<<unsigned((H.nterms + 7) / 8), 256, 0, st>>>(H.nterms, H.terms, H.V, xp, H.t);
+    const long long warps = (H.nterms + kTermsPerWarp - 1) / kTermsPerWarp;
+    k_h_vt<T><<<unsigned((warps + 7) / 8), 256, 0, st>>>(H.nterms, H.terms, H.V, xp, H.t);
     note_launch();
-    k_h_ut<T><<<H.ngroups, 256, 0, st>>>(H.groups, H.rank, H.uoff, H.toff, H.U, H.t, y);
+    k_h_ut<T><<<H.ngroups, 256, 0, st>>>(H.groups, H.toff, H.terms, H.U, H.t, y);
   }
   note_launch();
   k_h_dirichlet<<<grid_for(n), kBlock, 0, st>>>(n, pos, y, bdir);

@@ -65,8 +65,9 @@ __device__ __forceinline__ bool grid_reduce(const double (&v)[K], double* partia
 }
 
 // Entries of a SELL-32 row are visited in chunks of kChunk: the chunk's column indices and
-// values are loaded first (coalesced across the warp), then its kChunk gathers are issued
-// together, so that a thread keeps kChunk gathers in flight (FEM rows hold 10-15 entries).
+// values are loaded first (coalesced across the warp, values kept in the operator's type), then
+// its kChunk gathers are issued together (FEM rows hold 10-15 entries; 16-entry chunks measured
+// slower: more registers, fewer resident threads).
 constexpr int kChunk = 8;
 
 // Dot of operator row g / rep with replica g % rep of x (state row g).
@@ -81,16 +82,16 @@ __device__ __forceinline__ double sell_row_dot(const SellView& s, const V* __res
   double acc = 0.0;
   for (int k0 = beg; k0 < end; k0 += kChunk * kSlice) {
     int j[kChunk];
-    double v[kChunk];
+    V v[kChunk];
 #pragma unroll
     for (int u = 0; u < kChunk; ++u) {
       const int k = k0 + u * kSlice;
       const bool ok = k < end;
       j[u] = ok ? __ldg(s.col + k) * R + r : g;
-      v[u] = ok ? static_cast<double>(__ldg(val + k)) : 0.0;
+      v[u] = ok ? __ldg(val + k) : V(0);
     }
 #pragma unroll
-    for (int u = 0; u < kChunk; ++u) acc = fma(v[u], __ldg(x + j[u]), acc);
+    for (int u = 0; u < kChunk; ++u) acc = fma(static_cast<double>(v[u]), __ldg(x + j[u]), acc);
   }
   return acc;
 }
@@ -147,16 +148,17 @@ __global__ void __launch_bounds__(kBlock) k_jacobi0_residual(SellView s, const V
   double acc = 0.0;
   for (int k0 = beg; k0 < end; k0 += kChunk * kSlice) {
     int j[kChunk];
-    double v[kChunk];
+    V v[kChunk];
 #pragma unroll
     for (int u = 0; u < kChunk; ++u) {
       const int k = k0 + u * kSlice;
       const bool ok = k < end;
       j[u] = ok ? __ldg(s.col + k) : row;
-      v[u] = ok ? static_cast<double>(__ldg(val + k)) : 0.0;
+      v[u] = ok ? __ldg(val + k) : V(0);
     }
 #pragma unroll
-    for (int u = 0; u < kChunk; ++u) acc = fma(v[u], __ldg(dinv + j[u]) * __ldg(b + j[u] * R + rr), acc);
+    for (int u = 0; u < kChunk; ++u)
+      acc = fma(static_cast<double>(v[u]), __ldg(dinv + j[u]) * __ldg(b + j[u] * R + rr), acc);
   }
   const double bi = b[g];
   x[g] = dinv[row] * bi;
@@ -173,6 +175,7 @@ __device__ __forceinline__ double group_sum(double v) {
 
 // Partial dot of a CSR row over the entries k = beg + sub, beg + sub + T, ... (x premultiplied by
 // w when w is not null).
+constexpr int kCsrChunk = 8;
 template <typename V, int T>
 __device__ __forceinline__ double csr_row_part(const CsrView& c, const V* __restrict__ val, const double* __restrict__ x,
                                                const double* __restrict__ w, int g, int sub) {
@@ -181,10 +184,22 @@ __device__ __forceinline__ double csr_row_part(const CsrView& c, const V* __rest
   if (g < c.n * R) {
     const int row = g / R, r = g - row * R;
     const int beg = __ldg(c.ptr + row), end = __ldg(c.ptr + row + 1);
-    for (int k = beg + sub; k < end; k += T) {
-      const int j = __ldg(c.col + k);
-      const double xj = w ? __ldg(w + j) * __ldg(x + j * R + r) : __ldg(x + j * R + r);
-      acc = fma(static_cast<double>(__ldg(val + k)), xj, acc);
+    // chunks of kCsrChunk entries per thread: indices and values first, then the gathers
+    for (int k0 = beg + sub; k0 < end; k0 += kCsrChunk * T) {
+      int j[kCsrChunk];
+      V v[kCsrChunk];
+#pragma unroll
+      for (int u = 0; u < kCsrChunk; ++u) {
+        const int k = k0 + u * T;
+        const bool ok = k < end;
+        j[u] = ok ? __ldg(c.col + k) : 0;
+        v[u] = ok ? __ldg(val + k) : V(0);
+      }
+#pragma unroll
+      for (int u = 0; u < kCsrChunk; ++u) {
+        const double xj = w ? __ldg(w + j[u]) * __ldg(x + j[u] * R + r) : __ldg(x + j[u] * R + r);
+        acc = fma(static_cast<double>(v[u]), xj, acc);
+      }
     }
   }
   return acc;
@@ -351,17 +366,48 @@ __global__ void __launch_bounds__(kBlock) k_jacobi_rz(SellView s, const V* __res
   }
 }
 
-// q = A p_new with p_new = z + beta p_old formed on the fly (two gathers), p_new written
-// for the own row into a second buffer; p.Ap reduced, the last block sets alpha.
+// New direction and its product without gathering p: p = z + beta p and q = A p = A z + beta q
+// (the previous q is A p_old), both updated in place for the own row, so the product gathers z
+// alone; p.q reduced, the last block sets alpha.  beta = 0 (first pass) reads neither old vector.
 template <typename V>
 __global__ void __launch_bounds__(kBlock) k_cg_dir_spmv(SellView s, const V* __restrict__ val,
-                                                        const double* __restrict__ z,
-                                                        const double* __restrict__ p_old, double* __restrict__ p_new,
+                                                        const double* __restrict__ z, double* __restrict__ p,
                                                         double* __restrict__ q, CgScalars* S, double* partials) {
   if (S->done) return;
   const double beta = S->beta;
   double v[1] = {0.0};
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < s.n * s.rep; g += gridDim.x * blockDim.x) {
+    const double az = sell_row_dot(s, val, z, g);
+    const double zi = z[g];
+    const double pi = (beta == 0.0) ? zi : fma(beta, p[g], zi);
+    const double qi = (beta == 0.0) ? az : fma(beta, q[g], az);
+    p[g] = pi;
+    q[g] = qi;
+    v[0] = fma(pi, qi, v[0]);
+  }
+  double tot[1];
+  if (grid_reduce<1>(v, partials, &S->ticket[2], tot) && threadIdx.x == 0) {
+    S->pq = tot[0];
+    S->alpha = S->rz / tot[0];
+  }
+}
+
+// The CG update fused with the first smoothing sweep of the V-cycle on the finest level:
+// x += alpha p and r_new = r - alpha q for the own row (||r_new||^2 reduced, the last block
+// decides convergence as k_cg_update does), then X = D_w^-1 r_new and R = r_new - A X, with the
+// neighbours' r_new formed on the fly from r and q.  r and r_new are different buffers.
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_cg_update_jacobi0(SellView s, const V* __restrict__ val,
+                                                              const double* __restrict__ dinv,
+                                                              const double* __restrict__ p,
+                                                              const double* __restrict__ q, double* __restrict__ x,
+                                                              const double* __restrict__ r, double* __restrict__ r_new,
+                                                              double* __restrict__ X, double* __restrict__ Rres,
+                                                              CgScalars* S, double* partials) {
+  if (S->done) return;
+  const double alpha = S->alpha;
   const int R = s.rep;
+  double v[1] = {0.0};
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < s.n * R; g += gridDim.x * blockDim.x) {
     const int row = g / R, rr = g - row * R;
     const int sl = row >> 5;
@@ -370,31 +416,40 @@ __global__ void __launch_bounds__(kBlock) k_cg_dir_spmv(SellView s, const V* __r
     double acc = 0.0;
     for (int k0 = beg; k0 < end; k0 += kChunk * kSlice) {
       int j[kChunk];
-      double v[kChunk];
+      V w[kChunk];
 #pragma unroll
       for (int u = 0; u < kChunk; ++u) {
         const int k = k0 + u * kSlice;
         const bool ok = k < end;
-        j[u] = ok ? __ldg(s.col + k) * R + rr : g;
-        v[u] = ok ? static_cast<double>(__ldg(val + k)) : 0.0;
+        j[u] = ok ? __ldg(s.col + k) : row;
+        w[u] = ok ? __ldg(val + k) : V(0);
       }
-      if (beta == 0.0) {
 #pragma unroll
-        for (int u = 0; u < kChunk; ++u) acc = fma(v[u], __ldg(z + j[u]), acc);
-      } else {
-#pragma unroll
-        for (int u = 0; u < kChunk; ++u) acc = fma(v[u], fma(beta, __ldg(p_old + j[u]), __ldg(z + j[u])), acc);
+      for (int u = 0; u < kChunk; ++u) {
+        const int jj = j[u] * R + rr;
+        acc = fma(static_cast<double>(w[u]), __ldg(dinv + j[u]) * fma(-alpha, __ldg(q + jj), __ldg(r + jj)), acc);
       }
     }
-    const double pi = (beta == 0.0) ? z[g] : fma(beta, p_old[g], z[g]);
-    p_new[g] = pi;
-    q[g] = acc;
-    v[0] = fma(pi, acc, v[0]);
+    const double ri = fma(-alpha, q[g], r[g]);
+    x[g] = fma(alpha, p[g], x[g]);
+    r_new[g] = ri;
+    X[g] = dinv[row] * ri;
+    Rres[g] = ri - acc;
+    v[0] = fma(ri, ri, v[0]);
   }
   double tot[1];
-  if (grid_reduce<1>(v, partials, &S->ticket[2], tot) && threadIdx.x == 0) {
-    S->pq = tot[0];
-    S->alpha = S->rz / tot[0];
+  if (grid_reduce<1>(v, partials, &S->ticket[3], tot) && threadIdx.x == 0) {
+    S->rr = tot[0];
+    S->iter += 1;
+    if (!(tot[0] == tot[0]) || !(S->pq > 0.0)) {
+      S->done = 1;
+      S->status = 5;  // breakdown / NaN
+    } else if (tot[0] <= S->tol2 * S->bb) {
+      S->done = 1;
+    } else if (S->iter >= S->maxit) {
+      S->done = 1;
+      S->status = 3;  // not converged within maxit
+    }
   }
 }
 
@@ -570,10 +625,18 @@ void launch_jacobi_rz(const SellView& s, const V* val, const double* dinv, const
   k_jacobi_rz<V><<<reduce_grid(1LL * s.n * s.rep), kBlock, 0, st>>>(s, val, dinv, r, xin, z, S, partials, first ? 1 : 0);
 }
 template <typename V>
-void launch_cg_dir_spmv(const SellView& s, const V* val, const double* z, const double* p_old, double* p_new,
-                        double* q, CgScalars* S, double* partials, cudaStream_t st) {
+void launch_cg_dir_spmv(const SellView& s, const V* val, const double* z, double* p, double* q, CgScalars* S,
+                        double* partials, cudaStream_t st) {
   note_launch();
-  k_cg_dir_spmv<V><<<reduce_grid(1LL * s.n * s.rep), kBlock, 0, st>>>(s, val, z, p_old, p_new, q, S, partials);
+  k_cg_dir_spmv<V><<<reduce_grid(1LL * s.n * s.rep), kBlock, 0, st>>>(s, val, z, p, q, S, partials);
+}
+template <typename V>
+void launch_cg_update_jacobi0(const SellView& s, const V* val, const double* dinv, const double* p, const double* q,
+                              double* x, const double* r, double* r_new, double* X, double* Rres, CgScalars* S,
+                              double* partials, cudaStream_t st) {
+  note_launch();
+  k_cg_update_jacobi0<V><<<reduce_grid(1LL * s.n * s.rep), kBlock, 0, st>>>(s, val, dinv, p, q, x, r, r_new, X,
+                                                                              Rres, S, partials);
 }
 
 void launch_cg_update(int n, const double* p, const double* q, double* x, double* r, CgScalars* S,
@@ -604,8 +667,11 @@ void launch_cg_update(int n, const double* p, const double* q, double* x, double
                                            double*, const int*, cudaStream_t);                              \
   template void launch_jacobi_rz<V>(const SellView&, const V*, const double*, const double*, const double*, \
                                     double*, CgScalars*, double*, bool, cudaStream_t);                      \
-  template void launch_cg_dir_spmv<V>(const SellView&, const V*, const double*, const double*, double*,     \
-                                      double*, CgScalars*, double*, cudaStream_t);
+  template void launch_cg_dir_spmv<V>(const SellView&, const V*, const double*, double*, double*, CgScalars*, \
+                                      double*, cudaStream_t);                                                 \
+  template void launch_cg_update_jacobi0<V>(const SellView&, const V*, const double*, const double*,         \
+                                            const double*, double*, const double*, double*, double*, double*, \
+                                            CgScalars*, double*, cudaStream_t);
 TMB_INST(double)
 TMB_INST(float)
 #undef TMB_INST

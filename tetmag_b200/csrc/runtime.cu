@@ -264,7 +264,7 @@ struct Solver {
   static constexpr int kAdjSlots = 4;   // one warm start per RK stage
   DevArray<double> ct, xfwd, xadj[kAdjSlots];
   bool has_xadj[kAdjSlots] = {false, false, false, false};
-  DevArray<double> x, r, z, p[2], q, bp, partials;
+  DevArray<double> x, rbuf[2], z, p, q, bp, partials;
   CgScalars* Sd = nullptr;
   CgScalars* Sh = nullptr;
   int last_iters = 0, last_status = 0;
@@ -291,9 +291,11 @@ struct Solver {
   // slot: which of kAdjSlots warm-start vectors to use (the adjoint keeps one per RK stage, since
   // the same stage's load changes little from one substep to the next)
   void solve_t(const double* c_dev, double* out, int precision, int slot = 0);
-  void vcycle(size_t l, const double* b, double* out, int precision, cudaStream_t st, int rz_mode);
+  // presmoothed: the finest level's first sweep (X, R) was already done by the fused CG update
+  void vcycle(size_t l, const double* b, double* out, int precision, cudaStream_t st, int rz_mode,
+              bool presmoothed = false);
   void precondition_rz(int precision, cudaStream_t st, bool first);
-  int pcur = 0;  // which of p[0], p[1] holds the current direction
+  int rc = 0;  // which of rbuf[0], rbuf[1] holds the current residual
   double nnz_fine = 0.0;
   void ctx_prof_begin(int id, cudaStream_t st, double bytes);
   void ctx_prof_end(cudaStream_t st);
@@ -495,16 +497,29 @@ bool Solver::ctx_prof_on() const { return ctx->prof.on; }
 void Solver::iteration_body(int precision, cudaStream_t st, bool profile) {
   const SellView A0 = lev[0].A.view(rep);
   const bool f64 = precision == TMB_FP64;
-  double* pold = p[pcur].p;
-  double* pnew = p[pcur ^ 1].p;
-  pcur ^= 1;
-  // direction update fused into A p: gathers z and p_old (two 8-byte gathers per entry)
+  // p = z + beta p and q = A z + beta q: the product gathers z only
   if (profile) ctx_prof_begin(6, st, nnz_fine * ((f64 ? 8.0 : 4.0) + 4.0) + 5.0 * 8.0 * n * rep);
-  if (f64) launch_cg_dir_spmv<double>(A0, lev[0].Ad.p, z.p, pold, pnew, q.p, Sd, partials.p, st);
-  else launch_cg_dir_spmv<float>(A0, lev[0].Af.p, z.p, pold, pnew, q.p, Sd, partials.p, st);
+  if (f64) launch_cg_dir_spmv<double>(A0, lev[0].Ad.p, z.p, p.p, q.p, Sd, partials.p, st);
+  else launch_cg_dir_spmv<float>(A0, lev[0].Af.p, z.p, p.p, q.p, Sd, partials.p, st);
   if (profile) ctx_prof_end(st);
-  launch_cg_update(n * rep, pnew, q.p, x.p, r.p, Sd, partials.p, st);
-  precondition_rz(precision, st, false);
+  if (lev.size() > 1 && rep < 8) {
+    // x, r update fused with the V-cycle's first sweep; the residual alternates between buffers
+    // (with many interleaved replicas the two gathered vectors no longer stay in L2: separate)
+    const double* rold = rbuf[rc].p;
+    double* rnew = rbuf[rc ^ 1].p;
+    rc ^= 1;
+    DevLevel& L = lev[0];
+    if (f64)
+      launch_cg_update_jacobi0<double>(A0, L.Ad.p, L.dinv.p, p.p, q.p, x.p, rold, rnew, L.X.p, L.R.p, Sd,
+                                       partials.p, st);
+    else
+      launch_cg_update_jacobi0<float>(A0, L.Af.p, L.dinv.p, p.p, q.p, x.p, rold, rnew, L.X.p, L.R.p, Sd,
+                                      partials.p, st);
+    vcycle(0, rnew, z.p, precision, st, 0, true);
+  } else {
+    launch_cg_update(n * rep, p.p, q.p, x.p, rbuf[rc].p, Sd, partials.p, st);
+    precondition_rz(precision, st, false);
+  }
 }
 
 cudaGraphExec_t Solver::graph_for(int precision) {
@@ -630,10 +645,10 @@ void Solver::compute() {
   const size_t nr = size_t(n) * rep;
   x.alloc(nr);
   x.zero(st);
-  r.alloc(nr);
+  rbuf[0].alloc(nr);
+  rbuf[1].alloc(nr);
   z.alloc(nr);
-  p[0].alloc(nr);
-  p[1].alloc(nr);
+  p.alloc(nr);
   q.alloc(nr);
   bp.alloc(nr);
   partials.alloc(size_t(2) * grid_for((long long)nr) + 64);
@@ -646,7 +661,8 @@ void Solver::compute() {
   computed = true;
 }
 
-void Solver::vcycle(size_t l, const double* b, double* out, int precision, cudaStream_t st, int rz_mode) {
+void Solver::vcycle(size_t l, const double* b, double* out, int precision, cudaStream_t st, int rz_mode,
+                    bool presmoothed) {
   DevLevel& L = lev[l];
   const int* done = &Sd->done;
   if (l + 1 == lev.size()) {
@@ -657,8 +673,10 @@ void Solver::vcycle(size_t l, const double* b, double* out, int precision, cudaS
   const bool f64 = precision == TMB_FP64;
   if (l == 0) {
     const SellView A = L.A.view(rep);
-    if (f64) launch_jacobi0_residual<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, L.R.p, done, st);
-    else launch_jacobi0_residual<float>(A, L.Af.p, L.dinv.p, b, L.X.p, L.R.p, done, st);
+    if (!presmoothed) {
+      if (f64) launch_jacobi0_residual<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, L.R.p, done, st);
+      else launch_jacobi0_residual<float>(A, L.Af.p, L.dinv.p, b, L.X.p, L.R.p, done, st);
+    }
   } else {
     const CsrView A = L.Ac.view(rep);
     if (f64) launch_csr_jacobi0_residual<double>(A, L.Ac.v.p, L.dinv.p, b, L.X.p, L.R.p, done, st, L.tA);
@@ -689,10 +707,10 @@ void Solver::vcycle(size_t l, const double* b, double* out, int precision, cudaS
 // Preconditioner application z = M r followed by rho = r.z (first: beta = 0).
 void Solver::precondition_rz(int precision, cudaStream_t st, bool first) {
   if (lev.size() > 1) {
-    vcycle(0, r.p, z.p, precision, st, first ? 1 : 0);
+    vcycle(0, rbuf[rc].p, z.p, precision, st, first ? 1 : 0);
   } else {
-    vcycle(0, r.p, z.p, precision, st, -1);
-    launch_cg_rz(n * rep, r.p, z.p, Sd, partials.p, first, st);
+    vcycle(0, rbuf[rc].p, z.p, precision, st, -1);
+    launch_cg_rz(n * rep, rbuf[rc].p, z.p, Sd, partials.p, first, st);
   }
 }
 
@@ -709,10 +727,10 @@ void Solver::solve(const double* b_dev, int precision) {
   const bool f64 = precision == TMB_FP64;
   if (f64) launch_cg_init<double>(n, lift.view(rep), lift.v.p, cmask.p, b_dev, bp.p, x.p, st);
   else launch_cg_init<float>(n, lift.view(rep), lift.vf.p, cmask.p, b_dev, bp.p, x.p, st);
-  if (f64) launch_cg_residual<double>(A0, lev[0].Ad.p, bp.p, x.p, r.p, Sd, partials.p, st);
-  else launch_cg_residual<float>(A0, lev[0].Af.p, bp.p, x.p, r.p, Sd, partials.p, st);
+  rc = 0;  // graphs are captured with the residual starting in rbuf[0]
+  if (f64) launch_cg_residual<double>(A0, lev[0].Ad.p, bp.p, x.p, rbuf[0].p, Sd, partials.p, st);
+  else launch_cg_residual<float>(A0, lev[0].Af.p, bp.p, x.p, rbuf[0].p, Sd, partials.p, st);
   precondition_rz(precision, st, true);
-  pcur = 0;  // graphs are captured with the direction starting in p[0]
   if (!ctx_prof_on()) {
     // Graph path: kGraphIters iterations per graph launch; the first batch covers the
     // previous solve's iteration count, then the done flag is polled after every launch.
@@ -1312,19 +1330,21 @@ void Ctx::h_compress(const double* bxyz, const double* bnrm, int leaf, double et
       std::vector<int> rk(H.nfar);
       std::vector<long long> uo(H.nfar), vo(H.nfar);
       long long su = 0, sv = 0, stt = 0;
-      std::vector<long long> to(H.nfar);
+      std::vector<long long> to(size_t(H.nfar) + 1);
       std::vector<HTerm> td;
       for (int q = 0; q < H.nfar; ++q) {
         rk[q] = ranks[size_t(3) * q + w];
         uo[q] = su;
         vo[q] = sv;
         to[q] = stt;
-        const int np = pad4(farb[q].n);
-        for (int l = 0; l < rk[q]; ++l) td.push_back(HTerm{sv + (long long)l * np, np, farb[q].cb});
+        const int np = pad4(farb[q].n), mp = pad4(farb[q].m);
+        for (int l = 0; l < rk[q]; ++l)
+          td.push_back(HTerm{sv + (long long)l * np, su + (long long)l * mp, np, farb[q].cb});
         su += (long long)rk[q] * pad4(farb[q].m);
         sv += (long long)rk[q] * np;
         stt += rk[q];
       }
+      to[H.nfar] = stt;
       H.toff[w].upload(to, st);
       H.termd[w].upload(td, st);
       // matvec work items: the admissible blocks of one row cluster, cut into runs of about

@@ -169,8 +169,12 @@ template <typename V>
 void launch_jacobi_rz(const SellView& s, const V* val, const double* dinv, const double* r, const double* xin,
                       double* z, CgScalars* S, double* partials, bool first, cudaStream_t st);
 template <typename V>
-void launch_cg_dir_spmv(const SellView& s, const V* val, const double* z, const double* p_old, double* p_new,
-                        double* q, CgScalars* S, double* partials, cudaStream_t st);
+void launch_cg_dir_spmv(const SellView& s, const V* val, const double* z, double* p, double* q, CgScalars* S,
+                        double* partials, cudaStream_t st);
+template <typename V>
+void launch_cg_update_jacobi0(const SellView& s, const V* val, const double* dinv, const double* p, const double* q,
+                              double* x, const double* r, double* r_new, double* X, double* Rres, CgScalars* S,
+                              double* partials, cudaStream_t st);
 
 // --- launchers (k_bem.cu) ----------------------------------------------------------------
 void launch_bem_assemble(int nb, int ntri, const double* bxyz, const int* tri, const double* area,
@@ -226,9 +230,10 @@ struct HFarGroup {
 // Low-rank factors are stored with leading dimensions padded to a multiple of 4 entries (zero
 // padding), so that every column of U and every row of V^T starts on a 16-byte boundary.
 __host__ __device__ inline int pad4(int x) { return (x + 3) & ~3; }
-// One term of the far-field product: t = V_l^T x[cb .. cb + n4) (n4 = pad4(n)), V_l at offset v.
+// One term of the far-field product: t = V_l^T x[cb .. cb + n4) (n4 = pad4(n)), V_l at offset v;
+// its column of U starts at offset u.
 struct HTerm {
-  long long v;
+  long long v, u;
   int n4, cb;
 };
 template <typename T>
@@ -247,7 +252,7 @@ struct HMatView {
   const T* V = nullptr;
   const HFarGroup* groups = nullptr;     // row clusters, largest work first
   const HTerm* terms = nullptr;          // every term of every admissible block, block by block
-  const long long* toff = nullptr;       // first term of each admissible block
+  const long long* toff = nullptr;       // first term of each admissible block, then the term count
   double* t = nullptr;                   // the terms' values V^T x (nterms)
 };
 // Where the entries of the boundary matrix (in cluster order) come from: the dense FP64
