@@ -99,6 +99,7 @@ __device__ __forceinline__ double sell_row_dot(const SellView& s, const V* __res
 template <typename V>
 __global__ void __launch_bounds__(kBlock) k_spmv(SellView s, const V* __restrict__ val, const double* __restrict__ x,
                                                  double* __restrict__ y, const int* done) {
+  pdl_enter();
   if (done && *done) return;
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g < s.n * s.rep) y[g] = sell_row_dot(s, val, x, g);
@@ -108,6 +109,7 @@ template <typename V>
 __global__ void __launch_bounds__(kBlock) k_residual(SellView s, const V* __restrict__ val,
                                                      const double* __restrict__ b, const double* __restrict__ x,
                                                      double* __restrict__ r, const int* done) {
+  pdl_enter();
   if (done && *done) return;
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g < s.n * s.rep) r[g] = b[g] - sell_row_dot(s, val, x, g);
@@ -115,6 +117,7 @@ __global__ void __launch_bounds__(kBlock) k_residual(SellView s, const V* __rest
 
 __global__ void k_jacobi0(int n, int R, const double* __restrict__ dinv, const double* __restrict__ b,
                           double* __restrict__ x, const int* done) {
+  pdl_enter();
   if (done && *done) return;
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g < n * R) x[g] = dinv[g / R] * b[g];
@@ -125,6 +128,7 @@ __global__ void __launch_bounds__(kBlock) k_jacobi(SellView s, const V* __restri
                                                    const double* __restrict__ dinv, const double* __restrict__ b,
                                                    const double* __restrict__ xin, double* __restrict__ xout,
                                                    const int* done) {
+  pdl_enter();
   if (done && *done) return;
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g < s.n * s.rep) xout[g] = xin[g] + dinv[g / s.rep] * (b[g] - sell_row_dot(s, val, xin, g));
@@ -137,6 +141,7 @@ __global__ void __launch_bounds__(kBlock) k_jacobi0_residual(SellView s, const V
                                                              const double* __restrict__ dinv,
                                                              const double* __restrict__ b, double* __restrict__ x,
                                                              double* __restrict__ r, const int* done) {
+  pdl_enter();
   if (done && *done) return;
   const int R = s.rep;
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -210,6 +215,7 @@ template <typename V, int T>
 __global__ void __launch_bounds__(kBlock) k_csr_spmv(CsrView c, const V* __restrict__ val,
                                                      const double* __restrict__ x, double* __restrict__ y,
                                                      int accumulate, const int* done) {
+  pdl_enter();
   if (done && *done) return;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int row = t / T, sub = t & (T - 1);
@@ -224,6 +230,7 @@ __global__ void __launch_bounds__(kBlock) k_csr_jacobi0_residual(CsrView c, cons
                                                                  const double* __restrict__ dinv,
                                                                  const double* __restrict__ b, double* __restrict__ x,
                                                                  double* __restrict__ r, const int* done) {
+  pdl_enter();
   if (done && *done) return;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int row = t / T, sub = t & (T - 1);
@@ -241,6 +248,7 @@ __global__ void __launch_bounds__(kBlock) k_csr_jacobi(CsrView c, const V* __res
                                                        const double* __restrict__ dinv, const double* __restrict__ b,
                                                        const double* __restrict__ xin, double* __restrict__ xout,
                                                        const int* done) {
+  pdl_enter();
   if (done && *done) return;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int row = t / T, sub = t & (T - 1);
@@ -252,6 +260,7 @@ __global__ void __launch_bounds__(kBlock) k_csr_jacobi(CsrView c, const V* __res
 // one warp per row and replica.
 __global__ void k_coarse_solve(int n, int ld, int R, const double* __restrict__ inv, const double* __restrict__ b,
                                double* __restrict__ x, const int* done) {
+  pdl_enter();
   if (done && *done) return;
   const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (g >= n * R) return;
@@ -268,6 +277,7 @@ __global__ void k_coarse_solve(int n, int ld, int R, const double* __restrict__ 
 __global__ void __launch_bounds__(128) k_coarse_solve_rows(int n, int ld, const double* __restrict__ inv,
                                                            const double* __restrict__ b, double* __restrict__ x,
                                                            const int* done) {
+  pdl_enter();
   if (done && *done) return;
   __shared__ double red[4];
   const double2* row = reinterpret_cast<const double2*>(inv + size_t(blockIdx.x) * ld);
@@ -288,6 +298,7 @@ __global__ void __launch_bounds__(128) k_coarse_solve_rows(int n, int ld, const 
 template <typename V>
 __global__ void k_cg_init(int n, CsrView lift, const V* __restrict__ lval, const int* __restrict__ cmask,
                           const double* __restrict__ b, double* __restrict__ bprime, double* __restrict__ x) {
+  pdl_enter();
   const int R = lift.rep;
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= n * R) return;
@@ -306,6 +317,7 @@ template <typename V>
 __global__ void __launch_bounds__(kBlock) k_cg_residual(SellView s, const V* __restrict__ val,
                                                         const double* __restrict__ bp, const double* __restrict__ x,
                                                         double* __restrict__ r, CgScalars* S, double* partials) {
+  pdl_enter();
   double v[2] = {0.0, 0.0};
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < s.n * s.rep; g += gridDim.x * blockDim.x) {
     const double ri = bp[g] - sell_row_dot(s, val, x, g);
@@ -330,6 +342,7 @@ __global__ void __launch_bounds__(kBlock) k_cg_residual(SellView s, const V* __r
 
 __global__ void __launch_bounds__(kBlock) k_cg_rz(int n, const double* __restrict__ r, const double* __restrict__ z,
                                                   CgScalars* S, double* partials, int first) {
+  pdl_enter();
   if (S->done) return;
   double v[1] = {0.0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[0] = fma(r[i], z[i], v[0]);
@@ -351,6 +364,7 @@ __global__ void __launch_bounds__(kBlock) k_jacobi_rz(SellView s, const V* __res
                                                       const double* __restrict__ dinv, const double* __restrict__ r,
                                                       const double* __restrict__ xin, double* __restrict__ z,
                                                       CgScalars* S, double* partials, int first) {
+  pdl_enter();
   if (S->done) return;
   double v[1] = {0.0};
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < s.n * s.rep; g += gridDim.x * blockDim.x) {
@@ -373,6 +387,7 @@ template <typename V>
 __global__ void __launch_bounds__(kBlock) k_cg_dir_spmv(SellView s, const V* __restrict__ val,
                                                         const double* __restrict__ z, double* __restrict__ p,
                                                         double* __restrict__ q, CgScalars* S, double* partials) {
+  pdl_enter();
   if (S->done) return;
   const double beta = S->beta;
   double v[1] = {0.0};
@@ -404,6 +419,7 @@ __global__ void __launch_bounds__(kBlock) k_cg_update_jacobi0(SellView s, const 
                                                               const double* __restrict__ r, double* __restrict__ r_new,
                                                               double* __restrict__ X, double* __restrict__ Rres,
                                                               CgScalars* S, double* partials) {
+  pdl_enter();
   if (S->done) return;
   const double alpha = S->alpha;
   const int R = s.rep;
@@ -454,6 +470,7 @@ __global__ void __launch_bounds__(kBlock) k_cg_update_jacobi0(SellView s, const 
 }
 
 __global__ void k_cg_pupdate(int n, const double* __restrict__ z, double* __restrict__ p, const CgScalars* S) {
+  pdl_enter();
   if (S->done) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -465,6 +482,7 @@ template <typename V>
 __global__ void __launch_bounds__(kBlock) k_cg_spmv_pq(SellView s, const V* __restrict__ val,
                                                        const double* __restrict__ p, double* __restrict__ q,
                                                        CgScalars* S, double* partials) {
+  pdl_enter();
   if (S->done) return;
   double v[1] = {0.0};
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < s.n * s.rep; g += gridDim.x * blockDim.x) {
@@ -482,6 +500,7 @@ __global__ void __launch_bounds__(kBlock) k_cg_spmv_pq(SellView s, const V* __re
 __global__ void __launch_bounds__(kBlock) k_cg_update(int n, const double* __restrict__ p,
                                                       const double* __restrict__ q, double* __restrict__ x,
                                                       double* __restrict__ r, CgScalars* S, double* partials) {
+  pdl_enter();
   if (S->done) return;
   const double alpha = S->alpha;
   double v[1] = {0.0};
@@ -525,23 +544,23 @@ int reduce_grid(long long n) {
 template <typename V>
 void launch_spmv(const SellView& s, const V* val, const double* x, double* y, const int* done, cudaStream_t st) {
   note_launch();
-  k_spmv<V><<<grid_for(1LL * s.n * s.rep), kBlock, 0, st>>>(s, val, x, y, done);
+  launch_pdl(k_spmv<V>, grid_for(1LL * s.n * s.rep), kBlock, 0, st, s, val, x, y, done);
 }
 template <typename V>
 void launch_residual(const SellView& s, const V* val, const double* b, const double* x, double* r,
                      const int* done, cudaStream_t st) {
   note_launch();
-  k_residual<V><<<grid_for(1LL * s.n * s.rep), kBlock, 0, st>>>(s, val, b, x, r, done);
+  launch_pdl(k_residual<V>, grid_for(1LL * s.n * s.rep), kBlock, 0, st, s, val, b, x, r, done);
 }
 void launch_jacobi0(int n, int rep, const double* dinv, const double* b, double* x, const int* done, cudaStream_t st) {
   note_launch();
-  k_jacobi0<<<grid_for(1LL * n * rep), kBlock, 0, st>>>(n, rep, dinv, b, x, done);
+  launch_pdl(k_jacobi0, grid_for(1LL * n * rep), kBlock, 0, st, n, rep, dinv, b, x, done);
 }
 template <typename V>
 void launch_jacobi(const SellView& s, const V* val, const double* dinv, const double* b, const double* xin,
                    double* xout, const int* done, cudaStream_t st) {
   note_launch();
-  k_jacobi<V><<<grid_for(1LL * s.n * s.rep), kBlock, 0, st>>>(s, val, dinv, b, xin, xout, done);
+  launch_pdl(k_jacobi<V>, grid_for(1LL * s.n * s.rep), kBlock, 0, st, s, val, dinv, b, xin, xout, done);
 }
 int csr_threads_per_row(long long nrows, long long nnz) {
   const double avg = nrows > 0 ? double(nnz) / double(nrows) : 0.0;
@@ -552,12 +571,12 @@ int csr_threads_per_row(long long nrows, long long nnz) {
 
 #define TMB_CSR_DISPATCH(T, KERNEL, NROWS, ...)                                                            \
   switch (T) {                                                                                            \
-    case 1: KERNEL<V, 1><<<grid_for(1LL * (NROWS)), kBlock, 0, st>>>(__VA_ARGS__); break;                 \
-    case 2: KERNEL<V, 2><<<grid_for(2LL * (NROWS)), kBlock, 0, st>>>(__VA_ARGS__); break;                 \
-    case 4: KERNEL<V, 4><<<grid_for(4LL * (NROWS)), kBlock, 0, st>>>(__VA_ARGS__); break;                 \
-    case 8: KERNEL<V, 8><<<grid_for(8LL * (NROWS)), kBlock, 0, st>>>(__VA_ARGS__); break;                 \
-    case 16: KERNEL<V, 16><<<grid_for(16LL * (NROWS)), kBlock, 0, st>>>(__VA_ARGS__); break;              \
-    default: KERNEL<V, 32><<<grid_for(32LL * (NROWS)), kBlock, 0, st>>>(__VA_ARGS__); break;              \
+    case 1: launch_pdl(KERNEL<V, 1>, grid_for(1LL * (NROWS)), kBlock, 0, st, __VA_ARGS__); break;                 \
+    case 2: launch_pdl(KERNEL<V, 2>, grid_for(2LL * (NROWS)), kBlock, 0, st, __VA_ARGS__); break;                 \
+    case 4: launch_pdl(KERNEL<V, 4>, grid_for(4LL * (NROWS)), kBlock, 0, st, __VA_ARGS__); break;                 \
+    case 8: launch_pdl(KERNEL<V, 8>, grid_for(8LL * (NROWS)), kBlock, 0, st, __VA_ARGS__); break;                 \
+    case 16: launch_pdl(KERNEL<V, 16>, grid_for(16LL * (NROWS)), kBlock, 0, st, __VA_ARGS__); break;              \
+    default: launch_pdl(KERNEL<V, 32>, grid_for(32LL * (NROWS)), kBlock, 0, st, __VA_ARGS__); break;              \
   }
 
 template <typename V>
@@ -582,67 +601,67 @@ void launch_csr_jacobi(const CsrView& c, const V* val, const double* dinv, const
 void launch_coarse_solve(int n, int ld, int rep, const double* inv, const double* b, double* x, const int* done,
                          cudaStream_t st) {
   note_launch();
-  if (rep == 1 && n >= 256) k_coarse_solve_rows<<<n, 128, 0, st>>>(n, ld, inv, b, x, done);
-  else k_coarse_solve<<<grid_for(32LL * n * rep), kBlock, 0, st>>>(n, ld, rep, inv, b, x, done);
+  if (rep == 1 && n >= 256) launch_pdl(k_coarse_solve_rows, n, 128, 0, st, n, ld, inv, b, x, done);
+  else launch_pdl(k_coarse_solve, grid_for(32LL * n * rep), kBlock, 0, st, n, ld, rep, inv, b, x, done);
 }
 template <typename V>
 void launch_cg_init(int n, const CsrView& lift, const V* lval, const int* cmask, const double* b,
                     double* bprime, double* x, cudaStream_t st) {
   note_launch();
-  k_cg_init<V><<<grid_for(1LL * n * lift.rep), kBlock, 0, st>>>(n, lift, lval, cmask, b, bprime, x);
+  launch_pdl(k_cg_init<V>, grid_for(1LL * n * lift.rep), kBlock, 0, st, n, lift, lval, cmask, b, bprime, x);
 }
 template <typename V>
 void launch_cg_residual(const SellView& s, const V* val, const double* bp, const double* x, double* r,
                         CgScalars* S, double* partials, cudaStream_t st) {
   note_launch();
-  k_cg_residual<V><<<reduce_grid(1LL * s.n * s.rep), kBlock, 0, st>>>(s, val, bp, x, r, S, partials);
+  launch_pdl(k_cg_residual<V>, reduce_grid(1LL * s.n * s.rep), kBlock, 0, st, s, val, bp, x, r, S, partials);
 }
 void launch_cg_rz(int n, const double* r, const double* z, CgScalars* S, double* partials, bool first,
                   cudaStream_t st) {
   note_launch();
-  k_cg_rz<<<reduce_grid(n), kBlock, 0, st>>>(n, r, z, S, partials, first ? 1 : 0);
+  launch_pdl(k_cg_rz, reduce_grid(n), kBlock, 0, st, n, r, z, S, partials, first ? 1 : 0);
 }
 void launch_cg_pupdate(int n, const double* z, double* p, CgScalars* S, cudaStream_t st) {
   note_launch();
-  k_cg_pupdate<<<grid_for(n), kBlock, 0, st>>>(n, z, p, S);
+  launch_pdl(k_cg_pupdate, grid_for(n), kBlock, 0, st, n, z, p, S);
 }
 template <typename V>
 void launch_cg_spmv_pq(const SellView& s, const V* val, const double* p, double* q, CgScalars* S,
                        double* partials, cudaStream_t st) {
   note_launch();
-  k_cg_spmv_pq<V><<<reduce_grid(1LL * s.n * s.rep), kBlock, 0, st>>>(s, val, p, q, S, partials);
+  launch_pdl(k_cg_spmv_pq<V>, reduce_grid(1LL * s.n * s.rep), kBlock, 0, st, s, val, p, q, S, partials);
 }
 template <typename V>
 void launch_jacobi0_residual(const SellView& s, const V* val, const double* dinv, const double* b, double* x,
                              double* r, const int* done, cudaStream_t st) {
   note_launch();
-  k_jacobi0_residual<V><<<grid_for(1LL * s.n * s.rep), kBlock, 0, st>>>(s, val, dinv, b, x, r, done);
+  launch_pdl(k_jacobi0_residual<V>, grid_for(1LL * s.n * s.rep), kBlock, 0, st, s, val, dinv, b, x, r, done);
 }
 template <typename V>
 void launch_jacobi_rz(const SellView& s, const V* val, const double* dinv, const double* r, const double* xin,
                       double* z, CgScalars* S, double* partials, bool first, cudaStream_t st) {
   note_launch();
-  k_jacobi_rz<V><<<reduce_grid(1LL * s.n * s.rep), kBlock, 0, st>>>(s, val, dinv, r, xin, z, S, partials, first ? 1 : 0);
+  launch_pdl(k_jacobi_rz<V>, reduce_grid(1LL * s.n * s.rep), kBlock, 0, st, s, val, dinv, r, xin, z, S, partials, first ? 1 : 0);
 }
 template <typename V>
 void launch_cg_dir_spmv(const SellView& s, const V* val, const double* z, double* p, double* q, CgScalars* S,
                         double* partials, cudaStream_t st) {
   note_launch();
-  k_cg_dir_spmv<V><<<reduce_grid(1LL * s.n * s.rep), kBlock, 0, st>>>(s, val, z, p, q, S, partials);
+  launch_pdl(k_cg_dir_spmv<V>, reduce_grid(1LL * s.n * s.rep), kBlock, 0, st, s, val, z, p, q, S, partials);
 }
 template <typename V>
 void launch_cg_update_jacobi0(const SellView& s, const V* val, const double* dinv, const double* p, const double* q,
                               double* x, const double* r, double* r_new, double* X, double* Rres, CgScalars* S,
                               double* partials, cudaStream_t st) {
   note_launch();
-  k_cg_update_jacobi0<V><<<reduce_grid(1LL * s.n * s.rep), kBlock, 0, st>>>(s, val, dinv, p, q, x, r, r_new, X,
+  launch_pdl(k_cg_update_jacobi0<V>, reduce_grid(1LL * s.n * s.rep), kBlock, 0, st, s, val, dinv, p, q, x, r, r_new, X,
                                                                               Rres, S, partials);
 }
 
 void launch_cg_update(int n, const double* p, const double* q, double* x, double* r, CgScalars* S,
                       double* partials, cudaStream_t st) {
   note_launch();
-  k_cg_update<<<reduce_grid(n), kBlock, 0, st>>>(n, p, q, x, r, S, partials);
+  launch_pdl(k_cg_update, reduce_grid(n), kBlock, 0, st, n, p, q, x, r, S, partials);
 }
 
 #define TMB_INST(V)                                                                                          \

@@ -18,6 +18,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <utility>
 
 namespace tmb {
 
@@ -351,6 +352,33 @@ void note_launches(long long k);  // k kernels launched at once (a CUDA graph)
 inline int grid_for(long long n, int block = kBlock) {
   long long g = (n + block - 1) / block;
   return int(g < 1 ? 1 : g);
+}
+
+// Programmatic dependent launch for chains of small dependent kernels (the CG iteration and its
+// V-cycle): a kernel launched by launch_pdl may be scheduled while its predecessor in the stream
+// still runs, so that its launch and CTA placement overlap the predecessor's execution instead
+// of following its completion.  Such a kernel calls pdl_enter() first, in every CTA: it waits
+// until the predecessor grid has completed and its writes are visible (griddepcontrol.wait),
+// then lets its own successor be scheduled (griddepcontrol.launch_dependents).  Waiting before
+// triggering keeps at most one pre-scheduled grid behind the running one; every CTA waits, so
+// completion stays ordered along the chain.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+template <typename... P, typename... A>
+inline void launch_pdl(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, A&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  TMB_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...));
 }
 
 }  // namespace tmb
