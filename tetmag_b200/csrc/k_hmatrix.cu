@@ -418,10 +418,11 @@ struct Vec16<double> {
 };
 
 // Far field, first pass: t_p = V_p^T x_sigma for every term p of every admissible block.  A warp
-// takes four consecutive terms and issues the 16-byte streaming loads of all four rows of V before
-// it uses them (each entry read once; x from cache), then reduces the four dots.  The padded tail
-// of V is zero and x has four zero entries past its end.
-constexpr int kTermsPerWarp = 4;
+// takes kTermsPerWarp consecutive terms and issues the 16-byte streaming loads of all their rows of
+// V before it uses them (each entry read once; x from cache), then reduces the dots.  Two terms
+// per warp (48 registers, five CTAs per SM) measured faster than four (80 registers, three CTAs).
+// The padded tail of V is zero and x has four zero entries past its end.
+constexpr int kTermsPerWarp = 2;
 template <typename T>
 __global__ void __launch_bounds__(256) k_h_vt(long long nterms, const HTerm* __restrict__ terms,
                                               const T* __restrict__ V, const T* __restrict__ xp,
