@@ -417,56 +417,39 @@ struct Vec16<double> {
   __device__ static double dot(const double2& v, const double* x) { return fma(v.x, x[0], v.y * x[1]); }
 };
 
-// Far field, first pass: t_p = V_p^T x_sigma for every term p of every admissible block.  A warp
-// takes kTermsPerWarp consecutive terms and issues the 16-byte streaming loads of all their rows of
-// V before it uses them (each entry read once; x from cache), then reduces the dots.  Two terms
-// per warp (48 registers, five CTAs per SM) measured faster than four (80 registers, three CTAs).
-// The padded tail of V is zero and x has four zero entries past its end.
-constexpr int kTermsPerWarp = 2;
+// Far field, first pass: t_p = V_p^T x_sigma for every term p of every admissible block.  Eight
+// lanes take one term (a warp four terms): each lane issues four 16-byte streaming loads of its
+// term's row of V before it uses them (each entry read once; x from cache), and the eight partial
+// dots are reduced with three shuffles.  The padded tail of V is zero and x has four zero entries
+// past its end.
+constexpr int kLanesPerTerm = 8;
 template <typename T>
 __global__ void __launch_bounds__(256) k_h_vt(long long nterms, const HTerm* __restrict__ terms,
                                               const T* __restrict__ V, const T* __restrict__ xp,
                                               double* __restrict__ t) {
   using W = Vec16<T>;
   using VT = typename W::type;
-  constexpr int P = kTermsPerWarp;
-  const long long p0 = ((long long)blockIdx.x * 8 + (threadIdx.x >> 5)) * P;
-  if (p0 >= nterms) return;
-  const int lane = threadIdx.x & 31;
-  const VT* v[P];
-  const T* x[P];
-  int nv[P];
-  int most = 0;
+  constexpr int L = kLanesPerTerm;
+  const long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / L;
+  const int sub = threadIdx.x & (L - 1);
+  const bool ok = p < nterms;
+  const HTerm h = terms[ok ? p : 0];
+  const VT* v = reinterpret_cast<const VT*>(V + h.v);
+  const T* x = xp + h.cb;
+  const int nv = ok ? h.n4 / W::n : 0;
+  double acc = 0.0;
+  int j = sub;
+  for (; j + 3 * L < nv; j += 4 * L) {
+    VT a[4];
 #pragma unroll
-  for (int i = 0; i < P; ++i) {
-    const bool ok = p0 + i < nterms;
-    const HTerm h = terms[ok ? p0 + i : p0];
-    v[i] = reinterpret_cast<const VT*>(V + h.v);
-    x[i] = xp + h.cb;
-    nv[i] = ok ? h.n4 / W::n : 0;
-    most = max(most, nv[i]);
+    for (int c = 0; c < 4; ++c) a[c] = __ldcs(v + j + c * L);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc += W::dot(a[c], x + W::n * (j + c * L));
   }
-  double acc[P];
+  for (; j < nv; j += L) acc += W::dot(__ldcs(v + j), x + W::n * j);
 #pragma unroll
-  for (int i = 0; i < P; ++i) acc[i] = 0.0;
-  for (int j = lane; j < most; j += 64) {
-    VT a[P], b[P];
-#pragma unroll
-    for (int i = 0; i < P; ++i) {
-      if (j < nv[i]) a[i] = __ldcs(v[i] + j);
-      if (j + 32 < nv[i]) b[i] = __ldcs(v[i] + j + 32);
-    }
-#pragma unroll
-    for (int i = 0; i < P; ++i) {
-      if (j < nv[i]) acc[i] += W::dot(a[i], x[i] + W::n * j);
-      if (j + 32 < nv[i]) acc[i] += W::dot(b[i], x[i] + W::n * (j + 32));
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < P; ++i) {
-    const double s = warp_sum_d(acc[i]);
-    if (lane == 0 && p0 + i < nterms) t[p0 + i] = s;
-  }
+  for (int o = L / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (sub == 0 && ok) t[p] = acc;
 }
 
 // Far field, second pass: y_tau += sum_b U_b t_b over the admissible blocks of one work item (a
@@ -612,8 +595,8 @@ void launch_h_matvec(const HMatView<T>& H, const double* u, double* y, T* xp, co
   k_h_near<T><<<H.nrows, 256, 0, st>>>(H.near_rows, H.near, H.D, xp, y);
   if (H.nterms > 0) {
     note_launch();
-    const long long warps = (H.nterms + kTermsPerWarp - 1) / kTermsPerWarp;
-    k_h_vt<T><<<unsigned((warps + 7) / 8), 256, 0, st>>>(H.nterms, H.terms, H.V, xp, H.t);
+    const long long threads = H.nterms * kLanesPerTerm;
+    k_h_vt<T><<<unsigned((threads + 255) / 256), 256, 0, st>>>(H.nterms, H.terms, H.V, xp, H.t);
     note_launch();
     k_h_ut<T><<<H.ngroups, 256, 0, st>>>(H.groups, H.toff, H.terms, H.U, H.t, y);
   }
