@@ -458,6 +458,7 @@ __global__ void __launch_bounds__(256) k_h_vt(long long nterms, const HTerm* __r
 // thread -> (16-byte row vector, term slice) streams its U entries with independent 16-byte loads
 // (each entry read once); one atomic add per row at the end.
 constexpr int kStage = 512;
+constexpr int kUtLoads = 4;  // U loads in flight per thread (8 measured slower: 443 against 437 us on c2)
 template <typename T>
 __global__ void __launch_bounds__(256) k_h_ut(const HFarGroup* __restrict__ grp, const long long* __restrict__ toff,
                                               const HTerm* __restrict__ terms, const T* __restrict__ U,
@@ -495,12 +496,13 @@ __global__ void __launch_bounds__(256) k_h_ut(const HFarGroup* __restrict__ grp,
         const int vv = vec + 256 * r;
         if (r < per && vv < nvec) {
           int i = slice;
-          for (; i + 3 * slices < nc; i += 4 * slices) {
-            VT uv[4];
+          for (; i + (kUtLoads - 1) * slices < nc; i += kUtLoads * slices) {
+            VT uv[kUtLoads];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) uv[c] = __ldcs(reinterpret_cast<const VT*>(U + su[i + c * slices]) + vv);
+            for (int c = 0; c < kUtLoads; ++c)
+              uv[c] = __ldcs(reinterpret_cast<const VT*>(U + su[i + c * slices]) + vv);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) W::add(acc[r], uv[c], st[i + c * slices]);
+            for (int c = 0; c < kUtLoads; ++c) W::add(acc[r], uv[c], st[i + c * slices]);
           }
           for (; i < nc; i += slices) W::add(acc[r], __ldcs(reinterpret_cast<const VT*>(U + su[i]) + vv), st[i]);
         }

@@ -295,6 +295,31 @@ __global__ void __launch_bounds__(128) k_coarse_solve_rows(int n, int ld, const 
   if (threadIdx.x == 0) x[blockIdx.x] = (red[0] + red[1]) + (red[2] + red[3]);
 }
 
+// The mixed path's form: an FP32 copy of the inverse (rows padded to a multiple of 4, 16-byte loads
+// of four entries), FP64 products and sums.  The coarsest solve only feeds the preconditioner.
+__global__ void __launch_bounds__(128) k_coarse_solve_rows_f32(int n, int ld, const float* __restrict__ inv,
+                                                               const double* __restrict__ b, double* __restrict__ x,
+                                                               const int* done) {
+  pdl_enter();
+  if (done && *done) return;
+  __shared__ double red[4];
+  const float4* row = reinterpret_cast<const float4*>(inv + size_t(blockIdx.x) * ld);
+  const int nq = ld / 4;
+  double a0 = 0.0, a1 = 0.0;
+  for (int j = threadIdx.x; j < nq; j += 128) {
+    const float4 v = __ldg(row + j);
+    const int c = 4 * j;  // padded entries are zero; b is read only below n
+    a0 = fma(double(v.x), __ldg(b + c), a0);
+    if (c + 1 < n) a1 = fma(double(v.y), __ldg(b + c + 1), a1);
+    if (c + 2 < n) a0 = fma(double(v.z), __ldg(b + c + 2), a0);
+    if (c + 3 < n) a1 = fma(double(v.w), __ldg(b + c + 3), a1);
+  }
+  double a = warp_sum(a0 + a1);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = a;
+  __syncthreads();
+  if (threadIdx.x == 0) x[blockIdx.x] = (red[0] + red[1]) + (red[2] + red[3]);
+}
+
 template <typename V>
 __global__ void k_cg_init(int n, CsrView lift, const V* __restrict__ lval, const int* __restrict__ cmask,
                           const double* __restrict__ b, double* __restrict__ bprime, double* __restrict__ x) {
@@ -599,9 +624,10 @@ void launch_csr_jacobi(const CsrView& c, const V* val, const double* dinv, const
 }
 #undef TMB_CSR_DISPATCH
 void launch_coarse_solve(int n, int ld, int rep, const double* inv, const double* b, double* x, const int* done,
-                         cudaStream_t st) {
+                         cudaStream_t st, const float* invf, int ldf) {
   note_launch();
-  if (rep == 1 && n >= 256) launch_pdl(k_coarse_solve_rows, n, 128, 0, st, n, ld, inv, b, x, done);
+  if (rep == 1 && n >= 256 && invf) launch_pdl(k_coarse_solve_rows_f32, n, 128, 0, st, n, ldf, invf, b, x, done);
+  else if (rep == 1 && n >= 256) launch_pdl(k_coarse_solve_rows, n, 128, 0, st, n, ld, inv, b, x, done);
   else launch_pdl(k_coarse_solve, grid_for(32LL * n * rep), kBlock, 0, st, n, ld, rep, inv, b, x, done);
 }
 template <typename V>

@@ -255,7 +255,8 @@ struct Solver {
   AmgHierarchy H;
   std::vector<DevLevel> lev;
   DevArray<double> cinv;
-  int ncoarse = 0, cld = 0;
+  DevArray<float> cinvf;
+  int ncoarse = 0, cld = 0, cldf = 0;
   DevCsr lift;
   DevArray<int> cmask;
   // transposed solve (the adjoint): lift^T, masked load, and a warm start kept apart from the
@@ -637,6 +638,11 @@ void Solver::compute() {
       std::copy(H.coarse_inv.begin() + size_t(i) * ncoarse, H.coarse_inv.begin() + size_t(i + 1) * ncoarse,
                 ci.begin() + size_t(i) * cld);
     cinv.upload(ci, st);
+    cldf = (ncoarse + 3) & ~3;  // FP32 copy for the mixed path, rows padded to a multiple of 4
+    std::vector<float> cf(size_t(ncoarse) * cldf, 0.0f);
+    for (int i = 0; i < ncoarse; ++i)
+      for (int k = 0; k < ncoarse; ++k) cf[size_t(i) * cldf + k] = float(H.coarse_inv[size_t(i) * ncoarse + k]);
+    cinvf.upload(cf, st);
   }
   lift.upload(L, st);
   liftT.upload(LT, st);
@@ -666,7 +672,8 @@ void Solver::vcycle(size_t l, const double* b, double* out, int precision, cudaS
   DevLevel& L = lev[l];
   const int* done = &Sd->done;
   if (l + 1 == lev.size()) {
-    launch_coarse_solve(ncoarse, cld, rep, cinv.p, b, out, done, st);
+    launch_coarse_solve(ncoarse, cld, rep, cinv.p, b, out, done, st, precision == TMB_FP64 ? nullptr : cinvf.p,
+                        cldf);
     return;
   }
   DevLevel& C = lev[l + 1];

@@ -146,7 +146,7 @@ template <typename V>
 void launch_csr_jacobi(const CsrView& c, const V* val, const double* dinv, const double* b, const double* xin,
                        double* xout, const int* done, cudaStream_t st, int tpr);
 void launch_coarse_solve(int n, int ld, int rep, const double* inv, const double* b, double* x, const int* done,
-                         cudaStream_t st);
+                         cudaStream_t st, const float* invf = nullptr, int ldf = 0);
 
 template <typename V>
 void launch_cg_init(int n, const CsrView& lift, const V* lval, const int* cmask, const double* b,
