@@ -70,14 +70,16 @@ class MeshOps:
         check(lib().tmb_mesh_create(self.xyz.shape[0], self.tets.shape[0], _dptr(self.xyz), _iptr(self.tets),
                                     C.byref(h)))
         self.h = h
+        self._L = lib()
         info = (C.c_longlong * 6)()
         check(lib().tmb_mesh_info(self.h, info))
         self.nx, self.ntet, self.nnz, self.nb, self.ntri = (int(info[i]) for i in range(5))
 
     def __del__(self):
-        h = getattr(self, "h", None)
-        if h:
-            lib().tmb_mesh_destroy(h)
+        # the library handle taken at construction: at interpreter exit module globals may be gone
+        h, L = getattr(self, "h", None), getattr(self, "_L", None)
+        if h and L is not None:
+            L.tmb_mesh_destroy(h)
             self.h = None
 
     def operators(self) -> dict:
@@ -108,14 +110,16 @@ class Context:
         h = C.c_void_p()
         check(lib().tmb_ctx_create(device, C.byref(h)))
         self.h = h
+        self._L = lib()
         self.n = 0
         self.nb = 0
         self.rep = 1
 
     def __del__(self):
-        h = getattr(self, "h", None)
-        if h:
-            lib().tmb_ctx_destroy(h)
+        # the library handle taken at construction: at interpreter exit module globals may be gone
+        h, L = getattr(self, "h", None), getattr(self, "_L", None)
+        if h and L is not None:
+            L.tmb_ctx_destroy(h)
             self.h = None
 
     # --- setup ---------------------------------------------------------------------------
@@ -507,6 +511,7 @@ class B200Solver:
         h = C.c_void_p()
         check(lib().tmb_solver_create(ctx.h, C.byref(h)))
         self.h = h
+        self._L = lib()
         self.n = 0
         self.b = None
         self.x = None
@@ -516,9 +521,10 @@ class B200Solver:
         self._ok = False
 
     def __del__(self):
-        h = getattr(self, "h", None)
-        if h:
-            lib().tmb_solver_destroy(h)
+        # the library handle taken at construction: at interpreter exit module globals may be gone
+        h, L = getattr(self, "h", None), getattr(self, "_L", None)
+        if h and L is not None:
+            L.tmb_solver_destroy(h)
             self.h = None
 
     def setMatrix(self, A):
