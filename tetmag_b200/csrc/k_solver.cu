@@ -96,6 +96,41 @@ __device__ __forceinline__ double sell_row_dot(const SellView& s, const V* __res
   return acc;
 }
 
+// Interleaved replicas in pairs (an even replica count of 8 or more): state rows g and g + 1 (g
+// even) are two replicas of one operator row, so one thread gathers both replicas' entries with one
+// 16-byte load (the pair's offset j R + r is even, so the load is aligned).
+__device__ __forceinline__ double2 ld2(const double* p) { return *reinterpret_cast<const double2*>(p); }
+__device__ __forceinline__ void st2(double* p, double2 v) { *reinterpret_cast<double2*>(p) = v; }
+
+template <typename V>
+__device__ __forceinline__ double2 sell_row_dot2(const SellView& s, const V* __restrict__ val,
+                                                 const double* __restrict__ x, int g) {
+  const int R = s.rep;
+  const int row = g / R, r = g - row * R;
+  const int sl = row >> 5;
+  const int beg = __ldg(s.soff + sl) + (row & 31);
+  const int end = __ldg(s.soff + sl + 1);
+  double2 acc = make_double2(0.0, 0.0);
+  for (int k0 = beg; k0 < end; k0 += kChunk * kSlice) {
+    int j[kChunk];
+    V v[kChunk];
+#pragma unroll
+    for (int u = 0; u < kChunk; ++u) {
+      const int k = k0 + u * kSlice;
+      const bool ok = k < end;
+      j[u] = ok ? __ldg(s.col + k) * R + r : g;
+      v[u] = ok ? __ldg(val + k) : V(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kChunk; ++u) {
+      const double2 xv = __ldg(reinterpret_cast<const double2*>(x + j[u]));
+      acc.x = fma(static_cast<double>(v[u]), xv.x, acc.x);
+      acc.y = fma(static_cast<double>(v[u]), xv.y, acc.y);
+    }
+  }
+  return acc;
+}
+
 template <typename V>
 __global__ void __launch_bounds__(kBlock) k_spmv(SellView s, const V* __restrict__ val, const double* __restrict__ x,
                                                  double* __restrict__ y, const int* done) {
@@ -551,7 +586,107 @@ __global__ void __launch_bounds__(kBlock) k_cg_update(int n, const double* __res
   }
 }
 
+// Pair forms of the three finest-level kernels for interleaved replicas (see sell_row_dot2).
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_jacobi0_residual2(SellView s, const V* __restrict__ val,
+                                                              const double* __restrict__ dinv,
+                                                              const double* __restrict__ b, double* __restrict__ x,
+                                                              double* __restrict__ r, const int* done) {
+  pdl_enter();
+  if (done && *done) return;
+  const int R = s.rep;
+  const int g = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  if (g >= s.n * R) return;
+  const int row = g / R, rr = g - row * R;
+  const int sl = row >> 5;
+  const int beg = __ldg(s.soff + sl) + (row & 31);
+  const int end = __ldg(s.soff + sl + 1);
+  double2 acc = make_double2(0.0, 0.0);
+  for (int k0 = beg; k0 < end; k0 += kChunk * kSlice) {
+    int j[kChunk];
+    V v[kChunk];
+#pragma unroll
+    for (int u = 0; u < kChunk; ++u) {
+      const int k = k0 + u * kSlice;
+      const bool ok = k < end;
+      j[u] = ok ? __ldg(s.col + k) : row;
+      v[u] = ok ? __ldg(val + k) : V(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kChunk; ++u) {
+      const double w = static_cast<double>(v[u]) * __ldg(dinv + j[u]);
+      const double2 bj = __ldg(reinterpret_cast<const double2*>(b + j[u] * R + rr));
+      acc.x = fma(w, bj.x, acc.x);
+      acc.y = fma(w, bj.y, acc.y);
+    }
+  }
+  const double2 bi = ld2(b + g);
+  const double d = dinv[row];
+  st2(x + g, make_double2(d * bi.x, d * bi.y));
+  st2(r + g, make_double2(bi.x - acc.x, bi.y - acc.y));
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_jacobi_rz2(SellView s, const V* __restrict__ val,
+                                                       const double* __restrict__ dinv, const double* __restrict__ r,
+                                                       const double* __restrict__ xin, double* __restrict__ z,
+                                                       CgScalars* S, double* partials, int first) {
+  pdl_enter();
+  if (S->done) return;
+  double v[1] = {0.0};
+  const int n2 = s.n * s.rep / 2;
+  for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < n2; h += gridDim.x * blockDim.x) {
+    const int g = 2 * h;
+    const double2 ax = sell_row_dot2(s, val, xin, g);
+    const double2 ri = ld2(r + g), xi = ld2(xin + g);
+    const double d = dinv[g / s.rep];
+    const double2 zi = make_double2(xi.x + d * (ri.x - ax.x), xi.y + d * (ri.y - ax.y));
+    st2(z + g, zi);
+    v[0] = fma(ri.x, zi.x, v[0]);
+    v[0] = fma(ri.y, zi.y, v[0]);
+  }
+  double tot[1];
+  if (grid_reduce<1>(v, partials, &S->ticket[1], tot) && threadIdx.x == 0) {
+    S->beta = first ? 0.0 : tot[0] / S->rz;
+    S->rz = tot[0];
+  }
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_cg_dir_spmv2(SellView s, const V* __restrict__ val,
+                                                         const double* __restrict__ z, double* __restrict__ p,
+                                                         double* __restrict__ q, CgScalars* S, double* partials) {
+  pdl_enter();
+  if (S->done) return;
+  const double beta = S->beta;
+  double v[1] = {0.0};
+  const int n2 = s.n * s.rep / 2;
+  for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < n2; h += gridDim.x * blockDim.x) {
+    const int g = 2 * h;
+    const double2 az = sell_row_dot2(s, val, z, g);
+    const double2 zi = ld2(z + g);
+    double2 pi = zi, qi = az;
+    if (beta != 0.0) {
+      const double2 po = ld2(p + g), qo = ld2(q + g);
+      pi = make_double2(fma(beta, po.x, zi.x), fma(beta, po.y, zi.y));
+      qi = make_double2(fma(beta, qo.x, az.x), fma(beta, qo.y, az.y));
+    }
+    st2(p + g, pi);
+    st2(q + g, qi);
+    v[0] = fma(pi.x, qi.x, v[0]);
+    v[0] = fma(pi.y, qi.y, v[0]);
+  }
+  double tot[1];
+  if (grid_reduce<1>(v, partials, &S->ticket[2], tot) && threadIdx.x == 0) {
+    S->pq = tot[0];
+    S->alpha = S->rz / tot[0];
+  }
+}
+
 }  // namespace
+
+// Interleaved replicas taken in pairs by the finest-level kernels: an even count of 8 or more.
+static bool paired(const SellView& s) { return s.rep >= 8 && s.rep % 2 == 0; }
 
 // Grid of the reduction kernels: at most eight 256-thread blocks per SM (a full SM); the rows
 // beyond are covered by a grid-stride loop, so that the blocks' publish-and-count tails are few.
@@ -661,19 +796,26 @@ template <typename V>
 void launch_jacobi0_residual(const SellView& s, const V* val, const double* dinv, const double* b, double* x,
                              double* r, const int* done, cudaStream_t st) {
   note_launch();
-  launch_pdl(k_jacobi0_residual<V>, grid_for(1LL * s.n * s.rep), kBlock, 0, st, s, val, dinv, b, x, r, done);
+  if (paired(s)) launch_pdl(k_jacobi0_residual2<V>, grid_for(1LL * s.n * s.rep / 2), kBlock, 0, st, s, val, dinv, b, x, r, done);
+  else launch_pdl(k_jacobi0_residual<V>, grid_for(1LL * s.n * s.rep), kBlock, 0, st, s, val, dinv, b, x, r, done);
 }
 template <typename V>
 void launch_jacobi_rz(const SellView& s, const V* val, const double* dinv, const double* r, const double* xin,
                       double* z, CgScalars* S, double* partials, bool first, cudaStream_t st) {
   note_launch();
-  launch_pdl(k_jacobi_rz<V>, reduce_grid(1LL * s.n * s.rep), kBlock, 0, st, s, val, dinv, r, xin, z, S, partials, first ? 1 : 0);
+  if (paired(s))
+    launch_pdl(k_jacobi_rz2<V>, reduce_grid(1LL * s.n * s.rep / 2), kBlock, 0, st, s, val, dinv, r, xin, z, S, partials,
+               first ? 1 : 0);
+  else
+    launch_pdl(k_jacobi_rz<V>, reduce_grid(1LL * s.n * s.rep), kBlock, 0, st, s, val, dinv, r, xin, z, S, partials,
+               first ? 1 : 0);
 }
 template <typename V>
 void launch_cg_dir_spmv(const SellView& s, const V* val, const double* z, double* p, double* q, CgScalars* S,
                         double* partials, cudaStream_t st) {
   note_launch();
-  launch_pdl(k_cg_dir_spmv<V>, reduce_grid(1LL * s.n * s.rep), kBlock, 0, st, s, val, z, p, q, S, partials);
+  if (paired(s)) launch_pdl(k_cg_dir_spmv2<V>, reduce_grid(1LL * s.n * s.rep / 2), kBlock, 0, st, s, val, z, p, q, S, partials);
+  else launch_pdl(k_cg_dir_spmv<V>, reduce_grid(1LL * s.n * s.rep), kBlock, 0, st, s, val, z, p, q, S, partials);
 }
 template <typename V>
 void launch_cg_update_jacobi0(const SellView& s, const V* val, const double* dinv, const double* p, const double* q,
