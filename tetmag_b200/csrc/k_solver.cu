@@ -683,10 +683,89 @@ __global__ void __launch_bounds__(kBlock) k_cg_dir_spmv2(SellView s, const V* __
   }
 }
 
+// Pair forms of the CSR kernels (coarser levels and transfer operators) for interleaved replicas:
+// thread -> state rows g, g + 1 (g even) of one operator row, one aligned 16-byte gather per entry.
+template <typename V>
+__device__ __forceinline__ double2 csr_row_part2(const CsrView& c, const V* __restrict__ val,
+                                                 const double* __restrict__ x, const double* __restrict__ w, int g) {
+  const int R = c.rep;
+  const int row = g / R, r = g - row * R;
+  const int beg = __ldg(c.ptr + row), end = __ldg(c.ptr + row + 1);
+  double2 acc = make_double2(0.0, 0.0);
+  for (int k0 = beg; k0 < end; k0 += kCsrChunk) {
+    int j[kCsrChunk];
+    V v[kCsrChunk];
+#pragma unroll
+    for (int u = 0; u < kCsrChunk; ++u) {
+      const int k = k0 + u;
+      const bool ok = k < end;
+      j[u] = ok ? __ldg(c.col + k) : 0;
+      v[u] = ok ? __ldg(val + k) : V(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kCsrChunk; ++u) {
+      const double wv = w ? static_cast<double>(v[u]) * __ldg(w + j[u]) : static_cast<double>(v[u]);
+      const double2 xv = __ldg(reinterpret_cast<const double2*>(x + j[u] * R + r));
+      acc.x = fma(wv, xv.x, acc.x);
+      acc.y = fma(wv, xv.y, acc.y);
+    }
+  }
+  return acc;
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_csr_spmv2(CsrView c, const V* __restrict__ val,
+                                                      const double* __restrict__ x, double* __restrict__ y,
+                                                      int accumulate, const int* done) {
+  pdl_enter();
+  if (done && *done) return;
+  const int g = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  if (g >= c.n * c.rep) return;
+  const double2 acc = csr_row_part2(c, val, x, nullptr, g);
+  if (accumulate) {
+    const double2 yo = ld2(y + g);
+    st2(y + g, make_double2(yo.x + acc.x, yo.y + acc.y));
+  } else {
+    st2(y + g, acc);
+  }
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_csr_jacobi0_residual2(CsrView c, const V* __restrict__ val,
+                                                                  const double* __restrict__ dinv,
+                                                                  const double* __restrict__ b, double* __restrict__ x,
+                                                                  double* __restrict__ r, const int* done) {
+  pdl_enter();
+  if (done && *done) return;
+  const int g = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  if (g >= c.n * c.rep) return;
+  const double2 acc = csr_row_part2(c, val, b, dinv, g);
+  const double2 bi = ld2(b + g);
+  const double d = dinv[g / c.rep];
+  st2(x + g, make_double2(d * bi.x, d * bi.y));
+  st2(r + g, make_double2(bi.x - acc.x, bi.y - acc.y));
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_csr_jacobi2(CsrView c, const V* __restrict__ val,
+                                                        const double* __restrict__ dinv, const double* __restrict__ b,
+                                                        const double* __restrict__ xin, double* __restrict__ xout,
+                                                        const int* done) {
+  pdl_enter();
+  if (done && *done) return;
+  const int g = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  if (g >= c.n * c.rep) return;
+  const double2 acc = csr_row_part2(c, val, xin, nullptr, g);
+  const double2 bi = ld2(b + g), xi = ld2(xin + g);
+  const double d = dinv[g / c.rep];
+  st2(xout + g, make_double2(xi.x + d * (bi.x - acc.x), xi.y + d * (bi.y - acc.y)));
+}
+
 }  // namespace
 
 // Interleaved replicas taken in pairs by the finest-level kernels: an even count of 8 or more.
 static bool paired(const SellView& s) { return s.rep >= 8 && s.rep % 2 == 0; }
+static bool paired(const CsrView& c, int tpr) { return tpr == 1 && c.rep >= 8 && c.rep % 2 == 0; }
 
 // Grid of the reduction kernels: at most eight 256-thread blocks per SM (a full SM); the rows
 // beyond are covered by a grid-stride loop, so that the blocks' publish-and-count tails are few.
@@ -743,18 +822,30 @@ template <typename V>
 void launch_csr_spmv(const CsrView& c, const V* val, const double* x, double* y, bool accumulate,
                      const int* done, cudaStream_t st, int tpr) {
   note_launch();
+  if (paired(c, tpr)) {
+    launch_pdl(k_csr_spmv2<V>, grid_for(1LL * c.n * c.rep / 2), kBlock, 0, st, c, val, x, y, accumulate ? 1 : 0, done);
+    return;
+  }
   TMB_CSR_DISPATCH(tpr, k_csr_spmv, 1LL * c.n * c.rep, c, val, x, y, accumulate ? 1 : 0, done)
 }
 template <typename V>
 void launch_csr_jacobi0_residual(const CsrView& c, const V* val, const double* dinv, const double* b, double* x,
                                  double* r, const int* done, cudaStream_t st, int tpr) {
   note_launch();
+  if (paired(c, tpr)) {
+    launch_pdl(k_csr_jacobi0_residual2<V>, grid_for(1LL * c.n * c.rep / 2), kBlock, 0, st, c, val, dinv, b, x, r, done);
+    return;
+  }
   TMB_CSR_DISPATCH(tpr, k_csr_jacobi0_residual, 1LL * c.n * c.rep, c, val, dinv, b, x, r, done)
 }
 template <typename V>
 void launch_csr_jacobi(const CsrView& c, const V* val, const double* dinv, const double* b, const double* xin,
                        double* xout, const int* done, cudaStream_t st, int tpr) {
   note_launch();
+  if (paired(c, tpr)) {
+    launch_pdl(k_csr_jacobi2<V>, grid_for(1LL * c.n * c.rep / 2), kBlock, 0, st, c, val, dinv, b, xin, xout, done);
+    return;
+  }
   TMB_CSR_DISPATCH(tpr, k_csr_jacobi, 1LL * c.n * c.rep, c, val, dinv, b, xin, xout, done)
 }
 #undef TMB_CSR_DISPATCH
