@@ -132,33 +132,6 @@ __device__ __forceinline__ double2 sell_row_dot2(const SellView& s, const V* __r
 }
 
 template <typename V>
-__global__ void __launch_bounds__(kBlock) k_spmv(SellView s, const V* __restrict__ val, const double* __restrict__ x,
-                                                 double* __restrict__ y, const int* done) {
-  pdl_enter();
-  if (done && *done) return;
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g < s.n * s.rep) y[g] = sell_row_dot(s, val, x, g);
-}
-
-template <typename V>
-__global__ void __launch_bounds__(kBlock) k_residual(SellView s, const V* __restrict__ val,
-                                                     const double* __restrict__ b, const double* __restrict__ x,
-                                                     double* __restrict__ r, const int* done) {
-  pdl_enter();
-  if (done && *done) return;
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g < s.n * s.rep) r[g] = b[g] - sell_row_dot(s, val, x, g);
-}
-
-__global__ void k_jacobi0(int n, int R, const double* __restrict__ dinv, const double* __restrict__ b,
-                          double* __restrict__ x, const int* done) {
-  pdl_enter();
-  if (done && *done) return;
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g < n * R) x[g] = dinv[g / R] * b[g];
-}
-
-template <typename V>
 __global__ void __launch_bounds__(kBlock) k_jacobi(SellView s, const V* __restrict__ val,
                                                    const double* __restrict__ dinv, const double* __restrict__ b,
                                                    const double* __restrict__ xin, double* __restrict__ xout,
@@ -529,34 +502,6 @@ __global__ void __launch_bounds__(kBlock) k_cg_update_jacobi0(SellView s, const 
   }
 }
 
-__global__ void k_cg_pupdate(int n, const double* __restrict__ z, double* __restrict__ p, const CgScalars* S) {
-  pdl_enter();
-  if (S->done) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double beta = S->beta;
-  p[i] = (beta == 0.0) ? z[i] : fma(beta, p[i], z[i]);
-}
-
-template <typename V>
-__global__ void __launch_bounds__(kBlock) k_cg_spmv_pq(SellView s, const V* __restrict__ val,
-                                                       const double* __restrict__ p, double* __restrict__ q,
-                                                       CgScalars* S, double* partials) {
-  pdl_enter();
-  if (S->done) return;
-  double v[1] = {0.0};
-  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < s.n * s.rep; g += gridDim.x * blockDim.x) {
-    const double qi = sell_row_dot(s, val, p, g);
-    q[g] = qi;
-    v[0] = fma(p[g], qi, v[0]);
-  }
-  double tot[1];
-  if (grid_reduce<1>(v, partials, &S->ticket[2], tot) && threadIdx.x == 0) {
-    S->pq = tot[0];
-    S->alpha = S->rz / tot[0];
-  }
-}
-
 __global__ void __launch_bounds__(kBlock) k_cg_update(int n, const double* __restrict__ p,
                                                       const double* __restrict__ q, double* __restrict__ x,
                                                       double* __restrict__ r, CgScalars* S, double* partials) {
@@ -781,21 +726,6 @@ int reduce_grid(long long n) {
 }
 
 template <typename V>
-void launch_spmv(const SellView& s, const V* val, const double* x, double* y, const int* done, cudaStream_t st) {
-  note_launch();
-  launch_pdl(k_spmv<V>, grid_for(1LL * s.n * s.rep), kBlock, 0, st, s, val, x, y, done);
-}
-template <typename V>
-void launch_residual(const SellView& s, const V* val, const double* b, const double* x, double* r,
-                     const int* done, cudaStream_t st) {
-  note_launch();
-  launch_pdl(k_residual<V>, grid_for(1LL * s.n * s.rep), kBlock, 0, st, s, val, b, x, r, done);
-}
-void launch_jacobi0(int n, int rep, const double* dinv, const double* b, double* x, const int* done, cudaStream_t st) {
-  note_launch();
-  launch_pdl(k_jacobi0, grid_for(1LL * n * rep), kBlock, 0, st, n, rep, dinv, b, x, done);
-}
-template <typename V>
 void launch_jacobi(const SellView& s, const V* val, const double* dinv, const double* b, const double* xin,
                    double* xout, const int* done, cudaStream_t st) {
   note_launch();
@@ -873,16 +803,6 @@ void launch_cg_rz(int n, const double* r, const double* z, CgScalars* S, double*
   note_launch();
   launch_pdl(k_cg_rz, reduce_grid(n), kBlock, 0, st, n, r, z, S, partials, first ? 1 : 0);
 }
-void launch_cg_pupdate(int n, const double* z, double* p, CgScalars* S, cudaStream_t st) {
-  note_launch();
-  launch_pdl(k_cg_pupdate, grid_for(n), kBlock, 0, st, n, z, p, S);
-}
-template <typename V>
-void launch_cg_spmv_pq(const SellView& s, const V* val, const double* p, double* q, CgScalars* S,
-                       double* partials, cudaStream_t st) {
-  note_launch();
-  launch_pdl(k_cg_spmv_pq<V>, reduce_grid(1LL * s.n * s.rep), kBlock, 0, st, s, val, p, q, S, partials);
-}
 template <typename V>
 void launch_jacobi0_residual(const SellView& s, const V* val, const double* dinv, const double* b, double* x,
                              double* r, const int* done, cudaStream_t st) {
@@ -924,9 +844,6 @@ void launch_cg_update(int n, const double* p, const double* q, double* x, double
 }
 
 #define TMB_INST(V)                                                                                          \
-  template void launch_spmv<V>(const SellView&, const V*, const double*, double*, const int*, cudaStream_t); \
-  template void launch_residual<V>(const SellView&, const V*, const double*, const double*, double*,        \
-                                   const int*, cudaStream_t);                                               \
   template void launch_jacobi<V>(const SellView&, const V*, const double*, const double*, const double*,    \
                                  double*, const int*, cudaStream_t);                                        \
   template void launch_csr_spmv<V>(const CsrView&, const V*, const double*, double*, bool, const int*,      \
@@ -939,8 +856,6 @@ void launch_cg_update(int n, const double* p, const double* q, double* x, double
                                   double*, cudaStream_t);                                                   \
   template void launch_cg_residual<V>(const SellView&, const V*, const double*, const double*, double*,     \
                                       CgScalars*, double*, cudaStream_t);                                   \
-  template void launch_cg_spmv_pq<V>(const SellView&, const V*, const double*, double*, CgScalars*,         \
-                                     double*, cudaStream_t);                                                \
   template void launch_jacobi0_residual<V>(const SellView&, const V*, const double*, const double*, double*, \
                                            double*, const int*, cudaStream_t);                              \
   template void launch_jacobi_rz<V>(const SellView&, const V*, const double*, const double*, const double*, \

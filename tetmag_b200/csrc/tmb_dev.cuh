@@ -125,12 +125,6 @@ void launch_add(int n, const double* a, const double* b, double* out, cudaStream
 
 // --- launchers (k_solver.cu) -------------------------------------------------------------
 template <typename V>
-void launch_spmv(const SellView& s, const V* val, const double* x, double* y, const int* done, cudaStream_t st);
-template <typename V>
-void launch_residual(const SellView& s, const V* val, const double* b, const double* x, double* r,
-                     const int* done, cudaStream_t st);
-void launch_jacobi0(int n, int rep, const double* dinv, const double* b, double* x, const int* done, cudaStream_t st);
-template <typename V>
 void launch_jacobi(const SellView& s, const V* val, const double* dinv, const double* b, const double* xin,
                    double* xout, const int* done, cudaStream_t st);
 // CSR kernels with tpr (1, 2, 4, 8, 16, 32) threads per row; csr_threads_per_row picks it from
@@ -156,10 +150,6 @@ void launch_cg_residual(const SellView& s, const V* val, const double* bp, const
                         CgScalars* S, double* partials, cudaStream_t st);
 void launch_cg_rz(int n, const double* r, const double* z, CgScalars* S, double* partials, bool first,
                   cudaStream_t st);
-void launch_cg_pupdate(int n, const double* z, double* p, CgScalars* S, cudaStream_t st);
-template <typename V>
-void launch_cg_spmv_pq(const SellView& s, const V* val, const double* p, double* q, CgScalars* S,
-                       double* partials, cudaStream_t st);
 void launch_cg_update(int n, const double* p, const double* q, double* x, double* r, CgScalars* S,
                       double* partials, cudaStream_t st);
 // fused variants used by the PCG iteration
