@@ -14,8 +14,9 @@
 //     After convergence a few unvisited rows are checked and, if any still has a
 //     significant residual, the approximation continues from that row;
 //   * the matvec y = H x works in the cluster-tree order: dense tiles by leaf row
-//     cluster (plain stores), then per row cluster tau, for each of its low-rank blocks,
-//     t_b = V_b^T x_sigma and y_tau += U_b t_b, with one atomic add per row and row cluster.
+//     cluster (plain stores); then t_b = V_b^T x_sigma for every term of every low-rank
+//     block (k_h_vt, eight lanes per term), and y_tau += U_b t_b per run of blocks of one
+//     row cluster (k_h_ut), with one atomic add per row and run.
 #include <cmath>
 
 #include "lindholm_accurate.cuh"
