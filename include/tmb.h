@@ -217,11 +217,13 @@ int tmb_llg_rhs(tmb_ctx* ctx, double t, const double* y, double* ydot, int ptr_k
  * evaluate the right-hand side (a fixed device-memory budget, a loop that must not pay
  * cudaMalloc's device-wide synchronisation, a stream under capture by other work).  y and
  * ydot are staged through one file-scope device array of 2 x 3 x 65536 doubles (3 MiB, held by
- * every GPU that loads the library until exit); meshes above 65536 nodes get TMB_ERR_ARG.
- * The first call on a device resolves that array's device address (cudaGetSymbolAddress); make
- * it before any stream capture.  Every call shares the array: calls that overlap on the GPU
- * (other threads, other contexts on the same device) race, so serialise them.  Nothing in the
- * array needs to start at zero: each call overwrites the 6N entries it uses.  Synchronises. */
+ * every GPU that loads the library until exit); contexts with nodes x replicas above 65536 get
+ * TMB_ERR_ARG.  tmb_ctx_create resolves that array's device address for its device
+ * (cudaGetSymbolAddress, which also loads the module holding the array), so no call of this
+ * entry point, the first included, allocates.  Every call shares the array: calls that overlap
+ * on the GPU (other threads, other contexts on the same device) race, so serialise them.
+ * Nothing in the array needs to start at zero: each call overwrites the 6N entries it uses.
+ * Synchronises. */
 int tmb_llg_rhs_noalloc(tmb_ctx* ctx, double t, const double* y, double* ydot);
 /* TheLLG::getMaxTorque (main/TheLLG.cpp:426-439): mu0 * max_i |m_i x H_i| with the frozen demag.
  * Synchronises.  Returns TMB_ERR_NAN if the torque is not finite. */

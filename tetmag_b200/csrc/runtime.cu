@@ -2111,6 +2111,12 @@ static int fail(int code, const std::string& msg) {
 #define TMB_CHECK_ARG(cond, msg) \
   if (!(cond)) return fail(TMB_ERR_ARG, msg);
 
+// Device address of the allocation-free right-hand side's staging array on `device` (the
+// current device), resolved once per device; defined with the array below.
+namespace tmb {
+static void resolve_staging_address(int device);
+}
+
 // Stages a host (or device) 3N vector into a device buffer.
 static const double* stage_in(Ctx& c, DevArray<double>& buf, const double* p, size_t count, int kind) {
   if (kind == TMB_PTR_DEVICE) return p;
@@ -2217,6 +2223,9 @@ int tmb_ctx_create(int device, tmb_ctx** out) {
   auto* h = new tmb_ctx();
   try {
     h->c = std::make_unique<Ctx>(device);
+    // the allocation-free right-hand side's staging array: its device address is resolved here,
+    // where allocating is allowed (resolving it loads the module that holds the array)
+    resolve_staging_address(device);
   } catch (...) {
     delete h;
     throw;
@@ -2634,15 +2643,26 @@ static __device__ __align__(256) double g_rhs_staging[2 * 3 * kNoAllocMaxNodes];
 static std::mutex g_staging_mutex;
 static double* g_staging_address[kNoAllocMaxDevices] = {};
 
-// Device address of g_rhs_staging on `device`, which must be the current device.  The
-// host-side name of the array is only a stand-in: kernels must be given this address.
-static double* staging_address(int device) {
+// Resolves the device address of g_rhs_staging on `device`, which must be the current device.
+// Called by tmb_ctx_create, once per device.  The host-side name of the array is only a
+// stand-in: kernels and copies must be given this address.  Resolving it loads the module that
+// holds the array (with lazy module loading that is the moment the 3 MiB are reserved), so it
+// happens at context creation, where allocating is allowed, and never inside
+// tmb_llg_rhs_noalloc.  Devices beyond kNoAllocMaxDevices are skipped (their contexts get
+// TMB_ERR_ARG from tmb_llg_rhs_noalloc).
+static void resolve_staging_address(int device) {
+  if (device < 0 || device >= kNoAllocMaxDevices) return;
   std::lock_guard<std::mutex> lock(g_staging_mutex);
   if (!g_staging_address[device]) {
     void* p = nullptr;
     TMB_CUDA(cudaGetSymbolAddress(&p, g_rhs_staging));
     g_staging_address[device] = static_cast<double*>(p);
   }
+}
+
+// The address resolved by tmb_ctx_create for `device`, or nullptr.
+static double* staging_address(int device) {
+  std::lock_guard<std::mutex> lock(g_staging_mutex);
   return g_staging_address[device];
 }
 
@@ -2658,13 +2678,14 @@ int tmb_llg_rhs_noalloc(tmb_ctx* ctx, double t, const double* y, double* ydot) {
   c.require_mesh();
   c.require_material();
   if (c.nr() > kNoAllocMaxNodes)
-    return fail(TMB_ERR_ARG, "tmb_llg_rhs_noalloc: the mesh has " + std::to_string(c.nr()) +
-                                 " nodes; its static staging array holds at most " +
+    return fail(TMB_ERR_ARG, "tmb_llg_rhs_noalloc: nodes x replicas = " + std::to_string(c.nr()) +
+                                 "; its static staging array holds at most " +
                                  std::to_string(kNoAllocMaxNodes) + " (use tmb_llg_rhs)");
   if (c.device < 0 || c.device >= kNoAllocMaxDevices)
     return fail(TMB_ERR_ARG, "tmb_llg_rhs_noalloc: device ordinal beyond the supported range");
-  TMB_CUDA(cudaSetDevice(c.device));
   double* const stage = staging_address(c.device);
+  if (!stage) return fail(TMB_ERR_STATE, "tmb_llg_rhs_noalloc: staging array not resolved for this device");
+  TMB_CUDA(cudaSetDevice(c.device));
   double* const yd = stage;                          // y, 3N
   double* const od = stage + 3 * kNoAllocMaxNodes;   // ydot, 3N
   const size_t n3 = size_t(3) * c.nr();
