@@ -282,8 +282,12 @@ int tmb_get_stats(tmb_ctx* ctx, double* out);
 /* Live profiling with CUDA events on the context stream (no reference counterpart; tetmag's
  * timers are host wall clocks, main/DemagField.cpp:155-160, utils/Timer.cpp:36-81).
  * Kernel ids: 0 local field + LLG, 1 divergence, 2 gradient, 3 BEM matvec, 4 Neumann solve,
- * 5 Dirichlet solve, 6 CG fine-level SpMV, 7 whole demag chain.
- * tmb_profile_read fills out[3*id + {0,1,2}] = launches, total ms, algorithmic bytes per launch. */
+ * 5 Dirichlet solve, 6 CG fine-level SpMV, 7 whole demag chain (4, 5 and 7 span several kernels),
+ * 8 fused CG update + first fine smoothing sweep, 9 fine post-smoothing sweep + r.z, 10 fine
+ * pre-smoothing sweep (unfused), 11 restriction, 12 prolongation, 13 coarse-level smoothing
+ * sweeps, 14 coarsest dense solve, 15 CG start (lift, initial residual), 16 CG vector update
+ * (unfused).  tmb_profile_read fills out[3*id + {0,1,2}] = launches, total ms, algorithmic bytes
+ * per launch, for the 17 ids (51 doubles). */
 int tmb_profile_enable(tmb_ctx* ctx, int on);
 int tmb_profile_read(tmb_ctx* ctx, double* out);
 

@@ -455,7 +455,10 @@ def kernel_launches() -> int:
 
 
 PROFILE_IDS = ["local_llg", "divergence", "gradient", "bem_matvec", "solve_neumann", "solve_dirichlet",
-               "cg_spmv", "demag_chain"]
+               "cg_spmv", "demag_chain", "cg_update_smooth", "fine_post_smooth_rz", "fine_pre_smooth",
+               "restriction", "prolongation", "coarse_smooth", "coarsest_solve", "cg_start", "cg_update"]
+# ids that span several kernels (not candidates for a per-kernel roofline)
+PROFILE_CONTAINERS = ("solve_neumann", "solve_dirichlet", "demag_chain")
 
 
 def profile_enable(ctx: "Context", on: bool = True):

@@ -249,20 +249,42 @@ void amg_build(const Csr& A0, const AmgParams& prm, AmgHierarchy& H) {
     }
 
     if (coarsest) {
-      if (n > 4096) throw std::runtime_error("AMG: coarsest level too large for a dense solve");
-      H.ncoarse = n;
-      std::vector<double> dense(size_t(n) * n, 0.0);
-      for (int i = 0; i < n; ++i)
-        for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) dense[size_t(i) * n + A.col[k]] += A.val[k];
+      constexpr int kMaxDense = 4096;
+      // rows without off-diagonal entries (the eliminated constraints of a Dirichlet matrix whose
+      // nodes are nearly all on the boundary, for instance) decouple: solve them by their
+      // diagonal and invert the coupled rows only
+      std::vector<int> core;
+      H.coarse_idx.clear();
+      H.coarse_diag_inv.clear();
+      if (n > kMaxDense) {
+        for (int i = 0; i < n; ++i)
+          if (A.ptr[i + 1] - A.ptr[i] > 1) core.push_back(i);
+        if (int(core.size()) > kMaxDense) throw std::runtime_error("AMG: coarsest level too large for a dense solve");
+        H.coarse_idx = core;
+        H.coarse_diag_inv.resize(n);
+        for (int i = 0; i < n; ++i) H.coarse_diag_inv[i] = 1.0 / d[i];
+      }
+      const bool subset = n > kMaxDense;
+      const int nd = subset ? int(core.size()) : n;
+      std::vector<int> where(n, -1);
+      for (int q = 0; q < nd; ++q) where[subset ? core[q] : q] = q;
+      H.ncoarse = nd;
+      std::vector<double> dense(size_t(nd) * nd, 0.0);
+      for (int q = 0; q < nd; ++q) {
+        const int i = subset ? core[q] : q;
+        for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k)
+          if (where[A.col[k]] >= 0) dense[size_t(q) * nd + where[A.col[k]]] += A.val[k];
+      }
       if (prm.singular) {
         // constants span the null space on every level (P 1 = 1 since A 1 = 0): invert
         // A_c + a 1 1^T, which acts as the pseudo-inverse on the range of A_c
         double tr = 0.0;
-        for (int i = 0; i < n; ++i) tr += dense[size_t(i) * n + i];
-        const double a = tr / (double(n) * n);
+        for (int i = 0; i < nd; ++i) tr += dense[size_t(i) * nd + i];
+        if (nd == 0) tr = 0.0;
+        const double a = tr / (double(nd) * nd);
         for (auto& v : dense) v += a;
       }
-      dense_inverse(dense, n);
+      dense_inverse(dense, nd);
       H.coarse_inv.swap(dense);
       L.A = std::move(A);
       H.levels.push_back(std::move(L));

@@ -280,6 +280,29 @@ __global__ void k_coarse_solve(int n, int ld, int R, const double* __restrict__ 
   if (lane == 0) x[g] = acc;
 }
 
+// Coarsest level with decoupled rows (AmgHierarchy::coarse_idx): x = D^-1 b on every row, then the
+// coupled rows are gathered into a compact vector, solved densely, and scattered back.
+__global__ void k_coarse_diag(int n, int R, const double* __restrict__ dinv, const double* __restrict__ b,
+                              double* __restrict__ x, const int* done) {
+  pdl_enter();
+  if (done && *done) return;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n * R) return;
+  x[g] = dinv[g / R] * b[g];
+}
+
+// dst[k * R + r] = src[idx[k] * R + r] (gather), or dst[idx[k] * R + r] = src[k * R + r] (scatter)
+__global__ void k_rows_move(int m, int R, const int* __restrict__ idx, const double* __restrict__ src,
+                            double* __restrict__ dst, int scatter, const int* done) {
+  pdl_enter();
+  if (done && *done) return;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= m * R) return;
+  const int k = g / R, r = g - k * R;
+  if (scatter) dst[idx[k] * R + r] = src[g];
+  else dst[g] = src[idx[k] * R + r];
+}
+
 // The same product for one replica and a larger coarsest level: one 128-thread CTA per row, all
 // of a thread's 16-byte loads of the row issued together.
 __global__ void __launch_bounds__(128) k_coarse_solve_rows(int n, int ld, const double* __restrict__ inv,
@@ -785,6 +808,17 @@ void launch_coarse_solve(int n, int ld, int rep, const double* inv, const double
   if (rep == 1 && n >= 256 && invf) launch_pdl(k_coarse_solve_rows_f32, n, 128, 0, st, n, ldf, invf, b, x, done);
   else if (rep == 1 && n >= 256) launch_pdl(k_coarse_solve_rows, n, 128, 0, st, n, ld, inv, b, x, done);
   else launch_pdl(k_coarse_solve, grid_for(32LL * n * rep), kBlock, 0, st, n, ld, rep, inv, b, x, done);
+}
+void launch_coarse_diag(int n, int rep, const double* dinv, const double* b, double* x, const int* done,
+                        cudaStream_t st) {
+  note_launch();
+  launch_pdl(k_coarse_diag, grid_for(1LL * n * rep), kBlock, 0, st, n, rep, dinv, b, x, done);
+}
+void launch_rows_move(int m, int rep, const int* idx, const double* src, double* dst, bool scatter,
+                      const int* done, cudaStream_t st) {
+  if (m <= 0) return;
+  note_launch();
+  launch_pdl(k_rows_move, grid_for(1LL * m * rep), kBlock, 0, st, m, rep, idx, src, dst, scatter ? 1 : 0, done);
 }
 template <typename V>
 void launch_cg_init(int n, const CsrView& lift, const V* lval, const int* cmask, const double* b,

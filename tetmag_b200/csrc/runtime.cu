@@ -168,9 +168,13 @@ struct Ctx;
 // ------------------------------------------------------------------------------------------
 // Live kernel profiler: CUDA events around the main kernels on the launching stream.
 // ids: 0 local field + LLG, 1 divergence, 2 gradient, 3 BEM matvec, 4 Neumann solve,
-//      5 Dirichlet solve, 6 CG fine-level SpMV, 7 whole demag chain
+//      5 Dirichlet solve, 6 CG fine-level SpMV, 7 whole demag chain (4, 5, 7 are containers),
+//      8 fused CG update + first fine smoothing sweep, 9 fine post-smoothing sweep + r.z,
+//      10 fine pre-smoothing sweep (unfused), 11 restriction (every level), 12 prolongation
+//      (every level), 13 coarse-level smoothing sweeps, 14 coarsest dense solve, 15 CG start
+//      (lift, initial residual), 16 CG vector update (unfused)
 // ------------------------------------------------------------------------------------------
-constexpr int kProfIds = 8;
+constexpr int kProfIds = 17;
 struct Prof {
   bool on = false;
   struct Rec {
@@ -257,6 +261,11 @@ struct Solver {
   DevArray<double> cinv;
   DevArray<float> cinvf;
   int ncoarse = 0, cld = 0, cldf = 0;
+  // coarsest level with decoupled rows (AmgHierarchy::coarse_idx): its coupled rows, the exact
+  // inverse diagonal of every row, and compact vectors for the dense solve of the coupled rows
+  bool csubset = false;
+  DevArray<int> cidx;
+  DevArray<double> cdiag, cb, cx;
   DevCsr lift;
   DevArray<int> cmask;
   // transposed solve (the adjoint): lift^T, masked load, and a warm start kept apart from the
@@ -510,15 +519,19 @@ void Solver::iteration_body(int precision, cudaStream_t st, bool profile) {
     double* rnew = rbuf[rc ^ 1].p;
     rc ^= 1;
     DevLevel& L = lev[0];
+    if (profile) ctx_prof_begin(8, st, nnz_fine * ((f64 ? 8.0 : 4.0) + 4.0) + 9.0 * 8.0 * n * rep);
     if (f64)
       launch_cg_update_jacobi0<double>(A0, L.Ad.p, L.dinv.p, p.p, q.p, x.p, rold, rnew, L.X.p, L.R.p, Sd,
                                        partials.p, st);
     else
       launch_cg_update_jacobi0<float>(A0, L.Af.p, L.dinv.p, p.p, q.p, x.p, rold, rnew, L.X.p, L.R.p, Sd,
                                       partials.p, st);
+    if (profile) ctx_prof_end(st);
     vcycle(0, rnew, z.p, precision, st, 0, true);
   } else {
+    if (profile) ctx_prof_begin(16, st, 6.0 * 8.0 * n * rep);
     launch_cg_update(n * rep, p.p, q.p, x.p, rbuf[rc].p, Sd, partials.p, st);
+    if (profile) ctx_prof_end(st);
     precondition_rz(precision, st, false);
   }
 }
@@ -631,6 +644,13 @@ void Solver::compute() {
     }
   }
   ncoarse = H.ncoarse;
+  csubset = !H.coarse_idx.empty() || !H.coarse_diag_inv.empty();
+  if (csubset) {
+    cidx.upload(H.coarse_idx, st);
+    cdiag.upload(H.coarse_diag_inv, st);
+    cb.alloc(size_t(std::max(ncoarse, 1)) * rep);
+    cx.alloc(size_t(std::max(ncoarse, 1)) * rep);
+  }
   cld = ncoarse + (ncoarse & 1);  // even rows: 16-byte loads
   {
     std::vector<double> ci(size_t(ncoarse) * cld, 0.0);
@@ -671,31 +691,62 @@ void Solver::vcycle(size_t l, const double* b, double* out, int precision, cudaS
                     bool presmoothed) {
   DevLevel& L = lev[l];
   const int* done = &Sd->done;
+  const bool f64 = precision == TMB_FP64;
+  // live profile (kernel by kernel, never inside a graph capture): algorithmic bytes per launch
+  const bool prof = ctx_prof_on();
+  const double sv = f64 ? 8.0 : 4.0, R = double(rep);
+  auto pb = [&](int id, double bytes) {
+    if (prof) ctx_prof_begin(id, st, bytes);
+  };
+  auto pe = [&]() {
+    if (prof) ctx_prof_end(st);
+  };
   if (l + 1 == lev.size()) {
-    launch_coarse_solve(ncoarse, cld, rep, cinv.p, b, out, done, st, precision == TMB_FP64 ? nullptr : cinvf.p,
-                        cldf);
+    pb(14, double(ncoarse) * ncoarse * sv + 2.0 * 8.0 * ncoarse * R);
+    if (csubset) {
+      launch_coarse_diag(L.n, rep, cdiag.p, b, out, done, st);
+      if (ncoarse > 0) {
+        launch_rows_move(ncoarse, rep, cidx.p, b, cb.p, false, done, st);
+        launch_coarse_solve(ncoarse, cld, rep, cinv.p, cb.p, cx.p, done, st, f64 ? nullptr : cinvf.p, cldf);
+        launch_rows_move(ncoarse, rep, cidx.p, cx.p, out, true, done, st);
+      }
+    } else {
+      launch_coarse_solve(ncoarse, cld, rep, cinv.p, b, out, done, st, f64 ? nullptr : cinvf.p, cldf);
+    }
+    pe();
     return;
   }
   DevLevel& C = lev[l + 1];
-  const bool f64 = precision == TMB_FP64;
+  const double nl = double(L.n) * R, nc = double(C.n) * R;
+  const double nnz_l = l == 0 ? nnz_fine : double(L.Ac.col.n);
+  const double sweep = nnz_l * (sv + 4.0) + (l == 0 ? 0.0 : 4.0 * (L.n + 1));
   if (l == 0) {
     const SellView A = L.A.view(rep);
     if (!presmoothed) {
+      pb(10, sweep + 4.0 * 8.0 * nl);
       if (f64) launch_jacobi0_residual<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, L.R.p, done, st);
       else launch_jacobi0_residual<float>(A, L.Af.p, L.dinv.p, b, L.X.p, L.R.p, done, st);
+      pe();
     }
   } else {
     const CsrView A = L.Ac.view(rep);
+    pb(13, sweep + 4.0 * 8.0 * nl);
     if (f64) launch_csr_jacobi0_residual<double>(A, L.Ac.v.p, L.dinv.p, b, L.X.p, L.R.p, done, st, L.tA);
     else launch_csr_jacobi0_residual<float>(A, L.Ac.vf.p, L.dinv.p, b, L.X.p, L.R.p, done, st, L.tA);
+    pe();
   }
+  pb(11, double(L.Rop.col.n) * (sv + 4.0) + 4.0 * (C.n + 1) + 8.0 * (nl + nc));
   if (f64) launch_csr_spmv<double>(L.Rop.view(rep), L.Rop.v.p, L.R.p, C.b.p, false, done, st, L.tR);
   else launch_csr_spmv<float>(L.Rop.view(rep), L.Rop.vf.p, L.R.p, C.b.p, false, done, st, L.tR);
+  pe();
   vcycle(l + 1, C.b.p, C.out.p, precision, st, -1);
+  pb(12, double(L.P.col.n) * (sv + 4.0) + 4.0 * (L.n + 1) + 8.0 * (nc + 2.0 * nl));
   if (f64) launch_csr_spmv<double>(L.P.view(rep), L.P.v.p, C.out.p, L.X.p, true, done, st, L.tP);
   else launch_csr_spmv<float>(L.P.view(rep), L.P.vf.p, C.out.p, L.X.p, true, done, st, L.tP);
+  pe();
   if (l == 0) {
     const SellView A = L.A.view(rep);
+    pb(9, sweep + 5.0 * 8.0 * nl);
     if (rz_mode >= 0) {
       // finest level: the post-smoothing sweep also reduces r.z for the next CG direction
       if (f64) launch_jacobi_rz<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, out, Sd, partials.p, rz_mode == 1, st);
@@ -704,10 +755,13 @@ void Solver::vcycle(size_t l, const double* b, double* out, int precision, cudaS
       if (f64) launch_jacobi<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, out, done, st);
       else launch_jacobi<float>(A, L.Af.p, L.dinv.p, b, L.X.p, out, done, st);
     }
+    pe();
   } else {
     const CsrView A = L.Ac.view(rep);
+    pb(13, sweep + 4.0 * 8.0 * nl);
     if (f64) launch_csr_jacobi<double>(A, L.Ac.v.p, L.dinv.p, b, L.X.p, out, done, st, L.tA);
     else launch_csr_jacobi<float>(A, L.Ac.vf.p, L.dinv.p, b, L.X.p, out, done, st, L.tA);
+    pe();
   }
 }
 
@@ -732,11 +786,14 @@ void Solver::solve(const double* b_dev, int precision) {
   TMB_CUDA(cudaMemcpyAsync(Sd, Sh, sizeof(CgScalars), cudaMemcpyHostToDevice, st));
   const SellView A0 = lev[0].A.view(rep);
   const bool f64 = precision == TMB_FP64;
+  if (ctx_prof_on())
+    ctx_prof_begin(15, st, (double(lift.col.n) + nnz_fine) * ((f64 ? 8.0 : 4.0) + 4.0) + 8.0 * 8.0 * n * rep);
   if (f64) launch_cg_init<double>(n, lift.view(rep), lift.v.p, cmask.p, b_dev, bp.p, x.p, st);
   else launch_cg_init<float>(n, lift.view(rep), lift.vf.p, cmask.p, b_dev, bp.p, x.p, st);
   rc = 0;  // graphs are captured with the residual starting in rbuf[0]
   if (f64) launch_cg_residual<double>(A0, lev[0].Ad.p, bp.p, x.p, rbuf[0].p, Sd, partials.p, st);
   else launch_cg_residual<float>(A0, lev[0].Af.p, bp.p, x.p, rbuf[0].p, Sd, partials.p, st);
+  if (ctx_prof_on()) ctx_prof_end(st);
   precondition_rz(precision, st, true);
   if (!ctx_prof_on()) {
     // Graph path: kGraphIters iterations per graph launch; the first batch covers the

@@ -139,6 +139,12 @@ void launch_csr_jacobi0_residual(const CsrView& c, const V* val, const double* d
 template <typename V>
 void launch_csr_jacobi(const CsrView& c, const V* val, const double* dinv, const double* b, const double* xin,
                        double* xout, const int* done, cudaStream_t st, int tpr);
+// coarsest level with decoupled rows: x = D^-1 b, and the moves of the coupled rows to and from a
+// compact vector for the dense solve
+void launch_coarse_diag(int n, int rep, const double* dinv, const double* b, double* x, const int* done,
+                        cudaStream_t st);
+void launch_rows_move(int m, int rep, const int* idx, const double* src, double* dst, bool scatter,
+                      const int* done, cudaStream_t st);
 void launch_coarse_solve(int n, int ld, int rep, const double* inv, const double* b, double* x, const int* done,
                          cudaStream_t st, const float* invf = nullptr, int ldf = 0);
 

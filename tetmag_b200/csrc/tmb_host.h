@@ -88,6 +88,13 @@ struct AmgHierarchy {
   std::vector<AmgLevel> levels;            // levels[0].A is the fine operator
   int ncoarse = 0;
   std::vector<double> coarse_inv;          // dense ncoarse x ncoarse inverse (row-major), FP64
+  // when the coarsest level is too large for a dense inverse but only a few of its rows couple to
+  // others (a row with no off-diagonal entry has a decoupled column too, the operator being
+  // symmetric): coarse_inv inverts the submatrix of those rows, listed here (the level's row ids),
+  // and every other row is solved exactly by its diagonal (coarse_diag_inv, one per level row).
+  // Empty: coarse_inv covers all rows.
+  std::vector<int> coarse_idx;
+  std::vector<double> coarse_diag_inv;
   double setup_ms = 0.0;
 };
 
