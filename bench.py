@@ -58,19 +58,22 @@ def parse():
     p.add_argument("--sim-ps", type=float, default=2.0, help="simulated ps for the ns/hour figure")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--c5-steps", type=int, default=500, help="time steps of the adjoint workload (c5)")
-    p.add_argument("--bem", default="auto", choices=["auto", "hmatrix", "hmatrix-only", "hmatrix-dense", "dense"],
+    p.add_argument("--bem", default="auto", choices=["auto", "h2", "hmatrix", "hmatrix-only", "hmatrix-dense", "dense"],
                    help="BEM form of the timed paths (the dense FP64 path is measured too, except with "
                         "hmatrix-only: the hierarchical matrix built from the mesh with no dense copy on the "
-                        "device, for profiling captures that must stay a few GB); auto: the hierarchical "
-                        "matrix built from the mesh for c2 (its configuration names the H2-compressed BEM), "
-                        "the dense matrix otherwise")
+                        "device, for profiling captures that must stay a few GB); h2: the hierarchical "
+                        "matrix built from the mesh, recompressed into nested cluster bases; auto: h2 for c2 "
+                        "(its configuration names the H2-compressed BEM), the dense matrix otherwise")
     return p.parse_args()
+
+
+H2_EPS = (1e-9, 1e-6)     # recompression tolerances of the FP64 and FP32 H2 copies
 
 
 def bem_for(args, workload: str) -> str:
     if args.bem != "auto":
         return args.bem
-    return "hmatrix" if workload == "c2" else "dense"
+    return "h2" if workload == "c2" else "dense"
 
 
 def peak_hbm():
@@ -163,8 +166,9 @@ def config_for(w, bem: str, tol: float, world: int, sharded: bool) -> dict:
     ninst = workloads.instances(w)
     cfg = {"workload": w.name, "nodes": int(w.m0.size // 3), "mesh_nodes": int(w.mesh.nx), "boundary_nodes": nb,
            "nnz": nnz, "instances": ninst,
-           "bem": ("hierarchical, leaf 32, eta 2 (tetmag's H2 parameters)" if bem.startswith("hmatrix")
-                   else "dense double-layer (Lindholm)"),
+           "bem": ("H2, leaf 32, eta 2 (tetmag's H2 parameters)" if bem == "h2" else
+                "hierarchical, leaf 32, eta 2 (tetmag's H2 parameters)" if bem.startswith("hmatrix")
+                else "dense double-layer (Lindholm)"),
            "cg_tol": tol, "states": "W+K distinct seeded perturbed states, warm-started solves",
            "l2": "inputs larger than L2 (c2's boundary matrix alone streams over 1 GB per step)",
            "parallelism": (("instances sharded over %d ranks" % world) if sharded else
@@ -200,7 +204,7 @@ def cpu_field(w, bem: str, tol: float):
     t = time.perf_counter()
     cf = cpu_ref.CpuField(pb, tol=tol, maxiter=100)
     sa = O.solid_angles(pb.xyz, pb.tets, pb.bnd)
-    if bem.startswith("hmatrix"):
+    if bem.startswith("hmatrix") or bem == "h2":
         info = cf.build_hmatrix(sa, leaf=32, eta=2.0, eps=1e-6, kmax=64)
         desc = (f"hierarchical boundary matrix (ACA to 1e-6, {info['bytes'] / 1e9:.2f} GB FP64, built in "
                 f"{info['build_s']:.1f} s)")
@@ -349,12 +353,15 @@ def measure(args, name: str, dist: Dist, full: bool) -> dict:
     hier = bem != "dense"
     dense_ref = bem != "hmatrix-only"
     mo, ctx = workloads.setup_context(w, device=local, mixed=True, tol=args.tol, maxiter=100,
-                                      hmatrix={"hmatrix": "mesh", "hmatrix-only": "mesh",
+                                      hmatrix={"hmatrix": "mesh", "hmatrix-only": "mesh", "h2": "mesh",
                                                "hmatrix-dense": True}.get(bem, False),
-                                      keep_dense=dense_ref)
+                                      keep_dense=dense_ref, h2=H2_EPS if bem == "h2" else None)
+    hier_mode = 2 if bem == "h2" else 1
     bem_info = ctx.bem_info() if hier else None
     if hier and dense_ref:
         bem_info["verify"] = ctx.bem_verify()
+    if bem == "h2":
+        bem_info["h2"] = ctx.bem_h2_info()
     setup_s = time.perf_counter() - t0
     stream = torch.cuda.Stream(dev)
     ctx.set_stream(stream.cuda_stream)
@@ -376,7 +383,7 @@ def measure(args, name: str, dist: Dist, full: bool) -> dict:
     def timed(mixed: bool, profile: bool, dense: bool = False):
         ctx.set_precision(mixed)
         if hier:
-            ctx.set_bem_mode(not dense)
+            ctx.set_bem_mode(0 if dense else hier_mode)
         for k in range(W):
             ctx.field_eval(S[k], ydot, hdem)
         torch.cuda.synchronize(dev)
@@ -426,7 +433,7 @@ def measure(args, name: str, dist: Dist, full: bool) -> dict:
     y64 = ctx.field_eval(probe, torch.empty_like(ydot), h64)
     err64 = None
     if hier:
-        ctx.set_bem_mode(True)
+        ctx.set_bem_mode(hier_mode)
         h64h = hdem.clone()
         y64h = ctx.field_eval(probe, torch.empty_like(ydot), h64h)
     ctx.set_precision(True)

@@ -150,7 +150,20 @@ int tmb_bem_compress(tmb_ctx* ctx, const double* bxyz, const double* bnormal, in
  * assembly replaces the dense matrix (setupH2MatrixC, main/h2interface.c:315-399). */
 int tmb_bem_build_h(tmb_ctx* ctx, const tmb_mesh* mesh, int leaf, double eta, double eps_mixed, double eps_fp64,
                     int kmax);
-int tmb_set_bem_mode(tmb_ctx* ctx, int mode);  /* 0 dense, 1 hierarchical */
+int tmb_set_bem_mode(tmb_ctx* ctx, int mode);  /* 0 dense, 1 hierarchical, 2 H2 */
+/* H2 matrix: the hierarchical matrix's admissible blocks (its FP64 terms) recompressed into nested
+ * cluster bases -- orthogonal row and column bases per cluster, leaf bases explicit and parents'
+ * through transfer matrices, one small coupling matrix per admissible block -- truncated at
+ * eps_fp64 (the plain path's copy) and eps_mixed (the mixed path's FP32 copy) relative to the
+ * largest singular value of each cluster's total matrix, ranks at most kmax (<= 64); the near
+ * field stays the hierarchical matrix's dense tiles.  Restates H2Lib's recompression
+ * (compress_hmatrix_h2matrix at 1e-5, main/h2interface.c:362-369) and the H2 matvec of
+ * H2_mvp_sub (:77-95).  Needs tmb_bem_build_h / tmb_bem_compress first; selects mode 2. */
+int tmb_bem_h2(tmb_ctx* ctx, double eps_fp64, double eps_mixed, int kmax);
+/* out[8 * w + 0..7] for w = 0 (FP64 copy), 1 (FP32 copy): built, bytes streamed per matvec
+ * (near tiles + bases + couplings), coupling bytes, basis + transfer bytes, max row rank, max
+ * column rank, build ms, tolerance. */
+int tmb_bem_h2_info(tmb_ctx* ctx, double* out);
 /* out[0..11]: mode, dense tiles, low-rank blocks, FP64 terms, FP32 terms, FP64 bytes, FP32 bytes,
  * dense entries (Nb^2), blocks at the rank cap, max FP64 rank, compression ms, built flag */
 int tmb_bem_info(tmb_ctx* ctx, double* out);

@@ -1,0 +1,82 @@
+"""The H2 boundary matrix (nested cluster bases, tmb_bem_h2) against the dense matrix and the oracle.
+
+tetmag's c2-sized runs use H2Lib's H2 matrix (main/h2interface.c:315-399: cross approximation,
+then recompression into nested bases at 1e-5; matvec H2_mvp_sub, :77-95).  Here the hierarchical
+matrix built from the mesh is recompressed on the host into orthogonal nested row / column bases
+and couplings, and the device matvec runs the upward pass, the couplings and the downward pass.
+Checked: the demag field through the H2 matrix against the oracle's dense-matrix field at c4 size
+(FP64 copy within the compression tolerances, mixed copy within 1e-5), the H2 matrix against the
+hierarchical matrix it came from, and the storage it saves.
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from tetmag_b200 import meshgen, workloads
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).with_name("golden")
+MIXED_TOL = 1e-5
+
+
+def rel(a, b):
+    a, b = np.asarray(a).ravel(), np.asarray(b).ravel()
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.fixture(scope="module")
+def c4h2():
+    g = np.load(GOLDEN / "c4_field.npz")
+    w = workloads.c4_replica(replica=0)
+    mo, ctx = workloads.setup_context(w, tol=1e-13, maxiter=400, hmatrix="mesh", keep_dense=False)
+    m = meshgen.random_state(w.n, int(g["state_seed"]))
+    h_hier = np.empty(3 * w.n)
+    ctx.field_eval(m, hdem=h_hier)
+    ctx.bem_h2(eps_fp64=1e-9, eps_mixed=1e-6, kmax=64)
+    return g, w, mo, ctx, m, h_hier
+
+
+def test_h2_fp64_against_oracle_and_hierarchical(c4h2):
+    g, w, mo, ctx, m, h_hier = c4h2
+    ctx.set_precision(False)
+    ctx.set_solver_params(1e-13, 400)
+    h = np.empty(3 * w.n)
+    y = ctx.field_eval(m, hdem=h)
+    assert rel(h, h_hier) <= 1e-7          # recompression error on top of the hierarchical matrix
+    assert rel(h, g["hdem"]) <= 1e-6       # against the dense matrix of tetmag's arithmetic
+    assert rel(y, g["ydot"]) <= 1e-6
+
+
+def test_h2_mixed_against_oracle(c4h2):
+    g, w, mo, ctx, m, _ = c4h2
+    ctx.set_precision(True)
+    ctx.set_solver_params(1e-8, 400)
+    try:
+        h = np.empty(3 * w.n)
+        y = ctx.field_eval(m, hdem=h)
+        assert rel(h, g["hdem"]) <= MIXED_TOL
+        assert rel(y, g["ydot"]) <= MIXED_TOL
+    finally:
+        ctx.set_precision(False)
+        ctx.set_solver_params(1e-13, 400)
+
+
+def test_h2_storage_and_modes(c4h2):
+    g, w, mo, ctx, m, h_hier = c4h2
+    info = ctx.bem_h2_info()
+    hinfo = ctx.bem_info()
+    assert info["fp64"]["built"] == 1.0 and info["fp32"]["built"] == 1.0
+    assert 0 < info["fp64"]["max_rank_row"] <= 64 and 0 < info["fp32"]["max_rank_col"] <= 64
+    # the FP32 H2 copy streams less than the FP32 hierarchical matrix it replaces
+    assert info["fp32"]["bytes"] < hinfo["bytes_fp32"]
+    # switching back to the hierarchical matrix gives its field again, then H2 again
+    ctx.set_precision(False)
+    h = np.empty(3 * w.n)
+    ctx.set_bem_mode(1)
+    ctx.field_eval(m, hdem=h)
+    assert rel(h, h_hier) <= 1e-12
+    ctx.set_bem_mode(2)
+    ctx.field_eval(m, hdem=h)
+    assert rel(h, h_hier) <= 1e-7

@@ -194,9 +194,21 @@ class Context:
                                     int(kmax)))
         return self
 
-    def set_bem_mode(self, hierarchical: bool):
-        check(lib().tmb_set_bem_mode(self.h, 1 if hierarchical else 0))
+    def set_bem_mode(self, hierarchical):
+        """False / 0: dense; True / 1: hierarchical; 2: H2 (nested cluster bases)."""
+        check(lib().tmb_set_bem_mode(self.h, int(hierarchical)))
         return self
+
+    def bem_h2(self, eps_fp64: float = 1e-8, eps_mixed: float = 1e-6, kmax: int = 64):
+        """Recompress the hierarchical matrix into nested cluster bases (H2); selects the H2 matvec."""
+        check(lib().tmb_bem_h2(self.h, float(eps_fp64), float(eps_mixed), int(kmax)))
+        return self
+
+    def bem_h2_info(self) -> dict:
+        out = (C.c_double * 16)()
+        check(lib().tmb_bem_h2_info(self.h, out))
+        keys = ["built", "bytes", "coupling_bytes", "basis_bytes", "max_rank_row", "max_rank_col", "build_ms", "eps"]
+        return {p: {k: out[8 * w + i] for i, k in enumerate(keys)} for w, p in enumerate(("fp64", "fp32"))}
 
     def bem_info(self) -> dict:
         st = (C.c_double * 12)()

@@ -42,6 +42,7 @@ __global__ void __launch_bounds__(kBlock) k_local_field(SellView s, const V* __r
                                                         const V* __restrict__ tg0, const V* __restrict__ tg1,
                                                         const V* __restrict__ tg2, const V* __restrict__ gr0,
                                                         const V* __restrict__ gr1, LocalFieldArgs a) {
+  if (a.active && *a.active == 0) return;
   const int R = s.rep;
   const int g = blockIdx.x * blockDim.x + threadIdx.x;  // state row (node row of replica r)
   double torque = 0.0;
@@ -277,6 +278,102 @@ __global__ void k_rk_error(int n3, const double* __restrict__ y, const double* _
   if ((threadIdx.x & 31) == 0) atomicMax(err_bits, ordered_bits(r));
 }
 
+// --- device-side step control (one attempt of the Dormand-Prince loop per graph segment) -------
+__device__ __forceinline__ double bits_value(unsigned long long b) { return __longlong_as_double((long long)b); }
+
+__global__ void k_step_begin(StepCtl* c) {
+  if (c->done) {
+    c->active = 0;
+    return;
+  }
+  if (++c->attempts > c->max_attempts) {
+    c->status = 6;   // TMB_ERR_STEP
+    c->done = 1;
+    c->active = 0;
+    return;
+  }
+  double h = c->dt;
+  int last = 0;
+  if (c->t + h >= c->t1) {
+    h = c->t1 - c->t;
+    last = 1;
+  }
+  if (!(h > 0.0) || h < 1e-300) {
+    c->status = 6;
+    c->done = 1;
+    c->active = 0;
+    return;
+  }
+  c->h = h;
+  c->last = last;
+  c->err_bits = 0ull;
+  c->active = 1;
+}
+
+__global__ void k_rk_combine_dev(int n3, const double* __restrict__ y, Ptrs7 k, int nk, const StepCtl* __restrict__ c,
+                                 double* __restrict__ out) {
+  if (!c->active) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n3) return;
+  double acc = 0.0;
+  for (int j = 0; j < nk; ++j)
+    if (k.c[j] != 0.0) acc = fma(k.c[j], k.p[j][i], acc);
+  out[i] = fma(c->h, acc, y[i]);
+}
+
+__global__ void k_rk_error_dev(int n3, const double* __restrict__ y, const double* __restrict__ k1, Ptrs7 k, int nk,
+                               StepCtl* c) {
+  if (!c->active) return;
+  const double h = c->h;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double r = 0.0;
+  if (i < n3) {
+    double acc = 0.0;
+    for (int j = 0; j < nk; ++j)
+      if (k.c[j] != 0.0) acc = fma(k.c[j], k.p[j][i], acc);
+    const double sc = c->eps_abs + c->eps_rel * (fabs(y[i]) + h * fabs(k1[i]));
+    r = fabs(h * acc) / sc;
+  }
+  r = warp_max(r);
+  if ((threadIdx.x & 31) == 0) atomicMax(&c->err_bits, ordered_bits(r));
+}
+
+// accepted attempt (finite error <= 1): y <- y5 and, first-same-as-last, k1 <- k7
+__global__ void k_step_accept(int n3, const StepCtl* __restrict__ c, double* __restrict__ y,
+                              const double* __restrict__ y5, double* __restrict__ k1, const double* __restrict__ k7) {
+  if (!c->active) return;
+  const double err = bits_value(c->err_bits);
+  if (!(err <= 1.0)) return;   // NaN or > 1: rejected
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n3) return;
+  y[i] = y5[i];
+  k1[i] = k7[i];
+}
+
+// step-size control of odeint's controlled stepper (the host loop's arithmetic): reject with
+// dt = h max(0.9 err^-1/3, 0.2); accept, and grow dt = 0.9 h max(err, 5^-5)^-1/5 when err < 0.5
+__global__ void k_step_update(StepCtl* c, int rhs_per_attempt) {
+  if (!c->active) return;
+  c->rhs += rhs_per_attempt;
+  const double err = bits_value(c->err_bits), h = c->h;
+  if (!(err <= 1.0)) {
+    const double e = isfinite(err) ? err : 1e30;
+    c->dt = h * fmax(0.9 * pow(e, -1.0 / 3.0), 0.2);
+    c->rejected += 1;
+    return;
+  }
+  c->accepted += 1;
+  const double dtn = (err < 0.5) ? h * 0.9 * pow(fmax(err, pow(5.0, -5.0)), -1.0 / 5.0) : h;
+  if (c->last) {
+    c->t = c->t1;
+    c->dt = (h < c->dt) ? fmax(c->dt, dtn) : dtn;
+    c->done = 1;
+  } else {
+    c->t += h;
+    c->dt = dtn;
+  }
+}
+
 __global__ void k_fill(double* p, double v, size_t n) {
   const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i < n) p[i] = v;
@@ -299,7 +396,9 @@ template <typename V>
 __global__ void __launch_bounds__(kBlock) k_stt_add(SellView sv, const V* __restrict__ g0, const V* __restrict__ g1,
                                                     const V* __restrict__ g2, const double* __restrict__ m,
                                                     const double* __restrict__ eta, double alpha, double beta,
-                                                    double scale, double* __restrict__ ydot) {
+                                                    double scale, double* __restrict__ ydot,
+                                                    const int* __restrict__ active) {
+  if (active && *active == 0) return;
   const int R = sv.rep;
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= sv.n * R) return;
@@ -336,15 +435,16 @@ __global__ void __launch_bounds__(kBlock) k_stt_add(SellView sv, const V* __rest
 
 template <typename V>
 void launch_stt_add(const SellView& s, const V* g0, const V* g1, const V* g2, const double* m, const double* eta,
-                    double alpha, double beta, double scale, double* ydot, cudaStream_t st) {
+                    double alpha, double beta, double scale, double* ydot, cudaStream_t st, const int* active) {
   note_launch();
-  k_stt_add<V><<<grid_for(1LL * s.n * s.rep), kBlock, 0, st>>>(s, g0, g1, g2, m, eta, alpha, beta, scale, ydot);
+  k_stt_add<V><<<grid_for(1LL * s.n * s.rep), kBlock, 0, st>>>(s, g0, g1, g2, m, eta, alpha, beta, scale, ydot,
+                                                                active);
   TMB_CUDA(cudaGetLastError());
 }
 template void launch_stt_add<double>(const SellView&, const double*, const double*, const double*, const double*,
-                                     const double*, double, double, double, double*, cudaStream_t);
+                                     const double*, double, double, double, double*, cudaStream_t, const int*);
 template void launch_stt_add<float>(const SellView&, const float*, const float*, const float*, const double*,
-                                    const double*, double, double, double, double*, cudaStream_t);
+                                    const double*, double, double, double, double*, cudaStream_t, const int*);
 
 // Per-block partial sums of the energy terms (TheSimulation::calculateEnergies,
 // main/TheSimulation.cpp:385-396), state row g = i * R + r:
@@ -480,6 +580,43 @@ void launch_rk_error(int n3, const double* y, const double* k1, const double* co
   Ptrs7 P{};
   for (int j = 0; j < nk && j < 7; ++j) { P.p[j] = k[j]; P.c[j] = e[j]; }
   k_rk_error<<<grid_for(n3), kBlock, 0, st>>>(n3, y, k1, P, nk, h, eps_abs, eps_rel, err_bits);
+  TMB_CUDA(cudaGetLastError());
+}
+
+void launch_step_begin(StepCtl* c, cudaStream_t st) {
+  note_launch();
+  k_step_begin<<<1, 1, 0, st>>>(c);
+  TMB_CUDA(cudaGetLastError());
+}
+
+void launch_rk_combine_dev(int n3, const double* y, const double* const* k, const double* a, int nk,
+                           const StepCtl* c, double* out, cudaStream_t st) {
+  note_launch();
+  Ptrs7 P{};
+  for (int j = 0; j < nk && j < 7; ++j) { P.p[j] = k[j]; P.c[j] = a[j]; }
+  k_rk_combine_dev<<<grid_for(n3), kBlock, 0, st>>>(n3, y, P, nk, c, out);
+  TMB_CUDA(cudaGetLastError());
+}
+
+void launch_rk_error_dev(int n3, const double* y, const double* k1, const double* const* k, const double* e, int nk,
+                         StepCtl* c, cudaStream_t st) {
+  note_launch();
+  Ptrs7 P{};
+  for (int j = 0; j < nk && j < 7; ++j) { P.p[j] = k[j]; P.c[j] = e[j]; }
+  k_rk_error_dev<<<grid_for(n3), kBlock, 0, st>>>(n3, y, k1, P, nk, c);
+  TMB_CUDA(cudaGetLastError());
+}
+
+void launch_step_accept(int n3, const StepCtl* c, double* y, const double* y5, double* k1, const double* k7,
+                        cudaStream_t st) {
+  note_launch();
+  k_step_accept<<<grid_for(n3), kBlock, 0, st>>>(n3, c, y, y5, k1, k7);
+  TMB_CUDA(cudaGetLastError());
+}
+
+void launch_step_update(StepCtl* c, int rhs_per_attempt, cudaStream_t st) {
+  note_launch();
+  k_step_update<<<1, 1, 0, st>>>(c, rhs_per_attempt);
   TMB_CUDA(cudaGetLastError());
 }
 

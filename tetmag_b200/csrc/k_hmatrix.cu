@@ -608,6 +608,180 @@ void launch_h_matvec(const HMatView<T>& H, const double* u, double* y, T* xp, co
   TMB_CUDA(cudaGetLastError());
 }
 
+// ------------------------------------------------------------------------------------------
+// H2 matvec (nested cluster bases built by h2.cpp).  Coefficient vectors are FP64; basis,
+// transfer and coupling values are T.  Every kernel gives one warp to one cluster (ranks <= 64:
+// two coefficients per lane).
+// ------------------------------------------------------------------------------------------
+namespace {
+
+// column leaves: xh_l = W_l^T x_l (W_l row-major m x kc: lane j reads W[i * kc + j], coalesced)
+template <typename T>
+__global__ void k_h2_leaf_up(int nleaf, const int* __restrict__ leaves, const H2Node* __restrict__ node,
+                             const T* __restrict__ colb, const T* __restrict__ xp, double* __restrict__ xh) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= nleaf) return;
+  const H2Node c = node[leaves[w]];
+  if (c.kc == 0) return;
+  const T* W = colb + c.cl;
+  double a0 = 0.0, a1 = 0.0;
+  const bool two = lane + 32 < c.kc;
+  for (int i = 0; i < c.m; ++i) {
+    const double xi = double(xp[c.begin + i]);
+    if (lane < c.kc) a0 = fma(double(W[size_t(i) * c.kc + lane]), xi, a0);
+    if (two) a1 = fma(double(W[size_t(i) * c.kc + lane + 32]), xi, a1);
+  }
+  if (lane < c.kc) xh[c.xo + lane] = a0;
+  if (two) xh[c.xo + lane + 32] = a1;
+}
+
+// upward pass, one depth: xh_c = sum over children F_ch^T xh_ch (the transposed transfer of a
+// child is stored kc x kc_child column-major: lane j reads F[j + i * kc], coalesced)
+template <typename T>
+__global__ void k_h2_up(int count, const int* __restrict__ ids, const H2Node* __restrict__ node,
+                        const T* __restrict__ colb, double* __restrict__ xh) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= count) return;
+  const H2Node c = node[ids[w]];
+  if (c.child0 < 0 || c.kc == 0) return;
+  double a0 = 0.0, a1 = 0.0;
+  const bool two = lane + 32 < c.kc;
+  for (int s = 0; s < 2; ++s) {
+    const H2Node ch = node[s == 0 ? c.child0 : c.child1];
+    const T* F = colb + ch.ct;
+    for (int i = 0; i < ch.kc; ++i) {
+      const double xi = xh[ch.xo + i];
+      if (lane < c.kc) a0 = fma(double(F[size_t(i) * c.kc + lane]), xi, a0);
+      if (two) a1 = fma(double(F[size_t(i) * c.kc + lane + 32]), xi, a1);
+    }
+  }
+  if (lane < c.kc) xh[c.xo + lane] = a0;
+  if (two) xh[c.xo + lane + 32] = a1;
+}
+
+// couplings: yh_t = sum over the blocks of row cluster t of S_b xh_s (S_b kr x kc column-major)
+template <typename T>
+__global__ void k_h2_couple(int nruns, const H2Run* __restrict__ runs, const H2Blk* __restrict__ blk,
+                            const H2Node* __restrict__ node, const T* __restrict__ S, const double* __restrict__ xh,
+                            double* __restrict__ yh) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= nruns) return;
+  const H2Run r = runs[w];
+  const H2Node t = node[r.t];
+  double a0 = 0.0, a1 = 0.0;
+  const bool one = lane < t.kr, two = lane + 32 < t.kr;
+  for (int q = r.first; q < r.last; ++q) {
+    const H2Blk b = blk[q];
+    const H2Node s = node[b.s];
+    const T* Sq = S + b.so;
+#pragma unroll 4
+    for (int j = 0; j < s.kc; ++j) {
+      const double xj = xh[s.xo + j];
+      if (one) a0 = fma(double(Sq[size_t(j) * t.kr + lane]), xj, a0);
+      if (two) a1 = fma(double(Sq[size_t(j) * t.kr + lane + 32]), xj, a1);
+    }
+  }
+  if (one) yh[t.yo + lane] = a0;
+  if (two) yh[t.yo + lane + 32] = a1;
+}
+
+// downward pass, one depth: yh_c += E_c yh_parent (E_c kr x kr_parent column-major)
+template <typename T>
+__global__ void k_h2_down(int count, const int* __restrict__ ids, const H2Node* __restrict__ node,
+                          const T* __restrict__ rowb, double* __restrict__ yh) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= count) return;
+  const H2Node c = node[ids[w]];
+  if (c.parent < 0 || c.kr == 0 || c.child0 < 0) return;
+  const H2Node p = node[c.parent];
+  if (p.kr == 0) return;
+  const T* E = rowb + c.rt;
+  double a0 = 0.0, a1 = 0.0;
+  const bool one = lane < c.kr, two = lane + 32 < c.kr;
+  for (int j = 0; j < p.kr; ++j) {
+    const double yj = yh[p.yo + j];
+    if (one) a0 = fma(double(E[size_t(j) * c.kr + lane]), yj, a0);
+    if (two) a1 = fma(double(E[size_t(j) * c.kr + lane + 32]), yj, a1);
+  }
+  if (one) yh[c.yo + lane] += a0;
+  if (two) yh[c.yo + lane + 32] += a1;
+}
+
+// row leaves: y_l += V_l (yh_l + E_l yh_parent) (V_l m x kr column-major: lane i reads V[i + j m]);
+// the leaf's own share of its parent's coefficients is applied here instead of in k_h2_down
+template <typename T>
+__global__ void k_h2_leaf_down(int nleaf, const int* __restrict__ leaves, const H2Node* __restrict__ node,
+                               const T* __restrict__ rowb, const double* __restrict__ yh, double* __restrict__ y) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (w >= nleaf) return;
+  const H2Node c = node[leaves[w]];
+  if (c.kr == 0) return;
+  // coefficients of the leaf: its own couplings plus the transfer of the parent's
+  __shared__ double coef[8][64];
+  double* cf = coef[(threadIdx.x >> 5) & 7];
+  for (int i = lane; i < c.kr; i += 32) {
+    double a = yh[c.yo + i];
+    if (c.parent >= 0) {
+      const H2Node p = node[c.parent];
+      const T* E = rowb + c.rt;
+      for (int j = 0; j < p.kr; ++j) a = fma(double(E[size_t(j) * c.kr + i]), yh[p.yo + j], a);
+    }
+    cf[i] = a;
+  }
+  __syncwarp();
+  if (lane < c.m) {
+    const T* V = rowb + c.rl;
+    double a = 0.0;
+    for (int j = 0; j < c.kr; ++j) a = fma(double(V[size_t(j) * c.m + lane]), cf[j], a);
+    y[c.begin + lane] += a;
+  }
+}
+
+}  // namespace
+
+template <typename T>
+void launch_h2_matvec(const H2View<T>& H, const double* u, double* y, T* xp, const int* pos, int n, double* bdir,
+                      const std::vector<std::pair<int, int>>& up, const std::vector<std::pair<int, int>>& down,
+                      cudaStream_t st) {
+  const int wpb = 8;   // warps per 256-thread block
+  auto blocks = [&](int warps) { return unsigned((warps + wpb - 1) / wpb); };
+  note_launch();
+  k_h_gather<T><<<grid_for(H.nb), kBlock, 0, st>>>(H.nb, u, H.gidx, xp);
+  note_launch();
+  k_h_near<T><<<H.nrows, 256, 0, st>>>(H.near_rows, H.near, H.D, xp, y);
+  TMB_CUDA(cudaMemsetAsync(H.yh, 0, sizeof(double) * size_t(H.nyh), st));
+  if (H.nleaf > 0) {
+    note_launch();
+    k_h2_leaf_up<T><<<blocks(H.nleaf), 256, 0, st>>>(H.nleaf, H.leaves, H.node, H.colb, xp, H.xh);
+  }
+  for (const auto& d : up) {
+    note_launch();
+    k_h2_up<T><<<blocks(d.second), 256, 0, st>>>(d.second, H.lvl_nodes + d.first, H.node, H.colb, H.xh);
+  }
+  if (H.nruns > 0) {
+    note_launch();
+    k_h2_couple<T><<<blocks(H.nruns), 256, 0, st>>>(H.nruns, H.runs, H.blk, H.node, H.S, H.xh, H.yh);
+  }
+  for (const auto& d : down) {
+    note_launch();
+    k_h2_down<T><<<blocks(d.second), 256, 0, st>>>(d.second, H.lvl_nodes + d.first, H.node, H.rowb, H.yh);
+  }
+  if (H.nleaf > 0) {
+    note_launch();
+    k_h2_leaf_down<T><<<blocks(H.nleaf), 256, 0, st>>>(H.nleaf, H.leaves, H.node, H.rowb, H.yh, y);
+  }
+  note_launch();
+  k_h_dirichlet<<<grid_for(n), kBlock, 0, st>>>(n, pos, y, bdir);
+  TMB_CUDA(cudaGetLastError());
+}
+
+template void launch_h2_matvec<double>(const H2View<double>&, const double*, double*, double*, const int*, int,
+                                       double*, const std::vector<std::pair<int, int>>&,
+                                       const std::vector<std::pair<int, int>>&, cudaStream_t);
+template void launch_h2_matvec<float>(const H2View<float>&, const double*, double*, float*, const int*, int,
+                                      double*, const std::vector<std::pair<int, int>>&,
+                                      const std::vector<std::pair<int, int>>&, cudaStream_t);
+
 template void launch_h_compact<double>(int, const HBlockDev*, const double*, const double*, const long long*,
                                        const long long*, const int*, double*, double*, cudaStream_t);
 template void launch_h_compact<float>(int, const HBlockDev*, const double*, const double*, const long long*,

@@ -416,6 +416,11 @@ struct Ctx {
     DevArray<long long> uoff[2], voff[2], toff[2];
     DevArray<HTerm> termd[2];             // per-term descriptors of the far-field product
     DevArray<double> tval;                // the terms' values, one matvec at a time
+    // the partition and the FP64 factors' offsets and ranks (host), for the H2 recompression
+    HPartition part;
+    std::vector<long long> huoff, hvoff;
+    std::vector<int> hrank;
+    long long hsu = 0, hsv = 0;
     // boundary geometry in cluster order when the matrix was built from the mesh
     bool from_mesh = false;
     int ntri = 0;
@@ -423,8 +428,27 @@ struct Ctx {
     DevArray<int> gtri, gadj_ptr;
     DevArray<int2> gadj;
   } H;
+  // H2 matrix: nested cluster bases recompressed from H's admissible blocks (h2.cpp); one per
+  // precision ([0] FP64 for the plain path, [1] FP32 for the mixed path); the near field is H's
+  struct H2Mat {
+    bool built = false;
+    int nleaf = 0, nruns = 0, nlevels = 0, max_kr = 0, max_kc = 0;
+    long long ncoef_r = 0, ncoef_c = 0;
+    double bytes = 0.0, coupling_bytes = 0.0, basis_bytes = 0.0, ms = 0.0, eps = 0.0;
+    DevArray<H2Node> node;
+    DevArray<int> leaves, lvl_nodes;
+    DevArray<H2Run> runs;
+    DevArray<H2Blk> blk;
+    DevArray<double> xh, yh;
+    DevArray<double> rowb64, colb64, S64;
+    DevArray<float> rowb32, colb32, S32;
+    std::vector<std::pair<int, int>> up, down;
+  } H2[2];
+  void h2_build(double eps_fp64, double eps_mixed, int kmax);
+  template <typename T>
+  H2View<T> h2_view(int which) const;
   HSource h_source() const;
-  int bem_mode = 0;  // 0 dense, 1 hierarchical
+  int bem_mode = 0;  // 0 dense, 1 hierarchical, 2 H2
   void h_compress(const double* bxyz, const double* bnrm, int leaf, double eta, double eps_mixed, double eps_fp64,
                   int kmax, bool keep_dense, const MeshHost* mesh = nullptr);
   void h_verify(double* block_out, double* out);
@@ -452,6 +476,9 @@ struct Ctx {
     bits.alloc(4);
   }
   ~Ctx() {
+    drop_step_graphs();
+    if (ctl_d) cudaFree(ctl_d);
+    if (ctl_h) cudaFreeHost(ctl_h);
     neu.reset();
     dir.reset();
     if (bits_h) cudaFreeHost(bits_h);
@@ -478,6 +505,25 @@ struct Ctx {
   DevArray<double> ebuf[2], epart;
   int integrate_segment(double*& y, double*& yalt, double t0, double t1, double& dt, double eps_abs,
                         double eps_rel, double* stats);
+  // the same loop with the step control on the device: kStepAttempts attempts per CUDA graph
+  // launch, the host polls the control block once per launch instead of once per step
+  static constexpr int kStepAttempts = 8;
+  StepCtl* ctl_d = nullptr;
+  StepCtl* ctl_h = nullptr;
+  cudaGraphExec_t step_graph[2] = {nullptr, nullptr};
+  std::vector<unsigned char> step_sig[2];
+  bool device_steps = true;
+  long long step_nodes = 0;
+  void integrate_segment_dev(double* y, double* yalt, double t0, double t1, double& dt, double eps_abs,
+                             double eps_rel, double* stats);
+  cudaGraphExec_t step_graph_for(double* y, double* yalt);
+  void drop_step_graphs() {
+    for (auto& g : step_graph)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+  }
   int relax(double* m_dev, double duration_ps, double segment_ps, double eps_abs, double eps_rel, double* stats);
   // Fixed-step integration with the full field at every stage, and its discrete adjoint.
   std::vector<double> bz;               // Bz(t) samples [T], uniformly spaced over [bz_t0, bz_t1] ps
@@ -1135,7 +1181,18 @@ void Ctx::demag(const double* m) {
   prof.begin(4, st, 0.0);
   neu->solve(rhs.p, precision);
   prof.end(st);
-  if (bem_mode == 1) {
+  if (bem_mode == 2) {
+    // H2 matvec (nested bases) in cluster order, scattered straight into the Dirichlet load
+    const int w = f64 ? 0 : 1;
+    prof.begin(3, st, H2[w].bytes + B * (sv + 8 + 8));
+    if (f64)
+      launch_h2_matvec<double>(h2_view<double>(0), neu->x.p, H.y.p, H.xp64.p, H.pos.p, n, bdir.p, H2[0].up,
+                               H2[0].down, st);
+    else
+      launch_h2_matvec<float>(h2_view<float>(1), neu->x.p, H.y.p, H.xp32.p, H.pos.p, n, bdir.p, H2[1].up,
+                              H2[1].down, st);
+    prof.end(st);
+  } else if (bem_mode == 1) {
     // hierarchical matvec in cluster order, scattered straight into the Dirichlet load
     const int w = f64 ? 0 : 1;
     prof.begin(3, st, H.bytes[w] + B * (sv + 8 + 8));
@@ -1327,6 +1384,8 @@ void Ctx::h_compress(const double* bxyz, const double* bnrm, int leaf, double et
     farb.push_back(b);
   }
   H = HMat{};
+  H2[0] = H2Mat{};
+  H2[1] = H2Mat{};
   H.nnear = int(nearb.size());
   H.nfar = int(farb.size());
   H.nrows = int(rows.size());
@@ -1449,6 +1508,11 @@ void Ctx::h_compress(const double* bxyz, const double* bnrm, int leaf, double et
       H.uoff[w].upload(uo, st);
       H.voff[w].upload(vo, st);
       if (w == 0) {
+        H.huoff = uo;
+        H.hvoff = vo;
+        H.hrank = rk;
+        H.hsu = su;
+        H.hsv = sv;
         H.U64.alloc(size_t(std::max(su, 1LL)));
         H.V64.alloc(size_t(std::max(sv, 1LL)));
         launch_h_compact<double>(H.nfar, H.farb.p, Us.p, Vs.p, H.uoff[0].p, H.voff[0].p, H.rank[0].p, H.U64.p,
@@ -1472,6 +1536,7 @@ void Ctx::h_compress(const double* bxyz, const double* bnrm, int leaf, double et
     H.max_rank = std::max(H.max_rank, ranks[size_t(3) * q]);
   }
   H.ranks = ranks;
+  H.part = std::move(P);
   H.y.alloc(nb);
   // four zero entries past the end: the padded tail of a V row meets them
   H.xp64.alloc(size_t(nb) + 4);
@@ -1487,6 +1552,191 @@ void Ctx::h_compress(const double* bxyz, const double* bnrm, int leaf, double et
     Bf.reset();
   }
   H.ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// H2 recompression of the hierarchical matrix's admissible blocks (FP64 factors), once per
+// precision: eps_fp64 for the plain path, eps_mixed for the mixed path (stored in FP32).
+void Ctx::h2_build(double eps_fp64, double eps_mixed, int kmax) {
+  if (!H.built) throw Error(TMB_ERR_STATE, "tmb_bem_h2: no hierarchical matrix built");
+  if (!(eps_fp64 > 0.0) || !(eps_mixed > 0.0) || kmax < 1 || kmax > 64)
+    throw Error(TMB_ERR_ARG, "tmb_bem_h2: tolerances must be positive, rank cap in 1..64");
+  cudaStream_t st = stream;
+  const HPartition& P = H.part;
+  const int nf = int(P.far.size());
+  // the FP64 factors on the host
+  std::vector<double> hU(size_t(std::max(H.hsu, 1LL))), hV(size_t(std::max(H.hsv, 1LL)));
+  if (nf > 0) {
+    TMB_CUDA(cudaMemcpyAsync(hU.data(), H.U64.p, sizeof(double) * size_t(H.hsu), cudaMemcpyDeviceToHost, st));
+    TMB_CUDA(cudaMemcpyAsync(hV.data(), H.V64.p, sizeof(double) * size_t(H.hsv), cudaMemcpyDeviceToHost, st));
+    sync();
+  }
+  H2Factors F;
+  F.U.resize(nf);
+  F.V.resize(nf);
+  F.ldu.resize(nf);
+  F.ldv.resize(nf);
+  F.rank = H.hrank;
+  for (int q = 0; q < nf; ++q) {
+    const HCluster& ct = P.clusters[P.far[q].first];
+    const HCluster& cs = P.clusters[P.far[q].second];
+    F.U[q] = hU.data() + H.huoff[q];
+    F.V[q] = hV.data() + H.hvoff[q];
+    F.ldu[q] = pad4(ct.end - ct.begin);
+    F.ldv[q] = pad4(cs.end - cs.begin);
+  }
+  const size_t nc = P.clusters.size();
+  // depth of every cluster, leaves, non-leaf clusters by depth
+  std::vector<int> depth(nc, 0), parent(nc, -1);
+  for (size_t c = 0; c < nc; ++c)
+    for (int ch : P.clusters[c].child)
+      if (ch >= 0) parent[ch] = int(c);
+  std::vector<int> order{0};
+  for (size_t i = 0; i < order.size(); ++i)
+    for (int ch : P.clusters[order[i]].child)
+      if (ch >= 0) {
+        depth[ch] = depth[order[i]] + 1;
+        order.push_back(ch);
+      }
+  const int maxd = *std::max_element(depth.begin(), depth.end());
+  std::vector<int> leaves;
+  std::vector<std::vector<int>> bydepth(maxd + 1);
+  for (size_t c = 0; c < nc; ++c) {
+    if (P.clusters[c].child[0] < 0) leaves.push_back(int(c));
+    else bydepth[depth[c]].push_back(int(c));
+  }
+  for (int w = 0; w < 2; ++w) {
+    const auto t0 = std::chrono::steady_clock::now();
+    H2Host Hh;
+    h2_build_host(P, F, w == 0 ? eps_fp64 : eps_mixed, kmax, Hh);
+    H2Mat& M = H2[w];
+    M = H2Mat{};
+    M.eps = w == 0 ? eps_fp64 : eps_mixed;
+    std::vector<H2Node> nodes(nc);
+    std::vector<double> rowb, colb, S;
+    int xo = 0, yo = 0;
+    for (size_t c = 0; c < nc; ++c) {
+      const HCluster& C = P.clusters[c];
+      H2Node& d = nodes[c];
+      d.begin = C.begin;
+      d.m = C.end - C.begin;
+      d.kr = Hh.row.k[c];
+      d.kc = Hh.col.k[c];
+      d.parent = parent[c];
+      d.child0 = C.child[0];
+      d.child1 = C.child[1];
+      d.xo = xo;
+      d.yo = yo;
+      xo += d.kc;
+      yo += d.kr;
+      M.max_kr = std::max(M.max_kr, d.kr);
+      M.max_kc = std::max(M.max_kc, d.kc);
+      d.rl = d.rt = d.cl = d.ct = -1;
+      if (C.child[0] < 0) {
+        d.rl = (long long)rowb.size();
+        rowb.insert(rowb.end(), Hh.row.leaf_basis[c].begin(), Hh.row.leaf_basis[c].end());   // m x kr col-major
+        d.cl = (long long)colb.size();
+        const std::vector<double>& Wc = Hh.col.leaf_basis[c];                                  // m x kc col-major
+        for (int i = 0; i < d.m; ++i)
+          for (int j = 0; j < d.kc; ++j) colb.push_back(Wc[i + size_t(j) * d.m]);              // -> row-major
+      }
+      if (parent[c] >= 0) {
+        d.rt = (long long)rowb.size();
+        rowb.insert(rowb.end(), Hh.row.transfer[c].begin(), Hh.row.transfer[c].end());       // kr x kr_p
+        d.ct = (long long)colb.size();
+        const int kp = Hh.col.k[parent[c]];
+        const std::vector<double>& Fc = Hh.col.transfer[c];                                    // kc x kp col-major
+        for (int i = 0; i < d.kc; ++i)
+          for (int j = 0; j < kp; ++j) colb.push_back(Fc[i + size_t(j) * d.kc]);              // -> kp x kc col-major
+      }
+    }
+    M.ncoef_c = xo;
+    M.ncoef_r = yo;
+    std::vector<H2Run> runs;
+    std::vector<H2Blk> blks(nf);
+    for (int q = 0; q < nf; ++q) {
+      blks[q].s = P.far[q].second;
+      blks[q].so = (long long)S.size();
+      S.insert(S.end(), Hh.coupling[q].begin(), Hh.coupling[q].end());
+      if (runs.empty() || runs.back().t != P.far[q].first) runs.push_back(H2Run{P.far[q].first, q, q + 1});
+      else runs.back().last = q + 1;
+    }
+    std::vector<int> lvl;
+    for (int dd = maxd; dd >= 0; --dd) {           // upward: deepest first
+      int cnt = 0;
+      for (int c : bydepth[dd]) cnt += nodes[c].kc > 0;
+      if (cnt > 0) M.up.emplace_back(int(lvl.size()), int(bydepth[dd].size()));
+      if (cnt > 0) lvl.insert(lvl.end(), bydepth[dd].begin(), bydepth[dd].end());
+    }
+    for (int dd = 1; dd <= maxd; ++dd) {           // downward: root first
+      int cnt = 0;
+      for (int c : bydepth[dd]) cnt += nodes[c].kr > 0 && nodes[parent[c]].kr > 0;
+      if (cnt > 0) M.down.emplace_back(int(lvl.size()), int(bydepth[dd].size()));
+      if (cnt > 0) lvl.insert(lvl.end(), bydepth[dd].begin(), bydepth[dd].end());
+    }
+    M.nleaf = int(leaves.size());
+    M.nruns = int(runs.size());
+    M.nlevels = maxd + 1;
+    M.node.upload(nodes, st);
+    M.leaves.upload(leaves, st);
+    M.lvl_nodes.upload(lvl, st);
+    M.runs.upload(runs, st);
+    M.blk.upload(blks, st);
+    M.xh.alloc(size_t(std::max(xo, 1)));
+    M.yh.alloc(size_t(std::max(yo, 1)));
+    const double vs = w == 0 ? 8.0 : 4.0;
+    if (w == 0) {
+      M.rowb64.upload(rowb, st);
+      M.colb64.upload(colb, st);
+      M.S64.upload(S, st);
+    } else {
+      std::vector<float> r(rowb.begin(), rowb.end()), c2(colb.begin(), colb.end()), s2(S.begin(), S.end());
+      M.rowb32.upload(r, st);
+      M.colb32.upload(c2, st);
+      M.S32.upload(s2, st);
+    }
+    M.coupling_bytes = double(S.size()) * vs;
+    M.basis_bytes = double(rowb.size() + colb.size()) * vs;
+    const double near_bytes = H.bytes[w] > 0 ? double(H.D64.n) * vs : 0.0;
+    M.bytes = near_bytes + M.coupling_bytes + M.basis_bytes + double(nc) * sizeof(H2Node) +
+              double(nf) * sizeof(H2Blk) + double(runs.size()) * sizeof(H2Run) + 16.0 * (xo + yo);
+    sync();
+    M.built = true;
+    M.ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+  bem_mode = 2;
+}
+
+template <typename T>
+H2View<T> Ctx::h2_view(int w) const {
+  const H2Mat& M = H2[w];
+  H2View<T> v;
+  v.nb = nb;
+  v.nleaf = M.nleaf;
+  v.nruns = M.nruns;
+  v.gidx = H.gidx.p;
+  v.nrows = H.nrows;
+  v.near_rows = H.rows.p;
+  v.near = H.nearb.p;
+  v.node = M.node.p;
+  v.leaves = M.leaves.p;
+  v.lvl_nodes = M.lvl_nodes.p;
+  v.runs = M.runs.p;
+  v.blk = M.blk.p;
+  v.xh = const_cast<double*>(M.xh.p);
+  v.yh = const_cast<double*>(M.yh.p);
+  v.nyh = M.ncoef_r;
+  if constexpr (sizeof(T) == 8) {
+    v.D = H.D64.p;
+    v.rowb = M.rowb64.p;
+    v.colb = M.colb64.p;
+    v.S = M.S64.p;
+  } else {
+    v.D = H.D32.p;
+    v.rowb = M.rowb32.p;
+    v.colb = M.colb32.p;
+    v.S = M.S32.p;
+  }
+  return v;
 }
 
 HSource Ctx::h_source() const {
@@ -1605,6 +1855,7 @@ void Ctx::upload_extra() {
 
 LocalFieldArgs Ctx::local_args(const double* m, double* ydot, double* hout, unsigned long long* tq) const {
   LocalFieldArgs a;
+  std::memset(static_cast<void*>(&a), 0, sizeof a);   // padding too: the step graphs compare these bytes
   a.n = n;
   a.m = m;
   a.hfix = hfix.p;
@@ -1814,6 +2065,106 @@ int Ctx::integrate_segment(double*& y, double*& yalt, double t0, double t1, doub
   return TMB_OK;
 }
 
+// Signature of what a captured step graph depends on: buffers, precision, the local field's
+// arguments (material arrays, DMI form, extra terms) and the spin-transfer term.
+static void push_bytes(std::vector<unsigned char>& v, const void* p, size_t n) {
+  const unsigned char* b = static_cast<const unsigned char*>(p);
+  v.insert(v.end(), b, b + n);
+}
+
+cudaGraphExec_t Ctx::step_graph_for(double* y, double* yalt) {
+  const int n3 = 3 * nr();
+  std::vector<unsigned char> sig;
+  LocalFieldArgs a = local_args(ytmp.p, kst[1].p, nullptr, nullptr);
+  push_bytes(sig, &a, sizeof a);
+  const void* ptrs[] = {y, yalt, ytmp.p, kst[0].p, kst[1].p, kst[2].p, kst[3].p, kst[4].p, kst[5].p, kst[6].p,
+                        ctl_d, stt_eta.p, pat.soff.p, K.p, Kf.p};
+  push_bytes(sig, ptrs, sizeof ptrs);
+  const double vals[] = {double(n3), double(precision), double(has_stt), stt_beta, stt_scale, alpha};
+  push_bytes(sig, vals, sizeof vals);
+  const int w = precision == TMB_FP64 ? 0 : 1;
+  if (step_graph[w] && step_sig[w] == sig) return step_graph[w];
+  if (step_graph[w]) {
+    cudaGraphExecDestroy(step_graph[w]);
+    step_graph[w] = nullptr;
+  }
+  cudaStream_t st = stream;
+  cudaGraph_t graph = nullptr;
+  const long long before = launch_count();
+  TMB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  try {
+    const double* kp[7];
+    for (int j = 0; j < 7; ++j) kp[j] = kst[j].p;
+    for (int q = 0; q < kStepAttempts; ++q) {
+      launch_step_begin(ctl_d, st);
+      for (int s = 1; s < 7; ++s) {
+        double* dst = (s == 6) ? yalt : ytmp.p;
+        launch_rk_combine_dev(n3, y, kp, kDpA[s], s, ctl_d, dst, st);
+        LocalFieldArgs la = local_args(dst, kst[s].p, nullptr, nullptr);
+        la.active = &ctl_d->active;
+        const SellView S = pat.view(rep);
+        if (precision == TMB_FP64)
+          launch_local_field<double>(S, K.p, tg[0].p, tg[1].p, tg[2].p, g[0].p, g[1].p, la, st);
+        else
+          launch_local_field<float>(S, Kf.p, tgf[0].p, tgf[1].p, tgf[2].p, gf[0].p, gf[1].p, la, st);
+        if (has_stt) {
+          if (precision == TMB_FP64)
+            launch_stt_add<double>(S, g[0].p, g[1].p, g[2].p, dst, stt_eta.p, alpha, stt_beta, stt_scale, kst[s].p,
+                                   st, &ctl_d->active);
+          else
+            launch_stt_add<float>(S, gf[0].p, gf[1].p, gf[2].p, dst, stt_eta.p, alpha, stt_beta, stt_scale,
+                                  kst[s].p, st, &ctl_d->active);
+        }
+      }
+      launch_rk_error_dev(n3, y, kst[0].p, kp, kDpE, 7, ctl_d, st);
+      launch_step_accept(n3, ctl_d, y, yalt, kst[0].p, kst[6].p, st);
+      launch_step_update(ctl_d, 6, st);
+    }
+  } catch (...) {
+    cudaStreamEndCapture(st, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  TMB_CUDA(cudaStreamEndCapture(st, &graph));
+  step_nodes = launch_count() - before;
+  note_launches(-step_nodes);  // captured, not launched
+  const cudaError_t e = cudaGraphInstantiate(&step_graph[w], graph, 0);
+  cudaGraphDestroy(graph);
+  TMB_CUDA(e);
+  step_sig[w] = sig;
+  return step_graph[w];
+}
+
+void Ctx::integrate_segment_dev(double* y, double* yalt, double t0, double t1, double& dt, double eps_abs,
+                                double eps_rel, double* stats) {
+  cudaStream_t st = stream;
+  if (!ctl_d) TMB_CUDA(cudaMalloc(&ctl_d, sizeof(StepCtl)));
+  if (!ctl_h) TMB_CUDA(cudaMallocHost(&ctl_h, sizeof(StepCtl)));
+  local(y, kst[0].p, nullptr, nullptr);   // first same as last: k1 of the first attempt
+  stats[2] += 1;
+  std::memset(ctl_h, 0, sizeof(StepCtl));
+  ctl_h->t = t0;
+  ctl_h->t1 = t1;
+  ctl_h->dt = dt;
+  ctl_h->eps_abs = eps_abs;
+  ctl_h->eps_rel = eps_rel;
+  ctl_h->max_attempts = 50000000LL;
+  TMB_CUDA(cudaMemcpyAsync(ctl_d, ctl_h, sizeof(StepCtl), cudaMemcpyHostToDevice, st));
+  cudaGraphExec_t gx = step_graph_for(y, yalt);
+  for (;;) {
+    TMB_CUDA(cudaGraphLaunch(gx, st));
+    note_launches(step_nodes);
+    TMB_CUDA(cudaMemcpyAsync(ctl_h, ctl_d, sizeof(StepCtl), cudaMemcpyDeviceToHost, st));
+    sync();
+    if (ctl_h->done) break;
+  }
+  if (ctl_h->status != 0) throw Error(TMB_ERR_STEP, "integrator step size underflow or step cap");
+  stats[0] += double(ctl_h->accepted);
+  stats[1] += double(ctl_h->rejected);
+  stats[2] += double(ctl_h->rhs);
+  dt = ctl_h->dt;
+}
+
 int Ctx::relax(double* m, double duration_ps, double segment_ps, double eps_abs, double eps_rel, double* stats) {
   require_mesh();
   require_material();
@@ -1839,7 +2190,8 @@ int Ctx::relax(double* m, double duration_ps, double segment_ps, double eps_abs,
       stats[5] += dir->last_iters;
     }
     const double seg = std::min(segment_ps, duration_ps - t_ps);
-    integrate_segment(y, yalt, t_ps * ts, (t_ps + seg) * ts, dt, eps_abs, eps_rel, stats);
+    if (device_steps && !prof.on) integrate_segment_dev(y, yalt, t_ps * ts, (t_ps + seg) * ts, dt, eps_abs, eps_rel, stats);
+    else integrate_segment(y, yalt, t_ps * ts, (t_ps + seg) * ts, dt, eps_abs, eps_rel, stats);
     launch_normalize(nr(), y, st);
     t_ps += seg;
     stats[8] += 1;
@@ -2509,9 +2861,11 @@ int tmb_bem_build_h(tmb_ctx* ctx, const tmb_mesh* mesh, int leaf, double eta, do
 }
 
 int tmb_set_bem_mode(tmb_ctx* ctx, int mode) {
-  TMB_CHECK_ARG(ctx && (mode == 0 || mode == 1), "tmb_set_bem_mode: mode is 0 (dense) or 1 (hierarchical)");
+  TMB_CHECK_ARG(ctx && (mode >= 0 && mode <= 2), "tmb_set_bem_mode: mode is 0 (dense), 1 (hierarchical) or 2 (H2)");
   Ctx& c = *ctx->c;
   if (mode == 1 && !c.H.built) return fail(TMB_ERR_STATE, "tmb_set_bem_mode: no hierarchical matrix built");
+  if (mode == 2 && !(c.H2[0].built && c.H2[1].built))
+    return fail(TMB_ERR_STATE, "tmb_set_bem_mode: no H2 matrix built (tmb_bem_h2)");
   if (mode == 0 && (!c.Bd.p || !c.Bf.p)) return fail(TMB_ERR_STATE, "tmb_set_bem_mode: the dense matrix was released");
   c.bem_mode = mode;
   return TMB_OK;
@@ -2533,6 +2887,31 @@ int tmb_bem_info(tmb_ctx* ctx, double* out) {
   out[9] = H.max_rank;
   out[10] = H.ms;
   out[11] = H.built ? 1.0 : 0.0;
+  return TMB_OK;
+}
+
+int tmb_bem_h2(tmb_ctx* ctx, double eps_fp64, double eps_mixed, int kmax) {
+  TMB_CHECK_ARG(ctx, "tmb_bem_h2: null context");
+  TMB_API_BEGIN
+  ctx->c->h2_build(eps_fp64, eps_mixed, kmax);
+  TMB_API_END
+}
+
+int tmb_bem_h2_info(tmb_ctx* ctx, double* out) {
+  TMB_CHECK_ARG(ctx && out, "tmb_bem_h2_info: null argument");
+  const Ctx& c = *ctx->c;
+  for (int w = 0; w < 2; ++w) {
+    const auto& M = c.H2[w];
+    double* o = out + 8 * w;
+    o[0] = M.built ? 1.0 : 0.0;
+    o[1] = M.bytes;
+    o[2] = M.coupling_bytes;
+    o[3] = M.basis_bytes;
+    o[4] = M.max_kr;
+    o[5] = M.max_kc;
+    o[6] = M.ms;
+    o[7] = M.eps;
+  }
   return TMB_OK;
 }
 

@@ -19,6 +19,7 @@
 #include <stdexcept>
 #include <string>
 #include <utility>
+#include <vector>
 
 namespace tmb {
 
@@ -83,7 +84,31 @@ struct LocalFieldArgs {
   double* ydot;             // 3N out, may be null
   double* hout;             // 3N out (total field), may be null
   unsigned long long* torque_bits;  // max |m x H| (ordered bits), may be null
+  const int* active = nullptr;  // device flag: the kernel does nothing while it is 0 (null: always runs)
 };
+
+// Step control of the device-side Dormand-Prince loop (one per context, device memory): the
+// host sets t, t1, dt and the tolerances per segment, the graph of step attempts updates the rest.
+struct StepCtl {
+  double t, t1, dt, h;               // time, segment end, proposed step, step of this attempt
+  double eps_abs, eps_rel;
+  unsigned long long err_bits;       // scaled error of this attempt (ordered bits of a double)
+  int active;                        // this attempt runs (set by k_step_begin)
+  int last;                          // this attempt ends the segment
+  int done;                          // the segment is finished (or failed): later attempts do nothing
+  int status;                        // 0, or TMB_ERR_STEP on step-size underflow / attempt cap
+  long long accepted, rejected, rhs, attempts, max_attempts;
+};
+// one attempt's kernels: begin (h, last), stage combination y + h sum a_j k_j (h from the control
+// block), error reduction, acceptance copy (y <- y5, k1 <- k7 when accepted), update (t, dt, counts)
+void launch_step_begin(StepCtl* c, cudaStream_t st);
+void launch_rk_combine_dev(int n3, const double* y, const double* const* k, const double* a, int nk,
+                           const StepCtl* c, double* out, cudaStream_t st);
+void launch_rk_error_dev(int n3, const double* y, const double* k1, const double* const* k, const double* e, int nk,
+                         StepCtl* c, cudaStream_t st);
+void launch_step_accept(int n3, const StepCtl* c, double* y, const double* y5, double* k1, const double* k7,
+                        cudaStream_t st);
+void launch_step_update(StepCtl* c, int rhs_per_attempt, cudaStream_t st);
 
 template <typename V>
 void launch_local_field(const SellView& s, const V* K, const V* tg0, const V* tg1, const V* tg2, const V* gr0,
@@ -101,7 +126,8 @@ void launch_normalize(int n, double* m, cudaStream_t st);
 // Zhang-Li spin-transfer torque added to ydot (eta: 3N SoA per node)
 template <typename V>
 void launch_stt_add(const SellView& s, const V* g0, const V* g1, const V* g2, const double* m, const double* eta,
-                    double alpha, double beta, double scale, double* ydot, cudaStream_t st);
+                    double alpha, double beta, double scale, double* ydot, cudaStream_t st,
+                    const int* active = nullptr);
 // energy terms, R interleaved replicas: kEnergyTerms partial sums per block (see k_field.cu);
 // extra: cubic (raw Kc1, Kc2 [J/m^3], axes SoA 9N) and surface anisotropy (Ks * node area [J])
 struct EnergyExtra {
@@ -289,6 +315,56 @@ void launch_h_compact(int nblk, const HBlockDev* blk, const double* Us, const do
 template <typename T>
 void launch_h_matvec(const HMatView<T>& H, const double* u, double* y, T* xp, const int* pos, int n, double* bdir,
                      cudaStream_t st);
+
+// --- H2 matrix (nested cluster bases, h2.cpp) -----------------------------------------------
+// One cluster of the tree: position range, ranks of its row and column bases, tree links,
+// offsets of its coefficients (FP64 vectors xh, yh) and of its basis data (-1: none):
+//   rl  leaf row basis, m x kr column-major
+//   rt  row transfer E, kr x kr_parent column-major (the parent's basis restricted to this
+//       cluster is this cluster's basis times E)
+//   cl  leaf column basis, m x kc row-major
+//   ct  column transfer, stored transposed: kc_parent x kc column-major
+struct H2Node {
+  int begin, m, kr, kc;
+  int parent, child0, child1;
+  int xo, yo;
+  long long rl, rt, cl, ct;
+};
+struct H2Run {              // a row cluster and its admissible blocks [first, last)
+  int t, first, last;
+};
+struct H2Blk {              // admissible block: column cluster, coupling offset (kr_t x kc_s, column-major)
+  int s;
+  long long so;
+};
+template <typename T>
+struct H2View {
+  int nb = 0, nleaf = 0, nruns = 0;
+  const int* gidx = nullptr;
+  int nrows = 0;                           // near field: the H-matrix's dense leaf tiles
+  const HNearRow* near_rows = nullptr;
+  const HBlockDev* near = nullptr;
+  const T* D = nullptr;
+  const H2Node* node = nullptr;
+  const int* leaves = nullptr;             // leaf cluster ids
+  const int* lvl_nodes = nullptr;          // non-leaf cluster ids grouped by depth
+  const T* rowb = nullptr;
+  const T* colb = nullptr;
+  const H2Run* runs = nullptr;
+  const H2Blk* blk = nullptr;
+  const T* S = nullptr;
+  double* xh = nullptr;
+  double* yh = nullptr;
+  long long nyh = 0;
+};
+// the same product through the H2 matrix: near tiles, column basis upward pass, couplings, row
+// basis downward pass; up / down: host lists of the depths that have work (deepest first / root first)
+// up / down: (offset into lvl_nodes, count) of the clusters of each depth with work, in launch
+// order (deepest first for the upward pass, root first for the downward pass)
+template <typename T>
+void launch_h2_matvec(const H2View<T>& H, const double* u, double* y, T* xp, const int* pos, int n, double* bdir,
+                      const std::vector<std::pair<int, int>>& up, const std::vector<std::pair<int, int>>& down,
+                      cudaStream_t st);
 
 // --- discrete adjoint of the fixed-step integration (k_adjoint.cu) -------------------------
 struct AdjPreArgs {

@@ -117,6 +117,23 @@ struct HPartition {
 // bnrm (Nb x 3 node normals, may be null) makes faces of different orientation separate first
 void h_partition(const double* bxyz, const double* bnrm, int nb, int leaf, double eta, int max_block,
                  HPartition& P);
+// h2.cpp -- recompression of the admissible blocks into nested cluster bases (H2).
+struct H2Factors {                           // low-rank factors of P.far[q]: U (m x k), V (n x k)
+  std::vector<const double*> U, V;           // column-major
+  std::vector<int> ldu, ldv, rank;
+};
+struct H2Side {                              // cluster basis of one side (rows or columns)
+  std::vector<int> k;                        // rank per cluster
+  std::vector<std::vector<double>> leaf_basis;  // leaf clusters: |c| x k_c, column-major
+  std::vector<std::vector<double>> transfer;    // non-root clusters: k_c x k_parent, column-major
+};
+struct H2Host {
+  H2Side row, col;
+  std::vector<std::vector<double>> coupling;    // per admissible block: k_row x k_col, column-major
+};
+// eps: relative truncation of each cluster's total matrix (H2Lib's releucl mode); kmax: rank cap
+void h2_build_host(const HPartition& P, const H2Factors& F, double eps, int kmax, H2Host& out);
+
 void csr_transpose(const Csr& A, Csr& T);
 void csr_multiply(const Csr& A, const Csr& B, Csr& C);
 

@@ -211,11 +211,13 @@ WORKLOADS = {"c1": c1, "c2": c2, "c3": c3_dots, "c4": c4_replica, "c4x64": c4_ba
 
 def setup_context(w: Workload, device: int = 0, mixed: bool = False, tol: float = 1e-7, maxiter: int = 100,
                   mesh_ops=None, hmatrix: bool = False, keep_dense: bool = True, eps_mixed: float = 1e-6,
-                  eps_fp64: float = 1e-7, kmax: int = 64, normal_split: bool = True):
+                  eps_fp64: float = 1e-7, kmax: int = 64, normal_split: bool = True, h2=None):
     """MeshOps + Context with operators, device-assembled BEM (dense, optionally compressed to the
     hierarchical form with leaf 32 and eta 2), material and applied field.  hmatrix="mesh" builds
     the hierarchical matrix from the mesh boundary; the dense matrix is then assembled only when
-    keep_dense is set, in the far-field-accurate arithmetic the hierarchical matrix approximates."""
+    keep_dense is set, in the far-field-accurate arithmetic the hierarchical matrix approximates.
+    h2=(eps_fp64, eps_mixed) then recompresses the hierarchical matrix into nested cluster bases (H2)
+    and selects the H2 matvec."""
     from .api import Context, MeshOps
 
     mo = mesh_ops if mesh_ops is not None else MeshOps(w.mesh.xyz, w.mesh.tets)
@@ -237,6 +239,9 @@ def setup_context(w: Workload, device: int = 0, mixed: bool = False, tol: float 
         nrm = bd["node_normal"].reshape(3, -1).T[bn] if normal_split else None
         ctx.bem_compress(w.mesh.xyz[bn], bnormal=nrm, leaf=32, eta=2.0, eps_mixed=eps_mixed, eps_fp64=eps_fp64,
                          kmax=kmax, keep_dense=keep_dense)
+    if h2 is not None and hmatrix:
+        # h2: (eps_fp64, eps_mixed) of the recompression into nested cluster bases
+        ctx.bem_h2(eps_fp64=h2[0], eps_mixed=h2[1], kmax=64)
     Js, A, Ku, axis, D = w.material_arrays()
     ctx.set_material(Js, A, Ku=Ku, ku_axis=axis, D=D, alpha=w.alpha)
     if w.dmi_kind == "interfacial":
