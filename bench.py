@@ -67,13 +67,13 @@ def parse():
     return p.parse_args()
 
 
-H2_EPS = (1e-9, 1e-6)     # recompression tolerances of the FP64 and FP32 H2 copies
+H2_EPS = (1e-7, 1e-6)     # recompression tolerances of the FP64 and FP32 H2 copies
 
 
 def bem_for(args, workload: str) -> str:
     if args.bem != "auto":
         return args.bem
-    return "h2" if workload == "c2" else "dense"
+    return "hmatrix" if workload == "c2" else "dense"
 
 
 def peak_hbm():

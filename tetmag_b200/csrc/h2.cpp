@@ -10,8 +10,7 @@
 //
 //   row basis     for every row cluster t, the left singular vectors of the matrix of every
 //                 admissible block whose row cluster is t or an ancestor of t, restricted to the
-//                 rows of t, each block weighted by 1 / ||A_b||_F; kept down to eps times the
-//                 largest singular value.  A leaf basis is explicit (|t| x k_t); a parent's is
+//                 rows of t; kept down to eps times the largest singular value.  A leaf basis is explicit (|t| x k_t); a parent's is
 //                 [V_t1 E_t1; V_t2 E_t2], the transfers E from the singular vectors of the same
 //                 matrix projected onto the children's bases, so the Gram matrices of the
 //                 parents are (k_t1 + k_t2) square and the bases stay nested.
@@ -299,7 +298,10 @@ void h2_build_host(const HPartition& P, const H2Factors& F, double eps, int kmax
     double fro = 0.0;
     for (int i = 0; i < k; ++i)
       for (int j = 0; j < k; ++j) fro += a(i, j) * b(j, i);
-    w2[q] = fro > 0.0 ? 1.0 / fro : 0.0;
+    // unweighted total matrices (H2Lib's relative Euclidean truncation of the cluster's total
+    // matrix): weak far blocks may lose relatively more, their absolute error stays below eps
+    // times the cluster's largest singular value
+    w2[q] = fro > 0.0 ? 1.0 : 0.0;
     gU[q] = std::move(a);
     gV[q] = std::move(b);
   }

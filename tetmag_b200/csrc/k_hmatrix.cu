@@ -659,30 +659,42 @@ __global__ void k_h2_up(int count, const int* __restrict__ ids, const H2Node* __
   if (two) xh[c.xo + lane + 32] = a1;
 }
 
-// couplings: yh_t = sum over the blocks of row cluster t of S_b xh_s (S_b kr x kc column-major)
+// couplings: yh_t += S_b xh_s for every admissible block b = (t, s) (S_b kr x kc column-major);
+// one warp per block (row clusters own very different numbers of blocks: a warp per row cluster
+// left the largest clusters' warps running long after the rest), FP64 atomic adds into yh_t
 template <typename T>
-__global__ void k_h2_couple(int nruns, const H2Run* __restrict__ runs, const H2Blk* __restrict__ blk,
-                            const H2Node* __restrict__ node, const T* __restrict__ S, const double* __restrict__ xh,
-                            double* __restrict__ yh) {
+__global__ void __launch_bounds__(256) k_h2_couple(int nblk, const int* __restrict__ brow,
+                                                   const H2Blk* __restrict__ blk, const H2Node* __restrict__ node,
+                                                   const T* __restrict__ S, const double* __restrict__ xh,
+                                                   double* __restrict__ yh) {
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (w >= nruns) return;
-  const H2Run r = runs[w];
-  const H2Node t = node[r.t];
-  double a0 = 0.0, a1 = 0.0;
+  if (w >= nblk) return;
+  const H2Blk b = blk[w];
+  const H2Node t = node[brow[w]];
+  const H2Node s = node[b.s];
+  if (t.kr == 0 || s.kc == 0) return;
+  const T* Sq = S + b.so;
+  double a0 = 0.0, a1 = 0.0, c0 = 0.0, c1 = 0.0;
   const bool one = lane < t.kr, two = lane + 32 < t.kr;
-  for (int q = r.first; q < r.last; ++q) {
-    const H2Blk b = blk[q];
-    const H2Node s = node[b.s];
-    const T* Sq = S + b.so;
-#pragma unroll 4
-    for (int j = 0; j < s.kc; ++j) {
-      const double xj = xh[s.xo + j];
-      if (one) a0 = fma(double(Sq[size_t(j) * t.kr + lane]), xj, a0);
-      if (two) a1 = fma(double(Sq[size_t(j) * t.kr + lane + 32]), xj, a1);
+  int j = 0;
+  for (; j + 1 < s.kc; j += 2) {   // two independent accumulation chains
+    const double x0 = xh[s.xo + j], x1 = xh[s.xo + j + 1];
+    if (one) {
+      a0 = fma(double(Sq[size_t(j) * t.kr + lane]), x0, a0);
+      c0 = fma(double(Sq[size_t(j + 1) * t.kr + lane]), x1, c0);
+    }
+    if (two) {
+      a1 = fma(double(Sq[size_t(j) * t.kr + lane + 32]), x0, a1);
+      c1 = fma(double(Sq[size_t(j + 1) * t.kr + lane + 32]), x1, c1);
     }
   }
-  if (one) yh[t.yo + lane] = a0;
-  if (two) yh[t.yo + lane + 32] = a1;
+  if (j < s.kc) {
+    const double x0 = xh[s.xo + j];
+    if (one) a0 = fma(double(Sq[size_t(j) * t.kr + lane]), x0, a0);
+    if (two) a1 = fma(double(Sq[size_t(j) * t.kr + lane + 32]), x0, a1);
+  }
+  if (one) atomicAdd(yh + t.yo + lane, a0 + c0);
+  if (two) atomicAdd(yh + t.yo + lane + 32, a1 + c1);
 }
 
 // downward pass, one depth: yh_c += E_c yh_parent (E_c kr x kr_parent column-major)
@@ -758,9 +770,9 @@ void launch_h2_matvec(const H2View<T>& H, const double* u, double* y, T* xp, con
     note_launch();
     k_h2_up<T><<<blocks(d.second), 256, 0, st>>>(d.second, H.lvl_nodes + d.first, H.node, H.colb, H.xh);
   }
-  if (H.nruns > 0) {
+  if (H.nblk > 0) {
     note_launch();
-    k_h2_couple<T><<<blocks(H.nruns), 256, 0, st>>>(H.nruns, H.runs, H.blk, H.node, H.S, H.xh, H.yh);
+    k_h2_couple<T><<<blocks(H.nblk), 256, 0, st>>>(H.nblk, H.brow, H.blk, H.node, H.S, H.xh, H.yh);
   }
   for (const auto& d : down) {
     note_launch();

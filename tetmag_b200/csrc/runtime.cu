@@ -307,6 +307,7 @@ struct Solver {
   void precondition_rz(int precision, cudaStream_t st, bool first);
   int rc = 0;  // which of rbuf[0], rbuf[1] holds the current residual
   double nnz_fine = 0.0;
+
   void ctx_prof_begin(int id, cudaStream_t st, double bytes);
   void ctx_prof_end(cudaStream_t st);
   bool ctx_prof_on() const;
@@ -439,6 +440,7 @@ struct Ctx {
     DevArray<int> leaves, lvl_nodes;
     DevArray<H2Run> runs;
     DevArray<H2Blk> blk;
+    DevArray<int> brow;
     DevArray<double> xh, yh;
     DevArray<double> rowb64, colb64, S64;
     DevArray<float> rowb32, colb32, S32;
@@ -1681,6 +1683,11 @@ void Ctx::h2_build(double eps_fp64, double eps_mixed, int kmax) {
     M.lvl_nodes.upload(lvl, st);
     M.runs.upload(runs, st);
     M.blk.upload(blks, st);
+    {
+      std::vector<int> br(nf);
+      for (int q = 0; q < nf; ++q) br[q] = P.far[q].first;
+      M.brow.upload(br, st);
+    }
     M.xh.alloc(size_t(std::max(xo, 1)));
     M.yh.alloc(size_t(std::max(yo, 1)));
     const double vs = w == 0 ? 8.0 : 4.0;
@@ -1721,6 +1728,8 @@ H2View<T> Ctx::h2_view(int w) const {
   v.leaves = M.leaves.p;
   v.lvl_nodes = M.lvl_nodes.p;
   v.runs = M.runs.p;
+  v.nblk = int(M.blk.n);
+  v.brow = M.brow.p;
   v.blk = M.blk.p;
   v.xh = const_cast<double*>(M.xh.p);
   v.yh = const_cast<double*>(M.yh.p);

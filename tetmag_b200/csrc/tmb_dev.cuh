@@ -351,6 +351,8 @@ struct H2View {
   const T* rowb = nullptr;
   const T* colb = nullptr;
   const H2Run* runs = nullptr;
+  int nblk = 0;
+  const int* brow = nullptr;               // row cluster of every admissible block
   const H2Blk* blk = nullptr;
   const T* S = nullptr;
   double* xh = nullptr;
