@@ -58,6 +58,9 @@ def parse():
     p.add_argument("--sim-ps", type=float, default=2.0, help="simulated ps for the ns/hour figure")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--c5-steps", type=int, default=500, help="time steps of the adjoint workload (c5)")
+    p.add_argument("--c5-h", type=float, default=3.0,
+                   help="lattice spacing of the c5 disk in nm (3.0: 8,188 nodes; 1.75: 41,328 nodes, the "
+                        "configuration's 'about 40k')")
     p.add_argument("--bem", default="auto", choices=["auto", "h2", "hmatrix", "hmatrix-only", "hmatrix-dense", "dense"],
                    help="BEM form of the timed paths (the dense FP64 path is measured too, except with "
                         "hmatrix-only: the hierarchical matrix built from the mesh with no dense copy on the "
@@ -635,7 +638,7 @@ def run_adjoint(args, dist: Dist | None = None) -> dict:
     world, rank, local = dist_env()
     torch.cuda.set_device(local)
     nsteps = args.c5_steps
-    w = workloads.c5_disk(nsteps=nsteps)
+    w = workloads.c5_disk(nsteps=nsteps, h=args.c5_h)
     info = w.info
     t0 = time.perf_counter()
     mo, ctx = workloads.setup_context(w, device=local, mixed=True, tol=args.tol, maxiter=200)

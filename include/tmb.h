@@ -122,10 +122,12 @@ int tmb_set_replicas(tmb_ctx* ctx, int nrep);
 /* Boundary GEMM of shared-mesh replicas on the mixed path: 1 (default) the 3xTF32 tensor-core
  * kernel (tcgen05, FP32 accumulation per K split, FP64 sum of the splits), 0 the CUDA-core kernel
  * (FP32 products, FP64 accumulation).  The FP64 path always uses the CUDA-core kernel.  The K
- * split of the tensor-core kernel is chosen by timing the candidates on first use.  No tetmag
+ * split and the TMA ring depth of the tensor-core kernel are chosen by timing the candidates on
+ * first use.  No tetmag
  * counterpart (tetmag multiplies one boundary vector at a time, main/DemagField.cpp:145-147). */
 int tmb_set_bem_gemm_kind(tmb_ctx* ctx, int tensor_cores);
-/* out[0..9]: tensor cores on, chosen K split, tuned ms per launch for splits 1..8 (0: not tried). */
+/* out[0..10]: tensor cores on, chosen K split, tuned ms per launch for splits 1..8 (the best TMA
+ * ring depth of each; 0: not tried), chosen ring depth (2, 3 or 4 stages; 0: not tuned yet). */
 int tmb_bem_gemm_info(tmb_ctx* ctx, double* out);
 int tmb_get_bem_dense(tmb_ctx* ctx, double* B_colmajor);
 

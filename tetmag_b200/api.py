@@ -163,9 +163,9 @@ class Context:
         return self
 
     def bem_gemm_info(self) -> dict:
-        out = (C.c_double * 10)()
+        out = (C.c_double * 11)()
         check(lib().tmb_bem_gemm_info(self.h, out))
-        return {"tensor_cores": bool(out[0]), "split": int(out[1]),
+        return {"tensor_cores": bool(out[0]), "split": int(out[1]), "stages": int(out[10]),
                 "tuned_ms": {k + 1: out[2 + k] for k in range(8) if out[2 + k] > 0}}
 
     def set_bem_dense(self, B: np.ndarray):

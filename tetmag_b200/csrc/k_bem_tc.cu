@@ -12,7 +12,7 @@
 //
 // Structure (one CTA per 128-row tile x 64 replicas x K range; 192 threads):
 //   warp 0      TMA producer: cp.async.bulk.tensor 2D tiles of B (128 x 32) and of the
-//               pre-split X_hi, X_lo (64 x 32 each), 128-byte swizzle, into a 4-stage ring;
+//               pre-split X_hi, X_lo (64 x 32 each), 128-byte swizzle, into a 2- to 4-stage ring;
 //               one mbarrier "full" per stage
 //   warp 1      MMA issuer (one elected lane): tcgen05.mma.cta_group::1.kind::tf32,
 //               M = 128, N = 64, K = 8 per instruction, 12 per stage; groups of kGroup stages
@@ -33,7 +33,7 @@ namespace tmb {
 
 namespace {
 
-constexpr int kTcM = 128, kTcN = 64, kTcK = 32, kTcStages = 4;
+constexpr int kTcM = 128, kTcN = 64, kTcK = 32;
 constexpr int kTileA = kTcM * kTcK * 4;           // 16 KiB
 constexpr int kTileX = kTcN * kTcK * 4;           // 8 KiB
 constexpr int kStageBytes = 2 * (kTileA + kTileX);  // hi + lo tiles
@@ -141,6 +141,7 @@ __device__ __forceinline__ void split_tile(float4* hi, float4* lo, int nvec, int
   }
 }
 
+template <int kTcStages>
 struct TcSmem {
   uint64_t full[kTcStages], conv[kTcStages], empty[kTcStages], accf[2], acce[2];
   uint32_t tmem_base;
@@ -172,6 +173,9 @@ __device__ __forceinline__ void tmem_ld64(uint32_t taddr, uint32_t (&v)[kTcN]) {
 // Each 32-wide K stage is accumulated by the tensor cores in FP32 into one of two TMEM buffers
 // (64 columns each) and drained by the epilogue warps into FP64 registers while the next stage
 // runs, so the FP32 part of every sum is 32 products long.
+// kTcStages: depth of the TMA ring (2, 3 or 4 stages of 48 KiB), picked with the K split by the
+// autotuner (Ctx::tune_gemm_tc).
+template <int kTcStages>
 __global__ void __launch_bounds__(kTcThreads, 1)
     k_bem_gemm_tc(const __grid_constant__ CUtensorMap mapB, const __grid_constant__ CUtensorMap mapXhi,
                   const __grid_constant__ CUtensorMap mapXlo, int nbc,
@@ -179,7 +183,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   extern __shared__ uint8_t smem_raw[];
   // tiles need 1024-byte alignment (128-byte swizzle atoms)
   uint8_t* tiles = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  TcSmem* S = reinterpret_cast<TcSmem*>(tiles + kTcStages * kStageBytes);
+  TcSmem<kTcStages>* S = reinterpret_cast<TcSmem<kTcStages>*>(tiles + kTcStages * kStageBytes);
   volatile int* abort_flag = &S->abort_flag;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.x * kTcM, n0 = blockIdx.y * kTcN;
@@ -368,7 +372,23 @@ CUtensorMap make_map(const float* base, int rows, int cols, size_t pitch, int bo
   return m;
 }
 
-constexpr size_t kTcSmemBytes = size_t(kTcStages) * kStageBytes + sizeof(TcSmem) + 1024;
+template <int kTcStages>
+constexpr size_t tc_smem_bytes() {
+  return size_t(kTcStages) * kStageBytes + sizeof(TcSmem<kTcStages>) + 1024;
+}
+
+template <int kTcStages>
+void launch_tc_kernel(dim3 grid, cudaStream_t st, const CUtensorMap& mb, const CUtensorMap& mxh,
+                      const CUtensorMap& mxl, int nbc, int ncomp, int per, int nks, double* Y, int* err) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    TMB_CUDA(cudaFuncSetAttribute(k_bem_gemm_tc<kTcStages>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(tc_smem_bytes<kTcStages>())));
+    attr_set = true;
+  }
+  k_bem_gemm_tc<kTcStages><<<grid, kTcThreads, tc_smem_bytes<kTcStages>(), st>>>(mb, mxh, mxl, nbc, ncomp, per, nks,
+                                                                                  Y, err);
+}
 
 }  // namespace
 
@@ -378,12 +398,7 @@ bool bem_gemm_tc_supported(int nbc, size_t ld, int xs) {
 }
 
 void launch_bem_gemm_tc(int nbc, int ncomp, size_t ld, const float* B, const float* X, int xs, float* Xhi,
-                        float* Xlo, double* Y, int split, int* err, cudaStream_t st) {
-  static bool attr_set = false;
-  if (!attr_set) {
-    TMB_CUDA(cudaFuncSetAttribute(k_bem_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTcSmemBytes)));
-    attr_set = true;
-  }
+                        float* Xlo, double* Y, int split, int stages, int* err, cudaStream_t st) {
   const size_t nx = size_t(xs) * ncomp;
   note_launch();
   k_split_tf32<<<grid_for((long long)nx), kBlock, 0, st>>>(nx, X, Xhi, Xlo);
@@ -397,7 +412,9 @@ void launch_bem_gemm_tc(int nbc, int ncomp, size_t ld, const float* B, const flo
   if (split > 1) TMB_CUDA(cudaMemsetAsync(Y, 0, sizeof(double) * size_t(nbc) * ncomp, st));
   note_launch();
   const dim3 grid((nbc + kTcM - 1) / kTcM, (ncomp + kTcN - 1) / kTcN, split);
-  k_bem_gemm_tc<<<grid, kTcThreads, kTcSmemBytes, st>>>(mb, mxh, mxl, nbc, ncomp, per, nks, Y, err);
+  if (stages == 2) launch_tc_kernel<2>(grid, st, mb, mxh, mxl, nbc, ncomp, per, nks, Y, err);
+  else if (stages == 3) launch_tc_kernel<3>(grid, st, mb, mxh, mxl, nbc, ncomp, per, nks, Y, err);
+  else launch_tc_kernel<4>(grid, st, mb, mxh, mxl, nbc, ncomp, per, nks, Y, err);
   TMB_CUDA(cudaGetLastError());
 }
 

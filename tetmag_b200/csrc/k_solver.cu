@@ -64,6 +64,12 @@ __device__ __forceinline__ bool grid_reduce(const double (&v)[K], double* partia
   return true;
 }
 
+// Resident CTAs asked of the compiler for the fine post-smoothing sweep: eight (32 registers, no
+// spills) with FP32 operator values, five (48) with FP64 ones; the fused update keeps its natural
+// register count (a cap spilled it), and reduce_grid_for sizes every grid to what fits.
+template <typename V>
+constexpr int kReduceMinBlocks = sizeof(V) == 4 ? 8 : 5;
+
 // Entries of a SELL-32 row are visited in chunks of kChunk: the chunk's column indices and
 // values are loaded first (coalesced across the warp, values kept in the operator's type), then
 // its kChunk gathers are issued together (FEM rows hold 10-15 entries; 16-entry chunks measured
@@ -416,7 +422,7 @@ __global__ void __launch_bounds__(kBlock) k_cg_rz(int n, const double* __restric
 // Last post-smoothing sweep of the finest level fused with rho = r.z:
 // z = x + D_w^-1 (r - A x); the last block sets beta = rho_new / rho (0 on the first pass).
 template <typename V>
-__global__ void __launch_bounds__(kBlock) k_jacobi_rz(SellView s, const V* __restrict__ val,
+__global__ void __launch_bounds__(kBlock, kReduceMinBlocks<V>) k_jacobi_rz(SellView s, const V* __restrict__ val,
                                                       const double* __restrict__ dinv, const double* __restrict__ r,
                                                       const double* __restrict__ xin, double* __restrict__ z,
                                                       CgScalars* S, double* partials, int first) {
@@ -748,6 +754,26 @@ int reduce_grid(long long n) {
   return g < cap ? g : cap;
 }
 
+// The grid of a grid-stride reduction kernel: one wave of the CTAs that are resident at once for
+// this kernel (its register count decides how many fit on an SM), at most one thread per row.
+// A grid of eight CTAs per SM for a kernel of which only five or six fit left a partial second
+// wave running alone.
+template <typename K>
+int reduce_grid_for(K kernel, long long n) {
+  static int cap = 0;
+  if (cap == 0) {
+    int dev = 0, sms = 148, per_sm = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, 0) != cudaSuccess || per_sm < 1) {
+      cudaGetLastError();
+      per_sm = 8;
+    }
+    cap = std::min(per_sm, 8) * sms;
+  }
+  const int g = grid_for(n);
+  return g < cap ? g : cap;
+}
+
 template <typename V>
 void launch_jacobi(const SellView& s, const V* val, const double* dinv, const double* b, const double* xin,
                    double* xout, const int* done, cudaStream_t st) {
@@ -830,7 +856,8 @@ template <typename V>
 void launch_cg_residual(const SellView& s, const V* val, const double* bp, const double* x, double* r,
                         CgScalars* S, double* partials, cudaStream_t st) {
   note_launch();
-  launch_pdl(k_cg_residual<V>, reduce_grid(1LL * s.n * s.rep), kBlock, 0, st, s, val, bp, x, r, S, partials);
+  launch_pdl(k_cg_residual<V>, reduce_grid_for(k_cg_residual<V>, 1LL * s.n * s.rep), kBlock, 0, st, s, val, bp, x, r,
+             S, partials);
 }
 void launch_cg_rz(int n, const double* r, const double* z, CgScalars* S, double* partials, bool first,
                   cudaStream_t st) {
@@ -849,25 +876,32 @@ void launch_jacobi_rz(const SellView& s, const V* val, const double* dinv, const
                       double* z, CgScalars* S, double* partials, bool first, cudaStream_t st) {
   note_launch();
   if (paired(s))
-    launch_pdl(k_jacobi_rz2<V>, reduce_grid(1LL * s.n * s.rep / 2), kBlock, 0, st, s, val, dinv, r, xin, z, S, partials,
+    launch_pdl(k_jacobi_rz2<V>, reduce_grid_for(k_jacobi_rz2<V>, 1LL * s.n * s.rep / 2), kBlock, 0, st, s, val, dinv, r,
+               xin, z, S, partials,
                first ? 1 : 0);
   else
-    launch_pdl(k_jacobi_rz<V>, reduce_grid(1LL * s.n * s.rep), kBlock, 0, st, s, val, dinv, r, xin, z, S, partials,
+    launch_pdl(k_jacobi_rz<V>, reduce_grid_for(k_jacobi_rz<V>, 1LL * s.n * s.rep), kBlock, 0, st, s, val, dinv, r, xin,
+               z, S, partials,
                first ? 1 : 0);
 }
 template <typename V>
 void launch_cg_dir_spmv(const SellView& s, const V* val, const double* z, double* p, double* q, CgScalars* S,
                         double* partials, cudaStream_t st) {
   note_launch();
-  if (paired(s)) launch_pdl(k_cg_dir_spmv2<V>, reduce_grid(1LL * s.n * s.rep / 2), kBlock, 0, st, s, val, z, p, q, S, partials);
-  else launch_pdl(k_cg_dir_spmv<V>, reduce_grid(1LL * s.n * s.rep), kBlock, 0, st, s, val, z, p, q, S, partials);
+  if (paired(s))
+    launch_pdl(k_cg_dir_spmv2<V>, reduce_grid_for(k_cg_dir_spmv2<V>, 1LL * s.n * s.rep / 2), kBlock, 0, st, s, val, z, p,
+               q, S, partials);
+  else
+    launch_pdl(k_cg_dir_spmv<V>, reduce_grid_for(k_cg_dir_spmv<V>, 1LL * s.n * s.rep), kBlock, 0, st, s, val, z, p, q, S,
+               partials);
 }
 template <typename V>
 void launch_cg_update_jacobi0(const SellView& s, const V* val, const double* dinv, const double* p, const double* q,
                               double* x, const double* r, double* r_new, double* X, double* Rres, CgScalars* S,
                               double* partials, cudaStream_t st) {
   note_launch();
-  launch_pdl(k_cg_update_jacobi0<V>, reduce_grid(1LL * s.n * s.rep), kBlock, 0, st, s, val, dinv, p, q, x, r, r_new, X,
+  launch_pdl(k_cg_update_jacobi0<V>, reduce_grid_for(k_cg_update_jacobi0<V>, 1LL * s.n * s.rep), kBlock, 0, st, s, val,
+             dinv, p, q, x, r, r_new, X,
                                                                               Rres, S, partials);
 }
 

@@ -388,7 +388,7 @@ struct Ctx {
   // tensor-core (3xTF32) boundary GEMM of the mixed path: on by default, split-K picked by
   // tune_gemm_tc on first use; tc_err is the kernel's time-out word
   bool gemm_tc = true;
-  int tc_split = 0;
+  int tc_split = 0, tc_stages = 4;
   DevArray<int> tc_err;
   std::vector<double> tc_tune_ms;       // per candidate split 1..8 (0: not tried)
   void tune_gemm_tc();
@@ -1258,7 +1258,8 @@ void Ctx::bem_gemm(bool f64, cudaStream_t st) {
     return;
   }
   if (tc_split == 0) tune_gemm_tc();
-  launch_bem_gemm_tc(nbc, nc, bem_ld(nbc), Bf.p, xpad32.p, xstride, xhi32.p, xlo32.p, u2b.p, tc_split, tc_err.p, st);
+  launch_bem_gemm_tc(nbc, nc, bem_ld(nbc), Bf.p, xpad32.p, xstride, xhi32.p, xlo32.p, u2b.p, tc_split, tc_stages,
+                     tc_err.p, st);
   TMB_CUDA(cudaMemcpyAsync(bits_h + 2, tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
 }
 
@@ -1274,23 +1275,30 @@ void Ctx::tune_gemm_tc() {
   cudaEvent_t e0, e1;
   TMB_CUDA(cudaEventCreate(&e0));
   TMB_CUDA(cudaEventCreate(&e1));
+  // candidates: K split 1..8 (while the CTAs of a split stay within two waves) x TMA ring depth
+  // 2, 3, 4; tc_tune_ms[sp] keeps the best depth's time for each split
   tc_tune_ms.assign(9, 0.0);
   double best = 1e300;
-  int best_split = 1;
+  int best_split = 1, best_stages = 4;
   for (int sp = 1; sp <= 8; ++sp) {
     if (sp > nks || (sp > 1 && mt * (sp - 1) >= 2 * num_sms)) break;
-    launch_bem_gemm_tc(nbc, nc, bem_ld(nbc), Bf.p, xpad32.p, xstride, xhi32.p, xlo32.p, u2b.p, sp, tc_err.p, st);
-    TMB_CUDA(cudaEventRecord(e0, st));
-    for (int r = 0; r < 3; ++r)
-      launch_bem_gemm_tc(nbc, nc, bem_ld(nbc), Bf.p, xpad32.p, xstride, xhi32.p, xlo32.p, u2b.p, sp, tc_err.p, st);
-    TMB_CUDA(cudaEventRecord(e1, st));
-    TMB_CUDA(cudaEventSynchronize(e1));
-    float ms = 0.0f;
-    TMB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    tc_tune_ms[sp] = ms / 3.0;
-    if (ms < best) {
-      best = ms;
-      best_split = sp;
+    for (int stg = 2; stg <= 4; ++stg) {
+      launch_bem_gemm_tc(nbc, nc, bem_ld(nbc), Bf.p, xpad32.p, xstride, xhi32.p, xlo32.p, u2b.p, sp, stg, tc_err.p,
+                         st);
+      TMB_CUDA(cudaEventRecord(e0, st));
+      for (int r = 0; r < 3; ++r)
+        launch_bem_gemm_tc(nbc, nc, bem_ld(nbc), Bf.p, xpad32.p, xstride, xhi32.p, xlo32.p, u2b.p, sp, stg,
+                           tc_err.p, st);
+      TMB_CUDA(cudaEventRecord(e1, st));
+      TMB_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.0f;
+      TMB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (tc_tune_ms[sp] == 0.0 || ms / 3.0 < tc_tune_ms[sp]) tc_tune_ms[sp] = ms / 3.0;
+      if (ms < best) {
+        best = ms;
+        best_split = sp;
+        best_stages = stg;
+      }
     }
   }
   cudaEventDestroy(e0);
@@ -1299,6 +1307,7 @@ void Ctx::tune_gemm_tc() {
   TMB_CUDA(cudaMemcpy(&err, tc_err.p, sizeof(int), cudaMemcpyDeviceToHost));
   if (err) throw Error(TMB_ERR_CUDA, "tensor-core boundary GEMM timed out waiting on a barrier");
   tc_split = best_split;
+  tc_stages = best_stages;
 }
 
 template <typename T>
@@ -3349,10 +3358,11 @@ int tmb_bem_gemm_info(tmb_ctx* ctx, double* out) {
   TMB_CHECK_ARG(ctx && out, "tmb_bem_gemm_info: null argument");
   TMB_API_BEGIN
   const Ctx& c = *ctx->c;
-  for (int i = 0; i < 10; ++i) out[i] = 0.0;
+  for (int i = 0; i < 11; ++i) out[i] = 0.0;
   out[0] = c.gemm_tc ? 1.0 : 0.0;
   out[1] = c.tc_split;
   for (size_t i = 1; i < c.tc_tune_ms.size() && i <= 8; ++i) out[1 + i] = c.tc_tune_ms[i];
+  out[10] = c.tc_split > 0 ? c.tc_stages : 0;
   TMB_API_END
 }
 

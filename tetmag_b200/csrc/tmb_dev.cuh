@@ -235,7 +235,7 @@ void launch_bem_gemm(int nbc, int ncomp, const V* B, const V* X, int xs, double*
 // err is set when a barrier wait timed out.
 bool bem_gemm_tc_supported(int nbc, size_t ld, int xs);
 void launch_bem_gemm_tc(int nbc, int ncomp, size_t ld, const float* B, const float* X, int xs, float* Xhi,
-                        float* Xlo, double* Y, int split, int* err, cudaStream_t st);
+                        float* Xlo, double* Y, int split, int stages, int* err, cudaStream_t st);
 
 // --- hierarchical BEM matrix (k_hmatrix.cu) ---------------------------------------------
 struct HBlockDev {
