@@ -176,6 +176,13 @@ int tmb_bem_info(tmb_ctx* ctx, double* out);
  * rank, 1 if the block hit the rank cap.  Diagnostic only: tetmag's call path has no
  * counterpart. */
 int tmb_bem_verify(tmb_ctx* ctx, double* block_out, double* out);
+/* The boundary product alone, DemagField::mvp (main/DemagField.cpp:139-152: denseMVP or
+ * h2MVP -> H2_mvp_sub, main/h2interface.c:77-95): y = B x (transpose = 0) or B^T x (1) for
+ * boundary vectors of Nb entries in boundary-node order (tmb_mesh_get_boundary's bnodes), with
+ * the context's boundary matrix form (tmb_set_bem_mode) and precision.  The transposed
+ * product (the adjoint's) exists for the dense and hierarchical forms; one component, no
+ * replicas.  Host pointers synchronise. */
+int tmb_bem_apply(tmb_ctx* ctx, const double* x, double* y, int transpose, int ptr_kind);
 
 /* Material per node (SimulationData, specs/SimulationData.cpp:125-163): Js [T], A [J/m]
  * already divided by scale^2, Ku [J/m^3], ku_axis 3N SoA, D [J/m^2] already divided by

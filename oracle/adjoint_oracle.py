@@ -47,11 +47,11 @@ def pulse_weights(ns: int, t0_ps: float, t1_ps: float, t_ps: float):
 
 
 class Dynamics:
-    """Field, right-hand side and their transposes for one problem (interfacial or no DMI)."""
+    """Field, right-hand side and their transposes for one problem (bulk, interfacial or no DMI)."""
 
     def __init__(self, pb: O.Problem, dem: O.DemagOracle, bz=None, t0_ps=0.0, t1_ps=0.0):
-        if np.any(pb.D != 0.0) and pb.dmi_kind != "interfacial":
-            raise ValueError("the adjoint supports the interfacial DMI form only")
+        if np.any(pb.D != 0.0) and pb.dmi_kind not in ("bulk", "interfacial"):
+            raise ValueError(f"unknown DMI form {pb.dmi_kind!r}")
         self.pb, self.dem = pb, dem
         self.bz = np.zeros(0) if bz is None else np.asarray(bz, np.float64)
         self.t0, self.t1 = t0_ps, t1_ps
@@ -95,9 +95,27 @@ class Dynamics:
         out = pb.fem.stiff.T @ (self.xcK[:, None] * mu)
         km = np.sum(pb.ku_axis * mu, axis=1)
         out += (2.0 * pb.Ku * self.ij * km)[:, None] * pb.ku_axis
-        if np.any(pb.D != 0.0):
+        if np.any(pb.D != 0.0) and pb.dmi_kind == "interfacial":
             out += self.W[:, None] * O.interfacial_dmi_field(pb, mu / self.W[:, None]) * self.ij[:, None]
+        elif np.any(pb.D != 0.0):
+            out += self.bulk_dmi_t(mu)
         return out + self.demag_t(mu)
+
+    def bulk_dmi_t(self, mu):
+        """Transpose of m -> H_dmi / Js for the bulk form (EffFieldCalc::dmiField, surfIntDMI and
+        curlM, main/EffFieldCalc.cpp:159-170, 280-298): H = ds (a m x n - 2 curl m) with
+        ds = D / (V Js) and curl m built from -tGrad; the transpose is ds a (n x mu) plus the
+        explicit transposes of the tGrad matrices applied to ds mu."""
+        pb = self.pb
+        ds = pb.D / pb.fem.node_vol * self.ij
+        v = ds[:, None] * mu
+        tx, ty, tz = pb.fem.tgrad
+        out = (ds * pb.bnd.node_area)[:, None] * np.cross(pb.bnd.node_normal, mu)
+        # -2 curl m = 2 [ty mz - tz my, tz mx - tx mz, tx my - ty mx] (tGrad itself, not -tGrad)
+        out[:, 0] += 2.0 * (tz.T @ v[:, 1] - ty.T @ v[:, 2])
+        out[:, 1] += 2.0 * (tx.T @ v[:, 2] - tz.T @ v[:, 0])
+        out[:, 2] += 2.0 * (ty.T @ v[:, 0] - tx.T @ v[:, 1])
+        return out
 
     def vjp(self, m, H, abar, t_ps):
         """(df/dm)^T abar and the parameter pieces (dKu per node, dJ/dHz scalar) at one stage."""

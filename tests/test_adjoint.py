@@ -62,17 +62,46 @@ def test_oracle_adjoint_matches_finite_differences():
     assert abs(fd - np.sum(gm * v)) <= 1e-7 * abs(np.sum(gm * v))
 
 
-def test_oracle_adjoint_rejects_bulk_dmi():
-    mesh, pb, m0 = small_disk_problem()
+def bulk_disk_problem(seed=5):
+    """The small disk with tetmag's bulk DMI form (EffFieldCalc::dmiField, main/EffFieldCalc.cpp:159-170)."""
     import dataclasses
-    with pytest.raises(ValueError):
-        A.Dynamics(dataclasses.replace(pb, dmi_kind="bulk"), None)
+    mesh, pb, m0 = small_disk_problem(seed=seed, D=3e-3)
+    return mesh, dataclasses.replace(pb, dmi_kind="bulk"), m0
+
+
+def test_oracle_bulk_dmi_adjoint_matches_finite_differences():
+    mesh, pb, m0 = bulk_disk_problem()
+    dem = O.DemagOracle(pb)
+    rng = np.random.default_rng(2)
+    n = mesh.nx
+    ku = 2e4 * rng.uniform(0, 1, n)
+    nsteps, dt, nsub = 2, 1.0, 8
+    w = A.mean_mz_weights(pb)
+
+    def J(m_):
+        d = A.Dynamics(A.problem_with_ku(pb, ku), dem, None)
+        return float(np.sum(w * A.rk4_forward(d, m_, nsteps, dt, nsub)))
+
+    d = A.Dynamics(A.problem_with_ku(pb, ku), dem, None)
+    # the bulk form is what the forward map uses
+    assert np.abs(O.dmi_field(pb, m0)).max() > 0.0
+    Jv, yN, gm, gku, gbz = A.rk4_adjoint(d, m0, nsteps, dt, w, nsub)
+    assert abs(Jv - J(m0)) <= 1e-14
+    for k in range(2):
+        v = rng.standard_normal(m0.shape)
+        fd = (J(m0 + 1e-5 * v) - J(m0 - 1e-5 * v)) / 2e-5
+        assert abs(fd - np.sum(gm * v)) <= 1e-7 * abs(np.sum(gm * v)), k
+    # the DMI part of the transpose alone: <H_dmi(m), mu> = <m, H_dmi^T(mu)>
+    mu = rng.standard_normal(m0.shape)
+    lhs = np.sum(O.dmi_field(pb, m0) * O.inv_js(pb)[:, None] * mu)
+    rhs = np.sum(m0 * d.bulk_dmi_t(mu))
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
 
 
 # ------------------------------------------------------------------------------------------
 # GPU: the device adjoint through the C ABI
 # ------------------------------------------------------------------------------------------
-def _device_setup(mesh, tol=1e-13, mixed=False, Ku=None):
+def _device_setup(mesh, tol=1e-13, mixed=False, Ku=None, D=1.58e-3, interfacial=True):
     from tetmag_b200.api import Context, MeshOps
     n = mesh.nx
     mo = MeshOps(mesh.xyz, mesh.tets)
@@ -81,10 +110,10 @@ def _device_setup(mesh, tol=1e-13, mixed=False, Ku=None):
     ctx.bem_assemble(mo)
     Js = np.full(n, O.MU0 * 3.84e5)
     A_ = np.full(n, 8.78e-12 / 1e-18)
-    D = np.full(n, 1.58e-3 / 1e-9)
+    D = np.full(n, D / 1e-9)
     axis = np.concatenate([np.zeros(2 * n), np.ones(n)])
     ctx.set_material(Js, A_, Ku=Ku, ku_axis=axis, D=D, alpha=0.3)
-    ctx.set_dmi_kind(True)
+    ctx.set_dmi_kind(interfacial)
     ctx.set_applied_field(np.zeros(3 * n))
     ctx.set_precision(mixed)
     ctx.set_solver_params(tol, 400)
@@ -174,10 +203,102 @@ def MeshOpsForWeights(mesh):
 
 
 @pytest.mark.gpu
-def test_device_adjoint_rejects_bulk_dmi():
-    from tetmag_b200 import _lib
-    mesh, pb, m0 = small_disk_problem()
-    mo, ctx, _ = _device_setup(mesh)
-    ctx.set_dmi_kind(False)
-    with pytest.raises(_lib.TmbError):
-        ctx.adjoint_rk4(O.rows_to_soa(m0), np.zeros(3 * mesh.nx), 1, 1.0, 2)
+def test_device_bulk_dmi_adjoint_matches_oracle_fp64():
+    # tetmag's bulk DMI form (surface term and curl, main/EffFieldCalc.cpp:159-170, 280-298) through
+    # the device adjoint against the oracle's explicit transposes
+    mesh, pb, m0 = bulk_disk_problem()
+    dem = O.DemagOracle(pb)
+    rng = np.random.default_rng(12)
+    n = mesh.nx
+    bz = 0.05 * rng.standard_normal(5)
+    ku = 2e4 * rng.uniform(0, 1, n)
+    nsteps, dt, nsub = 2, 1.0, 8
+    w = A.mean_mz_weights(pb)
+    d = A.Dynamics(A.problem_with_ku(pb, ku), dem, bz, 0.0, nsteps * dt)
+    Jo, yo, gmo, gko, gbo = A.rk4_adjoint(d, m0, nsteps, dt, w, nsub)
+    mo, ctx, _ = _device_setup(mesh, Ku=ku, D=3e-3, interfacial=False)
+    ctx.set_bz_pulse(bz, 0.0, nsteps * dt)
+    r = ctx.adjoint_rk4(O.rows_to_soa(m0), O.rows_to_soa(w), nsteps, dt, nsub, ckpt_every=1, n_bz=bz.size)
+    assert abs(r["J"] - Jo) <= 1e-12
+    assert _relerr(r["m_final"], O.rows_to_soa(yo)) <= 1e-10
+    assert _relerr(r["grad_m0"], O.rows_to_soa(gmo)) <= 1e-8
+    assert _relerr(r["grad_ku"], gko) <= 1e-8
+    assert _relerr(r["grad_bz"], gbo) <= 1e-8
+
+
+def _hier_disk_context(mixed=False):
+    """A disk large enough for admissible boundary blocks: dense matrix kept, hierarchical form
+    (leaf 32, eta 2, ACA to 1e-10 / 1e-6) selected."""
+    mesh = meshgen.jittered_disk(90.0, 9.0, 3.0, seed=8)
+    mo, ctx, mat = _device_setup(mesh, tol=1e-13 if not mixed else 1e-10, mixed=mixed)
+    ctx.bem_assemble(mo, accurate=True)   # far-field-accurate weights: compressible to 1e-10
+    bd = mo.boundary()
+    bn = bd["bnodes"]
+    ctx.bem_compress(mesh.xyz[bn], leaf=32, eta=2.0, eps_mixed=1e-6, eps_fp64=1e-10, kmax=64, keep_dense=True)
+    assert ctx.bem_info()["lowrank_blocks"] > 0
+    return mesh, mo, ctx, mat, bn
+
+
+@pytest.mark.gpu
+def test_hierarchical_transposed_product():
+    # B^T through the hierarchical form (transposed tiles, U and V exchanged, column-cluster work
+    # lists) against the dense B^T, and <y, H x> = <H^T y, x> for the hierarchical matrix itself
+    mesh, mo, ctx, _, bn = _hier_disk_context()
+    nb = bn.size
+    rng = np.random.default_rng(3)
+    x, y = rng.standard_normal(nb), rng.standard_normal(nb)
+    for mixed, tol_dense, tol_sym in ((False, 1e-8, 1e-13), (True, 2e-5, 1e-6)):
+        ctx.set_precision(mixed)
+        ctx.set_bem_mode(0)
+        bx, bty = ctx.bem_apply(x), ctx.bem_apply(y, transpose=True)
+        ctx.set_bem_mode(1)
+        hx, hty = ctx.bem_apply(x), ctx.bem_apply(y, transpose=True)
+        assert _relerr(hx, bx) <= tol_dense, mixed
+        assert _relerr(hty, bty) <= tol_dense, mixed
+        assert abs(y @ hx - hty @ x) <= tol_sym * abs(y @ hx), mixed
+        if not mixed:
+            assert abs(y @ bx - bty @ x) <= 1e-13 * abs(y @ bx)
+    ctx.set_precision(False)
+    # the dense B^T against the dense matrix itself
+    B = ctx.get_bem_dense()
+    ctx.set_bem_mode(0)
+    assert _relerr(ctx.bem_apply(y, transpose=True), B.T @ y) <= 1e-14
+
+
+@pytest.mark.gpu
+def test_device_adjoint_hierarchical_bem():
+    # the adjoint through the hierarchical boundary matrix: directional finite differences of the
+    # same forward map, and the dense-matrix adjoint within the compression error
+    mesh, mo, ctx, (Js, A_, axis, D), bn = _hier_disk_context()
+    n = mesh.nx
+    m0 = meshgen.skyrmion_state(mesh.xyz, 4, radius=22.0, wall=5.0)
+    nsteps, dt, nsub = 2, 1.0, 6
+    rng = np.random.default_rng(9)
+    bz0 = 0.02 + 0.01 * rng.standard_normal(5)
+    ku0 = 1e4 * rng.uniform(0, 1, n)
+    ctx.set_material(Js, A_, Ku=ku0, ku_axis=axis, D=D, alpha=0.3)
+    ctx.set_dmi_kind(True)
+    ctx.set_bz_pulse(bz0, 0.0, nsteps * dt)
+    vol = mo.operators()["node_vol"]
+    wv = np.zeros(3 * n)
+    wv[2 * n:] = vol / vol.sum()
+    res = {}
+    for mode in (1, 0):
+        ctx.set_bem_mode(mode)
+        res[mode] = ctx.adjoint_rk4(m0.copy(), wv, nsteps, dt, nsub, ckpt_every=1, n_bz=bz0.size)
+    g1, g0 = res[1], res[0]
+    assert _relerr(g1["grad_m0"], g0["grad_m0"]) <= 1e-7
+    assert _relerr(g1["grad_ku"], g0["grad_ku"]) <= 1e-7
+    assert _relerr(g1["grad_bz"], g0["grad_bz"]) <= 1e-7
+    ctx.set_bem_mode(1)
+
+    def J(m_):
+        m = m_.copy()
+        ctx.step_rk4(m, nsteps, dt, nsub)
+        return float(wv @ m)
+
+    assert abs(J(m0) - g1["J"]) <= 1e-11
+    for k in range(2):
+        v = rng.standard_normal(3 * n)
+        fd = (J(m0 + 1e-5 * v) - J(m0 - 1e-5 * v)) / 2e-5
+        assert abs(fd - g1["grad_m0"] @ v) <= 1e-6 * abs(g1["grad_m0"] @ v), k

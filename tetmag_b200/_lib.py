@@ -50,6 +50,7 @@ SIGNATURES = {
     "tmb_bem_h2_info": [_P, _D],
     "tmb_bem_info": [_P, _D],
     "tmb_bem_verify": [_P, _D, _D],
+    "tmb_bem_apply": [_P, _P, _P, _int, _int],
     "tmb_set_material": [_P, _D, _D, _D, _D, _D, _dbl],
     "tmb_set_dmi_kind": [_P, _int],
     "tmb_set_applied_field": [_P, _P, _int],

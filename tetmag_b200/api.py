@@ -229,6 +229,20 @@ class Context:
         res = dict(zip(["rel_err_fp64", "rel_err_fp32", "worst_block_fp64", "worst_block_fp32"], list(out)))
         return (res, blk) if per_block else res
 
+    def bem_apply(self, x, transpose: bool = False, out=None):
+        """The boundary product alone (DemagField::mvp): B x or B^T x for a boundary vector in
+        boundary-node order, with the current boundary matrix form and precision."""
+        if out is None:
+            if isinstance(x, np.ndarray):
+                out = np.empty(x.size)
+            else:
+                import torch
+                out = torch.empty(x.numel(), dtype=torch.float64, device=x.device)
+        px, k = _vec(x)
+        po, _ = _vec(out)
+        check(lib().tmb_bem_apply(self.h, px, po, 1 if transpose else 0, k))
+        return out
+
     def set_dmi_kind(self, interfacial: bool):
         """DMI form of the material's D: bulk (tetmag's) or interfacial."""
         check(lib().tmb_set_dmi_kind(self.h, 1 if interfacial else 0))
@@ -471,6 +485,10 @@ PROFILE_IDS = ["local_llg", "divergence", "gradient", "bem_matvec", "solve_neuma
                "restriction", "prolongation", "coarse_smooth", "coarsest_solve", "cg_start", "cg_update"]
 # ids that span several kernels (not candidates for a per-kernel roofline)
 PROFILE_CONTAINERS = ("solve_neumann", "solve_dirichlet", "demag_chain")
+# ids whose every record is one launch of one kernel (the others group the kernels of a product,
+# or one kernel per AMG level)
+PROFILE_SINGLE = ("local_llg", "divergence", "gradient", "cg_spmv", "cg_update_smooth", "fine_post_smooth_rz",
+                  "fine_pre_smooth", "cg_update")
 
 
 def profile_enable(ctx: "Context", on: bool = True):

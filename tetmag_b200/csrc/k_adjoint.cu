@@ -136,12 +136,18 @@ __global__ void __launch_bounds__(kBlock) k_adj_pre(AdjPreArgs a) {
   }
 }
 
-// g_i += (K diag(xc) mu)_i + W_i H_idmi(mu / W)_i + ku2_i (k.mu_i) k_i - (Js_i V_i / mu0) q_i
-// with q = -grad a1 (the transposed demag chain's last step), W = V Js.
-template <typename V, bool UNI, bool IDMI>
+// g_i += (K diag(xc) mu)_i + [DMI transpose]_i + ku2_i (k.mu_i) k_i - (Js_i V_i / mu0) q_i
+// with q = -grad a1 (the transposed demag chain's last step).  DMI 2 (interfacial): W_i H_idmi(mu / W)_i,
+// W = V Js.  DMI 1 (bulk, H = ds (a m x n + 2 C m) with ds = D / (V Js) and the curl
+// C m = [ty mz - tz my, tz mx - tx mz, tx my - ty mx] of the tGrad operators t,
+// main/EffFieldCalc.cpp:159-170, 280-298): ds_i a_i (n_i x mu_i) + 2 C^T (ds mu), where the
+// transposed tGrad rows are read from the gradient operators, t_d^T = diag(V) grad_d (both come
+// from the same P1 integrals, tGrad = (V grad)^T).
+template <typename V, bool UNI, int DMI>
 __global__ void __launch_bounds__(kBlock) k_adj_local(SellView s, const V* __restrict__ K, const V* __restrict__ tg0,
                                                       const V* __restrict__ tg1, const V* __restrict__ gr0,
-                                                      const V* __restrict__ gr1, AdjLocalArgs a) {
+                                                      const V* __restrict__ gr1, const V* __restrict__ gr2,
+                                                      AdjLocalArgs a) {
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
   if (row >= a.n) return;
   const int n = a.n;
@@ -161,7 +167,7 @@ __global__ void __launch_bounds__(kBlock) k_adj_local(SellView s, const V* __res
     ex = fma(v, u0, ex);
     ey = fma(v, u1, ey);
     ez = fma(v, u2, ez);
-    if (IDMI) {
+    if (DMI == 2) {
       const double w = __ldg(a.idm_b + j);  // 1 / (V_j Js_j)
       const double n0 = u0 * w, n1 = u1 * w, n2 = u2 * w;
       const double g0 = ldv(gr0, k), g1 = ldv(gr1, k);
@@ -174,13 +180,39 @@ __global__ void __launch_bounds__(kBlock) k_adj_local(SellView s, const V* __res
       cyx = fma(t1, n2, cyx);
       czy = fma(t0, n0, fma(t1, n1, czy));
     }
+    if (DMI == 1) {
+      // c_ab = (grad_a (ds mu_b))_i
+      const double d = __ldg(a.dmi_s + j);
+      const double v0 = d * u0, v1 = d * u1, v2 = d * u2;
+      const double g0 = ldv(gr0, k), g1 = ldv(gr1, k), g2 = ldv(gr2, k);
+      cxy = fma(g0, v1, cxy);
+      cxz = fma(g0, v2, cxz);
+      cyx = fma(g1, v0, cyx);
+      cyz = fma(g1, v2, cyz);
+      czx = fma(g2, v0, czx);
+      czy = fma(g2, v1, czy);
+    }
   }
   double o0 = ex, o1 = ey, o2 = ez;
-  if (IDMI) {
+  if (DMI == 2) {
     const double vd = a.vol[row] * a.idm_d[row];
     o0 += vd * cxz - cxy;
     o1 += vd * cyz - cyx;
     o2 += czy - vd * czx;
+  }
+  if (DMI == 1) {
+    const double w = 2.0 * a.vol[row];
+    o0 += w * (czy - cyz);
+    o1 += w * (cxz - czx);
+    o2 += w * (cyx - cxy);
+    const double f = a.dmi_s[row] * a.area[row];
+    if (f != 0.0) {
+      const double n0 = a.nvn[row], n1 = a.nvn[row + n], n2 = a.nvn[row + 2 * n];
+      const double u0 = ux[row], u1 = uy[row], u2 = uz[row];
+      o0 = fma(f, n1 * u2 - n2 * u1, o0);
+      o1 = fma(f, n2 * u0 - n0 * u2, o1);
+      o2 = fma(f, n0 * u1 - n1 * u0, o2);
+    }
   }
   if (UNI) {
     const double e0 = a.kax[row], e1 = a.kax[row + n], e2 = a.kax[row + 2 * n];
@@ -297,15 +329,23 @@ void launch_adj_pre(const AdjPreArgs& a, cudaStream_t st) {
 }
 
 template <typename V>
-void launch_adj_local(const SellView& s, const V* K, const V* tg0, const V* tg1, const V* gr0, const V* gr1,
+void launch_adj_local(const SellView& s, const V* K, const V* tg0, const V* tg1, const V* gr0, const V* gr1, const V* gr2,
                       const AdjLocalArgs& a, cudaStream_t st) {
   note_launch();
   const int g = grid_for(a.n);
-  const bool uni = a.ku2 != nullptr, idmi = a.idm_b != nullptr;
-  if (uni && idmi) k_adj_local<V, true, true><<<g, kBlock, 0, st>>>(s, K, tg0, tg1, gr0, gr1, a);
-  else if (uni) k_adj_local<V, true, false><<<g, kBlock, 0, st>>>(s, K, tg0, tg1, gr0, gr1, a);
-  else if (idmi) k_adj_local<V, false, true><<<g, kBlock, 0, st>>>(s, K, tg0, tg1, gr0, gr1, a);
-  else k_adj_local<V, false, false><<<g, kBlock, 0, st>>>(s, K, tg0, tg1, gr0, gr1, a);
+  const bool uni = a.ku2 != nullptr;
+  const int dmi = a.idm_b ? 2 : (a.dmi_s ? 1 : 0);
+#define TMB_ADJ(U, D) k_adj_local<V, U, D><<<g, kBlock, 0, st>>>(s, K, tg0, tg1, gr0, gr1, gr2, a)
+  if (uni) {
+    if (dmi == 2) TMB_ADJ(true, 2);
+    else if (dmi == 1) TMB_ADJ(true, 1);
+    else TMB_ADJ(true, 0);
+  } else {
+    if (dmi == 2) TMB_ADJ(false, 2);
+    else if (dmi == 1) TMB_ADJ(false, 1);
+    else TMB_ADJ(false, 0);
+  }
+#undef TMB_ADJ
   TMB_CUDA(cudaGetLastError());
 }
 
@@ -351,7 +391,7 @@ void launch_scatter_add(int nb, const int* idx, const double* z, double* a, cuda
 
 #define TMB_INST(V)                                                                                          \
   template void launch_adj_local<V>(const SellView&, const V*, const V*, const V*, const V*, const V*,      \
-                                    const AdjLocalArgs&, cudaStream_t);                                     \
+                                    const V*, const AdjLocalArgs&, cudaStream_t);                           \
   template void launch_bem_gemv_t<V>(int, const V*, const double*, double*, int, double*, cudaStream_t);    \
   template void launch_lift_t<V>(int, const CsrView&, const V*, const int*, const double*, const double*,   \
                                  double*, cudaStream_t);

@@ -332,6 +332,32 @@ __global__ void __launch_bounds__(256) k_h_near(const HNearRow* __restrict__ row
   }
 }
 
+// Transposed near field: one CTA per leaf column cluster sigma, y_sigma = sum_b D_b^T x_tau over
+// its dense tiles (column-major m x n, so lane j reads tile column j, contiguous in i).
+template <typename T>
+__global__ void __launch_bounds__(256) k_h_near_t(const HNearRow* __restrict__ cols, const HBlockDev* __restrict__ blk,
+                                                  const T* __restrict__ D, const T* __restrict__ xp,
+                                                  double* __restrict__ y) {
+  __shared__ double acc[8][33];
+  const HNearRow C = cols[blockIdx.x];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double a = 0.0;
+  for (int q = C.first + warp; q < C.last; q += 8) {
+    const HBlockDev b = blk[q];
+    if (lane < b.n) {
+      const T* col = D + b.off + size_t(lane) * b.m;
+      for (int i = 0; i < b.m; ++i) a = fma(double(col[i]), double(xp[b.rb + i]), a);
+    }
+  }
+  acc[warp][lane] = a;
+  __syncthreads();
+  if (warp == 0 && lane < C.m) {
+    double s = 0.0;
+    for (int w = 0; w < 8; ++w) s += acc[w][lane];
+    y[C.rb + lane] = s;
+  }
+}
+
 // Deterministic probe value in [-1, 1) for position j (cluster order): splitmix64 of j.
 __device__ __forceinline__ double probe_value(long long j) {
   unsigned long long z = static_cast<unsigned long long>(j) + 0x9e3779b97f4a7c15ull;
@@ -798,6 +824,24 @@ template void launch_h_compact<double>(int, const HBlockDev*, const double*, con
                                        const long long*, const int*, double*, double*, cudaStream_t);
 template void launch_h_compact<float>(int, const HBlockDev*, const double*, const double*, const long long*,
                                       const long long*, const int*, float*, float*, cudaStream_t);
+template <typename T>
+void launch_h_matvec_t(const HMatView<T>& H, const double* u, double* y, T* xp, cudaStream_t st) {
+  note_launch();
+  k_h_gather<T><<<grid_for(H.nb), kBlock, 0, st>>>(H.nb, u, H.gidx, xp);
+  note_launch();
+  k_h_near_t<T><<<H.nrows, 256, 0, st>>>(H.near_rows, H.near, H.D, xp, y);
+  if (H.nterms > 0) {
+    note_launch();
+    const long long threads = H.nterms * kLanesPerTerm;
+    k_h_vt<T><<<unsigned((threads + 255) / 256), 256, 0, st>>>(H.nterms, H.terms, H.V, xp, H.t);
+    note_launch();
+    k_h_ut<T><<<H.ngroups, 256, 0, st>>>(H.groups, H.toff, H.terms, H.U, H.t, y);
+  }
+  TMB_CUDA(cudaGetLastError());
+}
+
+template void launch_h_matvec_t<double>(const HMatView<double>&, const double*, double*, double*, cudaStream_t);
+template void launch_h_matvec_t<float>(const HMatView<float>&, const double*, double*, float*, cudaStream_t);
 template void launch_h_matvec<double>(const HMatView<double>&, const double*, double*, double*, const int*, int,
                                       double*, cudaStream_t);
 template void launch_h_matvec<float>(const HMatView<float>&, const double*, double*, float*, const int*, int,

@@ -64,12 +64,6 @@ __device__ __forceinline__ bool grid_reduce(const double (&v)[K], double* partia
   return true;
 }
 
-// Resident CTAs asked of the compiler for the fine post-smoothing sweep: eight (32 registers, no
-// spills) with FP32 operator values, five (48) with FP64 ones; the fused update keeps its natural
-// register count (a cap spilled it), and reduce_grid_for sizes every grid to what fits.
-template <typename V>
-constexpr int kReduceMinBlocks = sizeof(V) == 4 ? 8 : 5;
-
 // Entries of a SELL-32 row are visited in chunks of kChunk: the chunk's column indices and
 // values are loaded first (coalesced across the warp, values kept in the operator's type), then
 // its kChunk gathers are issued together (FEM rows hold 10-15 entries; 16-entry chunks measured
@@ -270,6 +264,112 @@ __global__ void __launch_bounds__(kBlock) k_csr_jacobi(CsrView c, const V* __res
   if (row < c.n * c.rep && sub == 0) xout[row] = xin[row] + dinv[row / c.rep] * (b[row] - acc);
 }
 
+// Coarse levels, one replica: the first sweep from zero with its residual (x = D_w^-1 b,
+// r = b - A x) and the restriction of that residual in one launch.  The restricted residual needs
+// no sweep result: R r = R (I - A D_w^-1) b = M b with M = R - (R A) D_w^-1, so the first na
+// blocks run the sweep's rows (ta threads a row) and the others the rows of M (tm threads a row).
+__device__ __forceinline__ double group_sum_rt(double v, int T) {
+  for (int o = T >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+template <typename V>
+__device__ __forceinline__ double csr_row_part_rt(const CsrView& c, const V* __restrict__ val,
+                                                  const double* __restrict__ x, const double* __restrict__ w, int row,
+                                                  int sub, int T) {
+  double acc = 0.0;
+  if (row < c.n) {
+    const int beg = __ldg(c.ptr + row), end = __ldg(c.ptr + row + 1);
+    for (int k0 = beg + sub; k0 < end; k0 += kCsrChunk * T) {
+      int j[kCsrChunk];
+      V v[kCsrChunk];
+#pragma unroll
+      for (int u = 0; u < kCsrChunk; ++u) {
+        const int k = k0 + u * T;
+        const bool ok = k < end;
+        j[u] = ok ? __ldg(c.col + k) : 0;
+        v[u] = ok ? __ldg(val + k) : V(0);
+      }
+#pragma unroll
+      for (int u = 0; u < kCsrChunk; ++u) {
+        const double xj = w ? __ldg(w + j[u]) * __ldg(x + j[u]) : __ldg(x + j[u]);
+        acc = fma(static_cast<double>(v[u]), xj, acc);
+      }
+    }
+  }
+  return acc;
+}
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_csr_pre_restrict(CsrView a, const V* __restrict__ aval,
+                                                             const double* __restrict__ dinv,
+                                                             const double* __restrict__ b, double* __restrict__ x,
+                                                             double* __restrict__ r, int ta, int na, CsrView m,
+                                                             const V* __restrict__ mval, double* __restrict__ bc,
+                                                             int tm, const int* done) {
+  pdl_enter();
+  if (done && *done) return;
+  if (int(blockIdx.x) < na) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int row = t / ta, sub = t & (ta - 1);
+    const double acc = group_sum_rt(csr_row_part_rt(a, aval, b, dinv, row, sub, ta), ta);
+    if (row < a.n && sub == 0) {
+      const double bi = b[row];
+      x[row] = dinv[row] * bi;
+      r[row] = bi - acc;
+    }
+  } else {
+    const int t = (blockIdx.x - na) * blockDim.x + threadIdx.x;
+    const int row = t / tm, sub = t & (tm - 1);
+    const double acc = group_sum_rt(csr_row_part_rt(m, mval, b, nullptr, row, sub, tm), tm);
+    if (row < m.n && sub == 0) bc[row] = acc;
+  }
+}
+
+// Coarse levels: the prolongation x += P c and the post-smoothing sweep in one pass.  With X0, R0
+// the pre-smoothed iterate and its residual (R0 = b - A X0), the sweep from X0 + P c is
+//   out = X0 + P c + D_w^-1 (R0 - (A P) c),
+// so one product over the rows of A P (whose pattern holds P's, a row of each per entry: pv, apv)
+// replaces the transfer kernel and the sweep's product with A; c is the coarser level's result.
+template <typename V, int T>
+__global__ void __launch_bounds__(kBlock) k_csr_prolong_smooth(CsrView m, const V* __restrict__ apv,
+                                                               const V* __restrict__ pv,
+                                                               const double* __restrict__ dinv,
+                                                               const double* __restrict__ x0,
+                                                               const double* __restrict__ r0,
+                                                               const double* __restrict__ c, double* __restrict__ out,
+                                                               const int* done) {
+  pdl_enter();
+  if (done && *done) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int g = t / T, sub = t & (T - 1);
+  const int R = m.rep;
+  double ap = 0.0, pp = 0.0;
+  if (g < m.n * R) {
+    const int row = g / R, r = g - row * R;
+    const int beg = __ldg(m.ptr + row), end = __ldg(m.ptr + row + 1);
+    for (int k0 = beg + sub; k0 < end; k0 += kCsrChunk * T) {
+      int j[kCsrChunk];
+      V a[kCsrChunk], p[kCsrChunk];
+#pragma unroll
+      for (int u = 0; u < kCsrChunk; ++u) {
+        const int k = k0 + u * T;
+        const bool ok = k < end;
+        j[u] = ok ? __ldg(m.col + k) : 0;
+        a[u] = ok ? __ldg(apv + k) : V(0);
+        p[u] = ok ? __ldg(pv + k) : V(0);
+      }
+#pragma unroll
+      for (int u = 0; u < kCsrChunk; ++u) {
+        const double cj = __ldg(c + j[u] * R + r);
+        ap = fma(static_cast<double>(a[u]), cj, ap);
+        pp = fma(static_cast<double>(p[u]), cj, pp);
+      }
+    }
+  }
+  ap = group_sum<T>(ap);
+  pp = group_sum<T>(pp);
+  if (g < m.n * R && sub == 0) out[g] = x0[g] + pp + dinv[g / R] * (r0[g] - ap);
+}
+
 // x = A_c^-1 b on the coarsest level (dense FP64 inverse, row-major, even leading dimension ld):
 // one warp per row and replica.
 __global__ void k_coarse_solve(int n, int ld, int R, const double* __restrict__ inv, const double* __restrict__ b,
@@ -422,7 +522,7 @@ __global__ void __launch_bounds__(kBlock) k_cg_rz(int n, const double* __restric
 // Last post-smoothing sweep of the finest level fused with rho = r.z:
 // z = x + D_w^-1 (r - A x); the last block sets beta = rho_new / rho (0 on the first pass).
 template <typename V>
-__global__ void __launch_bounds__(kBlock, kReduceMinBlocks<V>) k_jacobi_rz(SellView s, const V* __restrict__ val,
+__global__ void __launch_bounds__(kBlock) k_jacobi_rz(SellView s, const V* __restrict__ val,
                                                       const double* __restrict__ dinv, const double* __restrict__ r,
                                                       const double* __restrict__ xin, double* __restrict__ z,
                                                       CgScalars* S, double* partials, int first) {
@@ -557,6 +657,156 @@ __global__ void __launch_bounds__(kBlock) k_cg_update(int n, const double* __res
       S->done = 1;
       S->status = 3;  // not converged within maxit
     }
+  }
+}
+
+// Row-pair forms of the three finest-level kernels for one replica: thread g takes rows g and
+// g + H (H = half the rows rounded up to a multiple of 32, so both rows sit in the same lane of
+// their slices) and issues both rows' chunk loads, then both rows' gathers, before it uses any: two
+// independent index -> gather chains per thread, and half the threads, so that one wave of CTAs
+// covers the finest level (the single-row kernels leave a partial second wave).
+__host__ __device__ inline int pair_half(int n) { return (((n + 1) >> 1) + 31) & ~31; }
+
+// (A x)_a and (A x)_b for rows a < n and b (b < n or not), x gathered through gx(j), C entries of
+// each row per round.
+template <int C = kChunk, typename V, typename G>
+__device__ __forceinline__ double2 sell_pair_dot(const SellView& s, const V* __restrict__ val, int a, int b,
+                                                 bool hb, G gx) {
+  const int ba = __ldg(s.soff + (a >> 5)) + (a & 31), ea = __ldg(s.soff + (a >> 5) + 1);
+  const int bb = hb ? __ldg(s.soff + (b >> 5)) + (b & 31) : 0, eb = hb ? __ldg(s.soff + (b >> 5) + 1) : 0;
+  double acc_a = 0.0, acc_b = 0.0;
+  for (int o = 0; ba + o < ea || bb + o < eb; o += C * kSlice) {
+    int ja[C], jb[C];
+    V va[C], vb[C];
+#pragma unroll
+    for (int u = 0; u < C; ++u) {
+      const int ka = ba + o + u * kSlice, kb = bb + o + u * kSlice;
+      const bool oka = ka < ea, okb = kb < eb;
+      ja[u] = oka ? __ldg(s.col + ka) : a;
+      va[u] = oka ? __ldg(val + ka) : V(0);
+      jb[u] = okb ? __ldg(s.col + kb) : a;
+      vb[u] = okb ? __ldg(val + kb) : V(0);
+    }
+#pragma unroll
+    for (int u = 0; u < C; ++u) {
+      acc_a = fma(static_cast<double>(va[u]), gx(ja[u]), acc_a);
+      acc_b = fma(static_cast<double>(vb[u]), gx(jb[u]), acc_b);
+    }
+  }
+  return make_double2(acc_a, acc_b);
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_cg_dir_spmv_p(SellView s, const V* __restrict__ val,
+                                                          const double* __restrict__ z, double* __restrict__ p,
+                                                          double* __restrict__ q, CgScalars* S, double* partials) {
+  pdl_enter();
+  if (S->done) return;
+  const double beta = S->beta;
+  const int n = s.n, H = pair_half(n);
+  double v[1] = {0.0};
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < H; g += gridDim.x * blockDim.x) {
+    if (g >= n) continue;
+    const int b = g + H;
+    const bool hb = b < n;
+    const double2 az = sell_pair_dot(s, val, g, b, hb, [=](int j) { return __ldg(z + j); });
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (h == 1 && !hb) break;
+      const int i = h ? b : g;
+      const double zi = z[i], a = h ? az.y : az.x;
+      const double pi = (beta == 0.0) ? zi : fma(beta, p[i], zi);
+      const double qi = (beta == 0.0) ? a : fma(beta, q[i], a);
+      p[i] = pi;
+      q[i] = qi;
+      v[0] = fma(pi, qi, v[0]);
+    }
+  }
+  double tot[1];
+  if (grid_reduce<1>(v, partials, &S->ticket[2], tot) && threadIdx.x == 0) {
+    S->pq = tot[0];
+    S->alpha = S->rz / tot[0];
+  }
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_cg_update_jacobi0_p(SellView s, const V* __restrict__ val,
+                                                                const double* __restrict__ dinv,
+                                                                const double* __restrict__ p,
+                                                                const double* __restrict__ q, double* __restrict__ x,
+                                                                const double* __restrict__ r,
+                                                                double* __restrict__ r_new, double* __restrict__ X,
+                                                                double* __restrict__ Rres, CgScalars* S,
+                                                                double* partials) {
+  pdl_enter();
+  if (S->done) return;
+  const double alpha = S->alpha;
+  const int n = s.n, H = pair_half(n);
+  double v[1] = {0.0};
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < H; g += gridDim.x * blockDim.x) {
+    if (g >= n) continue;
+    const int b = g + H;
+    const bool hb = b < n;
+    // three gathered vectors per entry: four entries of each row per round keep it in registers
+    const double2 acc = sell_pair_dot<4>(s, val, g, b, hb, [=](int j) {
+      return __ldg(dinv + j) * fma(-alpha, __ldg(q + j), __ldg(r + j));
+    });
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (h == 1 && !hb) break;
+      const int i = h ? b : g;
+      const double ri = fma(-alpha, q[i], r[i]);
+      x[i] = fma(alpha, p[i], x[i]);
+      r_new[i] = ri;
+      X[i] = dinv[i] * ri;
+      Rres[i] = ri - (h ? acc.y : acc.x);
+      v[0] = fma(ri, ri, v[0]);
+    }
+  }
+  double tot[1];
+  if (grid_reduce<1>(v, partials, &S->ticket[3], tot) && threadIdx.x == 0) {
+    S->rr = tot[0];
+    S->iter += 1;
+    if (!(tot[0] == tot[0]) || !(S->pq > 0.0)) {
+      S->done = 1;
+      S->status = 5;  // breakdown / NaN
+    } else if (tot[0] <= S->tol2 * S->bb) {
+      S->done = 1;
+    } else if (S->iter >= S->maxit) {
+      S->done = 1;
+      S->status = 3;  // not converged within maxit
+    }
+  }
+}
+
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_jacobi_rz_p(SellView s, const V* __restrict__ val,
+                                                        const double* __restrict__ dinv, const double* __restrict__ r,
+                                                        const double* __restrict__ xin, double* __restrict__ z,
+                                                        CgScalars* S, double* partials, int first) {
+  pdl_enter();
+  if (S->done) return;
+  const int n = s.n, H = pair_half(n);
+  double v[1] = {0.0};
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < H; g += gridDim.x * blockDim.x) {
+    if (g >= n) continue;
+    const int b = g + H;
+    const bool hb = b < n;
+    const double2 ax = sell_pair_dot(s, val, g, b, hb, [=](int j) { return __ldg(xin + j); });
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (h == 1 && !hb) break;
+      const int i = h ? b : g;
+      const double ri = r[i];
+      const double zi = xin[i] + dinv[i] * (ri - (h ? ax.y : ax.x));
+      z[i] = zi;
+      v[0] = fma(ri, zi, v[0]);
+    }
+  }
+  double tot[1];
+  if (grid_reduce<1>(v, partials, &S->ticket[1], tot) && threadIdx.x == 0) {
+    S->beta = first ? 0.0 : tot[0] / S->rz;
+    S->rz = tot[0];
   }
 }
 
@@ -740,6 +990,14 @@ __global__ void __launch_bounds__(kBlock) k_csr_jacobi2(CsrView c, const V* __re
 // Interleaved replicas taken in pairs by the finest-level kernels: an even count of 8 or more.
 static bool paired(const SellView& s) { return s.rep >= 8 && s.rep % 2 == 0; }
 static bool paired(const CsrView& c, int tpr) { return tpr == 1 && c.rep >= 8 && c.rep % 2 == 0; }
+// Row pairs for one replica with FP32 operator values on levels of at least kRowPairMin rows (the
+// FP64 forms would need 80 registers a thread and are not built).
+constexpr bool kRowPairs = true;
+constexpr int kRowPairMin = 4096;
+template <typename V>
+static bool row_pairs(const SellView& s) {
+  return kRowPairs && s.rep == 1 && s.n >= kRowPairMin;
+}
 
 // Grid of the reduction kernels: at most eight 256-thread blocks per SM (a full SM); the rows
 // beyond are covered by a grid-stride loop, so that the blocks' publish-and-count tails are few.
@@ -749,26 +1007,6 @@ int reduce_grid(long long n) {
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cap = 8 * sms;
-  }
-  const int g = grid_for(n);
-  return g < cap ? g : cap;
-}
-
-// The grid of a grid-stride reduction kernel: one wave of the CTAs that are resident at once for
-// this kernel (its register count decides how many fit on an SM), at most one thread per row.
-// A grid of eight CTAs per SM for a kernel of which only five or six fit left a partial second
-// wave running alone.
-template <typename K>
-int reduce_grid_for(K kernel, long long n) {
-  static int cap = 0;
-  if (cap == 0) {
-    int dev = 0, sms = 148, per_sm = 0;
-    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, 0) != cudaSuccess || per_sm < 1) {
-      cudaGetLastError();
-      per_sm = 8;
-    }
-    cap = std::min(per_sm, 8) * sms;
   }
   const int g = grid_for(n);
   return g < cap ? g : cap;
@@ -827,6 +1065,21 @@ void launch_csr_jacobi(const CsrView& c, const V* val, const double* dinv, const
   }
   TMB_CSR_DISPATCH(tpr, k_csr_jacobi, 1LL * c.n * c.rep, c, val, dinv, b, xin, xout, done)
 }
+template <typename V>
+void launch_csr_pre_restrict(const CsrView& a, const V* aval, const double* dinv, const double* b, double* x,
+                             double* r, int ta, const CsrView& m, const V* mval, double* bc, int tm, const int* done,
+                             cudaStream_t st) {
+  note_launch();
+  const int na = grid_for(1LL * ta * a.n), nm = grid_for(1LL * tm * m.n);
+  launch_pdl(k_csr_pre_restrict<V>, na + nm, kBlock, 0, st, a, aval, dinv, b, x, r, ta, na, m, mval, bc, tm, done);
+}
+template <typename V>
+void launch_csr_prolong_smooth(const CsrView& m, const V* apv, const V* pv, const double* dinv, const double* x0,
+                               const double* r0, const double* c, double* out, const int* done, cudaStream_t st,
+                               int tpr) {
+  note_launch();
+  TMB_CSR_DISPATCH(tpr, k_csr_prolong_smooth, 1LL * m.n * m.rep, m, apv, pv, dinv, x0, r0, c, out, done)
+}
 #undef TMB_CSR_DISPATCH
 void launch_coarse_solve(int n, int ld, int rep, const double* inv, const double* b, double* x, const int* done,
                          cudaStream_t st, const float* invf, int ldf) {
@@ -856,8 +1109,7 @@ template <typename V>
 void launch_cg_residual(const SellView& s, const V* val, const double* bp, const double* x, double* r,
                         CgScalars* S, double* partials, cudaStream_t st) {
   note_launch();
-  launch_pdl(k_cg_residual<V>, reduce_grid_for(k_cg_residual<V>, 1LL * s.n * s.rep), kBlock, 0, st, s, val, bp, x, r,
-             S, partials);
+  launch_pdl(k_cg_residual<V>, reduce_grid(1LL * s.n * s.rep), kBlock, 0, st, s, val, bp, x, r, S, partials);
 }
 void launch_cg_rz(int n, const double* r, const double* z, CgScalars* S, double* partials, bool first,
                   cudaStream_t st) {
@@ -875,34 +1127,47 @@ template <typename V>
 void launch_jacobi_rz(const SellView& s, const V* val, const double* dinv, const double* r, const double* xin,
                       double* z, CgScalars* S, double* partials, bool first, cudaStream_t st) {
   note_launch();
+  if constexpr (sizeof(V) == 4) {
+    if (row_pairs<V>(s)) {
+      launch_pdl(k_jacobi_rz_p<V>, reduce_grid(pair_half(s.n)), kBlock, 0, st, s, val, dinv, r, xin, z, S, partials,
+                 first ? 1 : 0);
+      return;
+    }
+  }
   if (paired(s))
-    launch_pdl(k_jacobi_rz2<V>, reduce_grid_for(k_jacobi_rz2<V>, 1LL * s.n * s.rep / 2), kBlock, 0, st, s, val, dinv, r,
-               xin, z, S, partials,
+    launch_pdl(k_jacobi_rz2<V>, reduce_grid(1LL * s.n * s.rep / 2), kBlock, 0, st, s, val, dinv, r, xin, z, S, partials,
                first ? 1 : 0);
   else
-    launch_pdl(k_jacobi_rz<V>, reduce_grid_for(k_jacobi_rz<V>, 1LL * s.n * s.rep), kBlock, 0, st, s, val, dinv, r, xin,
-               z, S, partials,
+    launch_pdl(k_jacobi_rz<V>, reduce_grid(1LL * s.n * s.rep), kBlock, 0, st, s, val, dinv, r, xin, z, S, partials,
                first ? 1 : 0);
 }
 template <typename V>
 void launch_cg_dir_spmv(const SellView& s, const V* val, const double* z, double* p, double* q, CgScalars* S,
                         double* partials, cudaStream_t st) {
   note_launch();
-  if (paired(s))
-    launch_pdl(k_cg_dir_spmv2<V>, reduce_grid_for(k_cg_dir_spmv2<V>, 1LL * s.n * s.rep / 2), kBlock, 0, st, s, val, z, p,
-               q, S, partials);
-  else
-    launch_pdl(k_cg_dir_spmv<V>, reduce_grid_for(k_cg_dir_spmv<V>, 1LL * s.n * s.rep), kBlock, 0, st, s, val, z, p, q, S,
-               partials);
+  if constexpr (sizeof(V) == 4) {
+    if (row_pairs<V>(s)) {
+      launch_pdl(k_cg_dir_spmv_p<V>, reduce_grid(pair_half(s.n)), kBlock, 0, st, s, val, z, p, q, S, partials);
+      return;
+    }
+  }
+  if (paired(s)) launch_pdl(k_cg_dir_spmv2<V>, reduce_grid(1LL * s.n * s.rep / 2), kBlock, 0, st, s, val, z, p, q, S, partials);
+  else launch_pdl(k_cg_dir_spmv<V>, reduce_grid(1LL * s.n * s.rep), kBlock, 0, st, s, val, z, p, q, S, partials);
 }
 template <typename V>
 void launch_cg_update_jacobi0(const SellView& s, const V* val, const double* dinv, const double* p, const double* q,
                               double* x, const double* r, double* r_new, double* X, double* Rres, CgScalars* S,
                               double* partials, cudaStream_t st) {
   note_launch();
-  launch_pdl(k_cg_update_jacobi0<V>, reduce_grid_for(k_cg_update_jacobi0<V>, 1LL * s.n * s.rep), kBlock, 0, st, s, val,
-             dinv, p, q, x, r, r_new, X,
-                                                                              Rres, S, partials);
+  if constexpr (sizeof(V) == 4) {
+    if (row_pairs<V>(s)) {
+      launch_pdl(k_cg_update_jacobi0_p<V>, reduce_grid(pair_half(s.n)), kBlock, 0, st, s, val, dinv, p, q, x, r, r_new,
+                 X, Rres, S, partials);
+      return;
+    }
+  }
+  launch_pdl(k_cg_update_jacobi0<V>, reduce_grid(1LL * s.n * s.rep), kBlock, 0, st, s, val, dinv, p, q, x, r, r_new,
+               X, Rres, S, partials);
 }
 
 void launch_cg_update(int n, const double* p, const double* q, double* x, double* r, CgScalars* S,
@@ -918,6 +1183,12 @@ void launch_cg_update(int n, const double* p, const double* q, double* x, double
                                    cudaStream_t, int);                                                      \
   template void launch_csr_jacobi0_residual<V>(const CsrView&, const V*, const double*, const double*,      \
                                                double*, double*, const int*, cudaStream_t, int);            \
+  template void launch_csr_pre_restrict<V>(const CsrView&, const V*, const double*, const double*, double*,  \
+                                           double*, int, const CsrView&, const V*, double*, int, const int*,  \
+                                           cudaStream_t);                                                     \
+  template void launch_csr_prolong_smooth<V>(const CsrView&, const V*, const V*, const double*,             \
+                                             const double*, const double*, const double*, double*,          \
+                                             const int*, cudaStream_t, int);                                \
   template void launch_csr_jacobi<V>(const CsrView&, const V*, const double*, const double*, const double*, \
                                      double*, const int*, cudaStream_t, int);                               \
   template void launch_cg_init<V>(int, const CsrView&, const V*, const int*, const double*, double*,        \

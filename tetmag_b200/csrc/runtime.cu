@@ -243,7 +243,34 @@ struct DevLevel {
   DevArray<double> Ad, dinv, X, R, b, out;
   DevArray<float> Af;
   DevCsr P, Rop;
+  // coarse levels with one replica: A P (values) with P's values on its pattern, for the fused
+  // prolongation + post-smoothing sweep
+  bool fused_post = false;
+  DevCsr AP;
+  DevArray<double> pv;
+  DevArray<float> pvf;
+  int tAP = 1;
+  // coarse levels with one replica: M = R - (R A) D_w^-1, the restriction of the first sweep's
+  // residual straight from the level's right-hand side (merged with that sweep's launch)
+  bool fused_pre = false;
+  DevCsr M;
+  int tM = 1;
 };
+
+// P's values on the pattern of M = A P (which holds P's pattern when A has its diagonal); false if
+// an entry of P has no place in M.
+static bool values_on_pattern(const Csr& M, const Csr& P, std::vector<double>& out) {
+  out.assign(size_t(M.nnz()), 0.0);
+  for (int i = 0; i < P.nrows; ++i) {
+    int k = M.ptr[i];
+    for (int q = P.ptr[i]; q < P.ptr[i + 1]; ++q) {
+      while (k < M.ptr[i + 1] && M.col[k] < P.col[q]) ++k;
+      if (k == M.ptr[i + 1] || M.col[k] != P.col[q]) return false;
+      out[size_t(k)] = P.val[q];
+    }
+  }
+  return true;
+}
 
 struct Solver {
   Ctx* ctx;
@@ -417,6 +444,16 @@ struct Ctx {
     DevArray<long long> uoff[2], voff[2], toff[2];
     DevArray<HTerm> termd[2];             // per-term descriptors of the far-field product
     DevArray<double> tval;                // the terms' values, one matvec at a time
+    // the transposed product (the adjoint's B^T), built on first use: blocks ordered by column
+    std::vector<HBlockDev> hnearb, hfarb;
+    bool tbuilt = false;
+    int ntcols = 0, ntgroups[2] = {0, 0};
+    DevArray<HBlockDev> tnearb;
+    DevArray<HNearRow> tcols;
+    DevArray<HFarGroup> tgroups[2];
+    DevArray<long long> ttoff[2];
+    DevArray<HTerm> ttermd[2];
+    DevArray<double> ty;
     // the partition and the FP64 factors' offsets and ranks (host), for the H2 recompression
     HPartition part;
     std::vector<long long> huoff, hvoff;
@@ -454,8 +491,15 @@ struct Ctx {
   void h_compress(const double* bxyz, const double* bnrm, int leaf, double eta, double eps_mixed, double eps_fp64,
                   int kmax, bool keep_dense, const MeshHost* mesh = nullptr);
   void h_verify(double* block_out, double* out);
+  // the boundary product alone (DemagField::mvp), boundary vectors in boundary-node order
+  void bem_apply(const double* xb, double* yb, bool transpose);
+  DevArray<double> bap_u, bap_w, bap_part;
+  DevArray<float> bap_f;
   template <typename T>
   HMatView<T> h_view(int which) const;
+  void h_transpose_build();
+  template <typename T>
+  HMatView<T> ht_view(int which) const;
   // demag
   std::unique_ptr<Solver> neu, dir;
   double tol = 1e-7;
@@ -689,6 +733,29 @@ void Solver::compute() {
       // with 8 or more interleaved replicas a warp already covers replicas of one row
       d.tP = rep >= 8 ? 1 : csr_threads_per_row(hl.P.nrows, hl.P.nnz());
       d.tR = rep >= 8 ? 1 : csr_threads_per_row(hl.R.nrows, hl.R.nnz());
+      if (l > 0 && rep == 1) {
+        Csr AP;
+        csr_multiply(hl.A, hl.P, AP);
+        std::vector<double> pvals;
+        if (values_on_pattern(AP, hl.P, pvals)) {
+          d.AP.upload(AP, st);
+          d.pv.upload(pvals, st);
+          std::vector<float> pf(pvals.begin(), pvals.end());
+          d.pvf.upload(pf, st);
+          d.tAP = csr_threads_per_row(AP.nrows, AP.nnz());
+          d.fused_post = true;
+        }
+        Csr RA;
+        csr_multiply(hl.R, hl.A, RA);
+        std::vector<double> rv;
+        if (values_on_pattern(RA, hl.R, rv)) {
+          for (int j = 0; j < RA.nrows; ++j)
+            for (int k = RA.ptr[j]; k < RA.ptr[j + 1]; ++k) RA.val[k] = rv[k] - RA.val[k] * hl.dinv[RA.col[k]];
+          d.M.upload(RA, st);
+          d.tM = csr_threads_per_row(RA.nrows, RA.nnz());
+          d.fused_pre = true;
+        }
+      }
     }
   }
   ncoarse = H.ncoarse;
@@ -776,6 +843,17 @@ void Solver::vcycle(size_t l, const double* b, double* out, int precision, cudaS
       else launch_jacobi0_residual<float>(A, L.Af.p, L.dinv.p, b, L.X.p, L.R.p, done, st);
       pe();
     }
+  } else if (L.fused_pre) {
+    // first sweep with its residual, and the restriction as M b, in one launch
+    const CsrView A = L.Ac.view(rep);
+    pb(13, sweep + 4.0 * 8.0 * nl + double(L.M.col.n) * (sv + 4.0) + 4.0 * (C.n + 1) + 8.0 * nc);
+    if (f64)
+      launch_csr_pre_restrict<double>(A, L.Ac.v.p, L.dinv.p, b, L.X.p, L.R.p, L.tA, L.M.view(rep), L.M.v.p, C.b.p,
+                                      L.tM, done, st);
+    else
+      launch_csr_pre_restrict<float>(A, L.Ac.vf.p, L.dinv.p, b, L.X.p, L.R.p, L.tA, L.M.view(rep), L.M.vf.p, C.b.p,
+                                     L.tM, done, st);
+    pe();
   } else {
     const CsrView A = L.Ac.view(rep);
     pb(13, sweep + 4.0 * 8.0 * nl);
@@ -783,11 +861,25 @@ void Solver::vcycle(size_t l, const double* b, double* out, int precision, cudaS
     else launch_csr_jacobi0_residual<float>(A, L.Ac.vf.p, L.dinv.p, b, L.X.p, L.R.p, done, st, L.tA);
     pe();
   }
-  pb(11, double(L.Rop.col.n) * (sv + 4.0) + 4.0 * (C.n + 1) + 8.0 * (nl + nc));
-  if (f64) launch_csr_spmv<double>(L.Rop.view(rep), L.Rop.v.p, L.R.p, C.b.p, false, done, st, L.tR);
-  else launch_csr_spmv<float>(L.Rop.view(rep), L.Rop.vf.p, L.R.p, C.b.p, false, done, st, L.tR);
-  pe();
+  if (l == 0 || !L.fused_pre) {
+    pb(11, double(L.Rop.col.n) * (sv + 4.0) + 4.0 * (C.n + 1) + 8.0 * (nl + nc));
+    if (f64) launch_csr_spmv<double>(L.Rop.view(rep), L.Rop.v.p, L.R.p, C.b.p, false, done, st, L.tR);
+    else launch_csr_spmv<float>(L.Rop.view(rep), L.Rop.vf.p, L.R.p, C.b.p, false, done, st, L.tR);
+    pe();
+  }
   vcycle(l + 1, C.b.p, C.out.p, precision, st, -1);
+  if (l > 0 && L.fused_post) {
+    // prolongation and post-smoothing sweep in one pass over the rows of A P
+    pb(13, double(L.AP.col.n) * (2.0 * sv + 4.0) + 4.0 * (L.n + 1) + 8.0 * (nc + 4.0 * nl));
+    if (f64)
+      launch_csr_prolong_smooth<double>(L.AP.view(rep), L.AP.v.p, L.pv.p, L.dinv.p, L.X.p, L.R.p, C.out.p, out, done,
+                                        st, L.tAP);
+    else
+      launch_csr_prolong_smooth<float>(L.AP.view(rep), L.AP.vf.p, L.pvf.p, L.dinv.p, L.X.p, L.R.p, C.out.p, out, done,
+                                       st, L.tAP);
+    pe();
+    return;
+  }
   pb(12, double(L.P.col.n) * (sv + 4.0) + 4.0 * (L.n + 1) + 8.0 * (nc + 2.0 * nl));
   if (f64) launch_csr_spmv<double>(L.P.view(rep), L.P.v.p, C.out.p, L.X.p, true, done, st, L.tP);
   else launch_csr_spmv<float>(L.P.view(rep), L.P.vf.p, C.out.p, L.X.p, true, done, st, L.tP);
@@ -1340,6 +1432,179 @@ HMatView<T> Ctx::h_view(int w) const {
   return v;
 }
 
+template <typename T>
+HMatView<T> Ctx::ht_view(int w) const {
+  HMatView<T> v = h_view<T>(w);
+  v.nrows = H.ntcols;
+  v.near_rows = H.tcols.p;
+  v.near = H.tnearb.p;
+  v.ngroups = H.ntgroups[w];
+  v.groups = H.tgroups[w].p;
+  v.terms = H.ttermd[w].p;
+  v.toff = H.ttoff[w].p;
+  v.far = nullptr;
+  v.rank = nullptr;
+  v.uoff = nullptr;
+  v.voff = nullptr;
+  std::swap(v.U, v.V);  // t = U^T x, then y += V t
+  return v;
+}
+
+// The transposed hierarchical product's work lists, from the host copies of the blocks: near
+// tiles grouped by leaf column cluster; per precision, the admissible blocks ordered by column
+// cluster, one term per rank with U's column as the streamed vector and V's column as the
+// accumulated one, cut into runs of about the same work as the forward product's.
+void Ctx::h_transpose_build() {
+  if (H.tbuilt) return;
+  cudaStream_t st = stream;
+  std::vector<int> ord(H.hnearb.size());
+  std::iota(ord.begin(), ord.end(), 0);
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) {
+    return H.hnearb[a].cb < H.hnearb[b].cb || (H.hnearb[a].cb == H.hnearb[b].cb && H.hnearb[a].rb < H.hnearb[b].rb);
+  });
+  std::vector<HBlockDev> tn;
+  std::vector<HNearRow> cols;
+  for (int q : ord) {
+    const HBlockDev& b = H.hnearb[q];
+    const int p = int(tn.size());
+    if (cols.empty() || cols.back().rb != b.cb) cols.push_back(HNearRow{b.cb, b.n, p, p + 1});
+    else cols.back().last = p + 1;
+    tn.push_back(b);
+  }
+  long long covered = 0;
+  for (const auto& c : cols) covered += c.m;
+  if (covered != nb) throw Error(TMB_ERR_INTERNAL, "H-matrix: leaf columns do not cover the boundary");
+  H.tnearb.upload(tn, st);
+  H.tcols.upload(cols, st);
+  H.ntcols = int(cols.size());
+  const int nf = int(H.hfarb.size());
+  std::vector<int> fo(nf);
+  std::iota(fo.begin(), fo.end(), 0);
+  std::stable_sort(fo.begin(), fo.end(), [&](int a, int b) {
+    return H.hfarb[a].cb < H.hfarb[b].cb || (H.hfarb[a].cb == H.hfarb[b].cb && H.hfarb[a].rb < H.hfarb[b].rb);
+  });
+  for (int w = 0; w < 2; ++w) {
+    // the compact factor offsets of precision w, in the forward block order
+    std::vector<long long> uo(nf), vo(nf);
+    std::vector<int> rk(nf);
+    long long su = 0, sv = 0;
+    for (int q = 0; q < nf; ++q) {
+      rk[q] = H.ranks[size_t(3) * q + w];
+      uo[q] = su;
+      vo[q] = sv;
+      su += (long long)rk[q] * pad4(H.hfarb[q].m);
+      sv += (long long)rk[q] * pad4(H.hfarb[q].n);
+    }
+    std::vector<HTerm> td;
+    std::vector<long long> to(size_t(nf) + 1);
+    long long stt = 0;
+    std::vector<HFarGroup> groups;
+    for (int p = 0; p < nf; ++p) {
+      const int q = fo[p];
+      const HBlockDev& b = H.hfarb[q];
+      to[p] = stt;
+      const int mp = pad4(b.m), np = pad4(b.n);
+      for (int l = 0; l < rk[q]; ++l) td.push_back(HTerm{uo[q] + (long long)l * mp, vo[q] + (long long)l * np, mp, b.rb});
+      stt += rk[q];
+      if (groups.empty() || groups.back().rb != b.cb) groups.push_back(HFarGroup{b.cb, b.n, p, p + 1});
+      else groups.back().last = p + 1;
+    }
+    to[nf] = stt;
+    if (stt != H.terms[w]) throw Error(TMB_ERR_INTERNAL, "H-matrix: transposed term count differs");
+    double total = 0.0;
+    for (int q = 0; q < nf; ++q) total += double(rk[q]) * (H.hfarb[q].m + H.hfarb[q].n);
+    const double wmax = std::max(4096.0, total / (64.0 * num_sms));
+    std::vector<HFarGroup> items;
+    std::vector<double> work;
+    for (const HFarGroup& g : groups) {
+      HFarGroup it{g.rb, g.m, g.first, g.first};
+      double wk = 0.0;
+      for (int p = g.first; p < g.last; ++p) {
+        const int q = fo[p];
+        const double wq = double(rk[q]) * (H.hfarb[q].m + H.hfarb[q].n);
+        if (wk > 0.0 && wk + wq > wmax) {
+          items.push_back(it);
+          work.push_back(wk);
+          it.first = p;
+          wk = 0.0;
+        }
+        it.last = p + 1;
+        wk += wq;
+      }
+      if (wk > 0.0) {
+        items.push_back(it);
+        work.push_back(wk);
+      }
+    }
+    std::vector<int> order(items.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
+    std::vector<HFarGroup> sorted;
+    for (int g : order) sorted.push_back(items[g]);
+    H.ntgroups[w] = int(sorted.size());
+    H.tgroups[w].upload(sorted, st);
+    H.ttoff[w].upload(to, st);
+    H.ttermd[w].upload(td, st);
+  }
+  H.ty.alloc(size_t(std::max(nb, 1)));
+  sync();
+  H.tbuilt = true;
+}
+
+// y = B x or B^T x for boundary vectors in boundary-node order (device pointers), with the
+// current boundary matrix form and precision: dense (mode 0), hierarchical (1) or H2 (2, forward
+// only).  One component, no replicas.
+void Ctx::bem_apply(const double* xb, double* yb, bool transpose) {
+  require_mesh();
+  if (!has_bem) throw Error(TMB_ERR_STATE, "bem_apply: no BEM matrix set");
+  if (ncomp() != 1 || rep != 1) throw Error(TMB_ERR_STATE, "bem_apply: one component, no replicas");
+  if (transpose && bem_mode == 2) throw Error(TMB_ERR_STATE, "bem_apply: the H2 form has no transposed product");
+  cudaStream_t st = stream;
+  const bool f64 = precision == TMB_FP64;
+  if (bem_mode == 0) {
+    if (f64 ? !Bd.p : !Bf.p) throw Error(TMB_ERR_STATE, "bem_apply: the dense matrix was not kept");
+    if (transpose) {
+      const int nch = bem_gemv_t_chunks(nb, num_sms);
+      bap_part.alloc(size_t(nch) * nb);
+      if (f64) launch_bem_gemv_t<double>(nb, Bd.p, xb, bap_part.p, nch, yb, st);
+      else launch_bem_gemv_t<float>(nb, Bf.p, xb, bap_part.p, nch, yb, st);
+    } else if (f64) {
+      launch_bem_gemv<double>(nb, Bd.p, xb, yb, st);
+    } else {
+      // the FP32 operand copy of x: scatter to a node vector, gather in FP32
+      bap_u.alloc(size_t(n));
+      bap_f.alloc(size_t(nb));
+      bap_u.zero(st);
+      launch_scatter_add(nb, bnodes.p, xb, bap_u.p, st);
+      launch_gather<float>(nb, bap_u.p, bnodes.p, bap_f.p, st);
+      launch_bem_gemv<float>(nb, Bf.p, bap_f.p, yb, st);
+    }
+    return;
+  }
+  bap_u.alloc(size_t(n));
+  bap_w.alloc(size_t(n));
+  bap_u.zero(st);
+  launch_scatter_add(nb, bnodes.p, xb, bap_u.p, st);
+  if (transpose) {
+    h_transpose_build();
+    if (f64) launch_h_matvec_t<double>(ht_view<double>(0), bap_u.p, H.ty.p, H.xp64.p, st);
+    else launch_h_matvec_t<float>(ht_view<float>(1), bap_u.p, H.ty.p, H.xp32.p, st);
+    bap_w.zero(st);
+    launch_scatter_add(nb, H.gidx.p, H.ty.p, bap_w.p, st);
+  } else if (bem_mode == 2) {
+    if (f64)
+      launch_h2_matvec<double>(h2_view<double>(0), bap_u.p, H.y.p, H.xp64.p, H.pos.p, n, bap_w.p, H2[0].up, H2[0].down,
+                               st);
+    else
+      launch_h2_matvec<float>(h2_view<float>(1), bap_u.p, H.y.p, H.xp32.p, H.pos.p, n, bap_w.p, H2[1].up, H2[1].down,
+                              st);
+  } else {
+    if (f64) launch_h_matvec<double>(h_view<double>(0), bap_u.p, H.y.p, H.xp64.p, H.pos.p, n, bap_w.p, st);
+    else launch_h_matvec<float>(h_view<float>(1), bap_u.p, H.y.p, H.xp32.p, H.pos.p, n, bap_w.p, st);
+  }
+  launch_gather<double>(nb, bap_w.p, bnodes.p, yb, st);
+}
+
 // Compresses the device-assembled dense FP64 BEM matrix into the hierarchical form:
 // dense leaf tiles plus ACA low-rank blocks, FP64 terms to eps_fp64 and FP32 terms to eps_mixed.
 // With `mesh` the entries come from the boundary mesh instead (no dense matrix needed): dense
@@ -1440,6 +1705,8 @@ void Ctx::h_compress(const double* bxyz, const double* bnrm, int leaf, double et
     H.gnrm.upload(Bm.tri_normal, st);
   }
   const HSource src = h_source();
+  H.hnearb = nearb;
+  H.hfarb = farb;
   H.nearb.upload(nearb, st);
   H.rows.upload(rows, st);
   H.farb.upload(farb, st);
@@ -2313,11 +2580,19 @@ void Ctx::vjp(const double* Y, const double* H, const double* abar, double* gout
     if (f64) launch_divergence<double>(S, tg[0].p, tg[1].p, tg[2].p, ab.mu.p, ab.ninvvol.p, 1.0, ab.w.p, stream);
     else launch_divergence<float>(S, tgf[0].p, tgf[1].p, tgf[2].p, ab.mu.p, ab.ninvvol.p, 1.0, ab.w.p, stream);
     dir->solve_t(ab.w.p, ab.v.p, precision, stage);
-    launch_gather<double>(nb, ab.v.p, bnodes.p, ab.vb.p, stream);
-    const int nch = bem_gemv_t_chunks(nb, num_sms);
-    if (f64) launch_bem_gemv_t<double>(nb, Bd.p, ab.vb.p, ab.bpart.p, nch, ab.z.p, stream);
-    else launch_bem_gemv_t<float>(nb, Bf.p, ab.vb.p, ab.bpart.p, nch, ab.z.p, stream);
-    launch_scatter_add(nb, bnodes.p, ab.z.p, ab.w.p, stream);
+    if (bem_mode == 1) {
+      // hierarchical B^T in cluster order, scattered back to the boundary nodes
+      HMat& Hm = this->H;  // H is the stage field here
+      if (f64) launch_h_matvec_t<double>(ht_view<double>(0), ab.v.p, Hm.ty.p, Hm.xp64.p, stream);
+      else launch_h_matvec_t<float>(ht_view<float>(1), ab.v.p, Hm.ty.p, Hm.xp32.p, stream);
+      launch_scatter_add(nb, Hm.gidx.p, Hm.ty.p, ab.w.p, stream);
+    } else {
+      launch_gather<double>(nb, ab.v.p, bnodes.p, ab.vb.p, stream);
+      const int nch = bem_gemv_t_chunks(nb, num_sms);
+      if (f64) launch_bem_gemv_t<double>(nb, Bd.p, ab.vb.p, ab.bpart.p, nch, ab.z.p, stream);
+      else launch_bem_gemv_t<float>(nb, Bf.p, ab.vb.p, ab.bpart.p, nch, ab.z.p, stream);
+      launch_scatter_add(nb, bnodes.p, ab.z.p, ab.w.p, stream);
+    }
     neu->solve_t(ab.w.p, ab.a1.p, precision, stage);
     cnt[4] += neu->last_iters + dir->last_iters;
     if (f64) launch_gradient<double>(S, g[0].p, g[1].p, g[2].p, ab.a1.p, nullptr, nullptr, ab.q.p, nullptr, stream);
@@ -2333,13 +2608,16 @@ void Ctx::vjp(const double* Y, const double* H, const double* abar, double* gout
   la.kax = kax.p;
   la.idm_d = idmi ? idm_d.p : nullptr;
   la.idm_b = idmi ? idm_b.p : nullptr;
+  la.dmi_s = (has_dmi && !idmi) ? dmi_s.p : nullptr;
+  la.area = area.p;
+  la.nvn = nvn.p;
   la.vol = node_vol.p;
   la.js = js.p;
   la.q = q;
   la.inv_mu0 = 1.0 / kMu0;
   la.g = gout;
-  if (f64) launch_adj_local<double>(S, K.p, tg[0].p, tg[1].p, g[0].p, g[1].p, la, stream);
-  else launch_adj_local<float>(S, Kf.p, tgf[0].p, tgf[1].p, gf[0].p, gf[1].p, la, stream);
+  if (f64) launch_adj_local<double>(S, K.p, tg[0].p, tg[1].p, g[0].p, g[1].p, g[2].p, la, stream);
+  else launch_adj_local<float>(S, Kf.p, tgf[0].p, tgf[1].p, gf[0].p, gf[1].p, gf[2].p, la, stream);
   cnt[2] += 1;
 }
 
@@ -2367,14 +2645,13 @@ void Ctx::adjoint_rk4(const double* m0, int nsteps, double dt_ps, int nsub, int 
                       const double* w, double* m_final, double* grad_m0, double* grad_ku, double* grad_bz) {
   require_mesh();
   require_material();
-  if (has_dmi && dmi_kind != 1)
-    throw Error(TMB_ERR_STATE, "adjoint: the bulk DMI form has no transpose here (interfacial or none)");
-  if (has_bem && (ncomp() != 1 || bem_mode != 0))
-    throw Error(TMB_ERR_STATE, "adjoint: needs one component and the dense BEM matrix");
+  if (has_bem && (ncomp() != 1 || (bem_mode != 0 && bem_mode != 1)))
+    throw Error(TMB_ERR_STATE, "adjoint: needs one component and the dense or hierarchical BEM matrix");
   if (rep != 1) throw Error(TMB_ERR_STATE, "adjoint: not for interleaved replicas");
   if (has_cub || has_srf || has_stt)
     throw Error(TMB_ERR_STATE, "adjoint: cubic / surface anisotropy and spin-transfer torque have no transpose here");
   if (has_bem) ensure_demag();
+  if (has_bem && bem_mode == 1) h_transpose_build();
   cudaStream_t st = stream;
   const size_t n3 = size_t(3) * n;
   const int nck = (nsteps + ckpt - 1) / ckpt;
@@ -2938,6 +3215,25 @@ int tmb_bem_verify(tmb_ctx* ctx, double* block_out, double* out) {
   TMB_API_BEGIN
   TMB_CUDA(cudaSetDevice(ctx->c->device));
   ctx->c->h_verify(block_out, out);
+  TMB_API_END
+}
+
+int tmb_bem_apply(tmb_ctx* ctx, const double* x, double* y, int transpose, int ptr_kind) {
+  TMB_CHECK_ARG(ctx && x && y, "tmb_bem_apply: null argument");
+  TMB_API_BEGIN
+  Ctx& c = *ctx->c;
+  TMB_CUDA(cudaSetDevice(c.device));
+  c.require_mesh();
+  const size_t nbv = size_t(c.nb);
+  const double* xd = stage_in(c, c.in3, x, nbv, ptr_kind);
+  if (ptr_kind == TMB_PTR_DEVICE) {
+    c.bem_apply(xd, y, transpose != 0);
+  } else {
+    c.out3.alloc(nbv);
+    c.bem_apply(xd, c.out3.p, transpose != 0);
+    TMB_CUDA(cudaMemcpyAsync(y, c.out3.p, nbv * sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+    c.sync();
+  }
   TMB_API_END
 }
 

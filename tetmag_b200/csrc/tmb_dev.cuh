@@ -162,6 +162,19 @@ void launch_csr_spmv(const CsrView& c, const V* val, const double* x, double* y,
 template <typename V>
 void launch_csr_jacobi0_residual(const CsrView& c, const V* val, const double* dinv, const double* b, double* x,
                                  double* r, const int* done, cudaStream_t st, int tpr);
+// Coarse levels, one replica: the first sweep from zero with its residual, and the restriction of
+// that residual as bc = M b (M = R - (R A) D_w^-1), in one launch (ta, tm threads per row).
+template <typename V>
+void launch_csr_pre_restrict(const CsrView& a, const V* aval, const double* dinv, const double* b, double* x,
+                             double* r, int ta, const CsrView& m, const V* mval, double* bc, int tm, const int* done,
+                             cudaStream_t st);
+// Coarse levels: prolongation x += P c fused with the post-smoothing sweep, over the rows of A P
+// (values apv) with P's values on the same pattern (pv); x0, r0 the pre-smoothed iterate and its
+// residual.
+template <typename V>
+void launch_csr_prolong_smooth(const CsrView& m, const V* apv, const V* pv, const double* dinv, const double* x0,
+                               const double* r0, const double* c, double* out, const int* done, cudaStream_t st,
+                               int tpr);
 template <typename V>
 void launch_csr_jacobi(const CsrView& c, const V* val, const double* dinv, const double* b, const double* xin,
                        double* xout, const int* done, cudaStream_t st, int tpr);
@@ -315,6 +328,13 @@ void launch_h_compact(int nblk, const HBlockDev* blk, const double* Us, const do
 template <typename T>
 void launch_h_matvec(const HMatView<T>& H, const double* u, double* y, T* xp, const int* pos, int n, double* bdir,
                      cudaStream_t st);
+// Transposed product y (cluster order, FP64) = H^T u[boundary], from a view whose near-field
+// groups are the leaf column clusters (near_rows: column cluster, its blocks [first, last) of
+// `near` ordered by column), whose far-field groups, terms and offsets are the admissible blocks
+// ordered by column cluster with U and V exchanged (t = U^T x, then y += V t); the dense tiles are
+// the forward ones, read by columns.
+template <typename T>
+void launch_h_matvec_t(const HMatView<T>& Ht, const double* u, double* y, T* xp, cudaStream_t st);
 
 // --- H2 matrix (nested cluster bases, h2.cpp) -----------------------------------------------
 // One cluster of the tree: position range, ranks of its row and column bases, tree links,
@@ -391,6 +411,9 @@ struct AdjLocalArgs {
   const double* kax;     // 3N
   const double* idm_d;   // N  D (interfacial DMI), null otherwise
   const double* idm_b;   // N  1 / (V Js), null without interfacial DMI
+  const double* dmi_s;   // N  D / (V Js) (bulk DMI), null otherwise
+  const double* area;    // N  boundary node areas (bulk DMI surface term)
+  const double* nvn;     // 3N boundary node normals (bulk DMI surface term)
   const double* vol;     // N  node volumes
   const double* js;      // N
   const double* q;       // 3N -grad a1 of the transposed demag chain, null without demag
@@ -407,7 +430,7 @@ void launch_adj_normalize(int n, const double* y, const double* zn, double* lam,
 int adj_pre_blocks(int n);
 void launch_adj_pre(const AdjPreArgs& a, cudaStream_t st);
 template <typename V>
-void launch_adj_local(const SellView& s, const V* K, const V* tg0, const V* tg1, const V* gr0, const V* gr1,
+void launch_adj_local(const SellView& s, const V* K, const V* tg0, const V* tg1, const V* gr0, const V* gr1, const V* gr2,
                       const AdjLocalArgs& a, cudaStream_t st);
 int bem_gemv_t_chunks(int nb, int num_sms);
 template <typename V>
