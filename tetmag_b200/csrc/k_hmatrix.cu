@@ -309,11 +309,10 @@ __global__ void k_h_gather(int nb, const double* __restrict__ u, const int* __re
 
 // Dense leaf tiles: one CTA per leaf row cluster (<= 32 rows), warps stride over its tiles.
 template <typename T>
-__global__ void __launch_bounds__(256) k_h_near(const HNearRow* __restrict__ rows, const HBlockDev* __restrict__ blk,
-                                                const T* __restrict__ D, const T* __restrict__ xp,
-                                                double* __restrict__ y) {
+__device__ __forceinline__ void h_near_row(int bx, const HNearRow* __restrict__ rows, const HBlockDev* __restrict__ blk,
+                                           const T* __restrict__ D, const T* __restrict__ xp, double* __restrict__ y) {
   __shared__ double acc[8][33];
-  const HNearRow R = rows[blockIdx.x];
+  const HNearRow R = rows[bx];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double a = 0.0;
   for (int q = R.first + warp; q < R.last; q += 8) {
@@ -330,6 +329,13 @@ __global__ void __launch_bounds__(256) k_h_near(const HNearRow* __restrict__ row
     for (int w = 0; w < 8; ++w) s += acc[w][lane];
     y[R.rb + lane] = s;
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_h_near(const HNearRow* __restrict__ rows, const HBlockDev* __restrict__ blk,
+                                                const T* __restrict__ D, const T* __restrict__ xp,
+                                                double* __restrict__ y) {
+  h_near_row<T>(blockIdx.x, rows, blk, D, xp, y);
 }
 
 // Transposed near field: one CTA per leaf column cluster sigma, y_sigma = sum_b D_b^T x_tau over
@@ -451,13 +457,12 @@ struct Vec16<double> {
 // past its end.
 constexpr int kLanesPerTerm = 8;
 template <typename T>
-__global__ void __launch_bounds__(256) k_h_vt(long long nterms, const HTerm* __restrict__ terms,
-                                              const T* __restrict__ V, const T* __restrict__ xp,
-                                              double* __restrict__ t) {
+__device__ __forceinline__ void h_vt_block(long long bx, long long nterms, const HTerm* __restrict__ terms,
+                                           const T* __restrict__ V, const T* __restrict__ xp, double* __restrict__ t) {
   using W = Vec16<T>;
   using VT = typename W::type;
   constexpr int L = kLanesPerTerm;
-  const long long p = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / L;
+  const long long p = (bx * blockDim.x + threadIdx.x) / L;
   const int sub = threadIdx.x & (L - 1);
   const bool ok = p < nterms;
   const HTerm h = terms[ok ? p : 0];
@@ -477,6 +482,26 @@ __global__ void __launch_bounds__(256) k_h_vt(long long nterms, const HTerm* __r
 #pragma unroll
   for (int o = L / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
   if (sub == 0 && ok) t[p] = acc;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_h_vt(long long nterms, const HTerm* __restrict__ terms,
+                                              const T* __restrict__ V, const T* __restrict__ xp,
+                                              double* __restrict__ t) {
+  h_vt_block<T>(blockIdx.x, nterms, terms, V, xp, t);
+}
+
+// The dense near field and the far field's first pass are independent: one launch whose first
+// nrows CTAs take the leaf row clusters' tiles and whose others take the terms, so the
+// latency-bound tile rows run beside the streaming V^T x instead of before it.
+template <typename T>
+__global__ void __launch_bounds__(256) k_h_near_vt(int nrows, const HNearRow* __restrict__ rows,
+                                                   const HBlockDev* __restrict__ blk, const T* __restrict__ D,
+                                                   double* __restrict__ y, long long nterms,
+                                                   const HTerm* __restrict__ terms, const T* __restrict__ V,
+                                                   const T* __restrict__ xp, double* __restrict__ t) {
+  if (int(blockIdx.x) < nrows) h_near_row<T>(blockIdx.x, rows, blk, D, xp, y);
+  else h_vt_block<T>((long long)blockIdx.x - nrows, nterms, terms, V, xp, t);
 }
 
 // Far field, second pass: y_tau += sum_b U_b t_b over the admissible blocks of one work item (a
@@ -621,11 +646,10 @@ void launch_h_matvec(const HMatView<T>& H, const double* u, double* y, T* xp, co
   note_launch();
   k_h_gather<T><<<grid_for(H.nb), kBlock, 0, st>>>(H.nb, u, H.gidx, xp);
   note_launch();
-  k_h_near<T><<<H.nrows, 256, 0, st>>>(H.near_rows, H.near, H.D, xp, y);
+  const long long vt_blocks = (H.nterms * kLanesPerTerm + 255) / 256;
+  k_h_near_vt<T><<<unsigned(H.nrows + vt_blocks), 256, 0, st>>>(H.nrows, H.near_rows, H.near, H.D, y, H.nterms,
+                                                                H.terms, H.V, xp, H.t);
   if (H.nterms > 0) {
-    note_launch();
-    const long long threads = H.nterms * kLanesPerTerm;
-    k_h_vt<T><<<unsigned((threads + 255) / 256), 256, 0, st>>>(H.nterms, H.terms, H.V, xp, H.t);
     note_launch();
     k_h_ut<T><<<H.ngroups, 256, 0, st>>>(H.groups, H.toff, H.terms, H.U, H.t, y);
   }

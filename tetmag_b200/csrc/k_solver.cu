@@ -660,156 +660,6 @@ __global__ void __launch_bounds__(kBlock) k_cg_update(int n, const double* __res
   }
 }
 
-// Row-pair forms of the three finest-level kernels for one replica: thread g takes rows g and
-// g + H (H = half the rows rounded up to a multiple of 32, so both rows sit in the same lane of
-// their slices) and issues both rows' chunk loads, then both rows' gathers, before it uses any: two
-// independent index -> gather chains per thread, and half the threads, so that one wave of CTAs
-// covers the finest level (the single-row kernels leave a partial second wave).
-__host__ __device__ inline int pair_half(int n) { return (((n + 1) >> 1) + 31) & ~31; }
-
-// (A x)_a and (A x)_b for rows a < n and b (b < n or not), x gathered through gx(j), C entries of
-// each row per round.
-template <int C = kChunk, typename V, typename G>
-__device__ __forceinline__ double2 sell_pair_dot(const SellView& s, const V* __restrict__ val, int a, int b,
-                                                 bool hb, G gx) {
-  const int ba = __ldg(s.soff + (a >> 5)) + (a & 31), ea = __ldg(s.soff + (a >> 5) + 1);
-  const int bb = hb ? __ldg(s.soff + (b >> 5)) + (b & 31) : 0, eb = hb ? __ldg(s.soff + (b >> 5) + 1) : 0;
-  double acc_a = 0.0, acc_b = 0.0;
-  for (int o = 0; ba + o < ea || bb + o < eb; o += C * kSlice) {
-    int ja[C], jb[C];
-    V va[C], vb[C];
-#pragma unroll
-    for (int u = 0; u < C; ++u) {
-      const int ka = ba + o + u * kSlice, kb = bb + o + u * kSlice;
-      const bool oka = ka < ea, okb = kb < eb;
-      ja[u] = oka ? __ldg(s.col + ka) : a;
-      va[u] = oka ? __ldg(val + ka) : V(0);
-      jb[u] = okb ? __ldg(s.col + kb) : a;
-      vb[u] = okb ? __ldg(val + kb) : V(0);
-    }
-#pragma unroll
-    for (int u = 0; u < C; ++u) {
-      acc_a = fma(static_cast<double>(va[u]), gx(ja[u]), acc_a);
-      acc_b = fma(static_cast<double>(vb[u]), gx(jb[u]), acc_b);
-    }
-  }
-  return make_double2(acc_a, acc_b);
-}
-
-template <typename V>
-__global__ void __launch_bounds__(kBlock) k_cg_dir_spmv_p(SellView s, const V* __restrict__ val,
-                                                          const double* __restrict__ z, double* __restrict__ p,
-                                                          double* __restrict__ q, CgScalars* S, double* partials) {
-  pdl_enter();
-  if (S->done) return;
-  const double beta = S->beta;
-  const int n = s.n, H = pair_half(n);
-  double v[1] = {0.0};
-  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < H; g += gridDim.x * blockDim.x) {
-    if (g >= n) continue;
-    const int b = g + H;
-    const bool hb = b < n;
-    const double2 az = sell_pair_dot(s, val, g, b, hb, [=](int j) { return __ldg(z + j); });
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      if (h == 1 && !hb) break;
-      const int i = h ? b : g;
-      const double zi = z[i], a = h ? az.y : az.x;
-      const double pi = (beta == 0.0) ? zi : fma(beta, p[i], zi);
-      const double qi = (beta == 0.0) ? a : fma(beta, q[i], a);
-      p[i] = pi;
-      q[i] = qi;
-      v[0] = fma(pi, qi, v[0]);
-    }
-  }
-  double tot[1];
-  if (grid_reduce<1>(v, partials, &S->ticket[2], tot) && threadIdx.x == 0) {
-    S->pq = tot[0];
-    S->alpha = S->rz / tot[0];
-  }
-}
-
-template <typename V>
-__global__ void __launch_bounds__(kBlock) k_cg_update_jacobi0_p(SellView s, const V* __restrict__ val,
-                                                                const double* __restrict__ dinv,
-                                                                const double* __restrict__ p,
-                                                                const double* __restrict__ q, double* __restrict__ x,
-                                                                const double* __restrict__ r,
-                                                                double* __restrict__ r_new, double* __restrict__ X,
-                                                                double* __restrict__ Rres, CgScalars* S,
-                                                                double* partials) {
-  pdl_enter();
-  if (S->done) return;
-  const double alpha = S->alpha;
-  const int n = s.n, H = pair_half(n);
-  double v[1] = {0.0};
-  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < H; g += gridDim.x * blockDim.x) {
-    if (g >= n) continue;
-    const int b = g + H;
-    const bool hb = b < n;
-    // three gathered vectors per entry: four entries of each row per round keep it in registers
-    const double2 acc = sell_pair_dot<4>(s, val, g, b, hb, [=](int j) {
-      return __ldg(dinv + j) * fma(-alpha, __ldg(q + j), __ldg(r + j));
-    });
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      if (h == 1 && !hb) break;
-      const int i = h ? b : g;
-      const double ri = fma(-alpha, q[i], r[i]);
-      x[i] = fma(alpha, p[i], x[i]);
-      r_new[i] = ri;
-      X[i] = dinv[i] * ri;
-      Rres[i] = ri - (h ? acc.y : acc.x);
-      v[0] = fma(ri, ri, v[0]);
-    }
-  }
-  double tot[1];
-  if (grid_reduce<1>(v, partials, &S->ticket[3], tot) && threadIdx.x == 0) {
-    S->rr = tot[0];
-    S->iter += 1;
-    if (!(tot[0] == tot[0]) || !(S->pq > 0.0)) {
-      S->done = 1;
-      S->status = 5;  // breakdown / NaN
-    } else if (tot[0] <= S->tol2 * S->bb) {
-      S->done = 1;
-    } else if (S->iter >= S->maxit) {
-      S->done = 1;
-      S->status = 3;  // not converged within maxit
-    }
-  }
-}
-
-template <typename V>
-__global__ void __launch_bounds__(kBlock) k_jacobi_rz_p(SellView s, const V* __restrict__ val,
-                                                        const double* __restrict__ dinv, const double* __restrict__ r,
-                                                        const double* __restrict__ xin, double* __restrict__ z,
-                                                        CgScalars* S, double* partials, int first) {
-  pdl_enter();
-  if (S->done) return;
-  const int n = s.n, H = pair_half(n);
-  double v[1] = {0.0};
-  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < H; g += gridDim.x * blockDim.x) {
-    if (g >= n) continue;
-    const int b = g + H;
-    const bool hb = b < n;
-    const double2 ax = sell_pair_dot(s, val, g, b, hb, [=](int j) { return __ldg(xin + j); });
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      if (h == 1 && !hb) break;
-      const int i = h ? b : g;
-      const double ri = r[i];
-      const double zi = xin[i] + dinv[i] * (ri - (h ? ax.y : ax.x));
-      z[i] = zi;
-      v[0] = fma(ri, zi, v[0]);
-    }
-  }
-  double tot[1];
-  if (grid_reduce<1>(v, partials, &S->ticket[1], tot) && threadIdx.x == 0) {
-    S->beta = first ? 0.0 : tot[0] / S->rz;
-    S->rz = tot[0];
-  }
-}
-
 // Pair forms of the three finest-level kernels for interleaved replicas (see sell_row_dot2).
 template <typename V>
 __global__ void __launch_bounds__(kBlock) k_jacobi0_residual2(SellView s, const V* __restrict__ val,
@@ -990,14 +840,6 @@ __global__ void __launch_bounds__(kBlock) k_csr_jacobi2(CsrView c, const V* __re
 // Interleaved replicas taken in pairs by the finest-level kernels: an even count of 8 or more.
 static bool paired(const SellView& s) { return s.rep >= 8 && s.rep % 2 == 0; }
 static bool paired(const CsrView& c, int tpr) { return tpr == 1 && c.rep >= 8 && c.rep % 2 == 0; }
-// Row pairs for one replica with FP32 operator values on levels of at least kRowPairMin rows (the
-// FP64 forms would need 80 registers a thread and are not built).
-constexpr bool kRowPairs = true;
-constexpr int kRowPairMin = 4096;
-template <typename V>
-static bool row_pairs(const SellView& s) {
-  return kRowPairs && s.rep == 1 && s.n >= kRowPairMin;
-}
 
 // Grid of the reduction kernels: at most eight 256-thread blocks per SM (a full SM); the rows
 // beyond are covered by a grid-stride loop, so that the blocks' publish-and-count tails are few.
@@ -1127,13 +969,6 @@ template <typename V>
 void launch_jacobi_rz(const SellView& s, const V* val, const double* dinv, const double* r, const double* xin,
                       double* z, CgScalars* S, double* partials, bool first, cudaStream_t st) {
   note_launch();
-  if constexpr (sizeof(V) == 4) {
-    if (row_pairs<V>(s)) {
-      launch_pdl(k_jacobi_rz_p<V>, reduce_grid(pair_half(s.n)), kBlock, 0, st, s, val, dinv, r, xin, z, S, partials,
-                 first ? 1 : 0);
-      return;
-    }
-  }
   if (paired(s))
     launch_pdl(k_jacobi_rz2<V>, reduce_grid(1LL * s.n * s.rep / 2), kBlock, 0, st, s, val, dinv, r, xin, z, S, partials,
                first ? 1 : 0);
@@ -1145,12 +980,6 @@ template <typename V>
 void launch_cg_dir_spmv(const SellView& s, const V* val, const double* z, double* p, double* q, CgScalars* S,
                         double* partials, cudaStream_t st) {
   note_launch();
-  if constexpr (sizeof(V) == 4) {
-    if (row_pairs<V>(s)) {
-      launch_pdl(k_cg_dir_spmv_p<V>, reduce_grid(pair_half(s.n)), kBlock, 0, st, s, val, z, p, q, S, partials);
-      return;
-    }
-  }
   if (paired(s)) launch_pdl(k_cg_dir_spmv2<V>, reduce_grid(1LL * s.n * s.rep / 2), kBlock, 0, st, s, val, z, p, q, S, partials);
   else launch_pdl(k_cg_dir_spmv<V>, reduce_grid(1LL * s.n * s.rep), kBlock, 0, st, s, val, z, p, q, S, partials);
 }
@@ -1159,13 +988,6 @@ void launch_cg_update_jacobi0(const SellView& s, const V* val, const double* din
                               double* x, const double* r, double* r_new, double* X, double* Rres, CgScalars* S,
                               double* partials, cudaStream_t st) {
   note_launch();
-  if constexpr (sizeof(V) == 4) {
-    if (row_pairs<V>(s)) {
-      launch_pdl(k_cg_update_jacobi0_p<V>, reduce_grid(pair_half(s.n)), kBlock, 0, st, s, val, dinv, p, q, x, r, r_new,
-                 X, Rres, S, partials);
-      return;
-    }
-  }
   launch_pdl(k_cg_update_jacobi0<V>, reduce_grid(1LL * s.n * s.rep), kBlock, 0, st, s, val, dinv, p, q, x, r, r_new,
                X, Rres, S, partials);
 }

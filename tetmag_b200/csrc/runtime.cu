@@ -345,6 +345,8 @@ struct Solver {
   cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
   long long graph_nodes[2] = {0, 0};
   cudaGraphExec_t graph_for(int precision);
+  // the start of a solve: lift, first residual, first V-cycle with r.z
+  void solve_start(const double* b_dev, int precision, cudaStream_t st);
   void drop_graphs() {
     for (auto& g : graph_exec)
       if (g) {
@@ -915,6 +917,23 @@ void Solver::precondition_rz(int precision, cudaStream_t st, bool first) {
   }
 }
 
+// The start of a solve: b' = b_F - L b_C with x_C pinned, r = b' - A x from the warm start, and the
+// first V-cycle with r.z (beta = 0).
+void Solver::solve_start(const double* b_dev, int precision, cudaStream_t st) {
+  const SellView A0 = lev[0].A.view(rep);
+  const bool f64 = precision == TMB_FP64;
+  const bool prof = ctx_prof_on();
+  if (prof)
+    ctx_prof_begin(15, st, (double(lift.col.n) + nnz_fine) * ((f64 ? 8.0 : 4.0) + 4.0) + 8.0 * 8.0 * n * rep);
+  if (f64) launch_cg_init<double>(n, lift.view(rep), lift.v.p, cmask.p, b_dev, bp.p, x.p, st);
+  else launch_cg_init<float>(n, lift.view(rep), lift.vf.p, cmask.p, b_dev, bp.p, x.p, st);
+  rc = 0;  // graphs are captured with the residual starting in rbuf[0]
+  if (f64) launch_cg_residual<double>(A0, lev[0].Ad.p, bp.p, x.p, rbuf[0].p, Sd, partials.p, st);
+  else launch_cg_residual<float>(A0, lev[0].Af.p, bp.p, x.p, rbuf[0].p, Sd, partials.p, st);
+  if (prof) ctx_prof_end(st);
+  precondition_rz(precision, st, true);
+}
+
 void Solver::solve(const double* b_dev, int precision) {
   if (!computed) throw Error(TMB_ERR_STATE, "solver: compute() not called");
   cudaStream_t st = ctx->stream;
@@ -924,17 +943,7 @@ void Solver::solve(const double* b_dev, int precision) {
   Sh->status = 0;
   Sh->iter = 0;
   TMB_CUDA(cudaMemcpyAsync(Sd, Sh, sizeof(CgScalars), cudaMemcpyHostToDevice, st));
-  const SellView A0 = lev[0].A.view(rep);
-  const bool f64 = precision == TMB_FP64;
-  if (ctx_prof_on())
-    ctx_prof_begin(15, st, (double(lift.col.n) + nnz_fine) * ((f64 ? 8.0 : 4.0) + 4.0) + 8.0 * 8.0 * n * rep);
-  if (f64) launch_cg_init<double>(n, lift.view(rep), lift.v.p, cmask.p, b_dev, bp.p, x.p, st);
-  else launch_cg_init<float>(n, lift.view(rep), lift.vf.p, cmask.p, b_dev, bp.p, x.p, st);
-  rc = 0;  // graphs are captured with the residual starting in rbuf[0]
-  if (f64) launch_cg_residual<double>(A0, lev[0].Ad.p, bp.p, x.p, rbuf[0].p, Sd, partials.p, st);
-  else launch_cg_residual<float>(A0, lev[0].Af.p, bp.p, x.p, rbuf[0].p, Sd, partials.p, st);
-  if (ctx_prof_on()) ctx_prof_end(st);
-  precondition_rz(precision, st, true);
+  solve_start(b_dev, precision, st);
   if (!ctx_prof_on()) {
     // Graph path: kGraphIters iterations per graph launch; the first batch covers the
     // previous solve's iteration count, then the done flag is polled after every launch.
@@ -1459,6 +1468,7 @@ void Ctx::h_transpose_build() {
   cudaStream_t st = stream;
   std::vector<int> ord(H.hnearb.size());
   std::iota(ord.begin(), ord.end(), 0);
+  // near blocks pair leaf clusters, whose position ranges are disjoint: the begin names the leaf
   std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) {
     return H.hnearb[a].cb < H.hnearb[b].cb || (H.hnearb[a].cb == H.hnearb[b].cb && H.hnearb[a].rb < H.hnearb[b].rb);
   });
@@ -1480,8 +1490,13 @@ void Ctx::h_transpose_build() {
   const int nf = int(H.hfarb.size());
   std::vector<int> fo(nf);
   std::iota(fo.begin(), fo.end(), 0);
+  // a column cluster is its position range: a cluster and its first child begin at the same
+  // position, so the blocks are grouped by (begin, size)
   std::stable_sort(fo.begin(), fo.end(), [&](int a, int b) {
-    return H.hfarb[a].cb < H.hfarb[b].cb || (H.hfarb[a].cb == H.hfarb[b].cb && H.hfarb[a].rb < H.hfarb[b].rb);
+    const HBlockDev &x = H.hfarb[a], &y = H.hfarb[b];
+    if (x.cb != y.cb) return x.cb < y.cb;
+    if (x.n != y.n) return x.n < y.n;
+    return x.rb < y.rb;
   });
   for (int w = 0; w < 2; ++w) {
     // the compact factor offsets of precision w, in the forward block order
@@ -1506,8 +1521,10 @@ void Ctx::h_transpose_build() {
       const int mp = pad4(b.m), np = pad4(b.n);
       for (int l = 0; l < rk[q]; ++l) td.push_back(HTerm{uo[q] + (long long)l * mp, vo[q] + (long long)l * np, mp, b.rb});
       stt += rk[q];
-      if (groups.empty() || groups.back().rb != b.cb) groups.push_back(HFarGroup{b.cb, b.n, p, p + 1});
-      else groups.back().last = p + 1;
+      if (groups.empty() || groups.back().rb != b.cb || groups.back().m != b.n)
+        groups.push_back(HFarGroup{b.cb, b.n, p, p + 1});
+      else
+        groups.back().last = p + 1;
     }
     to[nf] = stt;
     if (stt != H.terms[w]) throw Error(TMB_ERR_INTERNAL, "H-matrix: transposed term count differs");
