@@ -660,165 +660,6 @@ __global__ void __launch_bounds__(kBlock) k_cg_update(int n, const double* __res
   }
 }
 
-// ---- staged finest level (StagedView) -----------------------------------------------------
-// Every thread of the CTA (tile blockIdx.x, row tile * kTileRows + threadIdx.x) calls this: the
-// first kStagedRegs entries of the thread's row are loaded (index, value) before the staging, so
-// their loads and the staging loads are in flight together; the tile's windows of the gathered
-// vector, each entry given by gx(global index), are copied into xs; after the barrier the row's
-// product is summed from shared memory.  Returns 0 for rows past the end.
-constexpr int kStagedRegs = 8;
-constexpr int kStageUnroll = 8;
-template <typename V, typename G>
-__device__ __forceinline__ double staged_row_dot(const SellView& s, const StagedView& g, const V* __restrict__ val,
-                                                 double* xs, G gx) {
-  __shared__ int4 wd[kMaxWindows];
-  __shared__ int nwin_s;
-  const int tile = blockIdx.x;
-  const int row = tile * kTileRows + threadIdx.x;
-  int beg = 0, end = 0;
-  if (row < s.n) {
-    const int sl = row >> 5;
-    beg = __ldg(s.soff + sl) + (row & 31);
-    end = __ldg(s.soff + sl + 1);
-  }
-  int lc[kStagedRegs];
-  V v[kStagedRegs];
-#pragma unroll
-  for (int u = 0; u < kStagedRegs; ++u) {
-    const int k = beg + u * kSlice;
-    const bool ok = k < end;
-    lc[u] = ok ? int(__ldg(g.lcol + k)) : 0;
-    v[u] = ok ? __ldg(val + k) : V(0);
-  }
-  const int w0 = __ldg(g.woff + tile), nw = __ldg(g.woff + tile + 1) - w0;
-  if (threadIdx.x < nw) wd[threadIdx.x] = g.win[w0 + threadIdx.x];
-  if (threadIdx.x == 0) nwin_s = nw;
-  __syncthreads();
-  const int total = nw > 0 ? wd[nw - 1].z + wd[nw - 1].y : 0;
-  int q = 0;
-  for (int base = 0; base < total; base += kTileRows * kStageUnroll) {
-    double tv[kStageUnroll];
-    int dst[kStageUnroll];
-#pragma unroll
-    for (int u = 0; u < kStageUnroll; ++u) {
-      const int i = base + u * kTileRows + threadIdx.x;
-      dst[u] = -1;
-      tv[u] = 0.0;
-      if (i < total) {
-        while (i >= wd[q].z + wd[q].y) ++q;  // windows in shared order; i only grows
-        dst[u] = i;
-        tv[u] = gx(wd[q].x + (i - wd[q].z));
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < kStageUnroll; ++u)
-      if (dst[u] >= 0) xs[dst[u]] = tv[u];
-  }
-  __syncthreads();
-  double acc = 0.0;
-#pragma unroll
-  for (int u = 0; u < kStagedRegs; ++u) acc = fma(static_cast<double>(v[u]), xs[lc[u]], acc);
-  for (int k = beg + kStagedRegs * kSlice; k < end; k += kSlice)
-    acc = fma(static_cast<double>(__ldg(val + k)), xs[__ldg(g.lcol + k)], acc);
-  return acc;
-}
-
-template <typename V>
-__global__ void __launch_bounds__(kTileRows) k_cg_dir_spmv_st(SellView s, StagedView g, const V* __restrict__ val,
-                                                              const double* __restrict__ z, double* __restrict__ p,
-                                                              double* __restrict__ q, CgScalars* S, double* partials) {
-  extern __shared__ double xs[];
-  pdl_enter();
-  if (S->done) return;
-  const double beta = S->beta;
-  const double az = staged_row_dot(s, g, val, xs, [=](int j) { return __ldg(z + j); });
-  const int i = blockIdx.x * kTileRows + threadIdx.x;
-  double v[1] = {0.0};
-  if (i < s.n) {
-    const double zi = z[i];
-    const double pi = (beta == 0.0) ? zi : fma(beta, p[i], zi);
-    const double qi = (beta == 0.0) ? az : fma(beta, q[i], az);
-    p[i] = pi;
-    q[i] = qi;
-    v[0] = pi * qi;
-  }
-  double tot[1];
-  if (grid_reduce<1>(v, partials, &S->ticket[2], tot) && threadIdx.x == 0) {
-    S->pq = tot[0];
-    S->alpha = S->rz / tot[0];
-  }
-}
-
-template <typename V>
-__global__ void __launch_bounds__(kTileRows) k_cg_update_jacobi0_st(SellView s, StagedView g,
-                                                                    const V* __restrict__ val,
-                                                                    const double* __restrict__ dinv,
-                                                                    const double* __restrict__ p,
-                                                                    const double* __restrict__ q,
-                                                                    double* __restrict__ x,
-                                                                    const double* __restrict__ r,
-                                                                    double* __restrict__ r_new, double* __restrict__ X,
-                                                                    double* __restrict__ Rres, CgScalars* S,
-                                                                    double* partials) {
-  extern __shared__ double xs[];
-  pdl_enter();
-  if (S->done) return;
-  const double alpha = S->alpha;
-  // the staged vector is D_w^-1 r_new of the neighbours, formed on the fly from r and q
-  const double acc = staged_row_dot(s, g, val, xs, [=](int j) {
-    return __ldg(dinv + j) * fma(-alpha, __ldg(q + j), __ldg(r + j));
-  });
-  const int i = blockIdx.x * kTileRows + threadIdx.x;
-  double v[1] = {0.0};
-  if (i < s.n) {
-    const double ri = fma(-alpha, q[i], r[i]);
-    x[i] = fma(alpha, p[i], x[i]);
-    r_new[i] = ri;
-    X[i] = dinv[i] * ri;
-    Rres[i] = ri - acc;
-    v[0] = ri * ri;
-  }
-  double tot[1];
-  if (grid_reduce<1>(v, partials, &S->ticket[3], tot) && threadIdx.x == 0) {
-    S->rr = tot[0];
-    S->iter += 1;
-    if (!(tot[0] == tot[0]) || !(S->pq > 0.0)) {
-      S->done = 1;
-      S->status = 5;  // breakdown / NaN
-    } else if (tot[0] <= S->tol2 * S->bb) {
-      S->done = 1;
-    } else if (S->iter >= S->maxit) {
-      S->done = 1;
-      S->status = 3;  // not converged within maxit
-    }
-  }
-}
-
-template <typename V>
-__global__ void __launch_bounds__(kTileRows) k_jacobi_rz_st(SellView s, StagedView g, const V* __restrict__ val,
-                                                            const double* __restrict__ dinv,
-                                                            const double* __restrict__ r,
-                                                            const double* __restrict__ xin, double* __restrict__ z,
-                                                            CgScalars* S, double* partials, int first) {
-  extern __shared__ double xs[];
-  pdl_enter();
-  if (S->done) return;
-  const double ax = staged_row_dot(s, g, val, xs, [=](int j) { return __ldg(xin + j); });
-  const int i = blockIdx.x * kTileRows + threadIdx.x;
-  double v[1] = {0.0};
-  if (i < s.n) {
-    const double ri = r[i];
-    const double zi = xin[i] + dinv[i] * (ri - ax);
-    z[i] = zi;
-    v[0] = ri * zi;
-  }
-  double tot[1];
-  if (grid_reduce<1>(v, partials, &S->ticket[1], tot) && threadIdx.x == 0) {
-    S->beta = first ? 0.0 : tot[0] / S->rz;
-    S->rz = tot[0];
-  }
-}
-
 // Pair forms of the three finest-level kernels for interleaved replicas (see sell_row_dot2).
 template <typename V>
 __global__ void __launch_bounds__(kBlock) k_jacobi0_residual2(SellView s, const V* __restrict__ val,
@@ -1151,29 +992,6 @@ void launch_cg_update_jacobi0(const SellView& s, const V* val, const double* din
                X, Rres, S, partials);
 }
 
-template <typename V>
-void launch_jacobi_rz_st(const SellView& s, const StagedView& g, const V* val, const double* dinv, const double* r,
-                         const double* xin, double* z, CgScalars* S, double* partials, bool first, cudaStream_t st) {
-  note_launch();
-  launch_pdl(k_jacobi_rz_st<V>, g.ntiles, kTileRows, size_t(g.max_stage) * sizeof(double), st, s, g, val, dinv, r,
-             xin, z, S, partials, first ? 1 : 0);
-}
-template <typename V>
-void launch_cg_dir_spmv_st(const SellView& s, const StagedView& g, const V* val, const double* z, double* p, double* q,
-                           CgScalars* S, double* partials, cudaStream_t st) {
-  note_launch();
-  launch_pdl(k_cg_dir_spmv_st<V>, g.ntiles, kTileRows, size_t(g.max_stage) * sizeof(double), st, s, g, val, z, p, q,
-             S, partials);
-}
-template <typename V>
-void launch_cg_update_jacobi0_st(const SellView& s, const StagedView& g, const V* val, const double* dinv,
-                                 const double* p, const double* q, double* x, const double* r, double* r_new,
-                                 double* X, double* Rres, CgScalars* S, double* partials, cudaStream_t st) {
-  note_launch();
-  launch_pdl(k_cg_update_jacobi0_st<V>, g.ntiles, kTileRows, size_t(g.max_stage) * sizeof(double), st, s, g, val,
-             dinv, p, q, x, r, r_new, X, Rres, S, partials);
-}
-
 void launch_cg_update(int n, const double* p, const double* q, double* x, double* r, CgScalars* S,
                       double* partials, cudaStream_t st) {
   note_launch();
@@ -1203,14 +1021,6 @@ void launch_cg_update(int n, const double* p, const double* q, double* x, double
                                            double*, const int*, cudaStream_t);                              \
   template void launch_jacobi_rz<V>(const SellView&, const V*, const double*, const double*, const double*, \
                                     double*, CgScalars*, double*, bool, cudaStream_t);                      \
-  template void launch_jacobi_rz_st<V>(const SellView&, const StagedView&, const V*, const double*,          \
-                                       const double*, const double*, double*, CgScalars*, double*, bool,      \
-                                       cudaStream_t);                                                         \
-  template void launch_cg_dir_spmv_st<V>(const SellView&, const StagedView&, const V*, const double*, double*, \
-                                         double*, CgScalars*, double*, cudaStream_t);                         \
-  template void launch_cg_update_jacobi0_st<V>(const SellView&, const StagedView&, const V*, const double*,    \
-                                               const double*, const double*, double*, const double*, double*, \
-                                               double*, double*, CgScalars*, double*, cudaStream_t);          \
   template void launch_cg_dir_spmv<V>(const SellView&, const V*, const double*, double*, double*, CgScalars*, \
                                       double*, cudaStream_t);                                                 \
   template void launch_cg_update_jacobi0<V>(const SellView&, const V*, const double*, const double*,         \

@@ -128,70 +128,6 @@ static SellHost build_sell(int n, const int* ptr, const int* col) {
   return S;
 }
 
-// The staged finest level (StagedView): per tile of kTileRows rows, the sorted columns its rows
-// reference merged into windows (gaps of up to kStageGap unused entries are staged too, to keep
-// the windows few), their shared-memory offsets, and every SELL entry's shared-memory index.  ok is
-// false when a tile would stage more than kMaxStage entries or kMaxWindows windows (an ordering
-// without locality); the unstaged kernels serve then.
-struct StagedHost {
-  bool ok = false;
-  int ntiles = 0, max_stage = 0;
-  std::vector<int> woff;
-  std::vector<int4> win;
-  std::vector<unsigned short> lcol;
-};
-constexpr int kStageGap = 16;
-constexpr bool kStaged = true;
-
-static StagedHost build_staged(const SellHost& S, const int* ptr, const int* col) {
-  StagedHost G;
-  const int n = S.n;
-  G.ntiles = (n + kTileRows - 1) / kTileRows;
-  G.woff.assign(G.ntiles + 1, 0);
-  G.lcol.assign(S.col.size(), 0);
-  std::vector<int> cols;
-  std::vector<int4> w;
-  for (int t = 0; t < G.ntiles; ++t) {
-    const int r0 = t * kTileRows, r1 = std::min(n, r0 + kTileRows);
-    cols.clear();
-    for (int r = r0; r < r1; ++r) {
-      cols.push_back(r);  // the padding entries of a row point at the row itself
-      for (int k = ptr[r]; k < ptr[r + 1]; ++k) cols.push_back(col[k]);
-    }
-    std::sort(cols.begin(), cols.end());
-    cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
-    w.clear();
-    for (int c : cols) {
-      if (w.empty() || c > w.back().x + w.back().y - 1 + kStageGap) w.push_back(make_int4(c, 1, 0, 0));
-      else w.back().y = c - w.back().x + 1;
-    }
-    int off = 0;
-    for (int4& q : w) {
-      q.z = off;
-      off += q.y;
-    }
-    if (off > kMaxStage || int(w.size()) > kMaxWindows) return StagedHost{};
-    G.max_stage = std::max(G.max_stage, off);
-    for (const int4& q : w) G.win.push_back(q);
-    G.woff[t + 1] = int(G.win.size());
-    const int s0 = r0 / kSlice, s1 = (r1 + kSlice - 1) / kSlice;
-    for (int sl = s0; sl < s1; ++sl)
-      for (int pos = S.soff[sl]; pos < S.soff[sl + 1]; ++pos) {
-        const int c = S.col[pos];
-        int lo = 0, hi = int(w.size()) - 1;
-        while (lo < hi) {  // last window starting at or before c
-          const int mid = (lo + hi + 1) / 2;
-          if (w[mid].x <= c) lo = mid;
-          else hi = mid - 1;
-        }
-        const int4& q = w[lo];
-        G.lcol[pos] = (c >= q.x && c < q.x + q.y) ? (unsigned short)(q.z + c - q.x) : 0;
-      }
-  }
-  G.ok = true;
-  return G;
-}
-
 template <typename V>
 static std::vector<V> sell_values(const SellHost& S, const double* v) {
   std::vector<V> out(S.col.size(), V(0));
@@ -302,21 +238,6 @@ struct Prof {
 struct DevLevel {
   int n = 0;
   DevSell A;                 // fine level: SELL-32, one thread per row (about 14 entries per row)
-  // fine level, one replica: the gathered vector staged in shared memory per tile of rows
-  bool staged = false;
-  int sntiles = 0, smax = 0;
-  DevArray<int> swoff;
-  DevArray<int4> swin;
-  DevArray<unsigned short> slcol;
-  StagedView sview() const {
-    StagedView g;
-    g.ntiles = sntiles;
-    g.max_stage = smax;
-    g.woff = swoff.p;
-    g.win = swin.p;
-    g.lcol = slcol.p;
-    return g;
-  }
   DevCsr Ac;                 // coarser levels: CSR, tA threads per row (Galerkin rows of 20-60 entries)
   int tA = 1, tP = 1, tR = 1;
   DevArray<double> Ad, dinv, X, R, b, out;
@@ -682,14 +603,8 @@ void Solver::iteration_body(int precision, cudaStream_t st, bool profile) {
   const bool f64 = precision == TMB_FP64;
   // p = z + beta p and q = A z + beta q: the product gathers z only
   if (profile) ctx_prof_begin(6, st, nnz_fine * ((f64 ? 8.0 : 4.0) + 4.0) + 5.0 * 8.0 * n * rep);
-  if (lev[0].staged) {
-    const StagedView G = lev[0].sview();
-    if (f64) launch_cg_dir_spmv_st<double>(A0, G, lev[0].Ad.p, z.p, p.p, q.p, Sd, partials.p, st);
-    else launch_cg_dir_spmv_st<float>(A0, G, lev[0].Af.p, z.p, p.p, q.p, Sd, partials.p, st);
-  } else {
-    if (f64) launch_cg_dir_spmv<double>(A0, lev[0].Ad.p, z.p, p.p, q.p, Sd, partials.p, st);
-    else launch_cg_dir_spmv<float>(A0, lev[0].Af.p, z.p, p.p, q.p, Sd, partials.p, st);
-  }
+  if (f64) launch_cg_dir_spmv<double>(A0, lev[0].Ad.p, z.p, p.p, q.p, Sd, partials.p, st);
+  else launch_cg_dir_spmv<float>(A0, lev[0].Af.p, z.p, p.p, q.p, Sd, partials.p, st);
   if (profile) ctx_prof_end(st);
   if (lev.size() > 1 && rep < 8) {
     // x, r update fused with the V-cycle's first sweep; the residual alternates between buffers
@@ -699,21 +614,12 @@ void Solver::iteration_body(int precision, cudaStream_t st, bool profile) {
     rc ^= 1;
     DevLevel& L = lev[0];
     if (profile) ctx_prof_begin(8, st, nnz_fine * ((f64 ? 8.0 : 4.0) + 4.0) + 9.0 * 8.0 * n * rep);
-    if (L.staged) {
-      const StagedView G = L.sview();
-      if (f64)
-        launch_cg_update_jacobi0_st<double>(A0, G, L.Ad.p, L.dinv.p, p.p, q.p, x.p, rold, rnew, L.X.p, L.R.p, Sd,
-                                            partials.p, st);
-      else
-        launch_cg_update_jacobi0_st<float>(A0, G, L.Af.p, L.dinv.p, p.p, q.p, x.p, rold, rnew, L.X.p, L.R.p, Sd,
-                                           partials.p, st);
-    } else if (f64) {
+    if (f64)
       launch_cg_update_jacobi0<double>(A0, L.Ad.p, L.dinv.p, p.p, q.p, x.p, rold, rnew, L.X.p, L.R.p, Sd,
                                        partials.p, st);
-    } else {
+    else
       launch_cg_update_jacobi0<float>(A0, L.Af.p, L.dinv.p, p.p, q.p, x.p, rold, rnew, L.X.p, L.R.p, Sd,
                                       partials.p, st);
-    }
     if (profile) ctx_prof_end(st);
     vcycle(0, rnew, z.p, precision, st, 0, true);
   } else {
@@ -812,18 +718,6 @@ void Solver::compute() {
       d.A.upload(S, st);
       d.Ad.upload(sell_values<double>(S, hl.A.val.data()), st);
       d.Af.upload(sell_values<float>(S, hl.A.val.data()), st);
-      d.staged = false;
-      if (kStaged && rep == 1) {
-        StagedHost G = build_staged(S, hl.A.ptr.data(), hl.A.col.data());
-        if (G.ok) {
-          d.swoff.upload(G.woff, st);
-          d.swin.upload(G.win, st);
-          d.slcol.upload(G.lcol, st);
-          d.sntiles = G.ntiles;
-          d.smax = G.max_stage;
-          d.staged = true;
-        }
-      }
     } else {
       d.Ac.upload(hl.A, st);
       d.tA = rep >= 8 ? 1 : csr_threads_per_row(hl.A.nrows, hl.A.nnz());
@@ -995,11 +889,7 @@ void Solver::vcycle(size_t l, const double* b, double* out, int precision, cudaS
   if (l == 0) {
     const SellView A = L.A.view(rep);
     pb(9, sweep + 5.0 * 8.0 * nl);
-    if (rz_mode >= 0 && L.staged) {
-      const StagedView G = L.sview();
-      if (f64) launch_jacobi_rz_st<double>(A, G, L.Ad.p, L.dinv.p, b, L.X.p, out, Sd, partials.p, rz_mode == 1, st);
-      else launch_jacobi_rz_st<float>(A, G, L.Af.p, L.dinv.p, b, L.X.p, out, Sd, partials.p, rz_mode == 1, st);
-    } else if (rz_mode >= 0) {
+    if (rz_mode >= 0) {
       // finest level: the post-smoothing sweep also reduces r.z for the next CG direction
       if (f64) launch_jacobi_rz<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, out, Sd, partials.p, rz_mode == 1, st);
       else launch_jacobi_rz<float>(A, L.Af.p, L.dinv.p, b, L.X.p, out, Sd, partials.p, rz_mode == 1, st);

@@ -46,21 +46,6 @@ struct SellView {
   int rep;           // interleaved replicas (1: plain vectors)
 };
 
-// Finest level with its gathered vector staged in shared memory: one CTA per tile of kTileRows
-// rows (eight slices), which copies the windows of the vector its rows reference (a few ranges of
-// consecutive entries: the row block and the neighbouring layers) into shared memory, then gathers
-// from there through 16-bit local indices kept beside the SELL column indices.
-constexpr int kTileRows = 256;
-constexpr int kMaxStage = 6144;   // staged doubles per CTA (48 KB)
-constexpr int kMaxWindows = 256;
-struct StagedView {
-  int ntiles = 0;
-  int max_stage = 0;                       // staged entries of the largest tile
-  const int* woff = nullptr;               // ntiles + 1 offsets into win
-  const int4* win = nullptr;               // (global start, length, shared offset, 0) per window
-  const unsigned short* lcol = nullptr;    // shared-memory index of every SELL entry's column
-};
-
 struct CsrView {
   int n;
   const int* ptr;
@@ -226,17 +211,6 @@ template <typename V>
 void launch_cg_update_jacobi0(const SellView& s, const V* val, const double* dinv, const double* p, const double* q,
                               double* x, const double* r, double* r_new, double* X, double* Rres, CgScalars* S,
                               double* partials, cudaStream_t st);
-// the same three kernels on a staged finest level (one replica)
-template <typename V>
-void launch_jacobi_rz_st(const SellView& s, const StagedView& g, const V* val, const double* dinv, const double* r,
-                         const double* xin, double* z, CgScalars* S, double* partials, bool first, cudaStream_t st);
-template <typename V>
-void launch_cg_dir_spmv_st(const SellView& s, const StagedView& g, const V* val, const double* z, double* p, double* q,
-                           CgScalars* S, double* partials, cudaStream_t st);
-template <typename V>
-void launch_cg_update_jacobi0_st(const SellView& s, const StagedView& g, const V* val, const double* dinv,
-                                 const double* p, const double* q, double* x, const double* r, double* r_new,
-                                 double* X, double* Rres, CgScalars* S, double* partials, cudaStream_t st);
 
 // --- launchers (k_bem.cu) ----------------------------------------------------------------
 void launch_bem_assemble(int nb, int ntri, const double* bxyz, const int* tri, const double* area,
