@@ -13,8 +13,9 @@ The reference documents one run of its own (examples/example3, doc/examples/exam
 
 Its documentation quotes the mean magnetisation of the equilibrium reached after 14 ns:
 <M_x> = -1.7009e5 A/m, <M_y> = 1.566e4 A/m (example3.rst:68; tests/golden/make_stt.py extracts
-them with the mesh).  This test runs both stages through the C ABI and compares the
-volume-weighted mean magnetisation with them.  The STT coefficients are the reference's
+them with the mesh).  This test runs both stages through the C ABI on the plain FP64 path and
+compares the volume-weighted mean magnetisation with them (measured: -170,097.4 and 15,660.6 A/m;
+the static stage ends after 1,336 ps; 160 s on one B200).  The STT coefficients are the reference's
 (STT::setEta and the constructor's btimesMs, specs/ProgramSpecs.cpp:405-421): per node
 eta_d = j_d P mu_B mu0 / (gamma0 e (1 + beta^2) scale Js).
 """
@@ -32,8 +33,12 @@ MU_B = 9.274009994e-24             # J/T
 E_CHARGE = 1.6021766208e-19        # C
 SCALE = 1e-9
 
-# |<M>_here - <M>_reference| per component, in A/m (Ms = 8e5 A/m)
-MEAN_M_TOL = 2.0e3
+# |<M>_here - <M>_reference| per component, in A/m (Ms = 8e5 A/m).  Measured: 7.4 A/m (x) and
+# 0.6 A/m (y) on both precision paths, within the rounding of the quoted values (5 A/m); the
+# vortex still circles the equilibrium at 14 ns (the last nanosecond moves <M_y> by 84 A/m), so
+# the bound allows for a small phase difference of that residual motion.
+MEAN_M_TOL = 100.0
+SETTLE_TOL = 250.0    # |<M>(14 ns) - <M>(13 ns)| per component
 
 
 def vortex_xy(xyz):
@@ -111,6 +116,6 @@ def test_stt_standard_problem_against_reference_mean_m():
     assert torque <= float(g["torque_limit"]) and np.abs(m_static[:2]).max() < 0.02 and m_static[2] > 0.0, static
     assert abs(M[0] - float(g["mean_Mx"])) <= MEAN_M_TOL, (M, log[-3:])
     assert abs(M[1] - float(g["mean_My"])) <= MEAN_M_TOL, (M, log[-3:])
-    # settled: the last nanosecond moves the mean by far less than the tolerance
-    assert np.abs(log[-1][1] - log[-2][1]).max() <= 0.25 * MEAN_M_TOL, log[-3:]
+    # nearly settled: the last nanosecond moves the mean by little
+    assert np.abs(log[-1][1] - log[-2][1]).max() <= SETTLE_TOL, log[-3:]
     print(f"stt: static {t_static:g} ps, <M> after {log[-1][0]:g} ps = {M} A/m")
