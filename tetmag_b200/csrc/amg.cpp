@@ -12,9 +12,10 @@
 //   smoothed P   (I - w D_F^-1 A_F) P_tent, w = relax * 4/3 / rho(D_F^-1 A_F)
 //   coarse A     P^T A P (Galerkin)
 // Differences from AMGCL, chosen for a device V-cycle inside CG: the smoother
-// is damped Jacobi (symmetric and parallel) instead of ILU0, and the coarsest
-// level (<= coarse_enough unknowns) is solved exactly in FP64 with a dense
-// inverse.
+// is damped Jacobi (symmetric and parallel) instead of ILU0, the prolongation
+// smoother takes relax = 1 (fewer PCG iterations under the Jacobi cycle than
+// 0.75), and the coarsest level (<= coarse_enough unknowns) is solved exactly
+// in FP64 with a dense inverse.
 #include <algorithm>
 #include <chrono>
 #include <cmath>

@@ -266,8 +266,9 @@ __global__ void __launch_bounds__(kBlock) k_csr_jacobi(CsrView c, const V* __res
 
 // Coarse levels, one replica: the first sweep from zero with its residual (x = D_w^-1 b,
 // r = b - A x) and the restriction of that residual in one launch.  The restricted residual needs
-// no sweep result: R r = R (I - A D_w^-1) b = M b with M = R - (R A) D_w^-1, so the first na
-// blocks run the sweep's rows (ta threads a row) and the others the rows of M (tm threads a row).
+// no sweep result: R r = R (I - A D_w^-1) b = M b with M = R - (R A) D_w^-1, so the first nm
+// blocks run the rows of M (tm threads a row: few, long rows, placed first so that they start at
+// once) and the others the sweep's rows (ta threads a row).
 __device__ __forceinline__ double group_sum_rt(double v, int T) {
   for (int o = T >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
@@ -302,13 +303,18 @@ template <typename V>
 __global__ void __launch_bounds__(kBlock) k_csr_pre_restrict(CsrView a, const V* __restrict__ aval,
                                                              const double* __restrict__ dinv,
                                                              const double* __restrict__ b, double* __restrict__ x,
-                                                             double* __restrict__ r, int ta, int na, CsrView m,
+                                                             double* __restrict__ r, int ta, int nm, CsrView m,
                                                              const V* __restrict__ mval, double* __restrict__ bc,
                                                              int tm, const int* done) {
   pdl_enter();
   if (done && *done) return;
-  if (int(blockIdx.x) < na) {
+  if (int(blockIdx.x) < nm) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int row = t / tm, sub = t & (tm - 1);
+    const double acc = group_sum_rt(csr_row_part_rt(m, mval, b, nullptr, row, sub, tm), tm);
+    if (row < m.n && sub == 0) bc[row] = acc;
+  } else {
+    const int t = (blockIdx.x - nm) * blockDim.x + threadIdx.x;
     const int row = t / ta, sub = t & (ta - 1);
     const double acc = group_sum_rt(csr_row_part_rt(a, aval, b, dinv, row, sub, ta), ta);
     if (row < a.n && sub == 0) {
@@ -316,11 +322,6 @@ __global__ void __launch_bounds__(kBlock) k_csr_pre_restrict(CsrView a, const V*
       x[row] = dinv[row] * bi;
       r[row] = bi - acc;
     }
-  } else {
-    const int t = (blockIdx.x - na) * blockDim.x + threadIdx.x;
-    const int row = t / tm, sub = t & (tm - 1);
-    const double acc = group_sum_rt(csr_row_part_rt(m, mval, b, nullptr, row, sub, tm), tm);
-    if (row < m.n && sub == 0) bc[row] = acc;
   }
 }
 
@@ -913,7 +914,7 @@ void launch_csr_pre_restrict(const CsrView& a, const V* aval, const double* dinv
                              cudaStream_t st) {
   note_launch();
   const int na = grid_for(1LL * ta * a.n), nm = grid_for(1LL * tm * m.n);
-  launch_pdl(k_csr_pre_restrict<V>, na + nm, kBlock, 0, st, a, aval, dinv, b, x, r, ta, na, m, mval, bc, tm, done);
+  launch_pdl(k_csr_pre_restrict<V>, na + nm, kBlock, 0, st, a, aval, dinv, b, x, r, ta, nm, m, mval, bc, tm, done);
 }
 template <typename V>
 void launch_csr_prolong_smooth(const CsrView& m, const V* apv, const V* pv, const double* dinv, const double* x0,

@@ -373,6 +373,15 @@ struct Ctx {
   DevSell pat;
   DevArray<double> K, g[3], tg[3];
   DevArray<float> Kf, gf[3], tgf[3];
+  // K alone on its non-zero entries (and the diagonal), for local fields without DMI: on Kuhn-split
+  // cuboids half of the shared pattern holds exact zeros of K (the face-diagonal couplings).  Built
+  // only when it drops at least a tenth of the entries; otherwise the shared pattern serves.
+  bool has_patx = false;
+  long long nnz_x = 0;
+  DevSell patx;
+  DevArray<double> Kx;
+  DevArray<float> Kxf;
+  void launch_local_kernel(const LocalFieldArgs& a, cudaStream_t st);
   std::vector<int> hptr, hcol, hbnodes;
   std::vector<double> hK, hvol;
   DevArray<double> node_vol, area, nvn;
@@ -660,11 +669,20 @@ void Solver::compute() {
   n = A.nrows;
   rep = want_rep >= 1 ? want_rep : ctx->rep;
   if (n <= 0) throw Error(TMB_ERR_ARG, "solver: empty matrix");
-  // constraints: rows whose only entry is a unit diagonal
+  // constraints: rows whose only non-zero entry is a unit diagonal
   std::vector<int> cm(n, 0);
-  for (int i = 0; i < n; ++i)
-    if (A.ptr[i + 1] - A.ptr[i] == 1 && A.col[A.ptr[i]] == i && A.val[A.ptr[i]] == 1.0) cm[i] = 1;
-  // symmetric elimination: A' keeps free-free couplings, the free-constrained ones go to the lift
+  for (int i = 0; i < n; ++i) {
+    bool unit = false, other = false;
+    for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
+      if (A.col[k] == i && A.val[k] == 1.0) unit = true;
+      else if (A.val[k] != 0.0) other = true;
+    }
+    cm[i] = unit && !other;
+  }
+  // symmetric elimination: A' keeps free-free couplings, the free-constrained ones go to the lift.
+  // Stored entries that are exactly zero are dropped (they add nothing to any product): on meshes of
+  // Kuhn-split cuboids the face-diagonal couplings of the stiffness matrix vanish exactly, about
+  // half of the pattern, so every product over A' gathers half as many entries there.
   Csr Ap, L;
   Ap.nrows = Ap.ncols = L.nrows = L.ncols = n;
   Ap.ptr.assign(n + 1, 0);
@@ -676,6 +694,7 @@ void Solver::compute() {
     } else {
       for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
         const int j = A.col[k];
+        if (A.val[k] == 0.0 && j != i) continue;
         if (cm[j]) {
           L.col.push_back(j);
           L.val.push_back(A.val[k]);
@@ -1029,6 +1048,26 @@ void Ctx::set_operators(int nx, const int* ptr, const int* col, const double* K_
     gf[d].upload(sell_values<float>(S, g_[d]), st);
     tg[d].upload(sell_values<double>(S, tg_[d]), st);
     tgf[d].upload(sell_values<float>(S, tg_[d]), st);
+  }
+  {
+    std::vector<int> xp(nx + 1, 0), xcol;
+    std::vector<double> xv;
+    for (int i = 0; i < nx; ++i) {
+      for (int k = ptr[i]; k < ptr[i + 1]; ++k)
+        if (K_[k] != 0.0 || col[k] == i) {
+          xcol.push_back(col[k]);
+          xv.push_back(K_[k]);
+        }
+      xp[i + 1] = int(xcol.size());
+    }
+    has_patx = double(xcol.size()) < 0.9 * double(nnz);
+    nnz_x = (long long)xcol.size();
+    if (has_patx) {
+      SellHost SX = build_sell(nx, xp.data(), xcol.data());
+      patx.upload(SX, st);
+      Kx.upload(sell_values<double>(SX, xv.data()), st);
+      Kxf.upload(sell_values<float>(SX, xv.data()), st);
+    }
   }
   node_vol.upload(vol, nx, st);
   area.upload(area_, nx, st);
@@ -2183,12 +2222,20 @@ LocalFieldArgs Ctx::local_args(const double* m, double* ydot, double* hout, unsi
   return a;
 }
 
+// The local-field kernel on the shared pattern, or on K's own non-zero pattern when no DMI term
+// needs the gradient operators (the same sums: the dropped entries are exact zeros).
+void Ctx::launch_local_kernel(const LocalFieldArgs& a, cudaStream_t st) {
+  const bool compact = has_patx && !a.idm_a && !a.dmi_s;
+  const SellView S = compact ? patx.view(rep) : pat.view(rep);
+  if (precision == TMB_FP64)
+    launch_local_field<double>(S, compact ? Kx.p : K.p, tg[0].p, tg[1].p, tg[2].p, g[0].p, g[1].p, a, st);
+  else
+    launch_local_field<float>(S, compact ? Kxf.p : Kf.p, tgf[0].p, tgf[1].p, tgf[2].p, gf[0].p, gf[1].p, a, st);
+}
+
 void Ctx::launch_local(const LocalFieldArgs& a, cudaStream_t st) {
   const SellView S = pat.view(rep);
-  if (precision == TMB_FP64)
-    launch_local_field<double>(S, K.p, tg[0].p, tg[1].p, tg[2].p, g[0].p, g[1].p, a, st);
-  else
-    launch_local_field<float>(S, Kf.p, tgf[0].p, tgf[1].p, tgf[2].p, gf[0].p, gf[1].p, a, st);
+  launch_local_kernel(a, st);
   if (has_stt && a.ydot) {
     if (precision == TMB_FP64)
       launch_stt_add<double>(S, g[0].p, g[1].p, g[2].p, a.m, stt_eta.p, alpha, stt_beta, stt_scale, a.ydot, st);
@@ -2202,7 +2249,8 @@ void Ctx::local(const double* m, double* ydot, double* hout, unsigned long long*
   require_material();
   const LocalFieldArgs a = local_args(m, ydot, hout, tq);
   const double sv = precision == TMB_FP64 ? 8.0 : 4.0, z = double(hptr[n]), N = double(nr());
-  double bytes = z * (sv + 4) + N * 8 * (3 + 3 + 1) + (ydot ? N * 24 : 0.0) + (hout ? N * 24 : 0.0);
+  const double zx = (has_patx && !a.idm_a && !a.dmi_s) ? double(nnz_x) : z;  // entries of K read
+  double bytes = zx * (sv + 4) + N * 8 * (3 + 3 + 1) + (ydot ? N * 24 : 0.0) + (hout ? N * 24 : 0.0);
   if (a.ku2) bytes += N * 8 * 4;
   if (a.dmi_s) bytes += z * 3 * sv + N * 8 * 5;
   if (a.idm_a) bytes += z * 4 * sv + N * 8 * 3;
@@ -2380,7 +2428,7 @@ cudaGraphExec_t Ctx::step_graph_for(double* y, double* yalt) {
   LocalFieldArgs a = local_args(ytmp.p, kst[1].p, nullptr, nullptr);
   push_bytes(sig, &a, sizeof a);
   const void* ptrs[] = {y, yalt, ytmp.p, kst[0].p, kst[1].p, kst[2].p, kst[3].p, kst[4].p, kst[5].p, kst[6].p,
-                        ctl_d, stt_eta.p, pat.soff.p, K.p, Kf.p};
+                        ctl_d, stt_eta.p, pat.soff.p, K.p, Kf.p, patx.soff.p, Kx.p, Kxf.p};
   push_bytes(sig, ptrs, sizeof ptrs);
   const double vals[] = {double(n3), double(precision), double(has_stt), stt_beta, stt_scale, alpha};
   push_bytes(sig, vals, sizeof vals);
@@ -2405,10 +2453,7 @@ cudaGraphExec_t Ctx::step_graph_for(double* y, double* yalt) {
         LocalFieldArgs la = local_args(dst, kst[s].p, nullptr, nullptr);
         la.active = &ctl_d->active;
         const SellView S = pat.view(rep);
-        if (precision == TMB_FP64)
-          launch_local_field<double>(S, K.p, tg[0].p, tg[1].p, tg[2].p, g[0].p, g[1].p, la, st);
-        else
-          launch_local_field<float>(S, Kf.p, tgf[0].p, tgf[1].p, tgf[2].p, gf[0].p, gf[1].p, la, st);
+        launch_local_kernel(la, st);
         if (has_stt) {
           if (precision == TMB_FP64)
             launch_stt_add<double>(S, g[0].p, g[1].p, g[2].p, dst, stt_eta.p, alpha, stt_beta, stt_scale, kst[s].p,

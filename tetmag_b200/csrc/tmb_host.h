@@ -74,13 +74,15 @@ struct AmgParams {
   // face-diagonal couplings strong and cuts the Neumann PCG iterations about 3x (46 -> 15
   // on the 363,609-node film to 1e-7)
   double eps_strong = 0.02;
-  double relax = 0.75;                     // prolongation-smoother factor (main/AMGCLSolver.cpp:40)
+  // prolongation-smoother factor: tetmag gives AMGCL 0.75 (main/AMGCLSolver.cpp:40); 1.0 (Vanek's
+  // 4/3 / rho) measured 3-17 % faster under the Jacobi V-cycle here (fewer PCG iterations)
+  double relax = 1.0;
   // dense FP64 solve at or below this size: on the 363,609-node film the hierarchy then stops at
   // the 1,676-unknown level (one dense product instead of five latency-bound launches for the two
   // smallest levels per V-cycle)
   int coarse_enough = 2000;
   int max_levels = 12;
-  double jacobi_omega = 0.9;               // smoother damping (times 4 / (3 rho(D^-1 A)))
+  double jacobi_omega = 1.0;               // smoother damping (times 4 / (3 rho(D^-1 A)))
   bool singular = false;                   // operator annihilates constants (pure Neumann)
 };
 
