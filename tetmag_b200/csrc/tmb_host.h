@@ -82,7 +82,10 @@ struct AmgParams {
   // smallest levels per V-cycle)
   int coarse_enough = 2000;
   int max_levels = 12;
-  double jacobi_omega = 1.0;               // smoother damping (times 4 / (3 rho(D^-1 A)))
+  // smoother damping, times 4 / (3 rho(D^-1 A)): 1.25 puts the weight at 1.67 / rho, below the 2 / rho
+  // that keeps the symmetric V-cycle positive definite; measured fastest among 0.8-1.35 (fewer PCG
+  // iterations; 1.35 gave more)
+  double jacobi_omega = 1.25;
   bool singular = false;                   // operator annihilates constants (pure Neumann)
 };
 
