@@ -5,8 +5,8 @@ right-hand side) on B200.
 Default run: one JSON line for c2 -- a step is one full field evaluation of the 363,609-node
 permalloy film (500x500x20 nm at 2.5 nm, seeded vortex, 20 mT in-plane): divergence, Neumann
 PCG+AMG, hierarchical (leaf 32, eta 2) double-layer BEM matvec, Dirichlet PCG+AMG, gradient,
-fused local field + LLG right-hand side, on the mixed path (FP32 operator values, FP64 vectors /
-reductions / coarse solve).  The plain FP64 paths are measured in the same run as the speed bar,
+fused local field + LLG right-hand side, on the mixed path (FP32 operator values except the CG's
+own operator, FP64 vectors / reductions / coarse solve).  The plain FP64 paths are measured in the same run as the speed bar,
 with the relative error between them.  The same line carries, under "workloads", the other
 configurations measured in the same run: c3 (256 uneven dots in one batched context), c4x64
 (64 replicas of one mesh sharing one dense BEM, the boundary product a tensor-core GEMM) and c5
@@ -586,7 +586,7 @@ def headline_line(args, r: dict, world: int) -> dict:
         "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
         "scaling": "strong" if r["sharded"] else "weak", "vs_baseline": None,
         "dtype": "f32 operators / f64 vectors+reductions", "data": "synthetic", "config": r["config"],
-        "path": "mixed precision (FP32 operator values; FP64 vectors, reductions, coarse solve, step control)",
+        "path": "mixed precision (FP32 operator values except the CG's own operator; FP64 vectors, reductions, coarse solve, step control)",
         "e2e": r["e2e"], "gpu_launches": r["launches"], "roofline": r["roofline"], "clocks": r["clocks"],
     }
     for k in ("fp64_value", "fp64_dense_value", "rel_err_vs_fp64", "rel_err_fp64_hier_vs_dense", "bem_info",

@@ -34,7 +34,7 @@ extern "C" {
 #define TMB_ERR_INTERNAL 7
 
 #define TMB_FP64 0             /* plain path: FP64 operators and vectors */
-#define TMB_MIXED 1            /* FP32 operator values, FP64 vectors, reductions, coarse solve, step control */
+#define TMB_MIXED 1            /* FP32 operator values (the CG's own operator FP64), FP64 vectors, reductions, coarse solve, step control */
 
 #define TMB_PTR_HOST 0
 #define TMB_PTR_DEVICE 1

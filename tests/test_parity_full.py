@@ -6,6 +6,12 @@
 * c4 at full size (28,611 nodes, 7,002 boundary nodes, dense BEM): demag field and LLG right-hand
   side of a seeded random state against the oracle's direct solves, 1e-10 on the plain FP64 path
   and 1e-5 on the mixed path.
+* c4's whole configured run for replica 0 (1 ns at alpha = 0.5 from its seeded random state in its
+  applied field) and c3's whole 0.5 ns run for three dots of the 256-dot batch (the batch stepped in
+  one context, each dot run alone by the oracle): the mean magnetisation after every 100 ps within
+  1e-4 of the oracle's, on both paths.  c3's dots precess for the whole run (alpha = 0.1), so both
+  integrators run at tolerance 1e-8 there: at tetmag's 1e-6 the step control alone moves a dot's
+  mean m by up to 1e-3 within 200 ps.
 """
 from pathlib import Path
 
@@ -94,3 +100,35 @@ def test_c4_full_size_hierarchical_against_oracle(c4):
     ctx.set_solver_params(1e-8, 400)
     ctx.field_eval(m, hdem=h)
     assert rel(h, g["hdem"]) <= MIXED_TOL
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_c4_run_1ns_mean_m(mixed):
+    g = np.load(GOLDEN / "c4_relax_1ns.npz")
+    w = workloads.c4_replica(replica=0)
+    mo, ctx = workloads.setup_context(w, mixed=mixed, tol=1e-12 if not mixed else 1e-8, maxiter=300)
+    vol = mo.operators()["node_vol"]
+    m = w.m0.copy()
+    for k in range(len(g["mean_m"])):
+        ctx.relax(m, duration_ps=float(g["chunk_ps"]), segment_ps=float(g["segment_ps"]))
+        got = _mean_m(m, vol)
+        assert np.max(np.abs(got - g["mean_m"][k])) <= MEAN_M_TOL, (k, got, g["mean_m"][k])
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_c3_batch_run_sampled_dots_mean_m(mixed):
+    g = np.load(GOLDEN / "c3_dots_run.npz")
+    w = workloads.c3_dots(256, 3)
+    mo, ctx = workloads.setup_context(w, mixed=mixed, tol=1e-12 if not mixed else 1e-8, maxiter=300)
+    vol = mo.operators()["node_vol"]
+    off = np.asarray(w.components)
+    m = w.m0.copy()
+    eps = float(g["eps"])
+    for k in range(g["mean_m"].shape[1]):
+        ctx.relax(m, duration_ps=float(g["chunk_ps"]), segment_ps=float(g["segment_ps"]), eps_abs=eps, eps_rel=eps)
+        mm = m.reshape(3, -1)
+        for i, c in enumerate(g["dots"]):
+            lo, hi = int(off[c]), int(off[c + 1])
+            assert hi - lo == int(g["nodes"][i])
+            got = mm[:, lo:hi] @ vol[lo:hi] / vol[lo:hi].sum()
+            assert np.max(np.abs(got - g["mean_m"][i, k])) <= MEAN_M_TOL, (int(c), k, got, g["mean_m"][i, k])

@@ -235,6 +235,15 @@ struct Prof {
 // ------------------------------------------------------------------------------------------
 // Solver: PCG + smoothed-aggregation V-cycle for row-constrained SPD systems
 // ------------------------------------------------------------------------------------------
+// The mixed path keeps the CG's own operator (the lift of the constrained columns, the start
+// residual and the product A p) in FP64 and only the preconditioner (every V-cycle level and
+// transfer) in FP32.  A CG on FP32 operator values converges to the solution of the rounded system,
+// which differs from the FP64 one by up to the condition number times the FP32 rounding (about 1e-5
+// of the field on the small dots of the batched workload); with the FP64 operator the solution
+// matches the FP64 path to the CG tolerance and the FP32 preconditioner only changes the iteration
+// count.
+constexpr bool kCgOperatorF64 = true;
+
 struct DevLevel {
   int n = 0;
   DevSell A;                 // fine level: SELL-32, one thread per row (about 14 entries per row)
@@ -610,9 +619,11 @@ bool Solver::ctx_prof_on() const { return ctx->prof.on; }
 void Solver::iteration_body(int precision, cudaStream_t st, bool profile) {
   const SellView A0 = lev[0].A.view(rep);
   const bool f64 = precision == TMB_FP64;
-  // p = z + beta p and q = A z + beta q: the product gathers z only
-  if (profile) ctx_prof_begin(6, st, nnz_fine * ((f64 ? 8.0 : 4.0) + 4.0) + 5.0 * 8.0 * n * rep);
-  if (f64) launch_cg_dir_spmv<double>(A0, lev[0].Ad.p, z.p, p.p, q.p, Sd, partials.p, st);
+  // p = z + beta p and q = A z + beta q: the product gathers z only (FP64 operator values on both
+  // paths: the CG's own operator, see kCgOperatorF64)
+  const bool op64 = f64 || kCgOperatorF64;
+  if (profile) ctx_prof_begin(6, st, nnz_fine * ((op64 ? 8.0 : 4.0) + 4.0) + 5.0 * 8.0 * n * rep);
+  if (op64) launch_cg_dir_spmv<double>(A0, lev[0].Ad.p, z.p, p.p, q.p, Sd, partials.p, st);
   else launch_cg_dir_spmv<float>(A0, lev[0].Af.p, z.p, p.p, q.p, Sd, partials.p, st);
   if (profile) ctx_prof_end(st);
   if (lev.size() > 1 && rep < 8) {
@@ -942,12 +953,13 @@ void Solver::solve_start(const double* b_dev, int precision, cudaStream_t st) {
   const SellView A0 = lev[0].A.view(rep);
   const bool f64 = precision == TMB_FP64;
   const bool prof = ctx_prof_on();
+  const bool op64 = f64 || kCgOperatorF64;
   if (prof)
-    ctx_prof_begin(15, st, (double(lift.col.n) + nnz_fine) * ((f64 ? 8.0 : 4.0) + 4.0) + 8.0 * 8.0 * n * rep);
-  if (f64) launch_cg_init<double>(n, lift.view(rep), lift.v.p, cmask.p, b_dev, bp.p, x.p, st);
+    ctx_prof_begin(15, st, (double(lift.col.n) + nnz_fine) * ((op64 ? 8.0 : 4.0) + 4.0) + 8.0 * 8.0 * n * rep);
+  if (op64) launch_cg_init<double>(n, lift.view(rep), lift.v.p, cmask.p, b_dev, bp.p, x.p, st);
   else launch_cg_init<float>(n, lift.view(rep), lift.vf.p, cmask.p, b_dev, bp.p, x.p, st);
   rc = 0;  // graphs are captured with the residual starting in rbuf[0]
-  if (f64) launch_cg_residual<double>(A0, lev[0].Ad.p, bp.p, x.p, rbuf[0].p, Sd, partials.p, st);
+  if (op64) launch_cg_residual<double>(A0, lev[0].Ad.p, bp.p, x.p, rbuf[0].p, Sd, partials.p, st);
   else launch_cg_residual<float>(A0, lev[0].Af.p, bp.p, x.p, rbuf[0].p, Sd, partials.p, st);
   if (prof) ctx_prof_end(st);
   precondition_rz(precision, st, true);
