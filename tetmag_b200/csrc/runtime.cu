@@ -349,8 +349,12 @@ struct Solver {
   bool ctx_prof_on() const;
   // one PCG iteration: direction update, A p with p.Ap, x/r update with r.r, V-cycle, r.z
   void iteration_body(int precision, cudaStream_t st, bool profile);
-  // CUDA graph of kGraphIters iteration bodies per precision, captured on first use
+  // CUDA graph of kGraphIters iteration bodies per precision, captured on first use.  Each fused
+  // iteration swaps the two residual buffers and every graph is captured starting from rbuf[0], so
+  // a graph must hold an even count (an odd one makes the next launch read the wrong residual).
+  // 2 measured faster than 4.
   static constexpr int kGraphIters = 2;
+  static_assert(kGraphIters % 2 == 0, "CG graphs must end on the residual buffer they start from");
   cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
   long long graph_nodes[2] = {0, 0};
   cudaGraphExec_t graph_for(int precision);
