@@ -91,7 +91,7 @@ __device__ __forceinline__ double sell_row_dot(const SellView& s, const V* __res
       v[u] = ok ? __ldg(val + k) : V(0);
     }
 #pragma unroll
-    for (int u = 0; u < kChunk; ++u) acc = fma(static_cast<double>(v[u]), __ldg(x + j[u]), acc);
+    for (int u = 0; u < kChunk; ++u) acc = fma(opval(v[u], s.tab), __ldg(x + j[u]), acc);
   }
   return acc;
 }
@@ -124,8 +124,9 @@ __device__ __forceinline__ double2 sell_row_dot2(const SellView& s, const V* __r
 #pragma unroll
     for (int u = 0; u < kChunk; ++u) {
       const double2 xv = __ldg(reinterpret_cast<const double2*>(x + j[u]));
-      acc.x = fma(static_cast<double>(v[u]), xv.x, acc.x);
-      acc.y = fma(static_cast<double>(v[u]), xv.y, acc.y);
+      const double vu = opval(v[u], s.tab);
+      acc.x = fma(vu, xv.x, acc.x);
+      acc.y = fma(vu, xv.y, acc.y);
     }
   }
   return acc;
@@ -171,7 +172,7 @@ __global__ void __launch_bounds__(kBlock) k_jacobi0_residual(SellView s, const V
     }
 #pragma unroll
     for (int u = 0; u < kChunk; ++u)
-      acc = fma(static_cast<double>(v[u]), __ldg(dinv + j[u]) * __ldg(b + j[u] * R + rr), acc);
+      acc = fma(opval(v[u], s.tab), __ldg(dinv + j[u]) * __ldg(b + j[u] * R + rr), acc);
   }
   const double bi = b[g];
   x[g] = dinv[row] * bi;
@@ -606,7 +607,7 @@ __global__ void __launch_bounds__(kBlock) k_cg_update_jacobi0(SellView s, const 
 #pragma unroll
       for (int u = 0; u < kChunk; ++u) {
         const int jj = j[u] * R + rr;
-        acc = fma(static_cast<double>(w[u]), __ldg(dinv + j[u]) * fma(-alpha, __ldg(q + jj), __ldg(r + jj)), acc);
+        acc = fma(opval(w[u], s.tab), __ldg(dinv + j[u]) * fma(-alpha, __ldg(q + jj), __ldg(r + jj)), acc);
       }
     }
     const double ri = fma(-alpha, q[g], r[g]);
@@ -689,7 +690,7 @@ __global__ void __launch_bounds__(kBlock) k_jacobi0_residual2(SellView s, const 
     }
 #pragma unroll
     for (int u = 0; u < kChunk; ++u) {
-      const double w = static_cast<double>(v[u]) * __ldg(dinv + j[u]);
+      const double w = opval(v[u], s.tab) * __ldg(dinv + j[u]);
       const double2 bj = __ldg(reinterpret_cast<const double2*>(b + j[u] * R + rr));
       acc.x = fma(w, bj.x, acc.x);
       acc.y = fma(w, bj.y, acc.y);
@@ -1030,5 +1031,23 @@ void launch_cg_update(int n, const double* p, const double* q, double* x, double
 TMB_INST(double)
 TMB_INST(float)
 #undef TMB_INST
+
+// Finest-level kernels on dictionary-coded values (one-byte indices into SellView::tab).
+#define TMB_INST_SELL(V)                                                                                     \
+  template void launch_jacobi<V>(const SellView&, const V*, const double*, const double*, const double*,    \
+                                 double*, const int*, cudaStream_t);                                        \
+  template void launch_cg_residual<V>(const SellView&, const V*, const double*, const double*, double*,     \
+                                      CgScalars*, double*, cudaStream_t);                                   \
+  template void launch_jacobi0_residual<V>(const SellView&, const V*, const double*, const double*, double*, \
+                                           double*, const int*, cudaStream_t);                              \
+  template void launch_jacobi_rz<V>(const SellView&, const V*, const double*, const double*, const double*, \
+                                    double*, CgScalars*, double*, bool, cudaStream_t);                      \
+  template void launch_cg_dir_spmv<V>(const SellView&, const V*, const double*, double*, double*, CgScalars*, \
+                                      double*, cudaStream_t);                                                 \
+  template void launch_cg_update_jacobi0<V>(const SellView&, const V*, const double*, const double*,         \
+                                            const double*, double*, const double*, double*, double*, double*, \
+                                            CgScalars*, double*, cudaStream_t);
+TMB_INST_SELL(uint8_t)
+#undef TMB_INST_SELL
 
 }  // namespace tmb

@@ -22,6 +22,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/tmb.h"
@@ -244,9 +245,25 @@ struct Prof {
 // count.
 constexpr bool kCgOperatorF64 = true;
 
+// A finest-level operator with at most this many distinct values (0.0 included) stores them as
+// one-byte codes into an FP64 table.
+constexpr int kDictMax = 32;
+
 struct DevLevel {
   int n = 0;
   DevSell A;                 // fine level: SELL-32, one thread per row (about 14 entries per row)
+  // fine level, dictionary-coded values: the stiffness matrix of a Kuhn-split cuboid has about a
+  // dozen distinct entries, so one-byte codes into an FP64 table give exact FP64 values at a
+  // quarter of FP32's bytes (both precision paths then read the same exact operator)
+  bool dict = false;
+  DevArray<uint8_t> Aq;
+  DevArray<double> Atab;
+  SellView fine_view(int rep) const {
+    SellView v = A.view(rep);
+    v.tab = dict ? Atab.p : nullptr;
+    return v;
+  }
+  double fine_value_bytes(bool f64) const { return dict ? 1.0 : (f64 ? 8.0 : 4.0); }
   DevCsr Ac;                 // coarser levels: CSR, tA threads per row (Galerkin rows of 20-60 entries)
   int tA = 1, tP = 1, tR = 1;
   DevArray<double> Ad, dinv, X, R, b, out;
@@ -621,13 +638,14 @@ void Solver::ctx_prof_end(cudaStream_t st) { ctx->prof.end(st); }
 bool Solver::ctx_prof_on() const { return ctx->prof.on; }
 
 void Solver::iteration_body(int precision, cudaStream_t st, bool profile) {
-  const SellView A0 = lev[0].A.view(rep);
+  const SellView A0 = lev[0].fine_view(rep);
   const bool f64 = precision == TMB_FP64;
   // p = z + beta p and q = A z + beta q: the product gathers z only (FP64 operator values on both
-  // paths: the CG's own operator, see kCgOperatorF64)
+  // paths: the CG's own operator, see kCgOperatorF64; exact through the dictionary when coded)
   const bool op64 = f64 || kCgOperatorF64;
-  if (profile) ctx_prof_begin(6, st, nnz_fine * ((op64 ? 8.0 : 4.0) + 4.0) + 5.0 * 8.0 * n * rep);
-  if (op64) launch_cg_dir_spmv<double>(A0, lev[0].Ad.p, z.p, p.p, q.p, Sd, partials.p, st);
+  if (profile) ctx_prof_begin(6, st, nnz_fine * (lev[0].fine_value_bytes(op64) + 4.0) + 5.0 * 8.0 * n * rep);
+  if (lev[0].dict) launch_cg_dir_spmv<uint8_t>(A0, lev[0].Aq.p, z.p, p.p, q.p, Sd, partials.p, st);
+  else if (op64) launch_cg_dir_spmv<double>(A0, lev[0].Ad.p, z.p, p.p, q.p, Sd, partials.p, st);
   else launch_cg_dir_spmv<float>(A0, lev[0].Af.p, z.p, p.p, q.p, Sd, partials.p, st);
   if (profile) ctx_prof_end(st);
   if (lev.size() > 1 && rep < 8) {
@@ -637,8 +655,11 @@ void Solver::iteration_body(int precision, cudaStream_t st, bool profile) {
     double* rnew = rbuf[rc ^ 1].p;
     rc ^= 1;
     DevLevel& L = lev[0];
-    if (profile) ctx_prof_begin(8, st, nnz_fine * ((f64 ? 8.0 : 4.0) + 4.0) + 9.0 * 8.0 * n * rep);
-    if (f64)
+    if (profile) ctx_prof_begin(8, st, nnz_fine * (L.fine_value_bytes(f64) + 4.0) + 9.0 * 8.0 * n * rep);
+    if (L.dict)
+      launch_cg_update_jacobi0<uint8_t>(A0, L.Aq.p, L.dinv.p, p.p, q.p, x.p, rold, rnew, L.X.p, L.R.p, Sd,
+                                        partials.p, st);
+    else if (f64)
       launch_cg_update_jacobi0<double>(A0, L.Ad.p, L.dinv.p, p.p, q.p, x.p, rold, rnew, L.X.p, L.R.p, Sd,
                                        partials.p, st);
     else
@@ -752,6 +773,33 @@ void Solver::compute() {
       d.A.upload(S, st);
       d.Ad.upload(sell_values<double>(S, hl.A.val.data()), st);
       d.Af.upload(sell_values<float>(S, hl.A.val.data()), st);
+      {
+        std::vector<double> tab{0.0};
+        std::unordered_map<uint64_t, int> slot{{0ull, 0}};
+        std::vector<uint8_t> code(hl.A.val.size());
+        bool fits = true;
+        for (size_t k = 0; k < hl.A.val.size() && fits; ++k) {
+          uint64_t bits;
+          std::memcpy(&bits, &hl.A.val[k], sizeof bits);
+          auto it = slot.find(bits);
+          if (it == slot.end()) {
+            if (int(tab.size()) == kDictMax) {
+              fits = false;
+              break;
+            }
+            it = slot.emplace(bits, int(tab.size())).first;
+            tab.push_back(hl.A.val[k]);
+          }
+          code[k] = uint8_t(it->second);
+        }
+        d.dict = fits;
+        if (fits) {
+          std::vector<uint8_t> q(S.col.size(), 0);  // padding: code 0 = 0.0
+          for (size_t k = 0; k < S.map.size(); ++k) q[S.map[k]] = code[k];
+          d.Aq.upload(q, st);
+          d.Atab.upload(tab, st);
+        }
+      }
     } else {
       d.Ac.upload(hl.A, st);
       d.tA = rep >= 8 ? 1 : csr_threads_per_row(hl.A.nrows, hl.A.nnz());
@@ -870,12 +918,13 @@ void Solver::vcycle(size_t l, const double* b, double* out, int precision, cudaS
   DevLevel& C = lev[l + 1];
   const double nl = double(L.n) * R, nc = double(C.n) * R;
   const double nnz_l = l == 0 ? nnz_fine : double(L.Ac.col.n);
-  const double sweep = nnz_l * (sv + 4.0) + (l == 0 ? 0.0 : 4.0 * (L.n + 1));
+  const double sweep = nnz_l * ((l == 0 ? L.fine_value_bytes(f64) : sv) + 4.0) + (l == 0 ? 0.0 : 4.0 * (L.n + 1));
   if (l == 0) {
-    const SellView A = L.A.view(rep);
+    const SellView A = L.fine_view(rep);
     if (!presmoothed) {
       pb(10, sweep + 4.0 * 8.0 * nl);
-      if (f64) launch_jacobi0_residual<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, L.R.p, done, st);
+      if (L.dict) launch_jacobi0_residual<uint8_t>(A, L.Aq.p, L.dinv.p, b, L.X.p, L.R.p, done, st);
+      else if (f64) launch_jacobi0_residual<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, L.R.p, done, st);
       else launch_jacobi0_residual<float>(A, L.Af.p, L.dinv.p, b, L.X.p, L.R.p, done, st);
       pe();
     }
@@ -921,14 +970,16 @@ void Solver::vcycle(size_t l, const double* b, double* out, int precision, cudaS
   else launch_csr_spmv<float>(L.P.view(rep), L.P.vf.p, C.out.p, L.X.p, true, done, st, L.tP);
   pe();
   if (l == 0) {
-    const SellView A = L.A.view(rep);
+    const SellView A = L.fine_view(rep);
     pb(9, sweep + 5.0 * 8.0 * nl);
     if (rz_mode >= 0) {
       // finest level: the post-smoothing sweep also reduces r.z for the next CG direction
-      if (f64) launch_jacobi_rz<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, out, Sd, partials.p, rz_mode == 1, st);
+      if (L.dict) launch_jacobi_rz<uint8_t>(A, L.Aq.p, L.dinv.p, b, L.X.p, out, Sd, partials.p, rz_mode == 1, st);
+      else if (f64) launch_jacobi_rz<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, out, Sd, partials.p, rz_mode == 1, st);
       else launch_jacobi_rz<float>(A, L.Af.p, L.dinv.p, b, L.X.p, out, Sd, partials.p, rz_mode == 1, st);
     } else {
-      if (f64) launch_jacobi<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, out, done, st);
+      if (L.dict) launch_jacobi<uint8_t>(A, L.Aq.p, L.dinv.p, b, L.X.p, out, done, st);
+      else if (f64) launch_jacobi<double>(A, L.Ad.p, L.dinv.p, b, L.X.p, out, done, st);
       else launch_jacobi<float>(A, L.Af.p, L.dinv.p, b, L.X.p, out, done, st);
     }
     pe();
@@ -954,16 +1005,18 @@ void Solver::precondition_rz(int precision, cudaStream_t st, bool first) {
 // The start of a solve: b' = b_F - L b_C with x_C pinned, r = b' - A x from the warm start, and the
 // first V-cycle with r.z (beta = 0).
 void Solver::solve_start(const double* b_dev, int precision, cudaStream_t st) {
-  const SellView A0 = lev[0].A.view(rep);
+  const SellView A0 = lev[0].fine_view(rep);
   const bool f64 = precision == TMB_FP64;
   const bool prof = ctx_prof_on();
   const bool op64 = f64 || kCgOperatorF64;
   if (prof)
-    ctx_prof_begin(15, st, (double(lift.col.n) + nnz_fine) * ((op64 ? 8.0 : 4.0) + 4.0) + 8.0 * 8.0 * n * rep);
+    ctx_prof_begin(15, st, double(lift.col.n) * ((op64 ? 8.0 : 4.0) + 4.0) +
+                               nnz_fine * (lev[0].fine_value_bytes(op64) + 4.0) + 8.0 * 8.0 * n * rep);
   if (op64) launch_cg_init<double>(n, lift.view(rep), lift.v.p, cmask.p, b_dev, bp.p, x.p, st);
   else launch_cg_init<float>(n, lift.view(rep), lift.vf.p, cmask.p, b_dev, bp.p, x.p, st);
   rc = 0;  // graphs are captured with the residual starting in rbuf[0]
-  if (op64) launch_cg_residual<double>(A0, lev[0].Ad.p, bp.p, x.p, rbuf[0].p, Sd, partials.p, st);
+  if (lev[0].dict) launch_cg_residual<uint8_t>(A0, lev[0].Aq.p, bp.p, x.p, rbuf[0].p, Sd, partials.p, st);
+  else if (op64) launch_cg_residual<double>(A0, lev[0].Ad.p, bp.p, x.p, rbuf[0].p, Sd, partials.p, st);
   else launch_cg_residual<float>(A0, lev[0].Af.p, bp.p, x.p, rbuf[0].p, Sd, partials.p, st);
   if (prof) ctx_prof_end(st);
   precondition_rz(precision, st, true);

@@ -44,7 +44,20 @@ struct SellView {
   const int* soff;   // nslice + 1 element offsets (multiples of 32)
   const int* col;    // padded column indices
   int rep;           // interleaved replicas (1: plain vectors)
+  // value table of a dictionary-coded operator (values stored as one-byte indices into it, entry 0
+  // is 0.0 for the padding); null for plain FP32 / FP64 values
+  const double* tab;
 };
+
+// The value of one stored operator entry: the entry itself, or its table entry for one-byte codes.
+template <typename V>
+__device__ __forceinline__ double opval(V v, const double* /*tab*/) {
+  return static_cast<double>(v);
+}
+template <>
+__device__ __forceinline__ double opval<uint8_t>(uint8_t v, const double* tab) {
+  return __ldg(tab + v);
+}
 
 struct CsrView {
   int n;
