@@ -36,6 +36,17 @@ __device__ __forceinline__ double ld(const V* p, int k) {
   return static_cast<double>(__ldg(p + k));
 }
 
+// Stored entry k of an operator that may be dictionary-coded (one-byte codes into the FP64 table of
+// SellView::tab; the three operators of one kind share the table in sections of 32).
+template <typename V>
+__device__ __forceinline__ double ldc(const V* p, int k, const double* /*tab*/) {
+  return static_cast<double>(__ldg(p + k));
+}
+template <>
+__device__ __forceinline__ double ldc<uint8_t>(const uint8_t* p, int k, const double* tab) {
+  return __ldg(tab + __ldg(p + k));
+}
+
 // DMI: 0 none, 1 bulk (tetmag), 2 interfacial (no tetmag counterpart; see the epilogue).
 template <typename V, bool UNI, int DMI>
 __global__ void __launch_bounds__(kBlock) k_local_field(SellView s, const V* __restrict__ K,
@@ -198,7 +209,8 @@ __global__ void __launch_bounds__(kBlock) k_divergence(SellView s, const V* __re
     const int j = __ldg(s.col + k);
     const int jj = j * R + r;
     const double J = __ldg(js + j);
-    const double t = ld(tg0, k) * __ldg(m + jj) + ld(tg1, k) * __ldg(m + n + jj) + ld(tg2, k) * __ldg(m + 2 * n + jj);
+    const double t = ldc(tg0, k, s.tab) * __ldg(m + jj) + ldc(tg1, k, s.tab) * __ldg(m + n + jj) +
+                     ldc(tg2, k, s.tab) * __ldg(m + 2 * n + jj);
     acc = fma(t, J, acc);
   }
   rhs[g] = acc * inv_mu0;
@@ -222,9 +234,9 @@ __global__ void __launch_bounds__(kBlock) k_gradient(SellView s, const V* __rest
   for (int k = beg; k < end; k += kSlice) {
     const int j = __ldg(s.col + k) * R + r;
     const double u = u2 ? __ldg(u1 + j) + __ldg(u2 + j) : __ldg(u1 + j);
-    a0 = fma(ld(g0, k), u, a0);
-    a1 = fma(ld(g1, k), u, a1);
-    a2 = fma(ld(g2, k), u, a2);
+    a0 = fma(ldc(g0, k, s.tab), u, a0);
+    a1 = fma(ldc(g1, k, s.tab), u, a1);
+    a2 = fma(ldc(g2, k, s.tab), u, a2);
   }
   if (hdem) {
     hdem[g] = -a0;
@@ -643,5 +655,11 @@ void launch_add(int n, const double* a, const double* b, double* out, cudaStream
 TMB_INST(double)
 TMB_INST(float)
 #undef TMB_INST
+// divergence and gradient on dictionary-coded operators
+template void launch_divergence<uint8_t>(const SellView&, const uint8_t*, const uint8_t*, const uint8_t*,
+                                         const double*, const double*, double, double*, cudaStream_t);
+template void launch_gradient<uint8_t>(const SellView&, const uint8_t*, const uint8_t*, const uint8_t*,
+                                       const double*, const double*, const double*, double*, double*,
+                                       cudaStream_t);
 
 }  // namespace tmb

@@ -406,6 +406,14 @@ struct Ctx {
   // K alone on its non-zero entries (and the diagonal), for local fields without DMI: on Kuhn-split
   // cuboids half of the shared pattern holds exact zeros of K (the face-diagonal couplings).  Built
   // only when it drops at least a tenth of the entries; otherwise the shared pattern serves.
+  // grad and tGrad dictionary-coded (each of the three operators of a kind has at most 32 distinct
+  // values on a Kuhn-split cuboid): one-byte codes into a shared FP64 table, section 32 d for
+  // operator d; exact FP64 values for the divergence and gradient of both paths
+  bool g_coded = false, tg_coded = false;
+  DevArray<uint8_t> gq[3], tgq[3];
+  DevArray<double> gtab, tgtab;
+  void launch_div(const double* m, const double* js_, double scale, double* out, cudaStream_t st);
+  void launch_grad(const double* u1, const double* u2, const double* he, double* hd, double* hf, cudaStream_t st);
   bool has_patx = false;
   long long nnz_x = 0;
   DevSell patx;
@@ -1118,6 +1126,38 @@ void Ctx::set_operators(int nx, const int* ptr, const int* col, const double* K_
     tg[d].upload(sell_values<double>(S, tg_[d]), st);
     tgf[d].upload(sell_values<float>(S, tg_[d]), st);
   }
+  // dictionary codes of the three grad and the three tGrad operators (all or none of a kind)
+  auto code3 = [&](const double* const* ops, DevArray<uint8_t>* q, DevArray<double>& tab) {
+    std::vector<double> t(96, 0.0);
+    std::vector<std::vector<uint8_t>> codes(3);
+    for (int d = 0; d < 3; ++d) {
+      std::unordered_map<uint64_t, int> slot{{0ull, 0}};
+      int used = 1;  // local code 0 is 0.0 (the padding)
+      std::vector<uint8_t> c(nnz);
+      for (int k = 0; k < nnz; ++k) {
+        uint64_t bits;
+        std::memcpy(&bits, &ops[d][k], sizeof bits);
+        auto it = slot.find(bits);
+        if (it == slot.end()) {
+          if (used == 32) return false;
+          it = slot.emplace(bits, used).first;
+          t[32 * d + used] = ops[d][k];
+          ++used;
+        }
+        c[k] = uint8_t(32 * d + it->second);
+      }
+      codes[d] = std::move(c);
+    }
+    for (int d = 0; d < 3; ++d) {
+      std::vector<uint8_t> sc(S.col.size(), uint8_t(32 * d));  // padding: the section's 0.0
+      for (size_t k = 0; k < S.map.size(); ++k) sc[S.map[k]] = codes[d][k];
+      q[d].upload(sc, st);
+    }
+    tab.upload(t, st);
+    return true;
+  };
+  g_coded = code3(g_, gq, gtab);
+  tg_coded = code3(tg_, tgq, tgtab);
   {
     std::vector<int> xp(nx + 1, 0), xcol;
     std::vector<double> xv;
@@ -1385,9 +1425,8 @@ void Ctx::demag(const double* m) {
   const bool f64 = precision == TMB_FP64;
   const double sv = f64 ? 8.0 : 4.0, z = double(hptr[n]), N = double(nr()), B = double(nb) * rep;
   prof.begin(7, st, 0.0);
-  prof.begin(1, st, z * (3 * sv + 4) + N * 8 * 5);
-  if (f64) launch_divergence<double>(S, tg[0].p, tg[1].p, tg[2].p, m, js.p, 1.0 / kMu0, rhs.p, st);
-  else launch_divergence<float>(S, tgf[0].p, tgf[1].p, tgf[2].p, m, js.p, 1.0 / kMu0, rhs.p, st);
+  prof.begin(1, st, z * (3 * (tg_coded ? 1.0 : sv) + 4) + N * 8 * 5);
+  launch_div(m, js.p, 1.0 / kMu0, rhs.p, st);
   prof.end(st);
   prof.begin(4, st, 0.0);
   neu->solve(rhs.p, precision);
@@ -1446,9 +1485,8 @@ void Ctx::demag(const double* m) {
   if ((shared_bem || rep > 1) && !f64 && gemm_tc && bits_h[2] != 0)
     throw Error(TMB_ERR_CUDA, "tensor-core boundary GEMM timed out waiting on a barrier");
   prof.end(st);
-  prof.begin(2, st, z * (3 * sv + 4) + N * 8 * 11);
-  if (f64) launch_gradient<double>(S, g[0].p, g[1].p, g[2].p, neu->x.p, dir->x.p, hext.p, hdem.p, hfix.p, st);
-  else launch_gradient<float>(S, gf[0].p, gf[1].p, gf[2].p, neu->x.p, dir->x.p, hext.p, hdem.p, hfix.p, st);
+  prof.begin(2, st, z * (3 * (g_coded ? 1.0 : sv) + 4) + N * 8 * 11);
+  launch_grad(neu->x.p, dir->x.p, hext.p, hdem.p, hfix.p, st);
   prof.end(st);
   prof.end(st);
   TMB_CUDA(cudaGetLastError());
@@ -2291,6 +2329,32 @@ LocalFieldArgs Ctx::local_args(const double* m, double* ydot, double* hout, unsi
   return a;
 }
 
+// Divergence (sum_d tGrad_d (js m_d) scale) and gradient (-grad u) on the shared pattern, from the
+// dictionary-coded operators when they exist, else from the precision's value arrays.
+void Ctx::launch_div(const double* m, const double* js_, double scale, double* out, cudaStream_t st) {
+  SellView S = pat.view(rep);
+  if (tg_coded) {
+    S.tab = tgtab.p;
+    launch_divergence<uint8_t>(S, tgq[0].p, tgq[1].p, tgq[2].p, m, js_, scale, out, st);
+  } else if (precision == TMB_FP64) {
+    launch_divergence<double>(S, tg[0].p, tg[1].p, tg[2].p, m, js_, scale, out, st);
+  } else {
+    launch_divergence<float>(S, tgf[0].p, tgf[1].p, tgf[2].p, m, js_, scale, out, st);
+  }
+}
+void Ctx::launch_grad(const double* u1, const double* u2, const double* he, double* hd, double* hf,
+                      cudaStream_t st) {
+  SellView S = pat.view(rep);
+  if (g_coded) {
+    S.tab = gtab.p;
+    launch_gradient<uint8_t>(S, gq[0].p, gq[1].p, gq[2].p, u1, u2, he, hd, hf, st);
+  } else if (precision == TMB_FP64) {
+    launch_gradient<double>(S, g[0].p, g[1].p, g[2].p, u1, u2, he, hd, hf, st);
+  } else {
+    launch_gradient<float>(S, gf[0].p, gf[1].p, gf[2].p, u1, u2, he, hd, hf, st);
+  }
+}
+
 // The local-field kernel on the shared pattern, or on K's own non-zero pattern when no DMI term
 // needs the gradient operators (the same sums: the dropped entries are exact zeros).
 void Ctx::launch_local_kernel(const LocalFieldArgs& a, cudaStream_t st) {
@@ -2708,8 +2772,7 @@ void Ctx::vjp(const double* Y, const double* H, const double* abar, double* gout
   launch_adj_pre(pa, stream);
   const double* q = nullptr;
   if (has_bem) {
-    if (f64) launch_divergence<double>(S, tg[0].p, tg[1].p, tg[2].p, ab.mu.p, ab.ninvvol.p, 1.0, ab.w.p, stream);
-    else launch_divergence<float>(S, tgf[0].p, tgf[1].p, tgf[2].p, ab.mu.p, ab.ninvvol.p, 1.0, ab.w.p, stream);
+    launch_div(ab.mu.p, ab.ninvvol.p, 1.0, ab.w.p, stream);
     dir->solve_t(ab.w.p, ab.v.p, precision, stage);
     if (bem_mode == 1) {
       // hierarchical B^T in cluster order, scattered back to the boundary nodes
@@ -2726,8 +2789,7 @@ void Ctx::vjp(const double* Y, const double* H, const double* abar, double* gout
     }
     neu->solve_t(ab.w.p, ab.a1.p, precision, stage);
     cnt[4] += neu->last_iters + dir->last_iters;
-    if (f64) launch_gradient<double>(S, g[0].p, g[1].p, g[2].p, ab.a1.p, nullptr, nullptr, ab.q.p, nullptr, stream);
-    else launch_gradient<float>(S, gf[0].p, gf[1].p, gf[2].p, ab.a1.p, nullptr, nullptr, ab.q.p, nullptr, stream);
+    launch_grad(ab.a1.p, nullptr, nullptr, ab.q.p, nullptr, stream);
     q = ab.q.p;
   }
   const bool idmi = has_dmi && dmi_kind == 1;
