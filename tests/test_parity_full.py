@@ -2,7 +2,8 @@
 
 * c1, the whole configured run: 1 ns of frozen-demag Dormand-Prince relaxation (0.5 ps segments)
   of the 1,323-node cuboid from its seeded random state; the mean magnetisation after the run
-  within 1e-4 of the oracle's (the north star's bound), on the plain FP64 path and the mixed path.
+  within 1e-4 of the oracle's (the bound the workloads state for the mean magnetisation), on the plain
+  FP64 path and the mixed path.
 * c4 at full size (28,611 nodes, 7,002 boundary nodes, dense BEM): demag field and LLG right-hand
   side of a seeded random state against the oracle's direct solves, 1e-10 on the plain FP64 path
   and 1e-5 on the mixed path.
