@@ -67,6 +67,9 @@ def parse():
                         "device, for profiling captures that must stay a few GB); h2: the hierarchical "
                         "matrix built from the mesh, recompressed into nested cluster bases; auto: h2 for c2 "
                         "(its configuration names the H2-compressed BEM), the dense matrix otherwise")
+    p.add_argument("--matrix-share", type=float, default=0.0,
+                   help="accuracy measure of the hierarchical matrix: 0 block-relative cross approximation, "
+                        "s > 0 also a matrix-relative budget per block (tmb_set_bem_accuracy)")
     return p.parse_args()
 
 
@@ -360,9 +363,12 @@ def measure(args, name: str, dist: Dist, full: bool) -> dict:
     mo, ctx = workloads.setup_context(w, device=local, mixed=True, tol=args.tol, maxiter=100,
                                       hmatrix={"hmatrix": "mesh", "hmatrix-only": "mesh", "h2": "mesh",
                                                "hmatrix-dense": True}.get(bem, False),
-                                      keep_dense=dense_ref, h2=H2_EPS if bem == "h2" else None)
+                                      keep_dense=dense_ref, h2=H2_EPS if bem == "h2" else None,
+                                      matrix_share=args.matrix_share if hier else 0.0)
     hier_mode = 2 if bem == "h2" else 1
     bem_info = ctx.bem_info() if hier else None
+    if hier:
+        bem_info["matrix_share"] = args.matrix_share
     if hier and dense_ref:
         bem_info["verify"] = ctx.bem_verify()
     if bem == "h2":

@@ -152,6 +152,15 @@ int tmb_bem_compress(tmb_ctx* ctx, const double* bxyz, const double* bnormal, in
  * assembly replaces the dense matrix (setupH2MatrixC, main/h2interface.c:315-399). */
 int tmb_bem_build_h(tmb_ctx* ctx, const tmb_mesh* mesh, int leaf, double eta, double eps_mixed, double eps_fp64,
                     int kmax);
+/* Accuracy measure of the next tmb_bem_compress / tmb_bem_build_h.  matrix_share = 0 (the
+ * default): each admissible block's cross approximation stops at eps relative to the block's own
+ * Frobenius norm.  matrix_share = s > 0: a block may also stop at its share of a matrix-relative
+ * budget, eps * s * sqrt(m n) * ||N||_F / Nb, where N is the dense leaf tiles (the near field,
+ * which holds the diagonal); blocks far from each other, whose entries are orders of magnitude
+ * below the matrix's, then keep the few terms the product needs.  tetmag's recompression
+ * truncates relative to each cluster's total matrix rather than per block for the same reason
+ * (new_releucl_truncmode, main/h2interface.c:328, 362-369). */
+int tmb_set_bem_accuracy(tmb_ctx* ctx, double matrix_share);
 int tmb_set_bem_mode(tmb_ctx* ctx, int mode);  /* 0 dense, 1 hierarchical, 2 H2 */
 /* H2 matrix: the hierarchical matrix's admissible blocks (its FP64 terms) recompressed into nested
  * cluster bases -- orthogonal row and column bases per cluster, leaf bases explicit and parents'

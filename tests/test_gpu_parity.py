@@ -275,6 +275,36 @@ def test_hierarchical_bem_from_mesh_c4():
     assert rel(ctx.demag_field(m), H_dense) <= MIXED_TOL
 
 
+def test_hierarchical_matrix_relative_accuracy_c4():
+    # the same film built to matrix-relative accuracy (tmb_set_bem_accuracy): a low-rank block may
+    # stop at its share of eps * ||N||_F, so blocks far apart keep fewer terms; the demag field
+    # stays within the bounds of the block-relative build
+    w = workloads.c4_replica(replica=2)
+    mo, ctx = workloads.setup_context(w, tol=1e-12, maxiter=300, hmatrix="mesh", keep_dense=True)
+    base = ctx.bem_info()
+    ctx.set_bem_accuracy(1.0)
+    ctx.bem_build_h(mo, leaf=32, eta=2.0, eps_mixed=1e-6, eps_fp64=1e-7, kmax=64)
+    info = ctx.bem_info()
+    assert info["built"] == 1 and info["lowrank_blocks"] == base["lowrank_blocks"]
+    assert info["terms_fp64"] < base["terms_fp64"] and info["terms_fp32"] < base["terms_fp32"]
+    assert info["bytes_fp32"] < base["bytes_fp32"]
+    m = w.m0
+    ctx.set_bem_mode(False)
+    H_dense = ctx.demag_field(m)
+    ctx.set_bem_mode(True)
+    assert rel(ctx.demag_field(m), H_dense) <= 1e-6
+    ctx.set_precision(True)
+    ctx.set_solver_params(1e-9, 300)
+    assert rel(ctx.demag_field(m), H_dense) <= MIXED_TOL
+
+
+def test_bem_accuracy_rejects_bad_share(c1):
+    w, mo, ctx, pb, dem = c1
+    for bad in (-1.0, float("nan"), float("inf")):
+        with pytest.raises(_lib.TmbError):
+            ctx.set_bem_accuracy(bad)
+
+
 def test_hierarchical_from_mesh_all_dense_tiles_equal_dense_c1(c1):
     # with a vanishing admissibility parameter every block is a dense tile assembled from the
     # mesh: the matvec must reproduce the dense assembly to round-off

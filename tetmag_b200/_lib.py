@@ -45,6 +45,7 @@ SIGNATURES = {
     "tmb_get_bem_dense": [_P, _D],
     "tmb_bem_compress": [_P, _D, _D, _int, _dbl, _dbl, _dbl, _int, _int],
     "tmb_bem_build_h": [_P, _P, _int, _dbl, _dbl, _dbl, _int],
+    "tmb_set_bem_accuracy": [_P, _dbl],
     "tmb_set_bem_mode": [_P, _int],
     "tmb_bem_h2": [_P, _dbl, _dbl, _int],
     "tmb_bem_h2_info": [_P, _D],

@@ -194,6 +194,12 @@ class Context:
                                     int(kmax)))
         return self
 
+    def set_bem_accuracy(self, matrix_share: float):
+        """Accuracy measure of the next hierarchical build: 0 block-relative cross approximation;
+        s > 0 also lets a block stop at its share of a matrix-relative budget (tmb_set_bem_accuracy)."""
+        check(lib().tmb_set_bem_accuracy(self.h, float(matrix_share)))
+        return self
+
     def set_bem_mode(self, hierarchical):
         """False / 0: dense; True / 1: hierarchical; 2: H2 (nested cluster bases)."""
         check(lib().tmb_set_bem_mode(self.h, int(hierarchical)))

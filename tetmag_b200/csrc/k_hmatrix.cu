@@ -148,10 +148,14 @@ __device__ void aca_verify(const HBlockDev& b, const E& entry, const double* U, 
 // only bottom-face columns and vice versa), so each time the loose tolerance is reached the
 // residual is checked on the unvisited rows, and the approximation restarts from the worst
 // one if it is significant; the same check guards the final (tight) stop.
+// gscale > 0 is an entry scale of the whole matrix: a block may then also stop once its last
+// term is below eps * gscale * sqrt(m n) (and its unvisited rows below eps * gscale per entry),
+// i.e. at its share of a matrix-relative error budget instead of its own norm's.
 template <typename E>
 __global__ void __launch_bounds__(256) k_h_aca(const HBlockDev* __restrict__ blk, E entry, double* __restrict__ Us,
                                                double* __restrict__ Vs, unsigned char* __restrict__ used, int kmax,
-                                               double eps_tight, double eps_loose, int* __restrict__ out_rank) {
+                                               double eps_tight, double eps_loose, double gscale,
+                                               int* __restrict__ out_rank) {
   constexpr int kMaxPasses = 8;
   __shared__ double shv[32];
   __shared__ int shi[32];
@@ -231,7 +235,7 @@ __global__ void __launch_bounds__(256) k_h_aca(const HBlockDev* __restrict__ blk
       }
       norm2 += uu * vv + 2.0 * cross;
       ++k;
-      const double term = sqrt(uu * vv), fro = sqrt(fabs(norm2));
+      const double term = sqrt(uu * vv), fro = fmax(sqrt(fabs(norm2)), gscale * sqrt(double(m) * n));
       if (term <= eps_tight * fro) {
         if (k_tight < 0) k_tight = k;
       } else {
@@ -251,7 +255,7 @@ __global__ void __launch_bounds__(256) k_h_aca(const HBlockDev* __restrict__ blk
         double val;
         int row;
         aca_verify(b, entry, U, V, usd, k, passes++, shv, shi, val, row);
-        if (row != 0x7fffffff && val > eps_loose * sqrt(fabs(norm2) / (double(m) * n))) {
+        if (row != 0x7fffffff && val > eps_loose * fmax(sqrt(fabs(norm2) / (double(m) * n)), gscale)) {
           k_loose = k_tight = -1;  // a part of the block is still missing: restart there
           istar = row;
           continue;
@@ -265,7 +269,7 @@ __global__ void __launch_bounds__(256) k_h_aca(const HBlockDev* __restrict__ blk
       double val;
       int row;
       aca_verify(b, entry, U, V, usd, k, passes++, shv, shi, val, row);
-      if (row == 0x7fffffff || val <= eps_tight * sqrt(fabs(norm2) / (double(m) * n))) break;
+      if (row == 0x7fffffff || val <= eps_tight * fmax(sqrt(fabs(norm2) / (double(m) * n)), gscale)) break;
       nxt = row;
     }
     if (nxt < 0) break;
@@ -606,13 +610,13 @@ void launch_h_near_gather(int nblk, const HBlockDev* blk, const HSource& src, do
 }
 
 void launch_h_aca(int nblk, const HBlockDev* blk, const HSource& src, double* Us, double* Vs, unsigned char* used,
-                  int kmax, double eps_tight, double eps_loose, int* out_rank, cudaStream_t st) {
+                  int kmax, double eps_tight, double eps_loose, double gscale, int* out_rank, cudaStream_t st) {
   if (nblk == 0) return;
   note_launch();
   if (src.B)
-    k_h_aca<<<nblk, 256, 0, st>>>(blk, dense_entry(src), Us, Vs, used, kmax, eps_tight, eps_loose, out_rank);
+    k_h_aca<<<nblk, 256, 0, st>>>(blk, dense_entry(src), Us, Vs, used, kmax, eps_tight, eps_loose, gscale, out_rank);
   else
-    k_h_aca<<<nblk, 256, 0, st>>>(blk, mesh_entry(src), Us, Vs, used, kmax, eps_tight, eps_loose, out_rank);
+    k_h_aca<<<nblk, 256, 0, st>>>(blk, mesh_entry(src), Us, Vs, used, kmax, eps_tight, eps_loose, gscale, out_rank);
   TMB_CUDA(cudaGetLastError());
 }
 

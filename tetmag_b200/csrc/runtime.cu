@@ -537,6 +537,9 @@ struct Ctx {
   H2View<T> h2_view(int which) const;
   HSource h_source() const;
   int bem_mode = 0;  // 0 dense, 1 hierarchical, 2 H2
+  // matrix-relative accuracy of the next compression (tmb_set_bem_accuracy): 0 block-relative only
+  double h_share = 0.0;
+  double h_gscale = 0.0;  // the entry scale the last compression used
   void h_compress(const double* bxyz, const double* bnrm, int leaf, double eta, double eps_mixed, double eps_fp64,
                   int kmax, bool keep_dense, const MeshHost* mesh = nullptr);
   void h_verify(double* block_out, double* out);
@@ -1877,6 +1880,26 @@ void Ctx::h_compress(const double* bxyz, const double* bnrm, int leaf, double et
   H.D32.alloc(size_t(doff));
   if (mesh) launch_h_near_mesh(H.nnear, H.nearb.p, src, H.D64.p, H.D32.p, st);
   else launch_h_near_gather(H.nnear, H.nearb.p, src, H.D64.p, H.D32.p, st);
+  // matrix-relative accuracy: the entry scale share * ||N||_F / Nb from the dense leaf tiles N
+  // (the near field, which holds the diagonal and dominates the matrix's norm); the tiles' sums
+  // of squares are added in partition order, so the scale does not depend on the thread count
+  h_gscale = 0.0;
+  if (h_share > 0.0 && doff > 0) {
+    std::vector<double> tiles(static_cast<size_t>(doff));
+    TMB_CUDA(cudaMemcpyAsync(tiles.data(), H.D64.p, sizeof(double) * tiles.size(), cudaMemcpyDeviceToHost, st));
+    sync();
+    std::vector<double> part(nearb.size(), 0.0);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (long long q = 0; q < (long long)nearb.size(); ++q) {
+      const HBlockDev& b = nearb[size_t(q)];
+      double a = 0.0;
+      for (long long t = 0; t < (long long)b.m * b.n; ++t) a += tiles[size_t(b.off + t)] * tiles[size_t(b.off + t)];
+      part[size_t(q)] = a;
+    }
+    double ss = 0.0;
+    for (double a : part) ss += a;
+    h_gscale = h_share * std::sqrt(ss) / double(nb);
+  }
   // adaptive cross approximation of every admissible block
   std::vector<int> ranks(size_t(3) * H.nfar, 0);
   if (H.nfar > 0) {
@@ -1887,7 +1910,7 @@ void Ctx::h_compress(const double* bxyz, const double* bnrm, int leaf, double et
     Vs.alloc(size_t(vs));
     used.alloc(size_t(fl));
     dr.alloc(size_t(3) * H.nfar);
-    launch_h_aca(H.nfar, H.farb.p, src, Us.p, Vs.p, used.p, kmax, eps_fp64, eps_mixed, dr.p, st);
+    launch_h_aca(H.nfar, H.farb.p, src, Us.p, Vs.p, used.p, kmax, eps_fp64, eps_mixed, h_gscale, dr.p, st);
     TMB_CUDA(cudaMemcpyAsync(ranks.data(), dr.p, sizeof(int) * ranks.size(), cudaMemcpyDeviceToHost, st));
     sync();
     for (int w = 0; w < 2; ++w) {
@@ -3346,6 +3369,13 @@ int tmb_bem_build_h(tmb_ctx* ctx, const tmb_mesh* mesh, int leaf, double eta, do
     }
   c.h_compress(bxyz.data(), bnrm.data(), leaf, eta, eps_mixed, eps_fp64, kmax, true, &M);
   TMB_API_END
+}
+
+int tmb_set_bem_accuracy(tmb_ctx* ctx, double matrix_share) {
+  TMB_CHECK_ARG(ctx && matrix_share >= 0.0 && std::isfinite(matrix_share),
+                "tmb_set_bem_accuracy: matrix_share is a finite number >= 0");
+  ctx->c->h_share = matrix_share;
+  return TMB_OK;
 }
 
 int tmb_set_bem_mode(tmb_ctx* ctx, int mode) {

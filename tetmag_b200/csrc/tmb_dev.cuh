@@ -327,7 +327,7 @@ void launch_h_near_gather(int nblk, const HBlockDev* blk, const HSource& src, do
 void launch_h_near_mesh(int nblk, const HBlockDev* blk, const HSource& src, double* d64, float* d32,
                         cudaStream_t st);
 void launch_h_aca(int nblk, const HBlockDev* blk, const HSource& src, double* Us, double* Vs, unsigned char* used,
-                  int kmax, double eps_tight, double eps_loose, int* out_rank, cudaStream_t st);
+                  int kmax, double eps_tight, double eps_loose, double gscale, int* out_rank, cudaStream_t st);
 // per low-rank block {|A x|^2, |A x - U64 V64^T x|^2, |A x - U32 V32^T x|^2} for a fixed probe x
 // (ranks <= 128)
 void launch_h_verify(int nblk, const HBlockDev* blk, const HSource& src, const int* rk64, const long long* uo64,

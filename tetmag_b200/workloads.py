@@ -211,13 +211,15 @@ WORKLOADS = {"c1": c1, "c2": c2, "c3": c3_dots, "c4": c4_replica, "c4x64": c4_ba
 
 def setup_context(w: Workload, device: int = 0, mixed: bool = False, tol: float = 1e-7, maxiter: int = 100,
                   mesh_ops=None, hmatrix: bool = False, keep_dense: bool = True, eps_mixed: float = 1e-6,
-                  eps_fp64: float = 1e-7, kmax: int = 64, normal_split: bool = True, h2=None):
+                  eps_fp64: float = 1e-7, kmax: int = 64, normal_split: bool = True, h2=None,
+                  matrix_share: float = 0.0):
     """MeshOps + Context with operators, device-assembled BEM (dense, optionally compressed to the
     hierarchical form with leaf 32 and eta 2), material and applied field.  hmatrix="mesh" builds
     the hierarchical matrix from the mesh boundary; the dense matrix is then assembled only when
     keep_dense is set, in the far-field-accurate arithmetic the hierarchical matrix approximates.
     h2=(eps_fp64, eps_mixed) then recompresses the hierarchical matrix into nested cluster bases (H2)
-    and selects the H2 matvec."""
+    and selects the H2 matvec.  matrix_share > 0 builds the hierarchical matrix to matrix-relative
+    accuracy (tmb_set_bem_accuracy)."""
     from .api import Context, MeshOps
 
     mo = mesh_ops if mesh_ops is not None else MeshOps(w.mesh.xyz, w.mesh.tets)
@@ -227,6 +229,8 @@ def setup_context(w: Workload, device: int = 0, mixed: bool = False, tol: float 
         ctx.set_replicas(w.replicas)
     if w.components is not None:
         ctx.set_components(w.components, shared_bem=w.shared_bem)
+    if hmatrix:
+        ctx.set_bem_accuracy(matrix_share)
     if hmatrix == "mesh":
         if keep_dense:
             ctx.bem_assemble(mo, accurate=True)
