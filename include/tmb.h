@@ -250,8 +250,9 @@ int tmb_llg_rhs(tmb_ctx* ctx, double t, const double* y, double* ydot, int ptr_k
  * ydot are staged through one file-scope device array of 2 x 3 x 65536 doubles (3 MiB, held by
  * every GPU that loads the library until exit); contexts with nodes x replicas above 65536 get
  * TMB_ERR_ARG.  tmb_ctx_create resolves that array's device address for its device
- * (cudaGetSymbolAddress, which also loads the module holding the array), so no call of this
- * entry point, the first included, allocates.  Every call shares the array: calls that overlap
+ * (cudaGetSymbolAddress, which also loads the module holding the array) and loads the kernels
+ * this entry point launches (with lazy module loading a kernel's code is otherwise loaded at its
+ * first launch), so no call of this entry point, the first included, allocates.  Every call shares the array: calls that overlap
  * on the GPU (other threads, other contexts on the same device) race, so serialise them.
  * Nothing in the array needs to start at zero: each call overwrites the 6N entries it uses.
  * Synchronises. */

@@ -118,6 +118,63 @@ def test_noalloc_leaves_device_memory_unchanged():
     assert np.linalg.norm(got1 - ref1) <= TOL * np.linalg.norm(ref1)
 
 
+_FRESH_PROCESS = r"""
+import ctypes as C, sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+import torch
+from oracle import tetmag_oracle as O
+from tetmag_b200 import _lib, meshgen
+from tetmag_b200.api import Context, MeshOps
+
+mesh = meshgen.kuhn_cuboid(24, 20, 8, 3.0)
+mo = MeshOps(mesh.xyz, mesh.tets)
+c = Context(0)
+c.set_mesh(mo)
+n = mo.nx
+rng = np.random.default_rng(5)
+axis = rng.standard_normal((n, 3))
+axis /= np.linalg.norm(axis, axis=1, keepdims=True)
+c.set_material(np.full(n, O.MU0 * 8e5), np.full(n, 1.3e-11 / 1e-18), Ku=np.full(n, 5e4),
+               ku_axis=O.rows_to_soa(axis), D=np.full(n, 3e-3 / 1e-9), alpha=0.3)
+c.set_demag_frozen(1e4 * rng.standard_normal(3 * n))
+c.set_stt(O.rows_to_soa(rng.standard_normal((n, 3)) * 4e6), beta=0.05, scale=0.7)
+c.set_precision(int(sys.argv[2]))
+ptr = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+torch.cuda.mem_get_info(0)
+torch.cuda.synchronize()
+free0, _ = torch.cuda.mem_get_info(0)
+outs = []
+for seed in (1, 2):
+    y = meshgen.random_state(n, seed)
+    out = np.full_like(y, np.nan)
+    _lib.check(_lib.lib().tmb_llg_rhs_noalloc(c.h, 0.0, ptr(y), ptr(out)))
+    outs.append((y, out))
+free1, _ = torch.cuda.mem_get_info(0)
+err = max(float(np.linalg.norm(o - c.llg_rhs(0.0, y)) / np.linalg.norm(o)) for y, o in outs)
+print(free0 - free1, err)
+"""
+
+
+@pytest.mark.parametrize("mixed", [0, 1])
+def test_noalloc_first_call_of_a_fresh_process(mixed):
+    # In a process whose only earlier work on the device is the context's set-up, the first two
+    # calls (local field with uniaxial anisotropy, bulk DMI and the spin-transfer term) leave the
+    # device's free memory unchanged: tmb_ctx_create has resolved the array and loaded the
+    # kernels the entry point launches.  Their results equal the regular entry point's.
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    root = str(Path(__file__).resolve().parents[1])
+    r = subprocess.run([sys.executable, "-c", _FRESH_PROCESS, root, str(mixed)], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    delta, err = r.stdout.split()[-2:]
+    assert int(delta) == 0, f"the first calls changed free device memory by {delta} bytes"
+    assert float(err) <= TOL
+
+
 def test_noalloc_rejects_meshes_beyond_its_array():
     mesh = meshgen.kuhn_cuboid(40, 40, 41, 2.0)  # 41 * 41 * 42 = 70602 nodes > 65536
     mo = MeshOps(mesh.xyz, mesh.tets)

@@ -453,6 +453,28 @@ void launch_stt_add(const SellView& s, const V* g0, const V* g1, const V* g2, co
                                                                 active);
   TMB_CUDA(cudaGetLastError());
 }
+// Loads the code of every kernel the local right-hand side can launch (both operator types,
+// with and without uniaxial anisotropy, each DMI form, the spin-transfer term).  With lazy module
+// loading a kernel's code is otherwise loaded, and its device memory taken, at its first launch;
+// cudaFuncGetAttributes loads it now.
+void preload_local_kernels() {
+  cudaFuncAttributes at;
+  TMB_CUDA(cudaFuncGetAttributes(&at, k_local_field<double, false, 0>));
+  TMB_CUDA(cudaFuncGetAttributes(&at, k_local_field<double, false, 1>));
+  TMB_CUDA(cudaFuncGetAttributes(&at, k_local_field<double, false, 2>));
+  TMB_CUDA(cudaFuncGetAttributes(&at, k_local_field<double, true, 0>));
+  TMB_CUDA(cudaFuncGetAttributes(&at, k_local_field<double, true, 1>));
+  TMB_CUDA(cudaFuncGetAttributes(&at, k_local_field<double, true, 2>));
+  TMB_CUDA(cudaFuncGetAttributes(&at, k_local_field<float, false, 0>));
+  TMB_CUDA(cudaFuncGetAttributes(&at, k_local_field<float, false, 1>));
+  TMB_CUDA(cudaFuncGetAttributes(&at, k_local_field<float, false, 2>));
+  TMB_CUDA(cudaFuncGetAttributes(&at, k_local_field<float, true, 0>));
+  TMB_CUDA(cudaFuncGetAttributes(&at, k_local_field<float, true, 1>));
+  TMB_CUDA(cudaFuncGetAttributes(&at, k_local_field<float, true, 2>));
+  TMB_CUDA(cudaFuncGetAttributes(&at, k_stt_add<double>));
+  TMB_CUDA(cudaFuncGetAttributes(&at, k_stt_add<float>));
+}
+
 template void launch_stt_add<double>(const SellView&, const double*, const double*, const double*, const double*,
                                      const double*, double, double, double, double*, cudaStream_t, const int*);
 template void launch_stt_add<float>(const SellView&, const float*, const float*, const float*, const double*,

@@ -3619,16 +3619,17 @@ static double* g_staging_address[kNoAllocMaxDevices] = {};
 // Resolves the device address of g_rhs_staging on `device`, which must be the current device.
 // Called by tmb_ctx_create, once per device.  The host-side name of the array is only a
 // stand-in: kernels and copies must be given this address.  Resolving it loads the module that
-// holds the array (with lazy module loading that is the moment the 3 MiB are reserved), so it
-// happens at context creation, where allocating is allowed, and never inside
-// tmb_llg_rhs_noalloc.  Devices beyond kNoAllocMaxDevices are skipped (their contexts get
-// TMB_ERR_ARG from tmb_llg_rhs_noalloc).
+// holds the array (with lazy module loading that is the moment the 3 MiB are reserved), and the
+// kernels the entry point launches are loaded with it, so that both happen at context creation,
+// where allocating is allowed, and never inside tmb_llg_rhs_noalloc.  Devices beyond
+// kNoAllocMaxDevices are skipped (their contexts get TMB_ERR_ARG from tmb_llg_rhs_noalloc).
 static void resolve_staging_address(int device) {
   if (device < 0 || device >= kNoAllocMaxDevices) return;
   std::lock_guard<std::mutex> lock(g_staging_mutex);
   if (!g_staging_address[device]) {
     void* p = nullptr;
     TMB_CUDA(cudaGetSymbolAddress(&p, g_rhs_staging));
+    preload_local_kernels();
     g_staging_address[device] = static_cast<double*>(p);
   }
 }

@@ -136,6 +136,8 @@ void launch_gradient(const SellView& s, const V* g0, const V* g1, const V* g2, c
                      const double* u2, const double* hext, double* hdem, double* hfix, cudaStream_t st);
 
 void launch_normalize(int n, double* m, cudaStream_t st);
+// Loads the code of every kernel of the local right-hand side (see k_field.cu), once per device.
+void preload_local_kernels();
 // Zhang-Li spin-transfer torque added to ydot (eta: 3N SoA per node)
 template <typename V>
 void launch_stt_add(const SellView& s, const V* g0, const V* g1, const V* g2, const double* m, const double* eta,
