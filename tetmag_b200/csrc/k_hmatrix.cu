@@ -689,28 +689,65 @@ __global__ void k_h2_leaf_up(int nleaf, const int* __restrict__ leaves, const H2
   if (two) xh[c.xo + lane + 32] = a1;
 }
 
-// upward pass, one depth: xh_c = sum over children F_ch^T xh_ch (the transposed transfer of a
-// child is stored kc x kc_child column-major: lane j reads F[j + i * kc], coalesced)
+// Asynchronous element copies global -> shared (cp.async): a thread issues all of its copies
+// before waiting for any, so a CTA has its whole panel in flight at once.
 template <typename T>
-__global__ void k_h2_up(int count, const int* __restrict__ ids, const H2Node* __restrict__ node,
-                        const T* __restrict__ colb, double* __restrict__ xh) {
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (w >= count) return;
-  const H2Node c = node[ids[w]];
+__device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
+  static_assert(sizeof(T) == 4 || sizeof(T) == 8, "4- or 8-byte elements");
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  if constexpr (sizeof(T) == 4)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// One depth of the upward or downward pass: out[o] (+)= sum_i P[i * ld + o] v[i], o < nout,
+// i < nin (nin, nout <= 64), for one cluster per CTA of 256 threads.  The panel P (nin x ld
+// column-major, ld = nout) is staged in shared memory by cp.async, so its loads overlap instead
+// of forming one chain per warp; thread t then sums the terms i = t / 64 (mod 4) of output
+// t % 64 and the four partial sums are added in a fixed order.  The tree's upper depths have only
+// a few clusters each: with one warp per cluster they were bound by that chain (one memory
+// latency per term, over 60 long-scoreboard stalls per issued instruction).
+template <typename T>
+__device__ __forceinline__ double cta_panel_dot(const T* __restrict__ P, int nout, const double* __restrict__ v,
+                                                int nin, T* sp, double* sv, double* red) {
+  const int t = threadIdx.x;
+  const int total = nin * nout;
+  for (int k = t; k < total; k += 256) cp_async_elem(sp + k, P + k);
+  if (t < nin) sv[t] = v[t];
+  cp_async_wait_all();
+  __syncthreads();
+  const int o = t & 63, g = t >> 6;
+  double a = 0.0;
+  if (o < nout)
+    for (int i = g; i < nin; i += 4) a = fma(double(sp[i * nout + o]), sv[i], a);
+  red[t] = a;
+  __syncthreads();
+  double r = 0.0;
+  if (t < 64) r = ((red[t] + red[t + 64]) + red[t + 128]) + red[t + 192];
+  __syncthreads();  // sp, sv and red are reused by the caller's next panel
+  return r;
+}
+
+// upward pass, one depth: xh_c = sum over children F_ch^T xh_ch (the transposed transfer of a
+// child is stored kc x kc_child column-major: F[j + i * kc]); one CTA per cluster
+template <typename T>
+__global__ void __launch_bounds__(256) k_h2_up(int count, const int* __restrict__ ids,
+                                               const H2Node* __restrict__ node, const T* __restrict__ colb,
+                                               double* __restrict__ xh) {
+  __shared__ T sp[64 * 64];
+  __shared__ double sv[64], red[256];
+  if (int(blockIdx.x) >= count) return;
+  const H2Node c = node[ids[blockIdx.x]];
   if (c.child0 < 0 || c.kc == 0) return;
-  double a0 = 0.0, a1 = 0.0;
-  const bool two = lane + 32 < c.kc;
+  double acc = 0.0;
   for (int s = 0; s < 2; ++s) {
     const H2Node ch = node[s == 0 ? c.child0 : c.child1];
-    const T* F = colb + ch.ct;
-    for (int i = 0; i < ch.kc; ++i) {
-      const double xi = xh[ch.xo + i];
-      if (lane < c.kc) a0 = fma(double(F[size_t(i) * c.kc + lane]), xi, a0);
-      if (two) a1 = fma(double(F[size_t(i) * c.kc + lane + 32]), xi, a1);
-    }
+    if (ch.kc == 0) continue;
+    acc += cta_panel_dot(colb + ch.ct, c.kc, xh + ch.xo, ch.kc, sp, sv, red);
   }
-  if (lane < c.kc) xh[c.xo + lane] = a0;
-  if (two) xh[c.xo + lane + 32] = a1;
+  if (threadIdx.x < c.kc) xh[c.xo + threadIdx.x] = acc;
 }
 
 // couplings: yh_t += S_b xh_s for every admissible block b = (t, s) (S_b kr x kc column-major);
@@ -751,26 +788,21 @@ __global__ void __launch_bounds__(256) k_h2_couple(int nblk, const int* __restri
   if (two) atomicAdd(yh + t.yo + lane + 32, a1 + c1);
 }
 
-// downward pass, one depth: yh_c += E_c yh_parent (E_c kr x kr_parent column-major)
+// downward pass, one depth: yh_c += E_c yh_parent (E_c kr x kr_parent column-major); one CTA per
+// cluster (cta_panel_dot)
 template <typename T>
-__global__ void k_h2_down(int count, const int* __restrict__ ids, const H2Node* __restrict__ node,
-                          const T* __restrict__ rowb, double* __restrict__ yh) {
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  if (w >= count) return;
-  const H2Node c = node[ids[w]];
+__global__ void __launch_bounds__(256) k_h2_down(int count, const int* __restrict__ ids,
+                                                 const H2Node* __restrict__ node, const T* __restrict__ rowb,
+                                                 double* __restrict__ yh) {
+  __shared__ T sp[64 * 64];
+  __shared__ double sv[64], red[256];
+  if (int(blockIdx.x) >= count) return;
+  const H2Node c = node[ids[blockIdx.x]];
   if (c.parent < 0 || c.kr == 0 || c.child0 < 0) return;
   const H2Node p = node[c.parent];
   if (p.kr == 0) return;
-  const T* E = rowb + c.rt;
-  double a0 = 0.0, a1 = 0.0;
-  const bool one = lane < c.kr, two = lane + 32 < c.kr;
-  for (int j = 0; j < p.kr; ++j) {
-    const double yj = yh[p.yo + j];
-    if (one) a0 = fma(double(E[size_t(j) * c.kr + lane]), yj, a0);
-    if (two) a1 = fma(double(E[size_t(j) * c.kr + lane + 32]), yj, a1);
-  }
-  if (one) yh[c.yo + lane] += a0;
-  if (two) yh[c.yo + lane + 32] += a1;
+  const double a = cta_panel_dot(rowb + c.rt, c.kr, yh + p.yo, p.kr, sp, sv, red);
+  if (threadIdx.x < c.kr) yh[c.yo + threadIdx.x] += a;
 }
 
 // row leaves: y_l += V_l (yh_l + E_l yh_parent) (V_l m x kr column-major: lane i reads V[i + j m]);
@@ -822,7 +854,7 @@ void launch_h2_matvec(const H2View<T>& H, const double* u, double* y, T* xp, con
   }
   for (const auto& d : up) {
     note_launch();
-    k_h2_up<T><<<blocks(d.second), 256, 0, st>>>(d.second, H.lvl_nodes + d.first, H.node, H.colb, H.xh);
+    k_h2_up<T><<<unsigned(d.second), 256, 0, st>>>(d.second, H.lvl_nodes + d.first, H.node, H.colb, H.xh);
   }
   if (H.nblk > 0) {
     note_launch();
@@ -830,7 +862,7 @@ void launch_h2_matvec(const H2View<T>& H, const double* u, double* y, T* xp, con
   }
   for (const auto& d : down) {
     note_launch();
-    k_h2_down<T><<<blocks(d.second), 256, 0, st>>>(d.second, H.lvl_nodes + d.first, H.node, H.rowb, H.yh);
+    k_h2_down<T><<<unsigned(d.second), 256, 0, st>>>(d.second, H.lvl_nodes + d.first, H.node, H.rowb, H.yh);
   }
   if (H.nleaf > 0) {
     note_launch();
