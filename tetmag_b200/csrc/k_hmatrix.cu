@@ -703,8 +703,8 @@ __device__ __forceinline__ void cp_async_elem(T* smem, const T* gmem) {
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 // One depth of the upward or downward pass: out[o] (+)= sum_i P[i * ld + o] v[i], o < nout,
-// i < nin (nin, nout <= 64), for one cluster per CTA of 256 threads.  The panel P (nin x ld
-// column-major, ld = nout) is staged in shared memory by cp.async, so its loads overlap instead
+// i < nin (nin, nout <= 64), for one cluster per CTA of 256 threads.  The panel P (nout x nin,
+// column-major: entry (o, i) at i * nout + o) is staged in shared memory by cp.async, so its loads overlap instead
 // of forming one chain per warp; thread t then sums the terms i = t / 64 (mod 4) of output
 // t % 64 and the four partial sums are added in a fixed order.  The tree's upper depths have only
 // a few clusters each: with one warp per cluster they were bound by that chain (one memory
